@@ -1,0 +1,238 @@
+"""ctypes bindings for the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+`lib/libpivoracle.so` is the project's C restatement of the reference path;
+`_ref/libpeakfit_ref.so` and `_ref/libfusedwarp_ref.so` are the reference's own
+peak fitter and warp compiled from its sources by `make -C oracle ref`.  Only the
+tests, the smoke check and bench.py's CPU-baseline leg import this module.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libpivoracle.so")
+REF_PEAKFIT = os.path.join(HERE, "_ref", "libpeakfit_ref.so")
+REF_WARP = os.path.join(HERE, "_ref", "libfusedwarp_ref.so")
+REF_SRC = "/root/reference/pivtools_cli/lib"
+
+_f32 = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64 = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u8 = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_vp = ctypes.c_void_p
+_ci = ctypes.c_int
+
+
+def build(with_ref: bool = True) -> None:
+    """Compile the restatement (always) and the reference sources (when present)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+    if with_ref and os.path.isdir(REF_SRC):
+        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.isfile(LIB_PATH):
+        build(with_ref=False)
+    L = ctypes.CDLL(LIB_PATH)
+    L.orc_xcorr_plane.argtypes = [_f32, _f32, _ci, _ci, _f64]
+    L.orc_correl_weight.argtypes = [_f32, _ci, _ci, _f32]
+    L.orc_lsqpeaklocate_lm.argtypes = [_f32, _i32, _f32, _ci, _ci, _f32, _vp, _ci]
+    L.orc_lsqpeaklocate_lm.restype = None
+    L.orc_peak_detectability.argtypes = [_f32, _i32]
+    L.orc_peak_detectability.restype = ctypes.c_float
+    L.orc_bulkxcorr2d.argtypes = [_f32, _f32, _f32, _i32, _ci, _f32, _f32, _i32, _f32, _ci,
+                                  _f32, _i32, _ci, _ci, _f32, _f32, _f32, _f32, _f32, _f32,
+                                  _f32, _vp, _vp, _ci, _ci]
+    L.orc_bulkxcorr2d.restype = ctypes.c_ubyte
+    L.orc_accumulate_triple.argtypes = [_f32, _f32, _f32, _i32, _ci, _f32, _f32, _i32, _f32,
+                                        _f32, _f32, _f32, _i32, _vp, _ci, _ci, _f32, _f32,
+                                        _f32, _ci]
+    L.orc_accumulate_triple.restype = ctypes.c_ubyte
+    L.orc_accumulate.argtypes = [_f32, _f32, _f32, _i32, _ci, _f32, _f32, _i32, _f32, _f32,
+                                 _i32, _vp, _f32, _ci]
+    L.orc_accumulate.restype = ctypes.c_ubyte
+    L.orc_fused_warp_batch.argtypes = [_f32, _f32, _f32, _f32, _f32, _f32, _ci, _ci, _ci, _ci,
+                                       _ci, _f32, _f32, _ci, _ci, _ci, _ci]
+    L.orc_kspace_lm_fit_batch.argtypes = [_f64, _f64, _f64, _u8, _vp, _ci, _ci, _ci, _ci, _ci,
+                                          _f64, _i32, _f64, _f64, _f64, _f64, _f64, _f64, _i32,
+                                          _i32, _u8, _ci]
+    L.orc_kspace_fft2_centered.argtypes = [_f64, _ci, _ci, _f64, _f64]
+    L.orc_fminvec.argtypes = [_f32, _ci]
+    L.orc_fminvec.restype = ctypes.c_float
+    L.orc_fmaxvec.argtypes = [_f32, _ci]
+    L.orc_fmaxvec.restype = ctypes.c_float
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def ref_peakfit() -> ctypes.CDLL | None:
+    """The reference's own fitter compiled from source, or None if not built here."""
+    if not os.path.isfile(REF_PEAKFIT):
+        return None
+    L = ctypes.CDLL(REF_PEAKFIT)
+    L.lsqpeaklocate_lm.argtypes = [_f32, _i32, _f32, _ci, _ci, _f32, _vp]
+    L.lsqpeaklocate_lm.restype = None
+    L.lsqpeaklocate_lm_batch.argtypes = [_f32, _ci, _i32, _ci, _f32, _f32, _vp]
+    L.lsqpeaklocate_lm_batch.restype = None
+    L.peak_detectability.argtypes = [_f32, _i32]
+    L.peak_detectability.restype = ctypes.c_float
+    L.peakfit_batch_lanes.restype = ctypes.c_int
+    return L
+
+
+def ref_warp() -> ctypes.CDLL | None:
+    if not os.path.isfile(REF_WARP):
+        return None
+    L = ctypes.CDLL(REF_WARP)
+    L.fused_warp_set_impl.argtypes = [_ci]
+    L.fused_symmetric_warp_batch.argtypes = [_f32, _f32, _f32, _f32, _f32, _f32, _ci, _ci,
+                                             _ci, _ci, _ci, _f32, _f32, _ci, _ci, _ci]
+    L.fused_symmetric_warp_batch.restype = ctypes.c_int
+    return L
+
+
+# --------------------------------------------------------------------------- #
+# numpy-facing helpers                                                         #
+# --------------------------------------------------------------------------- #
+
+def xcorr_plane(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    out = np.zeros(a.shape, np.float64)
+    e = lib().orc_xcorr_plane(a, b, a.shape[0], a.shape[1], out)
+    if e:
+        raise ValueError(f"orc_xcorr_plane error {e}")
+    return out
+
+
+def correl_weight(w: np.ndarray) -> np.ndarray:
+    w = np.ascontiguousarray(w, np.float32)
+    out = np.zeros(w.shape, np.float32)
+    if lib().orc_correl_weight(w, w.shape[0], w.shape[1], out):
+        raise ValueError("orc_correl_weight failed")
+    return out
+
+
+def peakfit(plane, fit_type, n_peaks=1, weight=None, exp_mode=0):
+    plane = np.ascontiguousarray(plane, np.float32)
+    N = np.array(plane.shape, np.int32)
+    loc = np.zeros(3 * n_peaks, np.float32)
+    sd = np.zeros(3 * n_peaks, np.float32)
+    w = None if weight is None else np.ascontiguousarray(weight, np.float32)
+    lib().orc_lsqpeaklocate_lm(plane, N, loc, n_peaks, fit_type, sd, _ptr(w), exp_mode)
+    return loc, sd
+
+
+def detectability(plane) -> float:
+    plane = np.ascontiguousarray(plane, np.float32)
+    return float(lib().orc_peak_detectability(plane, np.array(plane.shape, np.int32)))
+
+
+def bulkxcorr2d(A, B, mask, ctr_x, ctr_y, win_size, weight_a, weight_b, n_peaks=1,
+                peak_finder=3, ensemble=False, want_planes=False, want_f64=False,
+                peakfit_impl=0, n_threads=0):
+    """Run the oracle bulkxcorr2d; returns a dict of outputs (numpy)."""
+    A = np.ascontiguousarray(A, np.float32)
+    B = np.ascontiguousarray(B, np.float32)
+    if A.ndim == 2:
+        A, B = A[None], B[None]
+    n, H, W = A.shape
+    ny, nx = len(ctr_y), len(ctr_x)
+    nwt = ny * nx
+    h, w = win_size
+    shp = (n, n_peaks, ny, nx)
+    out = {k: np.zeros(shp, np.float32) for k in ("pk_x", "pk_y", "pk_h", "sx", "sy", "sxy")}
+    out["pk_ratio"] = np.zeros((n, ny, nx), np.float32)
+    planes = np.zeros(n * nwt * h * w, np.float32) if want_planes else None
+    planes64 = np.zeros(n * nwt * h * w, np.float64) if want_f64 else None
+    e = lib().orc_bulkxcorr2d(
+        A, B, np.ascontiguousarray(mask, np.float32).ravel(), np.array([H, W], np.int32), n,
+        np.ascontiguousarray(ctr_x, np.float32), np.ascontiguousarray(ctr_y, np.float32),
+        np.array([ny, nx], np.int32), np.ascontiguousarray(weight_a, np.float32).ravel(),
+        int(bool(ensemble)), np.ascontiguousarray(weight_b, np.float32).ravel(),
+        np.array([h, w], np.int32), n_peaks, peak_finder, out["pk_x"], out["pk_y"],
+        out["pk_h"], out["sx"], out["sy"], out["sxy"], out["pk_ratio"], _ptr(planes),
+        _ptr(planes64), peakfit_impl, n_threads)
+    out["error"] = int(e)
+    if planes is not None:
+        out["planes"] = planes.reshape(n, ny, nx, h, w)
+    if planes64 is not None:
+        out["planes_f64"] = planes64.reshape(n, ny, nx, h, w)
+    return out
+
+
+def accumulate_triple(A, B, mask, ctr_x, ctr_y, win_size, w_ab_a, w_ab_b, w_auto_a,
+                      w_auto_b, fit_size=None, mean_subtract=0, per_pair_norm=0,
+                      n_threads=0):
+    A = np.ascontiguousarray(A, np.float32)
+    B = np.ascontiguousarray(B, np.float32)
+    n, H, W = A.shape
+    ny, nx = len(ctr_y), len(ctr_x)
+    oh, ow = fit_size if fit_size is not None else win_size
+    sums = [np.zeros(ny * nx * oh * ow, np.float32) for _ in range(3)]
+    fs = None if fit_size is None else np.array(fit_size, np.int32)
+    e = lib().orc_accumulate_triple(
+        A, B, np.ascontiguousarray(mask, np.float32).ravel(), np.array([H, W], np.int32), n,
+        np.ascontiguousarray(ctr_x, np.float32), np.ascontiguousarray(ctr_y, np.float32),
+        np.array([ny, nx], np.int32), *[np.ascontiguousarray(x, np.float32).ravel() for x in
+                                        (w_ab_a, w_ab_b, w_auto_a, w_auto_b)],
+        np.array(win_size, np.int32), _ptr(fs), mean_subtract, per_pair_norm, *sums, n_threads)
+    if e:
+        raise ValueError(f"orc_accumulate_triple error {e}")
+    return [s.reshape(ny, nx, oh, ow) for s in sums]
+
+
+def fused_warp_batch(imgs_a, imgs_b, pred_dy, pred_dx, ctrs_y, ctrs_x, interp_mode=0,
+                     shared_predictor=0, round_shifts=0, n_threads=0):
+    imgs_a = np.ascontiguousarray(imgs_a, np.float32)
+    imgs_b = np.ascontiguousarray(imgs_b, np.float32)
+    N, H, W = imgs_a.shape
+    pred_dy = np.ascontiguousarray(pred_dy, np.float32)
+    pred_dx = np.ascontiguousarray(pred_dx, np.float32)
+    nPY, nPX = pred_dy.shape[-2:]
+    oa = np.zeros_like(imgs_a)
+    ob = np.zeros_like(imgs_b)
+    r = lib().orc_fused_warp_batch(imgs_a, imgs_b, oa, ob, pred_dy, pred_dx, N, H, W, nPY, nPX,
+                                   np.ascontiguousarray(ctrs_y, np.float32),
+                                   np.ascontiguousarray(ctrs_x, np.float32), interp_mode,
+                                   shared_predictor, round_shifts, n_threads)
+    if r:
+        raise ValueError("orc_fused_warp_batch failed")
+    return oa, ob
+
+
+def kspace_fit(R_AA, R_BB, R_AB, mask, corr_size, use_kx4=0, use_ky4=0, P_win=None,
+               n_threads=0):
+    h, w = corr_size
+    R_AA = np.ascontiguousarray(R_AA, np.float64).ravel()
+    R_BB = np.ascontiguousarray(R_BB, np.float64).ravel()
+    R_AB = np.ascontiguousarray(R_AB, np.float64).ravel()
+    n = R_AA.size // (h * w)
+    m = np.ascontiguousarray(mask, np.uint8).ravel()
+    P = None if P_win is None else np.ascontiguousarray(P_win, np.float64).ravel()
+    o = dict(gauss_flat=np.zeros((n, 16)), status=np.zeros(n, np.int32),
+             initial_guess=np.zeros((n, 16)), gain=np.zeros(n), N0=np.zeros(n),
+             b4x=np.zeros(n), b4y=np.zeros(n), cost_per_pt=np.zeros(n),
+             n_valid=np.zeros(n, np.int32), iters=np.zeros(n, np.int32),
+             conv=np.zeros(n, np.uint8))
+    r = lib().orc_kspace_lm_fit_batch(R_AA, R_BB, R_AB, m, _ptr(P), n, h, w, use_kx4, use_ky4,
+                                      o["gauss_flat"], o["status"], o["initial_guess"],
+                                      o["gain"], o["N0"], o["b4x"], o["b4y"], o["cost_per_pt"],
+                                      o["n_valid"], o["iters"], o["conv"], n_threads)
+    o["ret"] = int(r)
+    return o

@@ -1,0 +1,355 @@
+// fusedwarp.cu -- libfusedwarp for sm_100a.
+//
+// Predictor-corrector image deformation (pivtools_cli/lib/fused_warp.c): per
+// output pixel, upsample the coarse predictor (dy, dx) bicubically (Keys
+// a = -0.75, replicate border), take half of it, and sample frame A at
+// pixel - half and frame B at pixel + half (bicubic 4x4 or Lanczos-3 6x6 with a
+// 4097-entry weight table; zero outside the image).
+//
+// impl 0 evaluates every product and sum in the order of the reference's scalar
+// route (fused_warp.c:70-105, 175-207, 224-250) with unfused float operations,
+// so results are bit-identical to it.  impl 1 (the default, as in the reference)
+// uses, for stencils that lie inside the image, the association of the
+// reference's AVX2 route (simd_warp.h:74-160): a column accumulator
+// c[n] = sum_m wy[m]*img[m][n] built with fused multiply-adds, then
+// val = (p0 + p1) + (p2 + p3) with p = wx*c (Lanczos: ((p0+p4) + (p1+p5)) + (p2+p3)).
+// Border stencils use the scalar route in both.
+#include <math.h>
+#include <stdio.h>
+
+#include <mutex>
+
+#include "piv_common.cuh"
+
+namespace {
+
+constexpr int kLutN = 4096;
+
+__device__ __forceinline__ float fm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fa(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fs(float a, float b) { return __fsub_rn(a, b); }
+
+// fused_warp.c:52-64
+__device__ __forceinline__ void keys4(float d, float *w)
+{
+    const float s0 = fa(1.0f, d), q2 = fs(1.0f, d), s3 = fs(2.0f, d);
+    w[1] = fa(fm(fm(fs(fm(1.25f, d), 2.25f), d), d), 1.0f);
+    w[2] = fa(fm(fm(fs(fm(1.25f, q2), 2.25f), q2), q2), 1.0f);
+    w[0] = fa(fm(fs(fm(fa(fm(-0.75f, s0), 3.75f), s0), 6.0f), s0), 3.0f);
+    w[3] = fa(fm(fs(fm(fa(fm(-0.75f, s3), 3.75f), s3), 6.0f), s3), 3.0f);
+}
+
+// Lanczos-3 kernel value (fused_warp.c:120-127): sin in double, rounded once.
+__device__ __forceinline__ float lanczos3(float t)
+{
+    const float at = fabsf(t);
+    if (at < 1e-6f) return 1.0f;
+    if (at >= 3.0f) return 0.0f;
+    const float pt = fm((float)M_PI, at);
+    const float pta = __fdiv_rn(pt, 3.0f);
+    const float s1 = (float)sin((double)pt), s2 = (float)sin((double)pta);
+    return fm(__fdiv_rn(s1, pt), __fdiv_rn(s2, pta));
+}
+
+__device__ __forceinline__ void lanczos_w(float d, const float *lut, float *w)
+{
+    const float pos = fm(d, (float)kLutN);
+    int k = (int)pos;
+    float fr = fs(pos, (float)k);
+    if (k >= kLutN) { k = kLutN - 1; fr = 0.0f; }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const float a = lut[k * 6 + q], b = lut[(k + 1) * 6 + q];
+        w[q] = fa(a, fm(fr, fs(b, a)));
+    }
+}
+
+template <int IMPL>
+__device__ __forceinline__ float sample_bicubic(const float *__restrict__ img, float fy, float fx, int H, int W)
+{
+    const float fyf = floorf(fy), fxf = floorf(fx);
+    const int iy = (int)fyf - 1, ix = (int)fxf - 1;
+    float wy[4], wx[4];
+    keys4(fs(fy, fyf), wy);
+    keys4(fs(fx, fxf), wx);
+    if (IMPL == 1 && iy >= 0 && iy + 3 < H && ix >= 0 && ix + 3 < W) {
+        const float *r = img + (long long)iy * W + ix;
+        float c[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) c[n] = fm(__ldg(r + n), wy[0]);
+#pragma unroll
+        for (int m = 1; m < 4; ++m)
+#pragma unroll
+            for (int n = 0; n < 4; ++n) c[n] = __fmaf_rn(__ldg(r + (long long)m * W + n), wy[m], c[n]);
+        const float p0 = fm(c[0], wx[0]), p1 = fm(c[1], wx[1]), p2 = fm(c[2], wx[2]), p3 = fm(c[3], wx[3]);
+        return fa(fa(p0, p1), fa(p2, p3));
+    }
+    float v = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int row = iy + m;
+        if (row < 0 || row >= H) continue;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const int col = ix + n;
+            if (col < 0 || col >= W) continue;
+            v = fa(v, fm(fm(wy[m], wx[n]), __ldg(img + (long long)row * W + col)));
+        }
+    }
+    return v;
+}
+
+template <int IMPL>
+__device__ __forceinline__ float sample_lanczos(const float *__restrict__ img, float fy, float fx, int H, int W,
+                                                const float *lut)
+{
+    const float fyf = floorf(fy), fxf = floorf(fx);
+    const int iy = (int)fyf - 2, ix = (int)fxf - 2;
+    float wy[6], wx[6];
+    lanczos_w(fs(fy, fyf), lut, wy);
+    lanczos_w(fs(fx, fxf), lut, wx);
+    if (IMPL == 1 && iy >= 0 && iy + 5 < H && ix >= 0 && ix + 5 < W) {
+        const float *r = img + (long long)iy * W + ix;
+        float c[6];
+#pragma unroll
+        for (int n = 0; n < 6; ++n) c[n] = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 6; ++m)
+#pragma unroll
+            for (int n = 0; n < 6; ++n) c[n] = __fmaf_rn(__ldg(r + (long long)m * W + n), wy[m], c[n]);
+        float p[6];
+#pragma unroll
+        for (int n = 0; n < 6; ++n) p[n] = fm(c[n], wx[n]);
+        return fa(fa(fa(p[0], p[4]), fa(p[1], p[5])), fa(p[2], p[3]));
+    }
+    float v = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        const int row = iy + m;
+        if (row < 0 || row >= H) continue;
+#pragma unroll
+        for (int n = 0; n < 6; ++n) {
+            const int col = ix + n;
+            if (col < 0 || col >= W) continue;
+            v = fa(v, fm(fm(wy[m], wx[n]), __ldg(img + (long long)row * W + col)));
+        }
+    }
+    return v;
+}
+
+// np.interp(pixel, ctrs, arange(n)) with clamped ends (fused_warp.c:259-307); the
+// segment is the one the reference's forward scan reaches for ascending centres.
+__global__ void pred_index_kernel(const float *ctrs, int nc, float *lut, int n)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    if (nc == 1) { lut[p] = 0.0f; return; }
+    const float x = (float)p;
+    if (x <= ctrs[0]) { lut[p] = 0.0f; return; }
+    if (x >= ctrs[nc - 1]) { lut[p] = (float)(nc - 1); return; }
+    int lo = 0, hi = nc - 2;     // largest seg <= nc-2 with seg == 0 or ctrs[seg] < x
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ctrs[mid] < x) lo = mid;
+        else hi = mid - 1;
+    }
+    const int seg = lo;
+    const float den = fs(ctrs[seg + 1], ctrs[seg]);
+    if (den < 1e-12f) { lut[p] = (float)seg; return; }
+    lut[p] = fa((float)seg, __fdiv_rn(fs(x, ctrs[seg]), den));
+}
+
+// Lanczos weight table at d = i / 4096, i = 0..4096 (fused_warp.c:148-158).
+__global__ void lanczos_lut_kernel(float *lut)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > kLutN) return;
+    const float d = __fdiv_rn((float)i, (float)kLutN);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) lut[i * 6 + k] = lanczos3(fs(d, (float)(k - 2)));
+}
+
+struct WarpParams {
+    const float *ia, *ib;
+    float *oa, *ob;
+    const float *pdy, *pdx;
+    long long pred_stride;     // 0 = shared predictor
+    long long img_stride;
+    int N, H, W, nPY, nPX;
+    const float *ly, *lx;      // pixel -> fractional predictor index
+    const float *lut;          // Lanczos table or null
+    int round_shifts;
+};
+
+template <int MODE, int IMPL>
+__global__ void __launch_bounds__(256) warp_kernel(WarpParams p)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    const int n = blockIdx.z;
+    if (j >= p.W || i >= p.H) return;
+    const float *dy = p.pdy + n * p.pred_stride, *dx = p.pdx + n * p.pred_stride;
+    // Phase A: bicubic predictor (fused_warp.c:224-250)
+    const float fiy = p.ly[i], fiyf = floorf(fiy);
+    const int by = (int)fiyf - 1;
+    float wy[4], wx[4];
+    keys4(fs(fiy, fiyf), wy);
+    const float fx = p.lx[j], fxf = floorf(fx);
+    const int bx = (int)fxf - 1;
+    keys4(fs(fx, fxf), wx);
+    float vy = 0.0f, vx = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int r = min(max(by + m, 0), p.nPY - 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = min(max(bx + q, 0), p.nPX - 1);
+            const float w = fm(wy[m], wx[q]);
+            vy = fa(vy, fm(w, __ldg(dy + r * p.nPX + c)));
+            vx = fa(vx, fm(w, __ldg(dx + r * p.nPX + c)));
+        }
+    }
+    // Phase B: symmetric half shifts
+    float hy = fm(0.5f, vy), hx = fm(0.5f, vx);
+    if (p.round_shifts) { hy = roundf(hy); hx = roundf(hx); }
+    // Phase C: samples
+    const float *a = p.ia + n * p.img_stride, *b = p.ib + n * p.img_stride;
+    const long long o = n * p.img_stride + (long long)i * p.W + j;
+    const float fi = (float)i, fj = (float)j;
+    if (MODE == 0) {
+        p.oa[o] = sample_bicubic<IMPL>(a, fs(fi, hy), fs(fj, hx), p.H, p.W);
+        p.ob[o] = sample_bicubic<IMPL>(b, fa(fi, hy), fa(fj, hx), p.H, p.W);
+    } else {
+        p.oa[o] = sample_lanczos<IMPL>(a, fs(fi, hy), fs(fj, hx), p.H, p.W, p.lut);
+        p.ob[o] = sample_lanczos<IMPL>(b, fa(fi, hy), fa(fj, hx), p.H, p.W, p.lut);
+    }
+}
+
+std::mutex g_mu;
+volatile int g_impl = 1;
+struct Ws {
+    void *dev = nullptr;
+    size_t cap = 0;
+    cudaStream_t s = nullptr;
+    int ensure(size_t b)
+    {
+        if (!s && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return 1;
+        if (b > cap) {
+            if (dev) cudaFree(dev);
+            dev = nullptr;
+            cap = 0;
+            if (cudaMalloc(&dev, b + b / 4) != cudaSuccess) { cudaGetLastError(); return 1; }
+            cap = b + b / 4;
+        }
+        return 0;
+    }
+} g_ws;
+
+inline size_t pad256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace
+
+// fused_warp.h:21-22
+PIV_EXPORT void fused_warp_set_impl(int impl) { g_impl = impl ? 1 : 0; }
+PIV_EXPORT int fused_warp_get_impl(void) { return g_impl; }
+
+// Bytes of device tables pivb_warp_dev needs: lut_y [H], lut_x [W], Lanczos [4097*6].
+PIV_EXPORT size_t pivb_warp_table_bytes(int H, int W)
+{
+    return pad256((size_t)H * 4) + pad256((size_t)W * 4) + pad256((size_t)(kLutN + 1) * 6 * 4);
+}
+
+// Build the per-call tables on the device (pixel -> predictor index, Lanczos weights).
+PIV_EXPORT int pivb_warp_setup_dev(const float *d_ctrs_y, int nPY, const float *d_ctrs_x, int nPX, int H,
+                                   int W, void *d_tables, void *stream)
+{
+    if (H <= 0 || W <= 0 || nPY <= 0 || nPX <= 0 || !d_ctrs_y || !d_ctrs_x || !d_tables) return 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    char *t = static_cast<char *>(d_tables);
+    float *ly = reinterpret_cast<float *>(t);
+    float *lx = reinterpret_cast<float *>(t + pad256((size_t)H * 4));
+    float *lut = reinterpret_cast<float *>(t + pad256((size_t)H * 4) + pad256((size_t)W * 4));
+    pred_index_kernel<<<(H + 255) / 256, 256, 0, s>>>(d_ctrs_y, nPY, ly, H);
+    pred_index_kernel<<<(W + 255) / 256, 256, 0, s>>>(d_ctrs_x, nPX, lx, W);
+    lanczos_lut_kernel<<<(kLutN + 1 + 255) / 256, 256, 0, s>>>(lut);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Warp N pairs on device pointers.  img_stride = elements between frames (>= H*W);
+// tables from pivb_warp_setup_dev.  Returns 0 or 1 (bad arguments / launch failure).
+PIV_EXPORT int pivb_warp_dev(const float *d_ia, const float *d_ib, float *d_oa, float *d_ob,
+                             const float *d_pdy, const float *d_pdx, int N, int H, int W, int nPY, int nPX,
+                             long long img_stride, const void *d_tables, int interp_mode, int shared_predictor,
+                             int round_shifts, int impl, void *stream)
+{
+    if (N <= 0 || H <= 0 || W <= 0 || nPY <= 0 || nPX <= 0) return 1;
+    if (!d_ia || !d_ib || !d_oa || !d_ob || !d_pdy || !d_pdx || !d_tables) return 1;
+    const char *t = static_cast<const char *>(d_tables);
+    WarpParams p;
+    p.ia = d_ia; p.ib = d_ib; p.oa = d_oa; p.ob = d_ob; p.pdy = d_pdy; p.pdx = d_pdx;
+    p.pred_stride = shared_predictor ? 0 : (long long)nPY * nPX;
+    p.img_stride = img_stride;
+    p.N = N; p.H = H; p.W = W; p.nPY = nPY; p.nPX = nPX;
+    p.ly = reinterpret_cast<const float *>(t);
+    p.lx = reinterpret_cast<const float *>(t + pad256((size_t)H * 4));
+    p.lut = reinterpret_cast<const float *>(t + pad256((size_t)H * 4) + pad256((size_t)W * 4));
+    p.round_shifts = round_shifts;
+    dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8, N);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (interp_mode == 0) {
+        if (impl) warp_kernel<0, 1><<<grd, blk, 0, s>>>(p);
+        else warp_kernel<0, 0><<<grd, blk, 0, s>>>(p);
+    } else {
+        if (impl) warp_kernel<1, 1><<<grd, blk, 0, s>>>(p);
+        else warp_kernel<1, 0><<<grd, blk, 0, s>>>(p);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// fused_warp.h:78-93
+PIV_EXPORT int fused_symmetric_warp_batch(const float *imgs_a, const float *imgs_b, float *outs_a, float *outs_b,
+                                          const float *pred_dy, const float *pred_dx, int N, int H, int W,
+                                          int nPY, int nPX, const float *ctrs_y, const float *ctrs_x,
+                                          int interp_mode, int shared_predictor, int round_shifts)
+{
+    if (N <= 0 || H <= 0 || W <= 0 || nPY <= 0 || nPX <= 0) return 1;
+    if (!imgs_a || !imgs_b || !outs_a || !outs_b || !pred_dy || !pred_dx || !ctrs_y || !ctrs_x) return 1;
+    std::lock_guard<std::mutex> lock(g_mu);
+    const int impl = g_impl;
+    const size_t img = (size_t)N * H * W;
+    const size_t npred = (size_t)(shared_predictor ? 1 : N) * nPY * nPX;
+    const size_t tb = pivb_warp_table_bytes(H, W);
+    const size_t bytes = 4 * pad256(img * 4) + 2 * pad256(npred * 4) + pad256(nPY * 4) + pad256(nPX * 4) + tb + 4096;
+    if (g_ws.ensure(bytes)) return 1;
+    cudaStream_t s = g_ws.s;
+    char *base = static_cast<char *>(g_ws.dev);
+    size_t off = 0;
+    auto take = [&](size_t b) { char *p = base + off; off += pad256(b); return p; };
+    float *ia = (float *)take(img * 4), *ib = (float *)take(img * 4);
+    float *oa = (float *)take(img * 4), *ob = (float *)take(img * 4);
+    float *py = (float *)take(npred * 4), *px = (float *)take(npred * 4);
+    float *cy = (float *)take((size_t)nPY * 4), *cx = (float *)take((size_t)nPX * 4);
+    void *tables = take(tb);
+    if (cudaMemcpyAsync(ia, imgs_a, img * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(ib, imgs_b, img * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(py, pred_dy, npred * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(px, pred_dx, npred * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(cy, ctrs_y, (size_t)nPY * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(cx, ctrs_x, (size_t)nPX * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
+    if (pivb_warp_setup_dev(cy, nPY, cx, nPX, H, W, tables, s)) return 1;
+    if (pivb_warp_dev(ia, ib, oa, ob, py, px, N, H, W, nPY, nPX, (long long)H * W, tables, interp_mode,
+                      shared_predictor, round_shifts, impl, s))
+        return 1;
+    if (cudaMemcpyAsync(outs_a, oa, img * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(outs_b, ob, img * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess) return 1;
+    return cudaStreamSynchronize(s) == cudaSuccess ? 0 : 1;
+}
+
+// fused_warp.h:55-64
+PIV_EXPORT int fused_symmetric_warp(const float *img_a, const float *img_b, float *out_a, float *out_b,
+                                    const float *pred_dy, const float *pred_dx, int H, int W, int nPY, int nPX,
+                                    const float *ctrs_y, const float *ctrs_x, int interp_mode, int round_shifts)
+{
+    return fused_symmetric_warp_batch(img_a, img_b, out_a, out_b, pred_dy, pred_dx, 1, H, W, nPY, nPX, ctrs_y,
+                                      ctrs_x, interp_mode, 1, round_shifts);
+}

@@ -1,0 +1,292 @@
+// xcorr_engine.cuh -- one interrogation window per thread group: FFT
+// cross-correlation with the plane kept in shared memory.
+//
+// Layout of work.  An N x N window is handled by T = N*P threads (P = 1 for
+// N <= 32, 2 for 48/64, 4 for 96/128); each thread owns M = N/P complex samples
+// of one column (column phase) or one row (row phase), decimated by P.  The
+// forward transform packs the two real windows into one complex plane
+// z = a + i*b (a = frame A, b = frame B), so one complex 2-D FFT yields both
+// spectra; the Hermitian split and the conjugate product
+//     C = F_B * conj(F_A)                                 (slot0 = B, slot1 = A)
+// are formed in one pass that reads Z(k) and Z(-k) from shared memory
+// (PIV_2d_cross_correlate.c:131-133, codelet_fft.c:342-352).  The inverse
+// transform then produces the real correlation surface; it is scaled by
+// 1/numel, fftshifted (codelet_fft.c:316-327) and written to shared memory as
+// floats, where the peak search reads it.  The surface never leaves the SM
+// unless the caller asks for the debug dump.
+#pragma once
+
+#include "fft_reg.cuh"
+#include "peakfit_dev.cuh"
+
+namespace piv {
+
+template <int N>
+struct WinGeo {
+    static constexpr int P = (N <= 32) ? 1 : ((N <= 64) ? 2 : 4);
+    static constexpr int M = N / P;
+    static constexpr int T = N * P;                                     // active threads per window
+    static constexpr int GW = (T <= 8) ? 8 : (T <= 16) ? 16 : (T <= 32) ? 32 : T;  // lanes per group
+    static constexpr int WPW = (GW <= 32) ? 32 / GW : 1;                // windows per warp
+    static constexpr int ST = N + ((P == 1) ? 1 : (P == 2 ? 2 : 4));    // complex row stride
+    static constexpr int STF = N + 1;                                   // float row stride
+    static constexpr int WARPS_PER_CTA = (GW <= 32) ? 4 : GW / 32;
+    static constexpr int CTA_THREADS = WARPS_PER_CTA * 32;
+    static constexpr int GROUPS_PER_CTA = (GW <= 32) ? WARPS_PER_CTA * WPW : 1;
+    static constexpr int PLANE_BYTES = N * ST * 8;
+    static constexpr int RED_SLOTS = (GW > 32) ? GW / 32 : 1;
+    static constexpr int SMEM_BYTES = GROUPS_PER_CTA * PLANE_BYTES + 64 * RED_SLOTS * 4 + 64;
+    static_assert(N * STF * 4 <= PLANE_BYTES, "float plane must alias the complex plane");
+};
+
+// Thread-group services: synchronisation and reductions over the T threads of
+// one window.  Groups of <= 32 lanes live inside one warp; larger groups are a
+// whole CTA.
+template <int N>
+struct Group {
+    using G = WinGeo<N>;
+    int t;            // thread index within the group (0..GW-1)
+    float *red;       // CTA reduction scratch (GW > 32 only)
+
+    __device__ __forceinline__ void sync() const
+    {
+        if constexpr (G::GW <= 32) __syncwarp();
+        else __syncthreads();
+    }
+
+    __device__ __forceinline__ float sum(float v) const
+    {
+        if constexpr (G::GW <= 32) {
+#pragma unroll
+            for (int o = G::GW / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            return v;
+        } else {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            const int w = t >> 5;
+            __syncthreads();
+            if ((t & 31) == 0) red[w] = v;
+            __syncthreads();
+            float s = 0.0f;
+#pragma unroll
+            for (int k = 0; k < G::RED_SLOTS; ++k) s += red[k];
+            return s;
+        }
+    }
+
+    __device__ __forceinline__ bool any(bool b) const
+    {
+        if constexpr (G::GW <= 32) {
+            unsigned m = __ballot_sync(0xffffffffu, b);
+            if constexpr (G::GW < 32) {
+                const unsigned seg = ((1u << G::GW) - 1u) << ((threadIdx.x & 31) & ~(G::GW - 1));
+                m &= seg;
+            }
+            return m != 0u;
+        } else {
+            return __syncthreads_or(b) != 0;
+        }
+    }
+
+    // Reduce the (argmax, top-2) accumulator over the group; result in every lane.
+    __device__ __forceinline__ void reduce_peak(PeakAcc &a) const
+    {
+        constexpr int W = (G::GW <= 32) ? G::GW : 32;
+#pragma unroll
+        for (int o = W / 2; o > 0; o >>= 1) {
+            float ob = __shfl_xor_sync(0xffffffffu, a.best, o);
+            int oi = __shfl_xor_sync(0xffffffffu, a.idx, o);
+            float o1 = __shfl_xor_sync(0xffffffffu, a.p1, o);
+            float o2 = __shfl_xor_sync(0xffffffffu, a.p2, o);
+            a.merge(ob, oi, o1, o2);
+        }
+        if constexpr (G::GW > 32) {
+            const int w = t >> 5;
+            float *r = red;
+            __syncthreads();
+            if ((t & 31) == 0) {
+                r[4 * w + 0] = a.best;
+                r[4 * w + 1] = __int_as_float(a.idx);
+                r[4 * w + 2] = a.p1;
+                r[4 * w + 3] = a.p2;
+            }
+            __syncthreads();
+            a.init();
+#pragma unroll 1
+            for (int k = 0; k < G::RED_SLOTS; ++k)
+                a.merge(r[4 * k], __float_as_int(r[4 * k + 1]), r[4 * k + 2], r[4 * k + 3]);
+        }
+    }
+};
+
+// Position of a group thread in the column/row phases: the P threads sharing
+// one column (row) are adjacent lanes.
+template <int N>
+__device__ __forceinline__ void lane_slot(int t, int &line, int &p)
+{
+    using G = WinGeo<N>;
+    if constexpr (G::P == 1) {
+        line = t;
+        p = 0;
+    } else {
+        line = (t >> 5) * (32 / G::P) + (t & 31) / G::P;
+        p = t % G::P;
+    }
+}
+
+struct PlaneView {
+    const float *s;
+    int ld;
+    __device__ __forceinline__ float operator()(int i, int j) const { return s[i * ld + j]; }
+};
+
+// Forward packed 2-D transform: z = a + i b (column samples P*n + p of each
+// thread) -> Z in shared memory, row-major natural order.
+template <int N>
+__device__ __forceinline__ void fft2_forward(const Group<N> &g, float2 *S, const float (&a)[WinGeo<N>::M],
+                                             const float (&b)[WinGeo<N>::M])
+{
+    using G = WinGeo<N>;
+    constexpr int M = G::M, P = G::P, ST = G::ST;
+    const bool active = g.t < G::T;
+    int line, p;
+    lane_slot<N>(active ? g.t : 0, line, p);
+    const int q = out_block<P>(p);
+    float2 z[M];
+#pragma unroll
+    for (int n = 0; n < M; ++n) z[n] = make_float2(a[n], b[n]);
+    RegFFT<M, -1>::run(z);                       // column transform (over rows)
+    lane_combine<P, M, -1>(z, p);
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < M; ++k) S[(M * q + k) * ST + line] = z[k];
+    }
+    g.sync();
+    if (active) {
+#pragma unroll
+        for (int n = 0; n < M; ++n) z[n] = S[line * ST + P * n + p];
+    }
+    RegFFT<M, -1>::run(z);                       // row transform
+    lane_combine<P, M, -1>(z, p);
+    g.sync();
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < M; ++k) S[line * ST + M * q + k] = z[k];
+    }
+    g.sync();
+}
+
+// Spectrum products of the packed transform, in the decimated order of the
+// inverse row transform.  With Zm = conj(Z(-k)): F_a = (Z + Zm)/2 and
+// F_b = (Z - Zm)/(2i).
+//   KIND 0 (cross):  4 F_b conj(F_a) = -i (Z - Zm) conj(Z + Zm)
+//   KIND 1 (powers): 4 (|F_a|^2 + i |F_b|^2) = |Z + Zm|^2 + i |Z - Zm|^2
+template <int N, int KIND>
+__device__ __forceinline__ void spectrum_product(const Group<N> &g, const float2 *S, float2 (&z)[WinGeo<N>::M])
+{
+    using G = WinGeo<N>;
+    constexpr int M = G::M, P = G::P, ST = G::ST;
+    if (g.t < G::T) {
+        int line, p;
+        lane_slot<N>(g.t, line, p);
+        const int rm = (N - line) % N;
+#pragma unroll
+        for (int n = 0; n < M; ++n) {
+            const int kx = P * n + p;
+            const float2 zk = S[line * ST + kx];
+            const float2 zn = S[rm * ST + (N - kx) % N];
+            const float2 d = make_float2(zk.x - zn.x, zk.y + zn.y);   // Z - Zm
+            const float2 s = make_float2(zk.x + zn.x, zk.y - zn.y);   // Z + Zm
+            if constexpr (KIND == 0) {
+                const float re = d.x * s.x + d.y * s.y;
+                const float im = d.y * s.x - d.x * s.y;
+                z[n] = make_float2(im, -re);
+            } else {
+                z[n] = make_float2(s.x * s.x + s.y * s.y, d.x * d.x + d.y * d.y);
+            }
+        }
+    } else {
+#pragma unroll
+        for (int n = 0; n < M; ++n) z[n] = make_float2(0.0f, 0.0f);
+    }
+    g.sync();
+}
+
+// Inverse 2-D transform of spectrum rows held in registers (decimated order);
+// on exit thread (line, p) holds sample rows M*q + k of column `line`.
+template <int N>
+__device__ __forceinline__ void fft2_inverse(const Group<N> &g, float2 *S, float2 (&z)[WinGeo<N>::M])
+{
+    using G = WinGeo<N>;
+    constexpr int M = G::M, P = G::P, ST = G::ST;
+    const bool active = g.t < G::T;
+    int line, p;
+    lane_slot<N>(active ? g.t : 0, line, p);
+    const int q = out_block<P>(p);
+    RegFFT<M, +1>::run(z);
+    lane_combine<P, M, +1>(z, p);
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < M; ++k) S[line * ST + M * q + k] = z[k];
+    }
+    g.sync();
+    if (active) {
+#pragma unroll
+        for (int n = 0; n < M; ++n) z[n] = S[(P * n + p) * ST + line];
+    }
+    RegFFT<M, +1>::run(z);
+    lane_combine<P, M, +1>(z, p);
+    g.sync();
+}
+
+// Forward packed transform of (a, b) -> C' = 4 F_b conj(F_a), inverse transform,
+// scaling and fftshift into the float plane `pl` (aliases S).  On entry each
+// active thread holds a[n], b[n] = samples (P*n + p) of its column.
+template <int N>
+__device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, const float (&a)[WinGeo<N>::M],
+                                                const float (&b)[WinGeo<N>::M], float scale)
+{
+    using G = WinGeo<N>;
+    constexpr int M = G::M, P = G::P;
+    float2 z[M];
+    fft2_forward<N>(g, S, a, b);
+    spectrum_product<N, 0>(g, S, z);
+    fft2_inverse<N>(g, S, z);
+    float *pl = reinterpret_cast<float *>(S);
+    if (g.t < G::T) {
+        int line, p;
+        lane_slot<N>(g.t, line, p);
+        const int q = out_block<P>(p);
+        const int col = (line + N / 2) % N;
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            const int row = (M * q + k + N / 2) % N;
+            pl[row * G::STF + col] = (z[k].x * 0.25f) * scale;
+        }
+    }
+    g.sync();
+}
+
+// Parallel Westerweel search + detectability over the plane in shared memory.
+// Returns, in every lane, the accumulator and whether a NaN was seen.
+template <int N>
+__device__ __forceinline__ void search_plane(const Group<N> &g, const float *pl, PeakAcc &acc, bool &has_nan)
+{
+    using G = WinGeo<N>;
+    constexpr int H2 = N / 2, NC = H2 * H2;
+    PlaneView v{pl, G::STF};
+    acc.init();
+    bool nan = false;
+    if (g.t < G::T) {
+#pragma unroll 1
+        for (int c = g.t; c < NC; c += G::T) {
+            const int i = N / 4 + c / H2, j = N / 4 + c % H2;
+            float val = candidate(v, i, j, &nan);
+            acc.add(val, i * N + j);
+        }
+    }
+    has_nan = g.any(nan);
+    g.reduce_peak(acc);
+}
+
+}  // namespace piv

@@ -1,0 +1,150 @@
+"""ctypes loading of the in-tree sm_100a libraries.
+
+The libraries are loaded from pivtools_b200/lib/ only.  A missing library is an
+error (FileNotFoundError), never a reason to compute elsewhere: this package has
+no CPU implementation of the path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+LIBDIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib")
+
+f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+vp = ctypes.c_void_p
+ci = ctypes.c_int
+cll = ctypes.c_longlong
+csz = ctypes.c_size_t
+
+_cache: dict[str, ctypes.CDLL] = {}
+
+
+def lib_path(name: str) -> str:
+    return os.path.join(LIBDIR, name)
+
+
+def _load(name: str) -> ctypes.CDLL:
+    if name in _cache:
+        return _cache[name]
+    path = lib_path(name)
+    if not os.path.isfile(path):
+        raise FileNotFoundError(
+            f"{path} is not built; run `python -m pivtools_b200.build` (or __graft_entry__.build())")
+    L = ctypes.CDLL(path)
+    _cache[name] = L
+    return L
+
+
+def bulkxcorr2d_lib() -> ctypes.CDLL:
+    L = _load("libbulkxcorr2d.so")
+    if getattr(L, "_pivb_bound", False):
+        return L
+    L.bulkxcorr2d.argtypes = [f32p, f32p, f32p, i32p, ci, f32p, f32p, i32p, f32p, ctypes.c_bool,
+                              f32p, i32p, ci, ci, f32p, f32p, f32p, f32p, f32p, f32p, f32p, vp]
+    L.bulkxcorr2d.restype = ctypes.c_ubyte
+    L.lsqpeaklocate_lm.argtypes = [f32p, i32p, f32p, ci, ci, f32p, vp]
+    L.lsqpeaklocate_lm.restype = None
+    L.lsqpeaklocate_lm_batch.argtypes = [f32p, ci, i32p, ci, f32p, f32p, vp]
+    L.lsqpeaklocate_lm_batch.restype = None
+    L.peak_detectability.argtypes = [f32p, i32p]
+    L.peak_detectability.restype = ctypes.c_float
+    L.pivtools_cpu_supported.restype = ci
+    L.peakfit_batch_available.restype = ci
+    L.peakfit_batch_lanes.restype = ci
+    L.codelet_lanes.restype = ci
+    L.bulkxcorr2d_set_peakfit_impl.argtypes = [ci]
+    L.bulkxcorr2d_set_peakfit_impl.restype = ci
+    L.bulkxcorr2d_get_peakfit_impl.restype = ci
+    L.bulkxcorr2d_peakfit_batch_available.restype = ci
+    L.bulkxcorr2d_set_timing_enabled.argtypes = [ci]
+    L.bulkxcorr2d_set_timing_enabled.restype = None
+    L.bulkxcorr2d_reset_timing.restype = None
+    L.bulkxcorr2d_get_timing.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.bulkxcorr2d_get_timing.restype = None
+    L.convolve.argtypes = [f32p, f32p, f32p, i32p]
+    L.convolve.restype = ctypes.c_uint
+    L.xcorr.argtypes = [f32p, f32p, f32p, i32p]
+    L.xcorr.restype = ctypes.c_uint
+    L.fminvec.argtypes = [f32p, ci]
+    L.fminvec.restype = ctypes.c_float
+    L.fmaxvec.argtypes = [f32p, ci]
+    L.fmaxvec.restype = ctypes.c_float
+    L.pivb_xcorr_scratch_bytes.argtypes = [cll, ci, ci]
+    L.pivb_xcorr_scratch_bytes.restype = csz
+    L.pivb_correl_weight_dev.argtypes = [vp, ci, ci, vp, vp]
+    L.pivb_correl_weight_dev.restype = ci
+    L.pivb_xcorr_dev.argtypes = [vp, vp, cll, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, vp, ci, ci, ci, ci,
+                                 ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, vp, csz, vp]
+    L.pivb_xcorr_dev.restype = ci
+    L.pivb_device_info.argtypes = [ctypes.c_char_p, ci]
+    L.pivb_device_info.restype = ci
+    for opt in ("bulkxcorr2d_accumulate", "bulkxcorr2d_accumulate_triple"):
+        if hasattr(L, opt):
+            getattr(L, opt).restype = ctypes.c_ubyte
+    if hasattr(L, "bulkxcorr2d_accumulate"):
+        L.bulkxcorr2d_accumulate.argtypes = [f32p, f32p, f32p, i32p, ci, f32p, f32p, i32p, f32p, f32p,
+                                             i32p, vp, f32p]
+    if hasattr(L, "bulkxcorr2d_accumulate_triple"):
+        L.bulkxcorr2d_accumulate_triple.argtypes = [f32p, f32p, f32p, i32p, ci, f32p, f32p, i32p, f32p,
+                                                    f32p, f32p, f32p, i32p, vp, ci, ci, f32p, f32p,
+                                                    f32p]
+    L.pivb_accumulate_triple_dev.argtypes = [vp, vp, cll, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, vp, vp,
+                                             ci, ci, ci, ci, ci, ci, vp, vp, vp, vp, vp, csz, vp]
+    L.pivb_accumulate_triple_dev.restype = ci
+    L.pivb_accumulate_dev.argtypes = [vp, vp, cll, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, ci, ci, ci, ci,
+                                      vp, vp, vp, csz, vp]
+    L.pivb_accumulate_dev.restype = ci
+    L.pivb_accumulate_scratch_bytes.argtypes = [ci, cll]
+    L.pivb_accumulate_scratch_bytes.restype = csz
+    L._pivb_bound = True
+    return L
+
+
+def fusedwarp_lib() -> ctypes.CDLL:
+    L = _load("libfusedwarp.so")
+    if getattr(L, "_pivb_bound", False):
+        return L
+    L.fused_warp_set_impl.argtypes = [ci]
+    L.fused_warp_set_impl.restype = None
+    L.fused_warp_get_impl.restype = ci
+    L.fused_symmetric_warp.argtypes = [f32p, f32p, f32p, f32p, f32p, f32p, ci, ci, ci, ci, f32p, f32p,
+                                       ci, ci]
+    L.fused_symmetric_warp.restype = ci
+    L.fused_symmetric_warp_batch.argtypes = [f32p, f32p, f32p, f32p, f32p, f32p, ci, ci, ci, ci, ci,
+                                             f32p, f32p, ci, ci, ci]
+    L.fused_symmetric_warp_batch.restype = ci
+    L.pivb_warp_dev.argtypes = [vp, vp, vp, vp, vp, vp, ci, ci, ci, ci, ci, cll, vp, ci, ci, ci, ci, vp]
+    L.pivb_warp_dev.restype = ci
+    L.pivb_warp_setup_dev.argtypes = [vp, ci, vp, ci, ci, ci, vp, vp]
+    L.pivb_warp_setup_dev.restype = ci
+    L.pivb_warp_table_bytes.argtypes = [ci, ci]
+    L.pivb_warp_table_bytes.restype = csz
+    L._pivb_bound = True
+    return L
+
+
+def kspacefit_lib() -> ctypes.CDLL:
+    L = _load("libkspacefit.so")
+    if getattr(L, "_pivb_bound", False):
+        return L
+    L.kspace_lm_fit_batch.argtypes = [f64p, f64p, f64p, u8p, vp, ci, ci, ci, ci, ci, ci, f64p, i32p,
+                                      f64p, f64p, f64p, f64p, f64p, f64p, i32p, i32p, u8p]
+    L.kspace_lm_fit_batch.restype = ci
+    L.kspace_lm_fit_max_threads.restype = ci
+    L.kspace_fft2_centered.argtypes = [f64p, ci, ci, f64p, f64p]
+    L.kspace_fft2_centered.restype = ci
+    L.kspace_debug_prep.argtypes = [f64p, f64p, f64p, vp, ci, ci, f64p, ctypes.POINTER(ctypes.c_double)]
+    L.kspace_debug_prep.restype = ci
+    L._pivb_bound = True
+    return L
+
+
+def loaded_paths() -> list[str]:
+    return [lib_path(n) for n in _cache]

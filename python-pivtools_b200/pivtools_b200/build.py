@@ -1,0 +1,73 @@
+"""Build the sm_100a shared libraries in-tree (pivtools_b200/lib/).
+
+Each reference library name gets its own shared object with the same exported
+C symbols: libbulkxcorr2d.so, libfusedwarp.so, libkspacefit.so.  nvcc
+cross-compiles on a machine without a GPU.
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(ROOT, "csrc")
+LIBDIR = os.path.join(PKG, "lib")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+    "-shared", "-cudart", "shared",
+]
+
+# library -> translation unit
+TARGETS = {
+    "libbulkxcorr2d.so": "bulkxcorr2d.cu",
+    "libfusedwarp.so": "fusedwarp.cu",
+    "libkspacefit.so": "kspacefit.cu",
+}
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.isfile(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def _stale(out: str, srcs: list[str]) -> bool:
+    if not os.path.isfile(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(s) > t for s in srcs)
+
+
+def build(force: bool = False, verbose: bool = False, only: list[str] | None = None) -> list[str]:
+    """Compile every target whose sources changed; return the paths built."""
+    os.makedirs(LIBDIR, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    built = []
+    for lib, tu in TARGETS.items():
+        if only and lib not in only:
+            continue
+        src = os.path.join(CSRC, tu)
+        if not os.path.isfile(src):
+            continue
+        out = os.path.join(LIBDIR, lib)
+        if not force and not _stale(out, [src] + headers):
+            continue
+        cmd = [_nvcc(), *NVCC_FLAGS, "-o", out + ".tmp", src]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        os.replace(out + ".tmp", out)
+        built.append(out)
+    return built
+
+
+if __name__ == "__main__":
+    for p in build(force="--force" in sys.argv, verbose=True):
+        print("built", p)

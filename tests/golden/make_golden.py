@@ -1,0 +1,242 @@
+"""Generate the golden fixtures from the reference itself.
+
+Run in a container that has the reference sources (it reads them only through
+the reference-compiled libraries `oracle/_ref/*.so`, built by
+`make -C oracle ref`, and, for the k-space fixture, by importing the reference's
+Python package).  The fixtures are committed; tests never need the reference.
+
+    python tests/golden/make_golden.py            # peakfit_ref.npz, warp_ref.npz
+    python tests/golden/make_golden.py kspace     # kspace_ref.npz
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import oracle as O  # noqa: E402
+
+REF_ROOT = "/root/reference"
+
+
+def gauss(shape, amp, i0, j0, s1, s2, cov, kind):
+    h, w = shape
+    ii, jj = np.meshgrid(np.arange(h), np.arange(w), indexing="ij")
+    y = ii - (h - 1) / 2 - i0
+    x = jj - (w - 1) / 2 - j0
+    if kind == 4:
+        z = amp * np.exp(-(y * y + x * x) / (s1 * s1))
+    elif kind == 5:
+        z = amp * np.exp(-(y * y / (s1 * s1) + x * x / (s2 * s2)))
+    else:
+        z = amp * np.exp(-0.5 * (y * y / s1 + x * x / s2 + 2.0 * y * x * cov))
+    return z.astype(np.float32)
+
+
+def peakfit_cases():
+    """Planes of the reference's own peak-fit tests (test_instantaneous_peaks.py,
+    test_peakfit_batch.py) plus a seeded noisy battery with plane weights."""
+    cases = []   # (plane, fit_type, n_peaks, weight or None)
+    for shape in [(17, 17), (33, 33), (65, 65), (33, 65)]:
+        for disp in [(0.0, 0.0), (0.35, 0.27), (0.1, -0.4)]:
+            for t in (3, 4, 5, 6):
+                if t in (3, 4):
+                    p = gauss(shape, 1000.0, *disp, 1.5, 1.5, 0.0, 4)
+                elif t == 5:
+                    p = gauss(shape, 1000.0, *disp, 1.5, 1.5, 0.0, 5)
+                else:
+                    p = gauss(shape, 1000.0, *disp, 2.25, 2.25, 0.0, 6)
+                cases.append((p, t, 1, None))
+    for t in (4, 5, 6):
+        for sr, sc in [(1.5, 1.5), (1.5, 2.0), (1.0, 3.0)]:
+            if t == 4:
+                s = np.sqrt((sr * sr + sc * sc) / 2)
+                p = gauss((33, 33), 1000.0, 0.35, 0.27, s, s, 0.0, 4)
+            elif t == 5:
+                p = gauss((33, 33), 1000.0, 0.35, 0.27, sr, sc, 0.0, 5)
+            else:
+                p = gauss((33, 33), 1000.0, 0.35, 0.27, sr * sr, sc * sc, 0.0, 6)
+            cases.append((p, t, 1, None))
+    ell = gauss((33, 33), 1000.0, 0.35, 0.27, 1.5, 2.5, 0.0, 5)
+    for t in (3, 4, 5, 6):
+        cases.append((ell, t, 1, None))
+    # failure sentinels
+    z = np.zeros((33, 33), np.float32)
+    ramp = (np.arange(33, dtype=np.float32)[:, None] * np.ones(33, np.float32)[None, :]) + 1.0
+    poison = gauss((33, 33), 1000.0, 0.0, 0.0, 1.5, 1.5, 0.0, 4)
+    poison[17, 17] = np.nan
+    spike = np.random.RandomState(0).uniform(0.0, 1.0, (33, 33)).astype(np.float32)
+    spike[16, 16] = 2.0
+    for t in (3, 4, 5, 6):
+        for p in (z, ramp, poison, spike):
+            cases.append((p, t, 1, None))
+    # seeded noisy battery, with and without a compensation weight, 1 and 3 peaks
+    rng = np.random.default_rng(20261203)
+    for k in range(72):
+        t = (3, 4, 5, 6)[k % 4]
+        kind = 4 if t == 3 else t
+        s1, s2 = rng.uniform(1.0, 2.5, 2)
+        if kind == 6:
+            s1, s2 = s1 * s1, s2 * s2
+        p = gauss((33, 33), rng.uniform(100, 1000), *rng.uniform(-0.45, 0.45, 2), s1, s2,
+                  rng.uniform(-0.2, 0.2) / np.sqrt(s1 * s2), kind)
+        p = (p + rng.normal(0.0, rng.choice([0.0, 2.0, 10.0]), p.shape)).astype(np.float32)
+        wt = (1.0 + 0.2 * rng.random((33, 33))).astype(np.float32) if k % 3 == 0 else None
+        cases.append((p, t, 3 if k % 9 == 0 else 1, wt))
+    return cases
+
+
+def make_peakfit():
+    R = O.ref_peakfit()
+    if R is None:
+        raise SystemExit("oracle/_ref/libpeakfit_ref.so missing: run `make -C oracle ref`")
+    cases = peakfit_cases()
+    shapes = sorted({c[0].shape for c in cases})
+    out = {"shapes": np.array(shapes, np.int32)}
+    for si, shape in enumerate(shapes):
+        sel = [c for c in cases if c[0].shape == shape]
+        planes = np.stack([c[0] for c in sel]).astype(np.float32)
+        types = np.array([c[1] for c in sel], np.int32)
+        npk = np.array([c[2] for c in sel], np.int32)
+        has_w = np.array([c[3] is not None for c in sel], bool)
+        weights = np.stack([c[3] if c[3] is not None else np.ones(shape, np.float32) for c in sel])
+        loc = np.full((len(sel), 9), np.nan, np.float32)
+        sd = np.full((len(sel), 9), np.nan, np.float32)
+        ratio = np.zeros(len(sel), np.float32)
+        N = np.array(shape, np.int32)
+        for k, (p, t, m, w) in enumerate(sel):
+            l = np.zeros(3 * m, np.float32)
+            s = np.zeros(3 * m, np.float32)
+            R.lsqpeaklocate_lm(np.ascontiguousarray(p), N, l, m, t, s,
+                               None if w is None else np.ascontiguousarray(w).ctypes.data)
+            loc[k, :3 * m] = l
+            sd[k, :3 * m] = s
+            ratio[k] = R.peak_detectability(np.ascontiguousarray(p), N)
+        out[f"s{si}_planes"] = planes
+        out[f"s{si}_types"] = types
+        out[f"s{si}_npeaks"] = npk
+        out[f"s{si}_hasw"] = has_w
+        out[f"s{si}_weights"] = weights.astype(np.float32)
+        out[f"s{si}_loc"] = loc
+        out[f"s{si}_sd"] = sd
+        out[f"s{si}_ratio"] = ratio
+    # batch route (reference lockstep fitter, 8 lanes in this build)
+    W = R.peakfit_batch_lanes()
+    rng = np.random.default_rng(7)
+    bplanes, btypes, bloc, bsd = [], [], [], []
+    for t in (4, 5, 6):
+        for rep in range(3):
+            pl = []
+            for _ in range(W):
+                s1, s2 = rng.uniform(1.0, 2.5, 2)
+                if t == 6:
+                    s1, s2 = s1 * s1, s2 * s2
+                p = gauss((33, 33), rng.uniform(100, 1000), *rng.uniform(-0.45, 0.45, 2), s1, s2,
+                          rng.uniform(-0.2, 0.2) / np.sqrt(s1 * s2), t)
+                pl.append((p + rng.normal(0.0, 3.0, p.shape)).astype(np.float32))
+            pl = np.stack(pl)
+            l = np.zeros(3 * W, np.float32)
+            s = np.zeros(3 * W, np.float32)
+            R.lsqpeaklocate_lm_batch(pl, W, np.array([33, 33], np.int32), t, l, s, None)
+            bplanes.append(pl)
+            btypes.append(np.full(W, t, np.int32))
+            bloc.append(l.reshape(3, W).T)
+            bsd.append(s.reshape(3, W).T)
+    out["batch_planes"] = np.concatenate(bplanes)
+    out["batch_types"] = np.concatenate(btypes)
+    out["batch_loc"] = np.concatenate(bloc)
+    out["batch_sd"] = np.concatenate(bsd)
+    np.savez_compressed(os.path.join(HERE, "peakfit_ref.npz"), **out)
+    print("peakfit_ref.npz:", sum(v.nbytes for v in out.values()), "bytes raw")
+
+
+def make_warp():
+    RW = O.ref_warp()
+    if RW is None:
+        raise SystemExit("oracle/_ref/libfusedwarp_ref.so missing: run `make -C oracle ref`")
+    RW.fused_warp_set_impl(0)
+    rng = np.random.default_rng(11)
+    N, H, W = 2, 48, 64
+    ia = rng.uniform(0, 255, (N, H, W)).astype(np.float32)
+    ib = rng.uniform(0, 255, (N, H, W)).astype(np.float32)
+    cy = np.linspace(-4.5, H + 3.5, 8).astype(np.float32)
+    cx = np.linspace(-4.5, W + 3.5, 10).astype(np.float32)
+    pdy = rng.normal(0, 2.5, (N, 8, 10)).astype(np.float32)
+    pdx = rng.normal(0, 2.5, (N, 8, 10)).astype(np.float32)
+    out = dict(imgs_a=ia, imgs_b=ib, ctrs_y=cy, ctrs_x=cx, pred_dy=pdy, pred_dx=pdx)
+    for mode in (0, 1):
+        for rs in (0, 1):
+            ra = np.zeros_like(ia)
+            rb = np.zeros_like(ib)
+            RW.fused_symmetric_warp_batch(ia, ib, ra, rb, pdy, pdx, N, H, W, 8, 10, cy, cx, mode, 0, rs)
+            out[f"out_a_m{mode}_r{rs}"] = ra
+            out[f"out_b_m{mode}_r{rs}"] = rb
+    # the reference's default SIMD route (AVX2 interior association in this build)
+    RW.fused_warp_set_impl(1)
+    for mode in (0, 1):
+        ra = np.zeros_like(ia)
+        rb = np.zeros_like(ib)
+        RW.fused_symmetric_warp_batch(ia, ib, ra, rb, pdy, pdx, N, H, W, 8, 10, cy, cx, mode, 0, 0)
+        out[f"simd_a_m{mode}"] = ra
+        out[f"simd_b_m{mode}"] = rb
+    RW.fused_warp_set_impl(0)
+    np.savez_compressed(os.path.join(HERE, "warp_ref.npz"), **out)
+    print("warp_ref.npz written")
+
+
+def make_kspace():
+    """Fixtures from the reference's NumPy k-space oracle (fit_windows_kspace_lm_numpy,
+    pivtools_cli/piv/piv_backend/kspace_lm_fitting.py:964) on its own test batch
+    generator (unit-tests/synthetic_correlations.py)."""
+    sys.path.insert(0, REF_ROOT)
+    sys.path.insert(0, os.path.join(REF_ROOT, "unit-tests"))
+    from synthetic_correlations import generate_correlation_triplet, make_mock_config
+
+    from pivtools_cli.piv.piv_backend.kspace_lm_fitting import fit_windows_kspace_lm_numpy
+
+    corr = (24, 24)
+    n = 24
+    rng = np.random.default_rng(7)
+    aa, bb, ab = [], [], []
+    for i in range(n):
+        A, B, C = generate_correlation_triplet(
+            corr, sigma_particle_x=1.8 + 0.4 * rng.random(), sigma_particle_y=1.8 + 0.4 * rng.random(),
+            sigma_stress_xx=0.3 * rng.random(), sigma_stress_yy=0.3 * rng.random(),
+            mu_x=rng.uniform(-1.5, 1.5), mu_y=rng.uniform(-1.5, 1.5), noise_std=0.002, seed=100 + i)
+        aa.append(A.ravel())
+        bb.append(B.ravel())
+        ab.append(C.ravel())
+    mask = np.zeros(n, bool)
+    mask[::7] = True
+    R_AA, R_BB, R_AB = (np.concatenate(x) for x in (aa, bb, ab))
+    ky, kx = np.meshgrid(np.linspace(-1, 1, corr[0]), np.linspace(-1, 1, corr[1]), indexing="ij")
+    P = np.tile((1.0 + 0.6 * np.exp(-(kx ** 2 + ky ** 2) / 0.25)).ravel(), n)
+    out = dict(R_AA=R_AA, R_BB=R_BB, R_AB=R_AB, mask=mask, P_win=P, corr=np.array(corr))
+    for shape in ("gaussian", "kx4", "ky4", "kx4+ky4"):
+        for floor in ("flat", "coloured"):
+            cfg = make_mock_config(ensemble_kspace_shape=shape, ensemble_kspace_floor=floor)
+            kw = {"P_win": P} if floor == "coloured" else {}
+            g, s, ig, diag = fit_windows_kspace_lm_numpy(R_AA, R_BB, R_AB, mask, corr, cfg, 0,
+                                                          return_diagnostics=True, **kw)
+            key = f"{shape}_{floor}"
+            out[f"{key}_gauss"] = np.asarray(g)
+            out[f"{key}_status"] = np.asarray(s)
+            out[f"{key}_init"] = np.asarray(ig)
+    np.savez_compressed(os.path.join(HERE, "kspace_ref.npz"), **out)
+    print("kspace_ref.npz written")
+
+
+if __name__ == "__main__":
+    what = sys.argv[1:] or ["peakfit", "warp"]
+    if "peakfit" in what:
+        make_peakfit()
+    if "warp" in what:
+        make_warp()
+    if "kspace" in what:
+        make_kspace()

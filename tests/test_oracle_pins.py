@@ -1,0 +1,119 @@
+"""Pin the CPU oracle (the checker) to the reference.
+
+The oracle's restatements must reproduce the reference's own outputs:
+  * peak fitter, scalar and batch routes: bit-exact against fixtures produced by
+    the reference's peak_locate_lm*.c compiled from source (tests/golden);
+  * fused warp: bit-exact against the reference's fused_warp.c scalar route;
+  * k-space fit: the reference's own parity contract against its NumPy oracle
+    (status equality, |dSigma|, |dmu| < 1e-8; test_kspace_c_fit.py:53-54);
+  * correlation planes: against a brute-force FP64 circular correlation, the
+    reference's codelet gate (test_codelet_gate.c:33-49).
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _eq(a, b):
+    return np.array_equal(np.asarray(a), np.asarray(b), equal_nan=True)
+
+
+def test_peakfit_scalar_matches_reference_fixture(oracle):
+    g = np.load(os.path.join(GOLD, "peakfit_ref.npz"))
+    n_checked = 0
+    for si, shape in enumerate(g["shapes"]):
+        planes = g[f"s{si}_planes"]
+        for k in range(planes.shape[0]):
+            t = int(g[f"s{si}_types"][k])
+            m = int(g[f"s{si}_npeaks"][k])
+            w = g[f"s{si}_weights"][k] if g[f"s{si}_hasw"][k] else None
+            loc, sd = oracle.peakfit(planes[k], t, n_peaks=m, weight=w)
+            assert _eq(loc, g[f"s{si}_loc"][k, :3 * m]), (tuple(shape), k, t, loc, g[f"s{si}_loc"][k])
+            assert _eq(sd, g[f"s{si}_sd"][k, :3 * m]), (tuple(shape), k, t)
+            assert _eq(np.float32(oracle.detectability(planes[k])), g[f"s{si}_ratio"][k])
+            n_checked += 1
+    assert n_checked >= 140
+
+
+def test_peakfit_batch_matches_reference_fixture(oracle):
+    g = np.load(os.path.join(GOLD, "peakfit_ref.npz"))
+    for k in range(g["batch_planes"].shape[0]):
+        loc, sd = oracle.peakfit(g["batch_planes"][k], int(g["batch_types"][k]), exp_mode=1)
+        assert _eq(loc, g["batch_loc"][k]), k
+        assert _eq(sd, g["batch_sd"][k]), k
+
+
+def test_warp_matches_reference_fixture(oracle):
+    g = np.load(os.path.join(GOLD, "warp_ref.npz"))
+    for mode in (0, 1):
+        for rs in (0, 1):
+            oa, ob = oracle.fused_warp_batch(g["imgs_a"], g["imgs_b"], g["pred_dy"], g["pred_dx"],
+                                             g["ctrs_y"], g["ctrs_x"], interp_mode=mode, round_shifts=rs)
+            assert _eq(oa, g[f"out_a_m{mode}_r{rs}"]), (mode, rs)
+            assert _eq(ob, g[f"out_b_m{mode}_r{rs}"]), (mode, rs)
+
+
+@pytest.mark.parametrize("shape", ["gaussian", "kx4", "ky4", "kx4+ky4"])
+@pytest.mark.parametrize("floor", ["flat", "coloured"])
+def test_kspace_matches_reference_numpy_oracle(oracle, shape, floor):
+    g = np.load(os.path.join(GOLD, "kspace_ref.npz"))
+    corr = tuple(int(v) for v in g["corr"])
+    o = oracle.kspace_fit(g["R_AA"], g["R_BB"], g["R_AB"], g["mask"], corr,
+                          use_kx4=int("kx4" in shape), use_ky4=int("ky4" in shape),
+                          P_win=g["P_win"] if floor == "coloured" else None)
+    key = f"{shape}_{floor}"
+    st_ref = g[f"{key}_status"]
+    assert np.array_equal(o["status"], st_ref)
+    ok = (o["status"] == 0) & (st_ref == 0)
+    assert ok.any()
+    gp = g[f"{key}_gauss"]
+    assert np.abs(o["gauss_flat"][ok, 9:12] - gp[ok, 9:12]).max() < 1e-8
+    assert np.abs(o["gauss_flat"][ok, 14:16] - gp[ok, 14:16]).max() < 1e-8
+    np.testing.assert_allclose(o["initial_guess"], g[f"{key}_init"], rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("n", [8, 12, 16, 24, 32, 48])
+def test_xcorr_plane_is_circular_correlation(oracle, n):
+    rng = np.random.default_rng(n)
+    a = rng.normal(size=(n, n)).astype(np.float32)
+    b = rng.normal(size=(n, n)).astype(np.float32)
+    got = oracle.xcorr_plane(a, b)
+    ref = np.zeros((n, n))
+    ad, bd = a.astype(np.float64), b.astype(np.float64)
+    for r in range(n):
+        for c in range(n):
+            s = (r - n // 2, c - n // 2)
+            ref[r, c] = np.sum(np.roll(ad, (-s[0], -s[1]), axis=(0, 1)) * bd)
+    np.testing.assert_allclose(got, ref, rtol=0, atol=1e-9 * np.abs(ref).max())
+
+
+def test_oracle_recovers_known_shift(oracle):
+    from pivtools_b200 import geometry, synthetic
+
+    A, B, _ = synthetic.particle_pair((128, 128), seed=3, flow="uniform", flow_kwargs={"u": 3.3, "v": -1.7})
+    g = geometry.compute_window_centers((128, 128), (32, 32), 50)
+    w = geometry.window_weight((32, 32), "gaussian")
+    o = oracle.bulkxcorr2d(A, B, np.zeros((g.n_win_y, g.n_win_x)), g.win_ctrs_x, g.win_ctrs_y, (32, 32), w, w)
+    dx = np.nanmedian(o["pk_x"])
+    dy = np.nanmedian(o["pk_y"])
+    assert abs(dx - 3.3) < 0.05 and abs(dy + 1.7) < 0.05
+
+
+def test_oracle_matches_live_reference_fitter(oracle):
+    R = oracle.ref_peakfit()
+    if R is None:
+        pytest.skip("reference fitter not compiled in this checkout (fixture test covers it)")
+    rng = np.random.default_rng(99)
+    for k in range(200):
+        t = (3, 4, 5, 6)[k % 4]
+        p = rng.gamma(2.0, 50.0, (33, 33)).astype(np.float32)
+        p[16, 16] += 800.0
+        loc, sd = oracle.peakfit(p, t)
+        l2 = np.zeros(3, np.float32)
+        s2 = np.zeros(3, np.float32)
+        R.lsqpeaklocate_lm(p, np.array([33, 33], np.int32), l2, 1, t, s2, None)
+        assert _eq(loc, l2) and _eq(sd, s2)
