@@ -1,0 +1,358 @@
+"""Benchmark: multipass window-deformation PIV, 64 pairs of 2048x2048 per GPU.
+
+Workload (one step): 64 image pairs of 2048^2 (0.05 ppp Gaussian particles,
+sigma 0.6 px, intensities U[1000, 4000], Poisson noise on a 100-count
+background; turbulent-channel-like flow with a 12 px log-law peak and 8% rms
+fluctuations), four passes of 128/64/32/32 px windows at 50/50/50/75% overlap,
+bicubic symmetric warp by the smoothed predictor before passes 2-4, 3-point
+Gaussian subpixel fit, normalised-median validation and infilling between
+passes.  Metric: output vectors (the final pass's 253x253 grid per pair) per
+second.  Inputs (4.3 GB of float32 frames) exceed the 126 MB L2, so no flush is
+needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun every rank processes its own 64 pairs (instantaneous PIV shards
+by pair, no collective): weak scaling, value = all ranks' vectors / max time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "python-pivtools_b200"))
+
+METRIC = "vectors/s and p50/p99 pair latency on 1 B200 at ≤0.01 px RMS vs FP64 oracle"
+WORKLOAD = "multipass window-deformation PIV, 64 pairs 2048x2048, passes 128/64/32/32 px at 50/50/50/75%"
+HW = (2048, 2048)
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--pairs", type=int, default=64)
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--cpu-pairs", type=int, default=1)
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
+                          and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+def _dist():
+    import torch
+
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                             device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def _cpu_baseline(n_pairs: int):
+    """CPU leg: the oracle port's correlation of all four passes plus the
+    reference's own warp (compiled from source, when present; else the oracle
+    warp), all host threads, on n_pairs pairs.  Returns (vectors/s, sample)."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from pivtools_b200 import geometry, synthetic
+
+    geo = geometry.multipass_geometry(HW, [(128, 128), (64, 64), (32, 32), (32, 32)], [50, 50, 50, 75])
+    pairs = [synthetic.particle_pair(HW, seed=900 + k, flow="channel")[:2] for k in range(n_pairs)]
+    ref_warp = O.ref_warp()
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    for A, B in pairs:
+        for k, g in enumerate(geo):
+            fa, fb = A, B
+            if k > 0:
+                prev = geo[k - 1]
+                pdy = np.zeros((len(prev.ctrs_y_all), len(prev.ctrs_x_all)), np.float32)
+                if ref_warp is not None:
+                    ref_warp.fused_warp_set_impl(1)
+                    fa = np.zeros_like(A)
+                    fb = np.zeros_like(B)
+                    ref_warp.fused_symmetric_warp_batch(A[None], B[None], fa, fb, pdy[None], pdy[None], 1, HW[0],
+                                                        HW[1], pdy.shape[0], pdy.shape[1], prev.ctrs_y_all,
+                                                        prev.ctrs_x_all, 0, 0, 0)
+                else:
+                    fa, fb = O.fused_warp_batch(A[None], B[None], pdy[None], pdy[None], prev.ctrs_y_all,
+                                                prev.ctrs_x_all)
+                    fa, fb = fa[0], fb[0]
+            w = geometry.window_weight(g.window_size, "gaussian")
+            O.bulkxcorr2d(fa, fb, np.zeros((g.grid.n_win_y, g.grid.n_win_x), np.float32), g.grid.win_ctrs_x,
+                          g.grid.win_ctrs_y, g.window_size, w, w, peak_finder=3)
+    dt = time.perf_counter() - t0
+    vec = n_pairs * geo[-1].grid.n_win_y * geo[-1].grid.n_win_x
+    sample = (f"{n_pairs} pair(s) of 2048^2: oracle-port FP64-FFT correlation of the 4 passes + "
+              f"{'reference fused_warp.c (SIMD route)' if ref_warp is not None else 'oracle warp'} x3, "
+              f"validation/infill omitted; {dt:.2f} s")
+    return vec / dt, sample, cores
+
+
+def run_reference(args):
+    ws, rank, _ = (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
+    if rank != 0:
+        return
+    vals = []
+    sample = ""
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        _cpu_baseline(args.cpu_pairs)
+    t_all = []
+    for _ in range(args.steps):
+        v, sample, cores = _cpu_baseline(args.cpu_pairs)
+        vals.append(v)
+    value = statistics.median(vals)
+    vec_step = 64009 * args.pairs
+    line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": vec_step / value * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "pairs_per_step": args.pairs, "timed_sample_pairs": args.cpu_pairs},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "vectors/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "vectors/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+
+    from pivtools_b200 import multipass, synthetic
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N = args.pairs
+    A, B = synthetic.channel_batch_torch(N, HW, seed=2026 + rank, device=dev)
+    mp = multipass.MultipassPIV(HW, N, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 1)):
+            mp.run(A, B)
+    stream.synchronize()
+    graph = None
+    if not args.no_graph:
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            mp.run(A, B)
+        for _ in range(args.warmup):
+            graph.replay()
+        torch.cuda.synchronize()
+
+    def step():
+        if graph is not None:
+            graph.replay()
+        else:
+            mp.run(A, B)
+
+    # ---- timed region: device events on the launching stream, max over ranks
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for k in range(args.steps):
+                step_ev[k][0].record(stream)
+                step()
+                step_ev[k][1].record(stream)
+            e1.record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    step_ms = sorted(a.elapsed_time(b) for a, b in step_ev)
+    if ws > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    vec_step = mp.vectors_per_step()
+    value = vec_step * ws / (ms * 1e-3)
+
+    # ---- dominant kernel: the final pass's correlation (32 px, 75%), timed alone
+    p = mp.passes[-1]
+    Lx = mp.Lx
+    o = p["out"]
+    nbytes = int(Lx.pivb_xcorr_scratch_bytes(N * p["ny"] * p["nx"], 1, 3))
+    import ctypes
+
+    def corr_launch():
+        s = ctypes.c_void_p(stream.cuda_stream)
+        Lx.pivb_xcorr_dev(mp.warped[0].data_ptr(), mp.warped[1].data_ptr(), HW[0] * HW[1], None, HW[0], HW[1], N,
+                          p["cx"].data_ptr(), p["cy"].data_ptr(), p["ny"], p["nx"], p["weight"].data_ptr(),
+                          p["weight"].data_ptr(), p["cw"].data_ptr(), 32, 32, 0, 1, 3, 0, o["pk_loc_x"].data_ptr(),
+                          o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(),
+                          o["sxy"].data_ptr(), p["ratio"].data_ptr(), None, mp.scratch.data_ptr(), nbytes, s)
+
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            corr_launch()
+        k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k0.record(stream)
+        R = 10
+        for _ in range(R):
+            corr_launch()
+        k1.record(stream)
+    stream.synchronize()
+    kern_ms = k0.elapsed_time(k1) / R
+    windows = N * p["ny"] * p["nx"]
+    alg_bytes = 2 * N * HW[0] * HW[1] * 4 + 7 * windows * 4
+    hbm_peak, bf16_peak, peak_kind = _peaks()
+    achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
+    fp32_flops = windows * 80.1e3
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "xcorr32_traffic.json")) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+    except Exception:
+        pass
+
+    # ---- end to end through host buffers: H2D of the step's frames from pinned
+    # memory, the step, D2H of the final vector field
+    Ah = torch.empty((N,) + HW, dtype=torch.float32, pin_memory=True)
+    Bh = torch.empty_like(Ah)
+    Ah.copy_(A)
+    Bh.copy_(B)
+    ux_h = torch.empty((N, p["ny"], p["nx"]), dtype=torch.float32, pin_memory=True)
+    uy_h = torch.empty_like(ux_h)
+    e2e_steps = max(2, min(args.steps, 5))
+    torch.cuda.synchronize()
+    if ws > 1:
+        torch.distributed.barrier()
+    with torch.cuda.stream(stream):
+        q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        for _ in range(e2e_steps):
+            A.copy_(Ah, non_blocking=True)
+            B.copy_(Bh, non_blocking=True)
+            step()
+            ux_h.copy_(p["ux"], non_blocking=True)
+            uy_h.copy_(p["uy"], non_blocking=True)
+        q1.record(stream)
+    stream.synchronize()
+    e2e_ms = q0.elapsed_time(q1) / e2e_steps
+    if ws > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = vec_step * ws / (e2e_ms * 1e-3)
+
+    cpu = None
+    if rank == 0 and ws == 1 and os.environ.get("PIVB_SKIP_CPU") != "1":
+        v, sample, cores = _cpu_baseline(args.cpu_pairs)
+        cpu = {"value": v, "unit": "vectors/s", "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "pairs_per_step_per_gpu": N, "image": "2048x2048",
+                       "passes": "128/64/32/32 px, 50/50/50/75%", "peak_finder": "gauss3", "warp": "bicubic",
+                       "vectors_per_step_per_gpu": vec_step, "windows_per_step_per_gpu": mp.windows_per_step(),
+                       "cuda_graph": graph is not None, "l2": "inputs 4.3 GB > L2, no flush",
+                       "parallelism": f"dp{ws} (pairs)"},
+            "pair_latency_ms": {"p50": step_ms[len(step_ms) // 2] / N, "p99": step_ms[-1] / N,
+                                "note": "per-pair share of a batched step; served latency comes from the serving loop"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "xcorr_kernel<32> (final pass, 4.1M windows)", "kernel_ms": kern_ms,
+                         "algorithmic_bytes": alg_bytes,
+                         "fp32_view": {"flops_per_launch": fp32_flops,
+                                       "achieved_tflops": fp32_flops / (kern_ms * 1e-3) / 1e12}},
+            "e2e": {"value": e2e_val, "unit": "vectors/s", "h2d_bytes_per_step": 2 * N * HW[0] * HW[1] * 4,
+                    "d2h_bytes_per_step": 2 * N * p["ny"] * p["nx"] * 4},
+            "gpu_launches": mp.launches_per_step * args.steps,
+            "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if graph is not None:
+        del graph
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

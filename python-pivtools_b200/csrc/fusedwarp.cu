@@ -39,18 +39,6 @@ __device__ __forceinline__ void keys4(float d, float *w)
     w[3] = fa(fm(fs(fm(fa(fm(-0.75f, s3), 3.75f), s3), 6.0f), s3), 3.0f);
 }
 
-// Lanczos-3 kernel value (fused_warp.c:120-127): sin in double, rounded once.
-__device__ __forceinline__ float lanczos3(float t)
-{
-    const float at = fabsf(t);
-    if (at < 1e-6f) return 1.0f;
-    if (at >= 3.0f) return 0.0f;
-    const float pt = fm((float)M_PI, at);
-    const float pta = __fdiv_rn(pt, 3.0f);
-    const float s1 = (float)sin((double)pt), s2 = (float)sin((double)pta);
-    return fm(__fdiv_rn(s1, pt), __fdiv_rn(s2, pta));
-}
-
 __device__ __forceinline__ void lanczos_w(float d, const float *lut, float *w)
 {
     const float pos = fm(d, (float)kLutN);
@@ -159,14 +147,29 @@ __global__ void pred_index_kernel(const float *ctrs, int nc, float *lut, int n)
     lut[p] = fa((float)seg, __fdiv_rn(fs(x, ctrs[seg]), den));
 }
 
-// Lanczos weight table at d = i / 4096, i = 0..4096 (fused_warp.c:148-158).
-__global__ void lanczos_lut_kernel(float *lut)
+// Lanczos-3 weight table at d = i / 4096, i = 0..4096 (fused_warp.c:120-158).
+// An input-independent constant of the algorithm: it is built once per process
+// with the host libm's sinf -- the function the reference's table is built
+// with, and not correctly rounded, so a device sin would differ from it in the
+// last bit of a few hundred entries -- and copied into each call's tables.
+float g_lut_host[(kLutN + 1) * 6];
+std::once_flag g_lut_once;
+void build_lut_host()
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > kLutN) return;
-    const float d = __fdiv_rn((float)i, (float)kLutN);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) lut[i * 6 + k] = lanczos3(fs(d, (float)(k - 2)));
+    for (int i = 0; i <= kLutN; ++i) {
+        const float d = (float)i / (float)kLutN;
+        for (int k = 0; k < 6; ++k) {
+            const float t = d - (float)(k - 2), at = fabsf(t);
+            float v;
+            if (at < 1e-6f) v = 1.0f;
+            else if (at >= 3.0f) v = 0.0f;
+            else {
+                const float pt = (float)M_PI * at, pta = pt / 3.0f;
+                v = (sinf(pt) / pt) * (sinf(pta) / pta);
+            }
+            g_lut_host[i * 6 + k] = v;
+        }
+    }
 }
 
 struct WarpParams {
@@ -271,7 +274,8 @@ PIV_EXPORT int pivb_warp_setup_dev(const float *d_ctrs_y, int nPY, const float *
     float *lut = reinterpret_cast<float *>(t + pad256((size_t)H * 4) + pad256((size_t)W * 4));
     pred_index_kernel<<<(H + 255) / 256, 256, 0, s>>>(d_ctrs_y, nPY, ly, H);
     pred_index_kernel<<<(W + 255) / 256, 256, 0, s>>>(d_ctrs_x, nPX, lx, W);
-    lanczos_lut_kernel<<<(kLutN + 1 + 255) / 256, 256, 0, s>>>(lut);
+    std::call_once(g_lut_once, build_lut_host);
+    if (cudaMemcpyAsync(lut, g_lut_host, sizeof(g_lut_host), cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

@@ -1,0 +1,342 @@
+// passglue.cu -- libpivb_pass: the work between multipass passes, on the GPU.
+//
+// The reference runs these steps in Python between its C calls
+// (pivtools_cli/piv/piv_backend/cpu_instantaneous.py:559-870, :1040-1071):
+//   validate  -- large-displacement gate, add the window-grid predictor, peak
+//                magnitude and normalised-median outlier tests
+//                (outlier_detection.py:56-84, :87-243);
+//   infill    -- harmonic inpainting of invalid vectors: minimise the squared
+//                gradients (physical units) over the invalid cells with the valid
+//                cells held fixed and zero flux at the grid edge
+//                (infilling.py:336-376), solved by Jacobi iteration;
+//   pad       -- edge-replicate padding onto the padded predictor grid
+//                (cpu_instantaneous.py:836-853) and the separable Gaussian
+//                smoothing of scipy.ndimage.gaussian_filter(mode='nearest')
+//                (cpu_instantaneous.py:1040-1048, :1140-1152);
+//   remap     -- Keys-cubic (a = -0.75) interpolation of the padded predictor at
+//                the next pass's window centres, replicate border
+//                (cpu_instantaneous.py:1050-1071).
+// The device has no libraries here: each step is a plain CUDA kernel over the
+// small vector grids, one launch per step for the whole batch of pairs.
+#include <math.h>
+
+#include "piv_common.cuh"
+
+namespace {
+
+__device__ __forceinline__ float qnanf() { return __int_as_float(0x7fc00000); }
+
+// Median of v[0..n) (n <= 24) for finite values only; NaN if none.
+__device__ float median_finite(float *v, int n)
+{
+    int m = 0;
+    for (int i = 0; i < n; ++i)
+        if (v[i] == v[i]) v[m++] = v[i];
+    if (m == 0) return qnanf();
+    for (int i = 1; i < m; ++i)
+        for (int j = i; j > 0 && v[j - 1] > v[j]; --j) { const float t = v[j]; v[j] = v[j - 1]; v[j - 1] = t; }
+    return (m & 1) ? v[m / 2] : 0.5f * (v[m / 2 - 1] + v[m / 2]);
+}
+
+struct ValParams {
+    const float *pk_x, *pk_y, *pk_h;      // (N, ny, nx), primary peak
+    const float *pred_dy, *pred_dx;       // (N, ny, nx) window-grid predictor, or null
+    const float *mask;                    // (ny, nx) 1 = masked, or null
+    int N, ny, nx;
+    float thresh_x, thresh_y;             // large-displacement gate
+    float peak_thr;                       // peak-magnitude threshold (<0 disables)
+    float med_eps, med_thr;               // normalised median (med_thr <= 0 disables)
+    int med_size;
+    float *ux, *uy;                       // out: displacement, NaN where invalid, 0 at masked
+    unsigned char *invalid;               // out: 1 where the vector must be infilled
+};
+
+// Stage 1: gate + predictor.  ux/uy receive the gated field (NaN where the
+// correlation failed or the displacement gate fired, 0 at masked windows);
+// invalid additionally marks peak-magnitude failures.  With the median test off
+// the invalid vectors are NaN-ed here, otherwise by median_kernel.
+__global__ void gate_kernel(ValParams p, int apply)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nv = (long long)p.N * p.ny * p.nx;
+    if (i >= nv) return;
+    const int w = (int)(i % ((long long)p.ny * p.nx));
+    const bool masked = p.mask && p.mask[w] != 0.0f;
+    float x = p.pk_x[i], y = p.pk_y[i], h = p.pk_h[i];
+    if (masked || fabsf(x) > p.thresh_x || fabsf(y) > p.thresh_y) { x = qnanf(); y = qnanf(); h = qnanf(); }
+    if (p.pred_dx) { x += p.pred_dx[i]; y += p.pred_dy[i]; }
+    bool bad = (x != x) || (y != y);
+    if (p.peak_thr >= 0.0f && ((h < p.peak_thr) || (h != h))) bad = true;
+    bad = bad && !masked;
+    if (apply && bad) { x = qnanf(); y = qnanf(); }
+    p.ux[i] = masked ? 0.0f : x;
+    p.uy[i] = masked ? 0.0f : y;
+    p.invalid[i] = bad ? 1 : 0;
+}
+
+// Stage 2: normalised-median test on the gated field gx/gy (vector-norm
+// residual over the size x size neighbourhood without the node, 3x3 presence
+// guard), OR-ed with the stage-1 flags; invalid vectors become NaN.
+__global__ void median_kernel(ValParams p, const float *gx, const float *gy)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nv = (long long)p.N * p.ny * p.nx;
+    if (i >= nv) return;
+    const int plane = p.ny * p.nx;
+    const int n = (int)(i / plane), w = (int)(i % plane), r = w / p.nx, c = w % p.nx;
+    const bool masked = p.mask && p.mask[w] != 0.0f;
+    if (masked) return;
+    const float *X = gx + (long long)n * plane, *Y = gy + (long long)n * plane;
+    const int h = p.med_size / 2;
+    float nu[24], nvv[24];
+    int k = 0, present = 0;
+    for (int dr = -h; dr <= h; ++dr)
+        for (int dc = -h; dc <= h; ++dc) {
+            const int rr = r + dr, cc = c + dc;
+            const bool inside = rr >= 0 && rr < p.ny && cc >= 0 && cc < p.nx;
+            float a = qnanf(), b = qnanf();
+            bool mk = false;
+            if (inside) {
+                mk = p.mask && p.mask[rr * p.nx + cc] != 0.0f;
+                if (!mk) { a = X[rr * p.nx + cc]; b = Y[rr * p.nx + cc]; }
+                if (abs(dr) <= 1 && abs(dc) <= 1 && (mk || a == a)) ++present;
+            }
+            if (!dr && !dc) continue;
+            nu[k] = a;
+            nvv[k] = b;
+            ++k;
+        }
+    float tu[24], tv[24];
+    for (int j = 0; j < k; ++j) { tu[j] = nu[j]; tv[j] = nvv[j]; }
+    const float mu = median_finite(tu, k), mv = median_finite(tv, k);
+    const float u0 = X[w], v0 = Y[w];
+    const float r0 = sqrtf((u0 - mu) * (u0 - mu) + (v0 - mv) * (v0 - mv));
+    float ri[24];
+    for (int j = 0; j < k; ++j)
+        ri[j] = sqrtf((nu[j] - mu) * (nu[j] - mu) + (nvv[j] - mv) * (nvv[j] - mv));
+    const float rm = median_finite(ri, k);
+    const float nr = r0 / (rm + p.med_eps);
+    const bool bad = p.invalid[i] || (nr > p.med_thr) || !isfinite(nr) || present < 6;
+    p.invalid[i] = bad ? 1 : 0;
+    p.ux[i] = bad ? qnanf() : u0;
+    p.uy[i] = bad ? qnanf() : v0;
+}
+
+// Harmonic inpainting: one CTA per pair, Jacobi sweeps over the invalid cells.
+// Weights 1/dx^2 (x neighbours) and 1/dy^2 (y neighbours); neighbours outside
+// the grid or masked drop out (zero flux).  Cells start from the mean of the
+// pair's valid vectors; iteration stops at max_iter or when the largest update
+// is below tol (px).
+__global__ void __launch_bounds__(512) infill_kernel(float *ux, float *uy, const unsigned char *invalid,
+                                                     const float *mask, int ny, int nx, float wy, float wx,
+                                                     int max_iter, float tol, float *work)
+{
+    const int n = blockIdx.x;
+    const int plane = ny * nx;
+    float *X = ux + (long long)n * plane, *Y = uy + (long long)n * plane;
+    const unsigned char *bad = invalid + (long long)n * plane;
+    float *X2 = work + (long long)n * 2 * plane, *Y2 = X2 + plane;
+    __shared__ float s_max;
+    __shared__ int s_any;
+    if (threadIdx.x == 0) s_any = 0;
+    __syncthreads();
+    for (int w = threadIdx.x; w < plane; w += blockDim.x)
+        if (bad[w]) s_any = 1;
+    __syncthreads();
+    if (!s_any) return;
+    // initial guess: mean of the valid vectors (the iteration converges to the
+    // unique harmonic solution from any start; a good start shortens it)
+    __shared__ float s_su, s_sv, s_n;
+    if (threadIdx.x == 0) { s_su = 0.0f; s_sv = 0.0f; s_n = 0.0f; }
+    __syncthreads();
+    {
+        float su = 0.0f, sv = 0.0f, cnt = 0.0f;
+        for (int w = threadIdx.x; w < plane; w += blockDim.x)
+            if (!bad[w] && !(mask && mask[w] != 0.0f)) { su += X[w]; sv += Y[w]; cnt += 1.0f; }
+        atomicAdd(&s_su, su);
+        atomicAdd(&s_sv, sv);
+        atomicAdd(&s_n, cnt);
+    }
+    __syncthreads();
+    const float mu = s_n > 0.0f ? s_su / s_n : 0.0f, mv = s_n > 0.0f ? s_sv / s_n : 0.0f;
+    for (int w = threadIdx.x; w < plane; w += blockDim.x) {
+        if (bad[w]) { X[w] = mu; Y[w] = mv; }
+        X2[w] = X[w];
+        Y2[w] = Y[w];
+    }
+    __syncthreads();
+    for (int it = 0; it < max_iter; ++it) {
+        if (threadIdx.x == 0) s_max = 0.0f;
+        __syncthreads();
+        float local = 0.0f;
+        const float *sx = (it & 1) ? X2 : X, *sy = (it & 1) ? Y2 : Y;
+        float *dx = (it & 1) ? X : X2, *dy = (it & 1) ? Y : Y2;
+        for (int w = threadIdx.x; w < plane; w += blockDim.x) {
+            if (!bad[w]) { dx[w] = sx[w]; dy[w] = sy[w]; continue; }
+            const int r = w / nx, c = w % nx;
+            float su = 0.0f, sv = 0.0f, sw = 0.0f;
+            const int nr[4] = {r - 1, r + 1, r, r};
+            const int nc[4] = {c, c, c - 1, c + 1};
+            const float ww[4] = {wy, wy, wx, wx};
+            for (int k = 0; k < 4; ++k) {
+                if (nr[k] < 0 || nr[k] >= ny || nc[k] < 0 || nc[k] >= nx) continue;
+                const int q = nr[k] * nx + nc[k];
+                if (mask && mask[q] != 0.0f) continue;
+                su += ww[k] * sx[q];
+                sv += ww[k] * sy[q];
+                sw += ww[k];
+            }
+            const float nu = sw > 0.0f ? su / sw : sx[w], nv = sw > 0.0f ? sv / sw : sy[w];
+            local = fmaxf(local, fmaxf(fabsf(nu - sx[w]), fabsf(nv - sy[w])));
+            dx[w] = nu;
+            dy[w] = nv;
+        }
+        atomicMax(reinterpret_cast<int *>(&s_max), __float_as_int(local));   // local >= 0
+        __syncthreads();
+        const bool done = s_max < tol;
+        __syncthreads();
+        if (done || it == max_iter - 1) {
+            if (!(it & 1)) {   // result is in X2/Y2
+                for (int w = threadIdx.x; w < plane; w += blockDim.x) { X[w] = X2[w]; Y[w] = Y2[w]; }
+            }
+            break;
+        }
+    }
+}
+
+// Edge-replicate padding (ny, nx) -> (nyp, nxp) with the measured grid at
+// (pre_y, pre_x); channel order (dy, dx) -> two planes.
+__global__ void pad_kernel(const float *ux, const float *uy, int N, int ny, int nx, int nyp, int nxp, int pre_y,
+                           int pre_x, float *pdy, float *pdx)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)N * nyp * nxp) return;
+    const int n = (int)(i / ((long long)nyp * nxp)), w = (int)(i % ((long long)nyp * nxp));
+    const int r = min(max(w / nxp - pre_y, 0), ny - 1), c = min(max(w % nxp - pre_x, 0), nx - 1);
+    const long long s = (long long)n * ny * nx + r * nx + c;
+    pdy[i] = uy[s];
+    pdx[i] = ux[s];
+}
+
+// One separable Gaussian pass (mode 'nearest'), along x (axis 1) or y (axis 0).
+__global__ void gauss_kernel(const float *in, float *out, int N, int ny, int nx, const float *taps, int radius, int axis)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)N * ny * nx) return;
+    const int n = (int)(i / ((long long)ny * nx)), w = (int)(i % ((long long)ny * nx));
+    const int r = w / nx, c = w % nx;
+    const float *P = in + (long long)n * ny * nx;
+    double acc = 0.0;
+    for (int k = -radius; k <= radius; ++k) {
+        const int rr = axis == 0 ? min(max(r + k, 0), ny - 1) : r;
+        const int cc = axis == 1 ? min(max(c + k, 0), nx - 1) : c;
+        acc += (double)taps[k + radius] * (double)P[rr * nx + cc];
+    }
+    out[i] = (float)acc;
+}
+
+__device__ __forceinline__ void keys4(float d, float *w)
+{
+    const float s0 = 1.0f + d, q2 = 1.0f - d, s3 = 2.0f - d;
+    w[1] = (1.25f * d - 2.25f) * d * d + 1.0f;
+    w[2] = (1.25f * q2 - 2.25f) * q2 * q2 + 1.0f;
+    w[0] = ((-0.75f * s0 + 3.75f) * s0 - 6.0f) * s0 + 3.0f;
+    w[3] = ((-0.75f * s3 + 3.75f) * s3 - 6.0f) * s3 + 3.0f;
+}
+
+// Cubic remap of both padded planes at fractional grid coordinates.
+__global__ void remap_kernel(const float *pdy, const float *pdx, int N, int nyp, int nxp, const float *map_y,
+                             const float *map_x, int ny, int nx, float *oy, float *ox)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)N * ny * nx) return;
+    const int n = (int)(i / ((long long)ny * nx)), w = (int)(i % ((long long)ny * nx));
+    const float fy = map_y[w], fx = map_x[w];
+    const float fyf = floorf(fy), fxf = floorf(fx);
+    float wy[4], wx[4];
+    keys4(fy - fyf, wy);
+    keys4(fx - fxf, wx);
+    const int by = (int)fyf - 1, bx = (int)fxf - 1;
+    const float *Py = pdy + (long long)n * nyp * nxp, *Px = pdx + (long long)n * nyp * nxp;
+    float vy = 0.0f, vx = 0.0f;
+    for (int m = 0; m < 4; ++m) {
+        const int r = min(max(by + m, 0), nyp - 1);
+        for (int q = 0; q < 4; ++q) {
+            const int c = min(max(bx + q, 0), nxp - 1);
+            const float wt = wy[m] * wx[q];
+            vy += wt * Py[r * nxp + c];
+            vx += wt * Px[r * nxp + c];
+        }
+    }
+    oy[i] = vy;
+    ox[i] = vx;
+}
+
+inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+// Validation of one pass for N pairs.  pred_* (nullable) is the window-grid
+// predictor added to the correlation result.  Outputs ux, uy (NaN = to infill,
+// 0 at masked windows) and invalid flags.  work: 2*N*ny*nx floats.
+PIV_EXPORT int pivb_validate_dev(const float *pk_x, const float *pk_y, const float *pk_h, const float *pred_dy,
+                                 const float *pred_dx, const float *mask, int N, int ny, int nx, float thresh_x,
+                                 float thresh_y, float peak_thr, float med_eps, float med_thr, int med_size,
+                                 float *ux, float *uy, unsigned char *invalid, float *work, void *stream)
+{
+    if (N <= 0 || ny <= 0 || nx <= 0 || med_size < 3 || med_size > 5 || !(med_size & 1)) return 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    ValParams p{pk_x, pk_y, pk_h, pred_dy, pred_dx, mask, N, ny, nx, thresh_x, thresh_y, peak_thr, med_eps,
+                med_thr, med_size, ux, uy, invalid};
+    const long long nv = (long long)N * ny * nx;
+    gate_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, med_thr > 0.0f ? 0 : 1);
+    if (med_thr > 0.0f) {
+        float *gx = work, *gy = work + nv;
+        cudaMemcpyAsync(gx, ux, nv * 4, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(gy, uy, nv * 4, cudaMemcpyDeviceToDevice, s);
+        median_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, gx, gy);
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Harmonic infilling of the invalid vectors, in place.  work: 2*N*ny*nx floats.
+PIV_EXPORT int pivb_infill_dev(float *ux, float *uy, const unsigned char *invalid, const float *mask, int N, int ny,
+                               int nx, float spacing_y, float spacing_x, int max_iter, float tol, float *work,
+                               void *stream)
+{
+    if (N <= 0 || ny <= 0 || nx <= 0 || spacing_y <= 0.0f || spacing_x <= 0.0f) return 1;
+    const float wy = 1.0f / (spacing_y * spacing_y), wx = 1.0f / (spacing_x * spacing_x);
+    infill_kernel<<<N, 512, 0, (cudaStream_t)stream>>>(ux, uy, invalid, mask, ny, nx, wy, wx, max_iter, tol, work);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Padding onto the predictor grid and optional Gaussian smoothing.  taps
+// (2*radius+1, device) are the normalised kernel; radius 0 skips smoothing.
+// work: N*nyp*nxp floats.
+PIV_EXPORT int pivb_pad_smooth_dev(const float *ux, const float *uy, int N, int ny, int nx, int nyp, int nxp,
+                                   int pre_y, int pre_x, const float *taps, int radius, float *pdy, float *pdx,
+                                   float *work, void *stream)
+{
+    if (N <= 0 || ny <= 0 || nx <= 0 || nyp < ny || nxp < nx) return 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long n = (long long)N * nyp * nxp;
+    pad_kernel<<<blocks(n, 256), 256, 0, s>>>(ux, uy, N, ny, nx, nyp, nxp, pre_y, pre_x, pdy, pdx);
+    if (radius > 0) {
+        for (float *f : {pdy, pdx}) {
+            gauss_kernel<<<blocks(n, 256), 256, 0, s>>>(f, work, N, nyp, nxp, taps, radius, 1);
+            gauss_kernel<<<blocks(n, 256), 256, 0, s>>>(work, f, N, nyp, nxp, taps, radius, 0);
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Predictor at the next pass's window centres.
+PIV_EXPORT int pivb_remap_dev(const float *pdy, const float *pdx, int N, int nyp, int nxp, const float *map_y,
+                              const float *map_x, int ny, int nx, float *out_dy, float *out_dx, void *stream)
+{
+    if (N <= 0 || ny <= 0 || nx <= 0 || nyp <= 0 || nxp <= 0) return 1;
+    const long long n = (long long)N * ny * nx;
+    remap_kernel<<<blocks(n, 256), 256, 0, (cudaStream_t)stream>>>(pdy, pdx, N, nyp, nxp, map_y, map_x, ny, nx,
+                                                                     out_dy, out_dx);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}

@@ -581,6 +581,7 @@ __global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS) accum_kernel(AccumPara
             }
             float x1[M], x2[M];
             float s_ab = 1.0f, s_aa = 1.0f, s_bb = 1.0f;
+            bool skip = false;
             if (!prm.triple) {
 #pragma unroll
                 for (int k = 0; k < M; ++k) {
@@ -628,7 +629,9 @@ __global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS) accum_kernel(AccumPara
                 if (prm.ppn) {
                     eaa = g.sum(eaa);
                     ebb = g.sum(ebb);
-                    if (eaa <= 0.0f || ebb <= 0.0f) continue;   // group-uniform
+                    // a pair without signal contributes to no plane; the group still
+                    // runs the transforms (groups share warps and their shuffles)
+                    if (eaa <= 0.0f || ebb <= 0.0f) skip = true;
                     s_ab = 1.0f / sqrtf(eaa * ebb);
                     s_aa = 1.0f / eaa;
                     s_bb = 1.0f / ebb;
@@ -638,7 +641,7 @@ __global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS) accum_kernel(AccumPara
                 fft2_forward<N>(g, S, x3, x4);
                 spectrum_product<N, 1>(g, S, z);
                 fft2_inverse<N>(g, S, z);
-                if (valid) {
+                if (valid && !skip) {
 #pragma unroll
                     for (int k = 0; k < M; ++k) {
                         const int row = (M * q + k + N / 2) % N - prm.sy0;
@@ -655,7 +658,7 @@ __global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS) accum_kernel(AccumPara
             fft2_forward<N>(g, S, x1, x2);
             spectrum_product<N, 0>(g, S, z);
             fft2_inverse<N>(g, S, z);
-            if (valid) {
+            if (valid && !skip) {
 #pragma unroll
                 for (int k = 0; k < M; ++k) {
                     const int row = (M * q + k + N / 2) % N - prm.sy0;

@@ -142,6 +142,29 @@ def kspacefit_lib() -> ctypes.CDLL:
     L.kspace_fft2_centered.restype = ci
     L.kspace_debug_prep.argtypes = [f64p, f64p, f64p, vp, ci, ci, f64p, ctypes.POINTER(ctypes.c_double)]
     L.kspace_debug_prep.restype = ci
+    L.pivb_kspace_scratch_bytes.argtypes = [ci, ci, ci]
+    L.pivb_kspace_scratch_bytes.restype = csz
+    L.pivb_kspace_fit_dev.argtypes = [vp, vp, vp, vp, vp, ci, ci, ci, ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                      vp, vp, vp, csz, vp]
+    L.pivb_kspace_fit_dev.restype = ci
+    L._pivb_bound = True
+    return L
+
+
+def pass_lib() -> ctypes.CDLL:
+    L = _load("libpivb_pass.so")
+    if getattr(L, "_pivb_bound", False):
+        return L
+    fl = ctypes.c_float
+    L.pivb_validate_dev.argtypes = [vp, vp, vp, vp, vp, vp, ci, ci, ci, fl, fl, fl, fl, fl, ci, vp, vp, vp, vp,
+                                    vp]
+    L.pivb_validate_dev.restype = ci
+    L.pivb_infill_dev.argtypes = [vp, vp, vp, vp, ci, ci, ci, fl, fl, ci, fl, vp, vp]
+    L.pivb_infill_dev.restype = ci
+    L.pivb_pad_smooth_dev.argtypes = [vp, vp, ci, ci, ci, ci, ci, ci, ci, vp, ci, vp, vp, vp, vp]
+    L.pivb_pad_smooth_dev.restype = ci
+    L.pivb_remap_dev.argtypes = [vp, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, vp]
+    L.pivb_remap_dev.restype = ci
     L._pivb_bound = True
     return L
 

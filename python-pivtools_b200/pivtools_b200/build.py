@@ -28,6 +28,7 @@ TARGETS = {
     "libbulkxcorr2d.so": "bulkxcorr2d.cu",
     "libfusedwarp.so": "fusedwarp.cu",
     "libkspacefit.so": "kspacefit.cu",
+    "libpivb_pass.so": "passglue.cu",
 }
 
 

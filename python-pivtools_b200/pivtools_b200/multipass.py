@@ -1,0 +1,210 @@
+"""GPU-resident multipass window-deformation PIV (instantaneous mode).
+
+Follows the pass loop of the reference driver
+(pivtools_cli/piv/piv_backend/cpu_instantaneous.py:381-927, :995-1133) for a
+batch of N image pairs kept on the device:
+
+  pass 0      correlate the raw frames;
+  pass k > 0  remap the (smoothed, padded) predictor of pass k-1 to this pass's
+              window centres, warp both frames symmetrically by it, correlate;
+  every pass  gate large displacements (win/2 on pass 0, win/4 after), add the
+              predictor, reject peak-magnitude and normalised-median outliers,
+              infill, then (not on the last pass) pad onto the padded grid and
+              smooth -- the predictor of the next pass.
+
+Every step is a CUDA kernel launched on the caller's stream with no host
+synchronisation, so a whole batch step can be captured as one CUDA graph.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib, geometry
+
+
+@dataclass
+class MultipassConfig:
+    window_sizes: list = field(default_factory=lambda: [(128, 128), (64, 64), (32, 32), (32, 32)])
+    overlaps: list = field(default_factory=lambda: [50, 50, 50, 75])
+    window_type: str = "gaussian"
+    peak_finder: int = 3
+    peakfit_impl: int = 0
+    interp_mode: int = 0            # 0 bicubic, 1 Lanczos-3
+    warp_impl: int = 1
+    predictor_smoothing: bool = True
+    peak_mag_threshold: float = 0.25
+    median_epsilon: float = 0.1
+    median_threshold: float = 2.0
+    median_size: int = 5
+    infill_iters: int = 400
+    infill_tol: float = 1e-3
+    final_infill: bool = True
+
+
+def _gauss_taps(sigma: float, ksize: int):
+    """Normalised taps of scipy.ndimage.gaussian_filter with truncate =
+    (ksize-1)/(2 sigma) (cpu_instantaneous.py:1042-1048)."""
+    if sigma <= 0:
+        return np.ones(1, np.float32), 0
+    truncate = (ksize - 1) / (2 * sigma)
+    radius = int(truncate * sigma + 0.5)
+    x = np.arange(-radius, radius + 1, dtype=np.float64)
+    w = np.exp(-0.5 * (x / sigma) ** 2)
+    return (w / w.sum()).astype(np.float32), radius
+
+
+class MultipassPIV:
+    """Multipass PIV for batches of N pairs of one image size on one GPU."""
+
+    def __init__(self, image_shape, n_pairs: int, cfg: MultipassConfig | None = None, device=None):
+        import torch
+
+        self.torch = torch
+        self.cfg = cfg or MultipassConfig()
+        self.device = torch.device("cuda" if device is None else device)
+        self.H, self.W = image_shape
+        self.N = n_pairs
+        self.geo = geometry.multipass_geometry(image_shape, self.cfg.window_sizes, self.cfg.overlaps,
+                                               self.cfg.window_type)
+        self.Lx = _lib.bulkxcorr2d_lib()
+        self.Lw = _lib.fusedwarp_lib()
+        self.Lp = _lib.pass_lib()
+        dev, f32 = self.device, torch.float32
+        N, H, W = self.N, self.H, self.W
+        self.warped = [torch.empty((N, H, W), dtype=f32, device=dev) for _ in range(2)]
+        self.passes = []
+        max_scratch = 0
+        max_vec = 0
+        max_pad = 0
+        for k, g in enumerate(self.geo):
+            ny, nx = g.grid.n_win_y, g.grid.n_win_x
+            nyp, nxp = len(g.ctrs_y_all), len(g.ctrs_x_all)
+            w = torch.tensor(geometry.window_weight(g.window_size, self.cfg.window_type), device=dev)
+            cw = torch.empty_like(w)
+            p = dict(
+                ny=ny, nx=nx, nyp=nyp, nxp=nxp, win=g.window_size[0], weight=w, cw=cw,
+                cx=torch.tensor(g.grid.win_ctrs_x, device=dev), cy=torch.tensor(g.grid.win_ctrs_y, device=dev),
+                cx_all=torch.tensor(g.ctrs_x_all, device=dev), cy_all=torch.tensor(g.ctrs_y_all, device=dev),
+                out={k2: torch.empty((N, 1, ny, nx), dtype=f32, device=dev)
+                     for k2 in ("pk_loc_x", "pk_loc_y", "pk_height", "sx", "sy", "sxy")},
+                ratio=torch.empty((N, ny, nx), dtype=f32, device=dev),
+                ux=torch.empty((N, ny, nx), dtype=f32, device=dev),
+                uy=torch.empty((N, ny, nx), dtype=f32, device=dev),
+                invalid=torch.empty((N, ny, nx), dtype=torch.uint8, device=dev),
+                pdy=torch.empty((N, nyp, nxp), dtype=f32, device=dev),
+                pdx=torch.empty((N, nyp, nxp), dtype=f32, device=dev),
+                spacing=(float(g.grid.win_spacing_y), float(g.grid.win_spacing_x)),
+                pre=g.n_pre,
+            )
+            if k > 0:
+                p["map_x"] = torch.tensor(g.pred_map_x, device=dev)
+                p["map_y"] = torch.tensor(g.pred_map_y, device=dev)
+                p["pred_dy"] = torch.empty((N, ny, nx), dtype=f32, device=dev)
+                p["pred_dx"] = torch.empty((N, ny, nx), dtype=f32, device=dev)
+            if k + 1 < len(self.geo):
+                taps, rad = _gauss_taps(self.geo[k + 1].sd if self.cfg.predictor_smoothing else 0.0,
+                                        self.geo[k + 1].ksize_filt[0])
+                p["taps"] = torch.tensor(taps, device=dev)
+                p["radius"] = rad
+            max_scratch = max(max_scratch, int(self.Lx.pivb_xcorr_scratch_bytes(N * ny * nx, 1, self.cfg.peak_finder)))
+            max_vec = max(max_vec, N * ny * nx)
+            max_pad = max(max_pad, N * nyp * nxp)
+            self.passes.append(p)
+        self.scratch = torch.empty(max(max_scratch, 256), dtype=torch.uint8, device=dev)
+        self.work = torch.empty(max(2 * max_vec, max_pad), dtype=f32, device=dev)
+        # warp tables per pass (centres of the previous pass's padded grid)
+        tb = int(self.Lw.pivb_warp_table_bytes(H, W))
+        self.tables = [None] + [torch.empty(tb, dtype=torch.uint8, device=dev) for _ in self.geo[1:]]
+        s = self._stream()
+        for k in range(1, len(self.geo)):
+            prev = self.passes[k - 1]
+            self._ok(self.Lw.pivb_warp_setup_dev(prev["cy_all"].data_ptr(), prev["nyp"], prev["cx_all"].data_ptr(),
+                                                 prev["nxp"], H, W, self.tables[k].data_ptr(), s), "warp setup")
+        for p in self.passes:
+            self._ok(self.Lx.pivb_correl_weight_dev(p["weight"].data_ptr(), p["win"], p["win"], p["cw"].data_ptr(), s),
+                     "correlation weight")
+        self.launches_per_step = self._count_launches()
+
+    # ------------------------------------------------------------------ #
+    def _stream(self):
+        return ctypes.c_void_p(self.torch.cuda.current_stream(self.device).cuda_stream)
+
+    @staticmethod
+    def _ok(code, what):
+        if code != 0:
+            raise RuntimeError(f"{what} failed with code {code}")
+
+    def _count_launches(self):
+        n = 0
+        for k in range(len(self.geo)):
+            n += 1                                        # correlation
+            n += 1 if (self.cfg.peak_finder >= 4) else 0  # deferred LM
+            n += 2 if self.cfg.median_threshold > 0 else 1  # validate (+ median)
+            if k + 1 < len(self.geo) or self.cfg.final_infill:
+                n += 1                                    # infill
+            if k + 1 < len(self.geo):
+                n += 1 + (4 if self.passes[k]["radius"] > 0 else 0)   # pad (+ smoothing)
+            if k > 0:
+                n += 2                                    # remap, warp
+        return n
+
+    def run(self, A, B):
+        """A, B: (N, H, W) float32 CUDA tensors.  Returns (ux, uy) of the final pass
+        (device tensors, views into internal buffers)."""
+        cfg = self.cfg
+        s = self._stream()
+        N, H, W = self.N, self.H, self.W
+        scr = self.scratch
+        for k, p in enumerate(self.passes):
+            if k == 0:
+                fa, fb = A, B
+                pred_dy = pred_dx = None
+            else:
+                prev = self.passes[k - 1]
+                self._ok(self.Lp.pivb_remap_dev(prev["pdy"].data_ptr(), prev["pdx"].data_ptr(), N, prev["nyp"],
+                                                prev["nxp"], p["map_y"].data_ptr(), p["map_x"].data_ptr(), p["ny"],
+                                                p["nx"], p["pred_dy"].data_ptr(), p["pred_dx"].data_ptr(), s), "remap")
+                fa, fb = self.warped
+                self._ok(self.Lw.pivb_warp_dev(A.data_ptr(), B.data_ptr(), fa.data_ptr(), fb.data_ptr(),
+                                               prev["pdy"].data_ptr(), prev["pdx"].data_ptr(), N, H, W, prev["nyp"],
+                                               prev["nxp"], H * W, self.tables[k].data_ptr(), cfg.interp_mode, 0, 0,
+                                               cfg.warp_impl, s), "warp")
+                pred_dy, pred_dx = p["pred_dy"], p["pred_dx"]
+            o = p["out"]
+            nbytes = int(self.Lx.pivb_xcorr_scratch_bytes(N * p["ny"] * p["nx"], 1, cfg.peak_finder))
+            self._ok(self.Lx.pivb_xcorr_dev(
+                fa.data_ptr(), fb.data_ptr(), H * W, None, H, W, N, p["cx"].data_ptr(), p["cy"].data_ptr(),
+                p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win"],
+                p["win"], 0, 1, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(),
+                o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(), o["sxy"].data_ptr(),
+                p["ratio"].data_ptr(), None, scr.data_ptr(), nbytes, s), "correlation")
+            thr = p["win"] / 2.0 if k == 0 else p["win"] / 4.0
+            self._ok(self.Lp.pivb_validate_dev(
+                o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(),
+                None if pred_dy is None else pred_dy.data_ptr(), None if pred_dx is None else pred_dx.data_ptr(),
+                None, N, p["ny"], p["nx"], thr, thr, cfg.peak_mag_threshold, cfg.median_epsilon,
+                cfg.median_threshold, cfg.median_size, p["ux"].data_ptr(), p["uy"].data_ptr(),
+                p["invalid"].data_ptr(), self.work.data_ptr(), s), "validate")
+            last = k + 1 == len(self.passes)
+            if not last or cfg.final_infill:
+                self._ok(self.Lp.pivb_infill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), None,
+                                                 N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
+                                                 cfg.infill_iters, cfg.infill_tol, self.work.data_ptr(), s), "infill")
+            if not last:
+                self._ok(self.Lp.pivb_pad_smooth_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), N, p["ny"], p["nx"],
+                                                     p["nyp"], p["nxp"], p["pre"][0], p["pre"][1],
+                                                     p["taps"].data_ptr(), p["radius"], p["pdy"].data_ptr(),
+                                                     p["pdx"].data_ptr(), self.work.data_ptr(), s), "pad/smooth")
+        last = self.passes[-1]
+        return last["ux"], last["uy"]
+
+    def vectors_per_step(self) -> int:
+        p = self.passes[-1]
+        return self.N * p["ny"] * p["nx"]
+
+    def windows_per_step(self) -> int:
+        return self.N * sum(p["ny"] * p["nx"] for p in self.passes)

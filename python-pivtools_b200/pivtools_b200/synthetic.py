@@ -129,3 +129,48 @@ def particle_pair(shape, seed, density=0.05, sigma=0.6, i_range=(1000.0, 4000.0)
     A = torch.clamp(torch.poisson(ia + background, generator=ga), 0, 65535).float()
     B = torch.clamp(torch.poisson(ib + background, generator=gb), 0, 65535).float()
     return A, B, (u, v)
+
+
+def channel_batch_torch(n_pairs, shape, seed, device, peak=12.0, re_tau=1000.0, rms_frac=0.08, corr_len=24.0,
+                        density=0.05, sigma=0.6, i_range=(1000.0, 4000.0), background=100.0):
+    """Benchmark batch of channel-flow pairs rendered on the GPU: (A, B) as
+    (n_pairs, H, W) float32 CUDA tensors.  Fluctuation fields are Gaussian random
+    fields made by spectral filtering on the device; particles come from
+    numpy.random.default_rng(seed + pair)."""
+    import torch
+
+    h, w = shape
+    y = (np.arange(h) + 0.5) / h
+    yw = np.minimum(y, 1.0 - y) * 2.0 * re_tau
+    uplus = np.where(yw < 11.0, yw, np.log(np.maximum(yw, 1e-9)) / 0.41 + 5.2)
+    prof = torch.tensor(uplus / uplus.max() * peak, device=device, dtype=torch.float64)
+    ky = torch.fft.fftfreq(h, device=device, dtype=torch.float64)[:, None]
+    kx = torch.fft.fftfreq(w, device=device, dtype=torch.float64)[None, :]
+    filt = torch.exp(-2.0 * (np.pi * corr_len / 2.0) ** 2 * (kx * kx + ky * ky))
+    A = torch.empty((n_pairs, h, w), dtype=torch.float32, device=device)
+    B = torch.empty_like(A)
+    for k in range(n_pairs):
+        g = torch.Generator(device=device).manual_seed(int(seed) * 1000003 + k)
+        fields = []
+        for _ in range(2):
+            f = torch.fft.ifft2(torch.fft.fft2(torch.randn((h, w), generator=g, device=device,
+                                                           dtype=torch.float64)) * filt).real
+            fields.append(f * (rms_frac * peak / f.std()))
+        u = prof[:, None] + fields[0]
+        v = fields[1]
+        rng = np.random.default_rng(seed * 7919 + k)
+        n = int(round(density * h * w))
+        xs = rng.uniform(-8.0, w + 8.0, n)
+        ys = rng.uniform(-8.0, h + 8.0, n)
+        amp = rng.uniform(i_range[0], i_range[1], n)
+        xi = torch.as_tensor(np.clip(np.round(xs), 0, w - 1).astype(np.int64), device=device)
+        yi = torch.as_tensor(np.clip(np.round(ys), 0, h - 1).astype(np.int64), device=device)
+        xs_t = torch.as_tensor(xs, device=device)
+        ys_t = torch.as_tensor(ys, device=device)
+        xb = (xs_t + u[yi, xi]).cpu().numpy()
+        yb = (ys_t + v[yi, xi]).cpu().numpy()
+        ia = _render_torch(shape, xs, ys, amp, sigma, device)
+        ib = _render_torch(shape, xb, yb, amp, sigma, device)
+        A[k] = torch.clamp(torch.poisson(ia + background, generator=g), 0, 65535).float()
+        B[k] = torch.clamp(torch.poisson(ib + background, generator=g), 0, 65535).float()
+    return A, B

@@ -16,6 +16,7 @@ HEADER_LIB = {
     "libbulkxcorr2d.h": "libbulkxcorr2d.so",
     "libfusedwarp.h": "libfusedwarp.so",
     "libkspacefit.h": "libkspacefit.so",
+    "libpivb_pass.h": "libpivb_pass.so",
 }
 
 

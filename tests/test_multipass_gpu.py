@@ -1,0 +1,223 @@
+"""GPU multipass: the inter-pass glue kernels against NumPy/SciPy restatements of
+the reference's Python steps, and the resident multipass driver against known
+displacement fields."""
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from pivtools_b200 import _lib, geometry, multipass, synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(x, dev, dtype=None):
+    import torch
+
+    return torch.as_tensor(np.ascontiguousarray(x), device=dev, dtype=dtype)
+
+
+def _stream():
+    import torch
+
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _median_ref(ux, uy, eps, thr, size):
+    """Normalised median (vector norm, size x size without the node, 3x3 guard)."""
+    ny, nx = ux.shape
+    h = size // 2
+    out = np.zeros((ny, nx), bool)
+    for r in range(ny):
+        for c in range(nx):
+            nu, nv, present = [], [], 0
+            for dr in range(-h, h + 1):
+                for dc in range(-h, h + 1):
+                    rr, cc = r + dr, c + dc
+                    a = b = np.nan
+                    if 0 <= rr < ny and 0 <= cc < nx:
+                        a, b = ux[rr, cc], uy[rr, cc]
+                        if abs(dr) <= 1 and abs(dc) <= 1 and not np.isnan(a):
+                            present += 1
+                    if dr == 0 and dc == 0:
+                        continue
+                    nu.append(a)
+                    nv.append(b)
+            nu, nv = np.array(nu, np.float32), np.array(nv, np.float32)
+            if np.all(np.isnan(nu)):
+                out[r, c] = True
+                continue
+            mu, mv = np.nanmedian(nu), np.nanmedian(nv)
+            r0 = np.sqrt((ux[r, c] - mu) ** 2 + (uy[r, c] - mv) ** 2)
+            ri = np.sqrt((nu - mu) ** 2 + (nv - mv) ** 2)
+            rm = np.nanmedian(ri) if np.any(~np.isnan(ri)) else np.nan
+            nr = r0 / (rm + eps)
+            out[r, c] = (not np.isfinite(nr)) or nr > thr or present < 6
+    return out
+
+
+def test_validate_matches_restatement(cuda):
+    import torch
+
+    L = _lib.pass_lib()
+    rng = np.random.default_rng(3)
+    N, ny, nx = 2, 23, 31
+    pk_x = rng.normal(0.5, 0.3, (N, ny, nx)).astype(np.float32)
+    pk_y = rng.normal(-0.2, 0.3, (N, ny, nx)).astype(np.float32)
+    pk_h = rng.uniform(0.1, 0.9, (N, ny, nx)).astype(np.float32)
+    pk_x[0, 5, 5] = 9.0            # gate
+    pk_x[1, 7, 8] = np.nan          # failed fit
+    pk_x[0, 10, 10] += 3.0          # outlier
+    pdx = rng.normal(4.0, 0.1, (N, ny, nx)).astype(np.float32)
+    pdy = rng.normal(1.0, 0.1, (N, ny, nx)).astype(np.float32)
+    ux = torch.empty((N, ny, nx), device=cuda)
+    uy = torch.empty_like(ux)
+    inv = torch.empty((N, ny, nx), dtype=torch.uint8, device=cuda)
+    work = torch.empty(2 * N * ny * nx, device=cuda)
+    T = [_t(a, cuda) for a in (pk_x, pk_y, pk_h, pdy, pdx)]
+    assert L.pivb_validate_dev(T[0].data_ptr(), T[1].data_ptr(), T[2].data_ptr(), T[3].data_ptr(), T[4].data_ptr(),
+                               None, N, ny, nx, 8.0, 8.0, 0.25, 0.1, 2.0, 5, ux.data_ptr(), uy.data_ptr(),
+                               inv.data_ptr(), work.data_ptr(), _stream()) == 0
+    torch.cuda.synchronize()
+    gx = np.where((np.abs(pk_x) > 8) | (np.abs(pk_y) > 8), np.nan, pk_x) + pdx
+    gy = np.where((np.abs(pk_x) > 8) | (np.abs(pk_y) > 8), np.nan, pk_y) + pdy
+    for n in range(N):
+        bad = np.isnan(gx[n]) | np.isnan(gy[n]) | (pk_h[n] < 0.25)
+        bad |= _median_ref(gx[n], gy[n], 0.1, 2.0, 5)
+        assert np.array_equal(inv[n].cpu().numpy().astype(bool), bad)
+    assert inv[0, 5, 5] and inv[1, 7, 8] and inv[0, 10, 10]
+
+
+def test_infill_harmonic_matches_sparse_solve(cuda):
+    import torch
+    from scipy.sparse import lil_matrix
+    from scipy.sparse.linalg import spsolve
+
+    L = _lib.pass_lib()
+    rng = np.random.default_rng(5)
+    ny, nx, sy, sx = 17, 21, 8.0, 16.0
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    u = (np.sin(xx / 5.0) + yy / 7.0).astype(np.float32)
+    v = (np.cos(yy / 4.0) - xx / 9.0).astype(np.float32)
+    bad = rng.random((ny, nx)) < 0.15
+    bad[0:3, 0:4] = True
+    U, V = u.copy(), v.copy()
+    U[bad] = np.nan
+    V[bad] = np.nan
+    tu, tv = _t(U[None], cuda), _t(V[None], cuda)
+    tb = _t(bad[None].astype(np.uint8), cuda)
+    work = torch.empty(2 * ny * nx, device=cuda)
+    assert L.pivb_infill_dev(tu.data_ptr(), tv.data_ptr(), tb.data_ptr(), None, 1, ny, nx, sy, sx, 20000, 1e-7,
+                             work.data_ptr(), _stream()) == 0
+    torch.cuda.synchronize()
+    # direct solve of the same Laplace system
+    idx = -np.ones((ny, nx), int)
+    idx[bad] = np.arange(bad.sum())
+    for F, got in ((u, tu), (v, tv)):
+        A = lil_matrix((bad.sum(), bad.sum()))
+        b = np.zeros(bad.sum())
+        for r, c in zip(*np.nonzero(bad)):
+            i = idx[r, c]
+            for dr, dc, w in ((-1, 0, 1 / sy ** 2), (1, 0, 1 / sy ** 2), (0, -1, 1 / sx ** 2), (0, 1, 1 / sx ** 2)):
+                rr, cc = r + dr, c + dc
+                if 0 <= rr < ny and 0 <= cc < nx:
+                    A[i, i] += w
+                    if bad[rr, cc]:
+                        A[i, idx[rr, cc]] -= w
+                    else:
+                        b[i] += w * F[rr, cc]
+        sol = spsolve(A.tocsr(), b)
+        np.testing.assert_allclose(got[0].cpu().numpy()[bad], sol, atol=2e-3)
+
+
+def test_pad_smooth_and_remap(cuda):
+    import torch
+    from scipy.ndimage import gaussian_filter
+
+    L = _lib.pass_lib()
+    rng = np.random.default_rng(9)
+    N, ny, nx, pre, post = 2, 9, 12, (2, 3), (2, 2)
+    ux = rng.normal(size=(N, ny, nx)).astype(np.float32)
+    uy = rng.normal(size=(N, ny, nx)).astype(np.float32)
+    nyp, nxp = ny + pre[0] + post[0], nx + pre[1] + post[1]
+    taps, rad = multipass._gauss_taps(0.65, 3)
+    tux, tuy = _t(ux, cuda), _t(uy, cuda)
+    pdy = torch.empty((N, nyp, nxp), device=cuda)
+    pdx = torch.empty_like(pdy)
+    work = torch.empty(N * nyp * nxp, device=cuda)
+    tt = _t(taps, cuda)
+    assert L.pivb_pad_smooth_dev(tux.data_ptr(), tuy.data_ptr(), N, ny, nx, nyp, nxp, pre[0], pre[1], tt.data_ptr(),
+                                 rad, pdy.data_ptr(), pdx.data_ptr(), work.data_ptr(), _stream()) == 0
+    torch.cuda.synchronize()
+    for n in range(N):
+        ref = np.pad(uy[n], ((pre[0], post[0]), (pre[1], post[1])), mode="edge")
+        ref = gaussian_filter(ref.astype(np.float64), sigma=0.65, truncate=2 / (2 * 0.65), mode="nearest")
+        np.testing.assert_allclose(pdy[n].cpu().numpy(), ref, atol=1e-5)
+    # remap at fractional coordinates vs a Keys-cubic restatement
+    my = rng.uniform(0, nyp - 1, (5, 7)).astype(np.float32)
+    mx = rng.uniform(0, nxp - 1, (5, 7)).astype(np.float32)
+    oy = torch.empty((N, 5, 7), device=cuda)
+    ox = torch.empty_like(oy)
+    tmy, tmx = _t(my, cuda), _t(mx, cuda)
+    assert L.pivb_remap_dev(pdy.data_ptr(), pdx.data_ptr(), N, nyp, nxp, tmy.data_ptr(), tmx.data_ptr(), 5, 7,
+                            oy.data_ptr(), ox.data_ptr(), _stream()) == 0
+    torch.cuda.synchronize()
+
+    def keys(t):
+        t = abs(t)
+        return np.where(t < 1, (1.25 * t - 2.25) * t * t + 1, np.where(t < 2, ((-0.75 * t + 3.75) * t - 6) * t + 3, 0))
+
+    P = pdy[0].cpu().numpy().astype(np.float64)
+    for a in range(5):
+        for b in range(7):
+            y0, x0 = np.floor(my[a, b]), np.floor(mx[a, b])
+            val = 0.0
+            for m in range(-1, 3):
+                for q in range(-1, 3):
+                    r = int(min(max(y0 + m, 0), nyp - 1))
+                    c = int(min(max(x0 + q, 0), nxp - 1))
+                    val += keys(my[a, b] - (y0 + m)) * keys(mx[a, b] - (x0 + q)) * P[r, c]
+            assert abs(oy[0, a, b].item() - val) < 1e-4
+
+
+@pytest.mark.parametrize("flow", ["uniform", "channel"])
+def test_multipass_recovers_displacement(cuda, flow):
+    import torch
+
+    H = W = 384
+    N = 2
+    kw = {"u": 3.3, "v": -1.7} if flow == "uniform" else {"peak": 6.0}
+    pairs = [synthetic.particle_pair((H, W), seed=60 + k, flow=flow, flow_kwargs=kw) for k in range(N)]
+    A = torch.tensor(np.stack([p[0] for p in pairs]), device=cuda)
+    B = torch.tensor(np.stack([p[1] for p in pairs]), device=cuda)
+    cfg = multipass.MultipassConfig(window_sizes=[(64, 64), (32, 32), (32, 32)], overlaps=[50, 50, 75])
+    mp = multipass.MultipassPIV((H, W), N, cfg, device=cuda)
+    ux, uy = mp.run(A, B)
+    torch.cuda.synchronize()
+    g = mp.geo[-1].grid
+    err = []
+    for n in range(N):
+        u, v = pairs[n][2]
+        # truth: flow at the window centre, symmetric-warp convention (midpoint)
+        iy = np.clip(np.round(g.win_ctrs_y).astype(int), 0, H - 1)
+        ix = np.clip(np.round(g.win_ctrs_x).astype(int), 0, W - 1)
+        tu = u[np.ix_(iy, ix)]
+        tv = v[np.ix_(iy, ix)]
+        inner = (slice(2, -2), slice(2, -2))
+        err.append(np.hypot(ux[n].cpu().numpy() - tu, uy[n].cpu().numpy() - tv)[inner])
+    err = np.concatenate([e.ravel() for e in err])
+    assert np.isfinite(err).all()
+    assert np.sqrt(np.mean(err ** 2)) < (0.1 if flow == "uniform" else 0.35)
+    # graph capture of a whole step reproduces the eager result
+    ref = (ux.clone(), uy.clone())
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        mp.run(A, B)
+    s.synchronize()
+    gph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(gph, stream=s):
+        mp.run(A, B)
+    gph.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(ux, ref[0]) and torch.equal(uy, ref[1])
