@@ -131,6 +131,23 @@ int pivb_accumulate_dev(const float *d_A, const float *d_B, long long img_stride
                         float *d_sum, float *d_comp, void *d_scratch, size_t scratch_bytes,
                         void *stream);
 
+/* Allocation-free variant of pivb_xcorr_dev (no counterpart in the reference),
+ * for callers that cannot allocate device memory: a host whose GPU memory is
+ * owned by another allocator, a stream being captured into a CUDA graph, or a
+ * pipeline that cannot take the device synchronisation cudaFree implies.  The
+ * deferred-LM scratch is a fixed 16 MiB file-scope device array: at most 131072
+ * windows per call when LM records are needed (nPeaks 1, finder 4-6); larger calls
+ * return 1 (NOMEM) with a message on stderr.  The first call on a device resolves
+ * the array's address (cudaGetSymbolAddress) and must precede any stream capture.
+ * All calls share the array; calls overlapping on the GPU race. */
+int pivb_xcorr_dev_noalloc(const float *d_A, const float *d_B, long long img_stride,
+                           const float *d_mask, int H, int W, int n_images, const float *d_ctr_x,
+                           const float *d_ctr_y, int n_win_y, int n_win_x, const float *d_wA,
+                           const float *d_wB, const float *d_cw, int win_h, int win_w, int ensemble,
+                           int n_peaks, int peak_finder, int peakfit_impl, float *d_pk_x,
+                           float *d_pk_y, float *d_pk_h, float *d_sx, float *d_sy, float *d_sxy,
+                           float *d_pk_ratio, float *d_planes, void *stream);
+
 /* Device ordinal (return) and name of the GPU in use; -1 if none. */
 int pivb_device_info(char *name, int len);
 

@@ -729,3 +729,99 @@ PIV_EXPORT int pivb_device_info(char *name, int len)
     }
     return d;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free correlation entry point
+// ---------------------------------------------------------------------------
+// For callers that cannot allocate device memory themselves: a host whose
+// device memory is owned by another allocator (a framework's caching pool that
+// has reserved the GPU), a stream that is being captured into a CUDA graph, or a
+// latency-bound pipeline that cannot afford the device-wide synchronisation
+// cudaFree implies.  The scratch of the deferred LM fits then lives in a
+// file-scope device array of fixed size instead of a caller-provided buffer.
+//
+// Limit: 16 MiB, i.e. 131072 windows (image pairs x windows per pair) per call
+// when the call needs LM records (nPeaks == 1 and peak finder 4, 5 or 6); larger
+// calls are refused with PIV_ERROR_NOMEM and a message on stderr.  Calls without
+// LM records use no scratch and have no limit.  Every GPU that loads this library
+// holds the array until the process exits.
+//
+// The array is shared by every call on a device and keeps the last call's
+// contents.  Nothing in it needs clearing: the correlation kernel writes every
+// record the LM kernel reads, earlier on the same stream.  Calls whose work
+// overlaps on the GPU (different streams or host threads without ordering)
+// race on the array.
+//
+// Set-up: the first call on a device (with that device current) resolves the
+// array's device address with cudaGetSymbolAddress and fixes each kernel's
+// launch configuration; make that first call before any stream capture.
+// Neither this set-up nor a call allocates memory: no cudaMalloc, cudaFree or
+// allocating library routine is used.
+#define PIVB_NOALLOC_SCRATCH_BYTES (16u << 20)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PIVB_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+void *g_noalloc_addr[kNoallocMaxDevices] = {};
+std::mutex g_noalloc_mu;
+}  // namespace
+
+// pivb_xcorr_dev without the scratch arguments (see the block comment above).
+PIV_EXPORT int pivb_xcorr_dev_noalloc(const float *d_A, const float *d_B, long long img_stride,
+                                      const float *d_mask, int H, int W, int n_images, const float *d_ctr_x,
+                                      const float *d_ctr_y, int n_win_y, int n_win_x, const float *d_wA,
+                                      const float *d_wB, const float *d_cw, int win_h, int win_w, int ensemble,
+                                      int n_peaks, int peak_finder, int peakfit_impl, float *d_pk_x, float *d_pk_y,
+                                      float *d_pk_h, float *d_sx, float *d_sy, float *d_sxy, float *d_pk_ratio,
+                                      float *d_planes, void *stream)
+{
+    if (!size_ok(win_h) || !size_ok(win_w)) return PIV_ERROR_NOPLAN_BWD;
+    if (win_h != win_w) return PIV_ERROR_NOPLAN;
+    if (n_peaks < 1 || n_images < 0) return PIV_ERROR_OUT_OF_BOUNDS;
+    const long long total = (long long)n_images * n_win_y * n_win_x;
+    if (total == 0) return PIV_ERROR_NONE;
+    const bool lm = !ensemble && n_peaks == 1 && peak_finder >= 4 && peak_finder <= 6;
+    LmRecord *records = nullptr;
+    if (lm) {
+        const size_t need = (size_t)total * sizeof(LmRecord);
+        if (need > PIVB_NOALLOC_SCRATCH_BYTES) {
+            fprintf(stderr,
+                    "pivb_xcorr_dev_noalloc: %lld windows need %zu bytes of LM scratch; the fixed array holds "
+                    "%u bytes (%u windows); split the call\n",
+                    total, need, PIVB_NOALLOC_SCRATCH_BYTES, (unsigned)(PIVB_NOALLOC_SCRATCH_BYTES / sizeof(LmRecord)));
+            return PIV_ERROR_NOMEM;
+        }
+        int dev = -1;
+        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) return PIV_ERROR_CUDA;
+        {
+            std::lock_guard<std::mutex> lock(g_noalloc_mu);
+            if (g_noalloc_addr[dev] == nullptr) {
+                void *addr = nullptr;
+                if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || addr == nullptr)
+                    return PIV_ERROR_CUDA;
+                g_noalloc_addr[dev] = addr;
+            }
+            records = static_cast<LmRecord *>(g_noalloc_addr[dev]);
+        }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    XcorrParams p{};
+    p.A = d_A; p.B = d_B; p.img_stride = img_stride; p.mask = d_mask;
+    p.H = H; p.W = W; p.n_img = n_images;
+    p.ctr_x = d_ctr_x; p.ctr_y = d_ctr_y; p.nwy = n_win_y; p.nwx = n_win_x;
+    p.wA = d_wA; p.wB = d_wB; p.cw = d_cw;
+    p.ensemble = ensemble; p.n_peaks = n_peaks; p.finder = peak_finder;
+    p.pk_x = d_pk_x; p.pk_y = d_pk_y; p.pk_h = d_pk_h; p.sx = d_sx; p.sy = d_sy; p.sxy = d_sxy;
+    p.pk_ratio = d_pk_ratio; p.planes = d_planes;
+    p.lm = records;
+    p.total = total;
+    const int e = (n_peaks > 1 && !ensemble) ? launch_xcorr<true>(win_h, p, s) : launch_xcorr<false>(win_h, p, s);
+    if (e) return e;
+    if (lm) {
+        const unsigned blocks = (unsigned)((total + 127) / 128);
+        if (peakfit_impl) lm_records_kernel<1><<<blocks, 128, 0, s>>>(p, win_h);
+        else lm_records_kernel<0><<<blocks, 128, 0, s>>>(p, win_h);
+        if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
+    }
+    return PIV_ERROR_NONE;
+}

@@ -83,6 +83,10 @@ def bulkxcorr2d_lib() -> ctypes.CDLL:
     L.pivb_xcorr_dev.argtypes = [vp, vp, cll, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, vp, ci, ci, ci, ci,
                                  ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, vp, csz, vp]
     L.pivb_xcorr_dev.restype = ci
+    if hasattr(L, "pivb_xcorr_dev_noalloc"):
+        L.pivb_xcorr_dev_noalloc.argtypes = [vp, vp, cll, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, vp, ci, ci, ci,
+                                             ci, ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.pivb_xcorr_dev_noalloc.restype = ci
     L.pivb_device_info.argtypes = [ctypes.c_char_p, ci]
     L.pivb_device_info.restype = ci
     for opt in ("bulkxcorr2d_accumulate", "bulkxcorr2d_accumulate_triple"):
