@@ -38,6 +38,10 @@ int pivb_pad_smooth_dev(const float *ux, const float *uy, int N, int ny, int nx,
 int pivb_remap_dev(const float *pdy, const float *pdx, int N, int nyp, int nxp, const float *map_y,
                    const float *map_x, int ny, int nx, float *out_dy, float *out_dx, void *stream);
 
+/* uint16 frames -> float32 (the reference's readers convert on the host,
+ * pivtools_core/image_handling/load_images.py:594,625).  in 8-byte, out 16-byte aligned. */
+int pivb_u16_to_f32_dev(const unsigned short *in, float *out, long long n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

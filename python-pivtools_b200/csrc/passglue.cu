@@ -26,16 +26,44 @@ namespace {
 
 __device__ __forceinline__ float qnanf() { return __int_as_float(0x7fc00000); }
 
-// Median of v[0..n) (n <= 24) for finite values only; NaN if none.
-__device__ float median_finite(float *v, int n)
+// Median of the finite values among v[0..24) (np.nanmedian convention; NaN if
+// none).  Register bitonic sort of 32 keys with NaN and padding mapped to +inf,
+// then a select of the middle order statistics: no local memory.
+__device__ __forceinline__ float median24(const float (&v)[24])
 {
+    float k[32];
     int m = 0;
-    for (int i = 0; i < n; ++i)
-        if (v[i] == v[i]) v[m++] = v[i];
+#pragma unroll
+    for (int i = 0; i < 24; ++i) {
+        const bool fin = v[i] == v[i];
+        k[i] = fin ? v[i] : INFINITY;
+        m += fin;
+    }
+#pragma unroll
+    for (int i = 24; i < 32; ++i) k[i] = INFINITY;
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1)
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1)
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const float a = k[i], b = k[j];
+                    k[i] = up ? fminf(a, b) : fmaxf(a, b);
+                    k[j] = up ? fmaxf(a, b) : fminf(a, b);
+                }
+            }
     if (m == 0) return qnanf();
-    for (int i = 1; i < m; ++i)
-        for (int j = i; j > 0 && v[j - 1] > v[j]; --j) { const float t = v[j]; v[j] = v[j - 1]; v[j - 1] = t; }
-    return (m & 1) ? v[m / 2] : 0.5f * (v[m / 2 - 1] + v[m / 2]);
+    const int hi = m / 2, lo = (m - 1) / 2;
+    float vh = 0.0f, vl = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 24; ++i) {
+        vh = (i == hi) ? k[i] : vh;
+        vl = (i == lo) ? k[i] : vl;
+    }
+    return (m & 1) ? vh : 0.5f * (vl + vh);
 }
 
 struct ValParams {
@@ -89,32 +117,30 @@ __global__ void median_kernel(ValParams p, const float *gx, const float *gy)
     const float *X = gx + (long long)n * plane, *Y = gy + (long long)n * plane;
     const int h = p.med_size / 2;
     float nu[24], nvv[24];
-    int k = 0, present = 0;
-    for (int dr = -h; dr <= h; ++dr)
-        for (int dc = -h; dc <= h; ++dc) {
-            const int rr = r + dr, cc = c + dc;
-            const bool inside = rr >= 0 && rr < p.ny && cc >= 0 && cc < p.nx;
-            float a = qnanf(), b = qnanf();
-            bool mk = false;
-            if (inside) {
-                mk = p.mask && p.mask[rr * p.nx + cc] != 0.0f;
-                if (!mk) { a = X[rr * p.nx + cc]; b = Y[rr * p.nx + cc]; }
-                if (abs(dr) <= 1 && abs(dc) <= 1 && (mk || a == a)) ++present;
-            }
-            if (!dr && !dc) continue;
-            nu[k] = a;
-            nvv[k] = b;
-            ++k;
+    int present = 0;
+#pragma unroll
+    for (int t = 0; t < 25; ++t) {
+        const int dr = t / 5 - 2, dc = t % 5 - 2;
+        const int rr = r + dr, cc = c + dc;
+        const bool inside = rr >= 0 && rr < p.ny && cc >= 0 && cc < p.nx && abs(dr) <= h && abs(dc) <= h;
+        float a = qnanf(), b = qnanf();
+        if (inside) {
+            const bool mk = p.mask && p.mask[rr * p.nx + cc] != 0.0f;
+            if (!mk) { a = X[rr * p.nx + cc]; b = Y[rr * p.nx + cc]; }
+            if (abs(dr) <= 1 && abs(dc) <= 1 && (mk || a == a)) ++present;
         }
-    float tu[24], tv[24];
-    for (int j = 0; j < k; ++j) { tu[j] = nu[j]; tv[j] = nvv[j]; }
-    const float mu = median_finite(tu, k), mv = median_finite(tv, k);
+        if (t == 12) continue;
+        nu[t < 12 ? t : t - 1] = a;
+        nvv[t < 12 ? t : t - 1] = b;
+    }
+    const float mu = median24(nu), mv = median24(nvv);
     const float u0 = X[w], v0 = Y[w];
     const float r0 = sqrtf((u0 - mu) * (u0 - mu) + (v0 - mv) * (v0 - mv));
     float ri[24];
-    for (int j = 0; j < k; ++j)
+#pragma unroll
+    for (int j = 0; j < 24; ++j)
         ri[j] = sqrtf((nu[j] - mu) * (nu[j] - mu) + (nvv[j] - mv) * (nvv[j] - mv));
-    const float rm = median_finite(ri, k);
+    const float rm = median24(ri);
     const float nr = r0 / (rm + p.med_eps);
     const bool bad = p.invalid[i] || (nr > p.med_thr) || !isfinite(nr) || present < 6;
     p.invalid[i] = bad ? 1 : 0;
@@ -338,5 +364,32 @@ PIV_EXPORT int pivb_remap_dev(const float *pdy, const float *pdx, int N, int nyp
     const long long n = (long long)N * ny * nx;
     remap_kernel<<<blocks(n, 256), 256, 0, (cudaStream_t)stream>>>(pdy, pdx, N, nyp, nxp, map_y, map_x, ny, nx,
                                                                      out_dy, out_dx);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+namespace {
+__global__ void u16_to_f32_kernel(const unsigned short *__restrict__ in, float *__restrict__ out, long long n)
+{
+    long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const long long stride = (long long)gridDim.x * blockDim.x * 4;
+    for (; i + 3 < n; i += stride) {
+        const ushort4 v = *reinterpret_cast<const ushort4 *>(in + i);
+        *reinterpret_cast<float4 *>(out + i) = make_float4(v.x, v.y, v.z, v.w);
+    }
+    for (; i < n; ++i) out[i] = (float)in[i];   // tail (n not a multiple of 4)
+}
+}  // namespace
+
+// uint16 camera frames -> float32, as the reference's image readers convert them
+// (pivtools_core/image_handling/load_images.py:594,625).  in must be 8-byte and out
+// 16-byte aligned.
+PIV_EXPORT int pivb_u16_to_f32_dev(const unsigned short *in, float *out, long long n, void *stream)
+{
+    if (n <= 0 || !in || !out) return 1;
+    if (((uintptr_t)in & 7) || ((uintptr_t)out & 15)) return 1;
+    const long long quads = (n + 3) / 4;
+    unsigned blocks = (unsigned)((quads + 255) / 256);
+    if (blocks > 148u * 32u) blocks = 148u * 32u;
+    u16_to_f32_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(in, out, n);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }

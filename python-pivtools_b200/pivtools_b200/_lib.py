@@ -169,6 +169,8 @@ def pass_lib() -> ctypes.CDLL:
     L.pivb_pad_smooth_dev.restype = ci
     L.pivb_remap_dev.argtypes = [vp, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, vp]
     L.pivb_remap_dev.restype = ci
+    L.pivb_u16_to_f32_dev.argtypes = [vp, vp, cll, vp]
+    L.pivb_u16_to_f32_dev.restype = ci
     L._pivb_bound = True
     return L
 

@@ -208,3 +208,59 @@ class MultipassPIV:
 
     def windows_per_step(self) -> int:
         return self.N * sum(p["ny"] * p["nx"] for p in self.passes)
+
+
+class HostPipeline:
+    """End-to-end multipass from pinned host memory: uint16 frames in, float32
+    vector fields out.
+
+    The batch is processed in chunks of `chunk` pairs (one MultipassPIV of that
+    batch size).  While chunk c is computed, chunk c+1's frames cross PCIe on a
+    copy stream into the other of two uint16 staging slots; frames are converted
+    to float32 on the GPU (the reference's readers convert on the host), and each
+    chunk's final field is read back right after its last pass.
+    """
+
+    def __init__(self, image_shape, chunk: int, cfg: MultipassConfig | None = None, device=None):
+        import torch
+
+        self.torch = torch
+        self.mp = MultipassPIV(image_shape, chunk, cfg, device)
+        dev = self.mp.device
+        H, W = image_shape
+        self.C = chunk
+        self.u16 = [[torch.empty((chunk, H, W), dtype=torch.uint16, device=dev) for _ in range(2)] for _ in range(2)]
+        self.f32 = [torch.empty((chunk, H, W), dtype=torch.float32, device=dev) for _ in range(2)]
+        self.copy_stream = torch.cuda.Stream(device=dev)
+        self.ev_h2d = [torch.cuda.Event() for _ in range(2)]
+        self.ev_conv = [torch.cuda.Event() for _ in range(2)]
+        self.Lp = _lib.pass_lib()
+
+    def run(self, Ah, Bh, ux_out, uy_out):
+        """Ah, Bh: pinned uint16 (N, H, W) host tensors, N a multiple of the chunk;
+        ux_out, uy_out: pinned float32 (N, ny, nx) host tensors."""
+        torch = self.torch
+        comp = torch.cuda.current_stream(self.mp.device)
+        C = self.C
+        n_chunks = Ah.shape[0] // C
+        for s in range(2):
+            self.ev_conv[s].record(comp)
+        for c in range(n_chunks):
+            s = c % 2
+            sl = slice(c * C, (c + 1) * C)
+            self.copy_stream.wait_event(self.ev_conv[s])
+            with torch.cuda.stream(self.copy_stream):
+                self.u16[s][0].copy_(Ah[sl], non_blocking=True)
+                self.u16[s][1].copy_(Bh[sl], non_blocking=True)
+                self.ev_h2d[s].record(self.copy_stream)
+            comp.wait_event(self.ev_h2d[s])
+            st = ctypes.c_void_p(comp.cuda_stream)
+            for k in range(2):
+                src, dst = self.u16[s][k], self.f32[k]
+                if self.Lp.pivb_u16_to_f32_dev(src.data_ptr(), dst.data_ptr(), src.numel(), st) != 0:
+                    raise RuntimeError("u16 -> f32 conversion failed")
+            self.ev_conv[s].record(comp)
+            ux, uy = self.mp.run(self.f32[0], self.f32[1])
+            ux_out[sl].copy_(ux, non_blocking=True)
+            uy_out[sl].copy_(uy, non_blocking=True)
+        return ux_out, uy_out

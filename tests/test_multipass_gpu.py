@@ -221,3 +221,53 @@ def test_multipass_recovers_displacement(cuda, flow):
     gph.replay()
     torch.cuda.synchronize()
     assert torch.equal(ux, ref[0]) and torch.equal(uy, ref[1])
+
+
+def test_u16_to_f32_conversion(cuda):
+    import torch
+
+    L = _lib.pass_lib()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(5)
+    for n in (1, 3, 4, 1021, 1 << 20):                   # ragged tails and a large case
+        src = torch.tensor(rng.integers(0, 65536, n).astype(np.int32)).to(torch.uint16).to(cuda)
+        dst = torch.full((n,), -1.0, device=cuda)
+        assert L.pivb_u16_to_f32_dev(src.data_ptr(), dst.data_ptr(), n, s) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(dst.cpu(), src.cpu().to(torch.int32).to(torch.float32))
+    # misaligned pointers are refused before any launch
+    buf = torch.zeros(64, dtype=torch.uint16, device=cuda)
+    out = torch.zeros(64, device=cuda)
+    assert L.pivb_u16_to_f32_dev(buf.data_ptr() + 2, out.data_ptr(), 16, s) == 1
+    assert L.pivb_u16_to_f32_dev(buf.data_ptr(), out.data_ptr() + 4, 16, s) == 1
+    assert L.pivb_u16_to_f32_dev(buf.data_ptr(), out.data_ptr(), 0, s) == 1
+
+
+def test_host_pipeline_matches_resident_batch(cuda):
+    """uint16 pinned frames, chunked and overlapped with compute, give the same
+    fields as one resident batch of float32 frames."""
+    import torch
+
+    H = W = 256
+    N, C = 4, 2
+    pairs = [synthetic.particle_pair((H, W), seed=80 + k, flow="channel", flow_kwargs={"peak": 5.0})
+             for k in range(N)]
+    A16 = np.stack([np.clip(np.round(p[0]), 0, 65535) for p in pairs]).astype(np.int32)
+    B16 = np.stack([np.clip(np.round(p[1]), 0, 65535) for p in pairs]).astype(np.int32)
+    cfg = multipass.MultipassConfig(window_sizes=[(64, 64), (32, 32)], overlaps=[50, 50])
+    mp = multipass.MultipassPIV((H, W), N, cfg, device=cuda)
+    ux, uy = mp.run(torch.tensor(A16, dtype=torch.float32, device=cuda),
+                    torch.tensor(B16, dtype=torch.float32, device=cuda))
+    torch.cuda.synchronize()
+    pipe = multipass.HostPipeline((H, W), C, cfg, device=cuda)
+    Ah = torch.tensor(A16).to(torch.uint16).pin_memory()
+    Bh = torch.tensor(B16).to(torch.uint16).pin_memory()
+    g = mp.geo[-1].grid
+    oux = torch.empty((N, g.n_win_y, g.n_win_x)).pin_memory()
+    ouy = torch.empty_like(oux).pin_memory()
+    for _ in range(2):                                   # twice: slots and events are reused
+        oux.fill_(7.0)
+        ouy.fill_(7.0)
+        pipe.run(Ah, Bh, oux, ouy)
+        torch.cuda.synchronize()
+        assert torch.equal(oux, ux.cpu()) and torch.equal(ouy, uy.cpu())
