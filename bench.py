@@ -312,7 +312,8 @@ def run_b200(args):
     e2e_val = vec_step * ws / (e2e_ms * 1e-3)
     e2e_launches = pipe.mp.launches_per_step * (N // chunk) + 2 * (N // chunk)
     fin = mp.passes[-1]
-    e2e_same = bool(torch.equal(ux_h, fin["ux"].cpu()) and torch.equal(uy_h, fin["uy"].cpu()))
+    e2e_same = bool(torch.allclose(ux_h, fin["ux"].cpu(), rtol=0, atol=0, equal_nan=True)
+                    and torch.allclose(uy_h, fin["uy"].cpu(), rtol=0, atol=0, equal_nan=True))
 
     cpu = None
     if rank == 0 and ws == 1 and os.environ.get("PIVB_SKIP_CPU") != "1":

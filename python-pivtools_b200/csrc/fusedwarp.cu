@@ -61,14 +61,14 @@ __device__ __forceinline__ float sample_bicubic(const float *__restrict__ img, f
     keys4(fs(fy, fyf), wy);
     keys4(fs(fx, fxf), wx);
     if (IMPL == 1 && iy >= 0 && iy + 3 < H && ix >= 0 && ix + 3 < W) {
-        const float *r = img + (long long)iy * W + ix;
+        const float *r = img + (iy * W + ix);
         float c[4];
 #pragma unroll
         for (int n = 0; n < 4; ++n) c[n] = fm(__ldg(r + n), wy[0]);
 #pragma unroll
         for (int m = 1; m < 4; ++m)
 #pragma unroll
-            for (int n = 0; n < 4; ++n) c[n] = __fmaf_rn(__ldg(r + (long long)m * W + n), wy[m], c[n]);
+            for (int n = 0; n < 4; ++n) c[n] = __fmaf_rn(__ldg(r + m * W + n), wy[m], c[n]);
         const float p0 = fm(c[0], wx[0]), p1 = fm(c[1], wx[1]), p2 = fm(c[2], wx[2]), p3 = fm(c[3], wx[3]);
         return fa(fa(p0, p1), fa(p2, p3));
     }
@@ -97,14 +97,14 @@ __device__ __forceinline__ float sample_lanczos(const float *__restrict__ img, f
     lanczos_w(fs(fy, fyf), lut, wy);
     lanczos_w(fs(fx, fxf), lut, wx);
     if (IMPL == 1 && iy >= 0 && iy + 5 < H && ix >= 0 && ix + 5 < W) {
-        const float *r = img + (long long)iy * W + ix;
+        const float *r = img + (iy * W + ix);
         float c[6];
 #pragma unroll
         for (int n = 0; n < 6; ++n) c[n] = 0.0f;
 #pragma unroll
         for (int m = 0; m < 6; ++m)
 #pragma unroll
-            for (int n = 0; n < 6; ++n) c[n] = __fmaf_rn(__ldg(r + (long long)m * W + n), wy[m], c[n]);
+            for (int n = 0; n < 6; ++n) c[n] = __fmaf_rn(__ldg(r + m * W + n), wy[m], c[n]);
         float p[6];
 #pragma unroll
         for (int n = 0; n < 6; ++n) p[n] = fm(c[n], wx[n]);
@@ -184,47 +184,73 @@ struct WarpParams {
     int round_shifts;
 };
 
+// Output rows per thread.  The rows of one thread share the column-side work
+// (predictor column weights and indices) and, while they fall in the same
+// predictor cell row, the 4x4 predictor patch, which stays in registers.
+constexpr int kWarpRows = 4;
+
 template <int MODE, int IMPL>
 __global__ void __launch_bounds__(256) warp_kernel(WarpParams p)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * kWarpRows;
     const int n = blockIdx.z;
-    if (j >= p.W || i >= p.H) return;
+    if (j >= p.W || i0 >= p.H) return;
     const float *dy = p.pdy + n * p.pred_stride, *dx = p.pdx + n * p.pred_stride;
-    // Phase A: bicubic predictor (fused_warp.c:224-250)
-    const float fiy = p.ly[i], fiyf = floorf(fiy);
-    const int by = (int)fiyf - 1;
-    float wy[4], wx[4];
-    keys4(fs(fiy, fiyf), wy);
+    // column side of the bicubic predictor (fused_warp.c:224-250)
     const float fx = p.lx[j], fxf = floorf(fx);
     const int bx = (int)fxf - 1;
+    float wx[4];
     keys4(fs(fx, fxf), wx);
-    float vy = 0.0f, vx = 0.0f;
+    int cq[4];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        const int r = min(max(by + m, 0), p.nPY - 1);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int c = min(max(bx + q, 0), p.nPX - 1);
-            const float w = fm(wy[m], wx[q]);
-            vy = fa(vy, fm(w, __ldg(dy + r * p.nPX + c)));
-            vx = fa(vx, fm(w, __ldg(dx + r * p.nPX + c)));
-        }
-    }
-    // Phase B: symmetric half shifts
-    float hy = fm(0.5f, vy), hx = fm(0.5f, vx);
-    if (p.round_shifts) { hy = roundf(hy); hx = roundf(hx); }
-    // Phase C: samples
+    for (int q = 0; q < 4; ++q) cq[q] = min(max(bx + q, 0), p.nPX - 1);
+    float py[4][4], px[4][4];
+    int cur_by = -0x7fffffff;
     const float *a = p.ia + n * p.img_stride, *b = p.ib + n * p.img_stride;
-    const long long o = n * p.img_stride + (long long)i * p.W + j;
-    const float fi = (float)i, fj = (float)j;
-    if (MODE == 0) {
-        p.oa[o] = sample_bicubic<IMPL>(a, fs(fi, hy), fs(fj, hx), p.H, p.W);
-        p.ob[o] = sample_bicubic<IMPL>(b, fa(fi, hy), fa(fj, hx), p.H, p.W);
-    } else {
-        p.oa[o] = sample_lanczos<IMPL>(a, fs(fi, hy), fs(fj, hx), p.H, p.W, p.lut);
-        p.ob[o] = sample_lanczos<IMPL>(b, fa(fi, hy), fa(fj, hx), p.H, p.W, p.lut);
+    const int i_end = min(i0 + kWarpRows, p.H);
+#pragma unroll 1
+    for (int i = i0; i < i_end; ++i) {
+        // Phase A: bicubic predictor, products and sums in the scalar route's order
+        const float fiy = p.ly[i], fiyf = floorf(fiy);
+        const int by = (int)fiyf - 1;
+        float wy[4];
+        keys4(fs(fiy, fiyf), wy);
+        if (by != cur_by) {          // warp-uniform: all lanes share row i
+            cur_by = by;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int r = min(max(by + m, 0), p.nPY - 1) * p.nPX;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    py[m][q] = __ldg(dy + r + cq[q]);
+                    px[m][q] = __ldg(dx + r + cq[q]);
+                }
+            }
+        }
+        float vy = 0.0f, vx = 0.0f;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const float w = fm(wy[m], wx[q]);
+                vy = fa(vy, fm(w, py[m][q]));
+                vx = fa(vx, fm(w, px[m][q]));
+            }
+        }
+        // Phase B: symmetric half shifts
+        float hy = fm(0.5f, vy), hx = fm(0.5f, vx);
+        if (p.round_shifts) { hy = roundf(hy); hx = roundf(hx); }
+        // Phase C: samples
+        const long long o = n * p.img_stride + (long long)i * p.W + j;
+        const float fi = (float)i, fj = (float)j;
+        if (MODE == 0) {
+            p.oa[o] = sample_bicubic<IMPL>(a, fs(fi, hy), fs(fj, hx), p.H, p.W);
+            p.ob[o] = sample_bicubic<IMPL>(b, fa(fi, hy), fa(fj, hx), p.H, p.W);
+        } else {
+            p.oa[o] = sample_lanczos<IMPL>(a, fs(fi, hy), fs(fj, hx), p.H, p.W, p.lut);
+            p.ob[o] = sample_lanczos<IMPL>(b, fa(fi, hy), fa(fj, hx), p.H, p.W, p.lut);
+        }
     }
 }
 
@@ -280,7 +306,8 @@ PIV_EXPORT int pivb_warp_setup_dev(const float *d_ctrs_y, int nPY, const float *
 }
 
 // Warp N pairs on device pointers.  img_stride = elements between frames (>= H*W);
-// tables from pivb_warp_setup_dev.  Returns 0 or 1 (bad arguments / launch failure).
+// tables from pivb_warp_setup_dev.  Frames must hold fewer than 2^31 pixels.
+// Returns 0 or 1 (bad arguments / launch failure).
 PIV_EXPORT int pivb_warp_dev(const float *d_ia, const float *d_ib, float *d_oa, float *d_ob,
                              const float *d_pdy, const float *d_pdx, int N, int H, int W, int nPY, int nPX,
                              long long img_stride, const void *d_tables, int interp_mode, int shared_predictor,
@@ -288,6 +315,8 @@ PIV_EXPORT int pivb_warp_dev(const float *d_ia, const float *d_ib, float *d_oa, 
 {
     if (N <= 0 || H <= 0 || W <= 0 || nPY <= 0 || nPX <= 0) return 1;
     if (!d_ia || !d_ib || !d_oa || !d_ob || !d_pdy || !d_pdx || !d_tables) return 1;
+    if ((long long)H * W >= (1LL << 31) - 64 || (long long)nPY * nPX >= (1LL << 31)) return 1;  // 32-bit offsets
+    if (img_stride < (long long)H * W) return 1;
     const char *t = static_cast<const char *>(d_tables);
     WarpParams p;
     p.ia = d_ia; p.ib = d_ib; p.oa = d_oa; p.ob = d_ob; p.pdy = d_pdy; p.pdx = d_pdx;
@@ -298,7 +327,7 @@ PIV_EXPORT int pivb_warp_dev(const float *d_ia, const float *d_ib, float *d_oa, 
     p.lx = reinterpret_cast<const float *>(t + pad256((size_t)H * 4));
     p.lut = reinterpret_cast<const float *>(t + pad256((size_t)H * 4) + pad256((size_t)W * 4));
     p.round_shifts = round_shifts;
-    dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8, N);
+    dim3 blk(32, 8), grd((W + 31) / 32, (H + 8 * kWarpRows - 1) / (8 * kWarpRows), N);
     cudaStream_t s = (cudaStream_t)stream;
     if (interp_mode == 0) {
         if (impl) warp_kernel<0, 1><<<grd, blk, 0, s>>>(p);

@@ -172,18 +172,31 @@ __global__ void __launch_bounds__(512) infill_kernel(float *ux, float *uy, const
     if (!s_any) return;
     // initial guess: mean of the valid vectors (the iteration converges to the
     // unique harmonic solution from any start; a good start shortens it)
+    // deterministic block reduction (fixed order), so repeated runs agree bit for bit
+    __shared__ float s_part[3][16];
     __shared__ float s_su, s_sv, s_n;
-    if (threadIdx.x == 0) { s_su = 0.0f; s_sv = 0.0f; s_n = 0.0f; }
-    __syncthreads();
     {
         float su = 0.0f, sv = 0.0f, cnt = 0.0f;
         for (int w = threadIdx.x; w < plane; w += blockDim.x)
             if (!bad[w] && !(mask && mask[w] != 0.0f)) { su += X[w]; sv += Y[w]; cnt += 1.0f; }
-        atomicAdd(&s_su, su);
-        atomicAdd(&s_sv, sv);
-        atomicAdd(&s_n, cnt);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            su += __shfl_xor_sync(0xffffffffu, su, o);
+            sv += __shfl_xor_sync(0xffffffffu, sv, o);
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            s_part[0][threadIdx.x >> 5] = su;
+            s_part[1][threadIdx.x >> 5] = sv;
+            s_part[2][threadIdx.x >> 5] = cnt;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float a = 0.0f, b = 0.0f, c = 0.0f;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a += s_part[0][k]; b += s_part[1][k]; c += s_part[2][k]; }
+            s_su = a; s_sv = b; s_n = c;
+        }
     }
-    __syncthreads();
     const float mu = s_n > 0.0f ? s_su / s_n : 0.0f, mv = s_n > 0.0f ? s_sv / s_n : 0.0f;
     for (int w = threadIdx.x; w < plane; w += blockDim.x) {
         if (bad[w]) { X[w] = mu; Y[w] = mv; }

@@ -32,6 +32,8 @@ struct WinGeo {
     static constexpr int STF = N + 1;                                   // float row stride
     static constexpr int WARPS_PER_CTA = (GW <= 32) ? 4 : GW / 32;
     static constexpr int CTA_THREADS = WARPS_PER_CTA * 32;
+    // resident CTAs per SM the correlation kernel is compiled for (register cap)
+    static constexpr int MIN_CTAS = (N == 32) ? 5 : 1;
     static constexpr int GROUPS_PER_CTA = (GW <= 32) ? WARPS_PER_CTA * WPW : 1;
     static constexpr int PLANE_BYTES = N * ST * 8;
     static constexpr int RED_SLOTS = (GW > 32) ? GW / 32 : 1;
@@ -242,21 +244,75 @@ __device__ __forceinline__ void fft2_inverse(const Group<N> &g, float2 *S, float
 // Forward packed transform of (a, b) -> C' = 4 F_b conj(F_a), inverse transform,
 // scaling and fftshift into the float plane `pl` (aliases S).  On entry each
 // active thread holds a[n], b[n] = samples (P*n + p) of its column.
+//
+// All four 1-D passes (forward columns, forward rows, inverse rows, inverse
+// columns) run the same forward transform code inside one loop, so the kernel
+// carries a single copy of the unrolled butterflies (the instruction footprint
+// of four inlined copies does not fit the instruction cache).  The inverse is
+// taken as conj(FFT(conj(C'))): the product stage emits conj(C') directly, and
+// only the real part of the result is used, which the final conjugation leaves
+// unchanged.  Negation is exact, so this equals the inverse transform bit for bit.
 template <int N>
 __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, const float (&a)[WinGeo<N>::M],
                                                 const float (&b)[WinGeo<N>::M], float scale)
 {
     using G = WinGeo<N>;
-    constexpr int M = G::M, P = G::P;
+    constexpr int M = G::M, P = G::P, ST = G::ST;
+    const bool active = g.t < G::T;
+    int line, p;
+    lane_slot<N>(active ? g.t : 0, line, p);
+    const int q = out_block<P>(p);
+    const int rm = (N - line) % N;
     float2 z[M];
-    fft2_forward<N>(g, S, a, b);
-    spectrum_product<N, 0>(g, S, z);
-    fft2_inverse<N>(g, S, z);
+#pragma unroll
+    for (int n = 0; n < M; ++n) z[n] = make_float2(a[n], b[n]);
+#pragma unroll 1
+    for (int pass = 0;; ++pass) {
+        RegFFT<M, -1>::run(z);
+        lane_combine<P, M, -1>(z, p);
+        if (pass == 3) break;
+        g.sync();
+        if (active) {
+            if (pass == 0) {
+#pragma unroll
+                for (int k = 0; k < M; ++k) S[(M * q + k) * ST + line] = z[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < M; ++k) S[line * ST + M * q + k] = z[k];
+            }
+        }
+        g.sync();
+        if (pass == 1) {
+            // conj(C') = conj(-i (Z - Zm) conj(Z + Zm)), Zm = conj(Z(-k))
+            if (active) {
+#pragma unroll
+                for (int n = 0; n < M; ++n) {
+                    const int kx = P * n + p;
+                    const float2 zk = S[line * ST + kx];
+                    const float2 zn = S[rm * ST + (N - kx) % N];
+                    const float2 d = make_float2(zk.x - zn.x, zk.y + zn.y);   // Z - Zm
+                    const float2 sm = make_float2(zk.x + zn.x, zk.y - zn.y);  // Z + Zm
+                    const float re = d.x * sm.x + d.y * sm.y;
+                    const float im = d.y * sm.x - d.x * sm.y;
+                    z[n] = make_float2(im, re);
+                }
+            } else {
+#pragma unroll
+                for (int n = 0; n < M; ++n) z[n] = make_float2(0.0f, 0.0f);
+            }
+        } else if (active) {
+            if (pass == 0) {
+#pragma unroll
+                for (int n = 0; n < M; ++n) z[n] = S[line * ST + P * n + p];
+            } else {
+#pragma unroll
+                for (int n = 0; n < M; ++n) z[n] = S[(P * n + p) * ST + line];
+            }
+        }
+    }
+    g.sync();
     float *pl = reinterpret_cast<float *>(S);
-    if (g.t < G::T) {
-        int line, p;
-        lane_slot<N>(g.t, line, p);
-        const int q = out_block<P>(p);
+    if (active) {
         const int col = (line + N / 2) % N;
 #pragma unroll
         for (int k = 0; k < M; ++k) {

@@ -61,7 +61,7 @@ __device__ __forceinline__ void write_peak(const XcorrParams &p, long long o, in
 // search, 3-point fit.  LM fits of single-peak calls are deferred to
 // lm_records_kernel; MULTI handles nPeaks > 1 entirely in the group leader.
 template <int N, bool MULTI>
-__global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS)
+__global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS, MULTI ? 1 : WinGeo<N>::MIN_CTAS)
 xcorr_kernel(XcorrParams prm)
 {
     using G = WinGeo<N>;
