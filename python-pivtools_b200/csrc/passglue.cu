@@ -197,6 +197,7 @@ __global__ void __launch_bounds__(512) infill_kernel(float *ux, float *uy, const
             s_su = a; s_sv = b; s_n = c;
         }
     }
+    __syncthreads();
     const float mu = s_n > 0.0f ? s_su / s_n : 0.0f, mv = s_n > 0.0f ? s_sv / s_n : 0.0f;
     for (int w = threadIdx.x; w < plane; w += blockDim.x) {
         if (bad[w]) { X[w] = mu; Y[w] = mv; }

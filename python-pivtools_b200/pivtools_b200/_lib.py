@@ -175,5 +175,15 @@ def pass_lib() -> ctypes.CDLL:
     return L
 
 
+def dft_lib() -> ctypes.CDLL:
+    L = _load("libpivb_dft.so")
+    if getattr(L, "_pivb_bound", False):
+        return L
+    L.pivb_umma_selftest.argtypes = [vp, vp, vp, ci, ci, ci, vp, vp]
+    L.pivb_umma_selftest.restype = ci
+    L._pivb_bound = True
+    return L
+
+
 def loaded_paths() -> list[str]:
     return [lib_path(n) for n in _cache]

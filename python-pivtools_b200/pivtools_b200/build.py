@@ -29,6 +29,7 @@ TARGETS = {
     "libfusedwarp.so": "fusedwarp.cu",
     "libkspacefit.so": "kspacefit.cu",
     "libpivb_pass.so": "passglue.cu",
+    "libpivb_dft.so": "dftcorr.cu",
 }
 
 

@@ -17,6 +17,7 @@ HEADER_LIB = {
     "libfusedwarp.h": "libfusedwarp.so",
     "libkspacefit.h": "libkspacefit.so",
     "libpivb_pass.h": "libpivb_pass.so",
+    "libpivb_dft.h": "libpivb_dft.so",
 }
 
 
