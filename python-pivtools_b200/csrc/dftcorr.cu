@@ -1,10 +1,41 @@
 // dftcorr.cu -- libpivb_dft: tensor-core (tcgen05) building blocks and the
 // DFT-as-GEMM correlation path for sm_100a.
+//
+// DFT-as-GEMM correlation of 32 x 32 windows.  Each CTA takes groups of eight
+// windows through four chained GEMMs on the tensor core, with the FP32
+// accumulators in tensor memory and the CUDA cores doing only the splits,
+// transposes and the spectrum product between them:
+//
+//   stage 1  Y = X W1            rows (window, y), K = x (32): the real row DFT
+//                                 to the half spectrum, 16 complex columns, the
+//                                 Nyquist column packed into Im of column 0;
+//   stage 2  F^T = Y^T W2        rows (window, image, kx), K = (Re, Im) x y (64):
+//                                 the complex column DFT;
+//            C = F_B conj(F_A)    per element (slot0 = B, slot1 = A as in
+//                                 PIV_2d_cross_correlate.c:131-133); row kx = 0
+//                                 carries DC and Nyquist together and is unpacked
+//                                 by Hermitian symmetry, multiplied, repacked;
+//   stage 3  G^T = C^T W3        rows (window, kx), K = (Re, Im) x ky (64): the
+//                                 inverse column DFT;
+//   stage 4  c = G W4            rows (window, y), K = (Re, Im) x kx (32): the
+//                                 Hermitian inverse row DFT to the real plane.
+//
+// Every operand is split x = hi + lo into two BF16 numbers (hi = bf16(x),
+// lo = bf16(x - hi)) and each GEMM accumulates the three products hi*hi +
+// hi*lo + lo*hi in FP32, which keeps about 16 significant bits per operand.
+// The plane is then scaled by 1/numel, fftshifted into shared memory and goes
+// through the same peak search, fit and outputs as the FFT path.
+#include <math.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <string.h>
+
+#include <cuda_bf16.h>
+#include <mutex>
 
 #include "piv_common.cuh"
 #include "umma.cuh"
+#include "xcorr_kernels.cuh"
 
 namespace {
 
@@ -59,6 +90,411 @@ __global__ void __launch_bounds__(128) umma_selftest_kernel(const uint16_t *__re
     if (warp == 0) umma::tmem_free(tbase, ncols);
 }
 
+// ---------------------------------------------------------------------------
+// DFT-as-GEMM correlation, 32 x 32 windows
+// ---------------------------------------------------------------------------
+namespace dft32 {
+
+using namespace piv;
+
+constexpr int N = 32;
+constexpr int G = 8;                      // windows per group
+// constant operands (K-major, hi then lo), byte offsets in the constant block
+constexpr uint32_t B1 = 0, B1_BYTES = 32 * 32 * 2;
+constexpr uint32_t B2 = B1 + 2 * B1_BYTES, B2_BYTES = 64 * 64 * 2;
+constexpr uint32_t B3 = B2 + 2 * B2_BYTES, B3_BYTES = 64 * 64 * 2;
+constexpr uint32_t B4 = B3 + 2 * B3_BYTES, B4_BYTES = 32 * 32 * 2;
+constexpr uint32_t CONST_BYTES = B4 + 2 * B4_BYTES;          // 40 KB
+constexpr uint32_t WORK_BYTES = 64 * 1024;
+constexpr uint32_t PLANE_LD = N + 1;
+constexpr uint32_t SMEM_BYTES = CONST_BYTES + WORK_BYTES + 64;
+constexpr uint32_t TMEM_COLS = 256;
+static_assert(G * N * PLANE_LD * 4 <= WORK_BYTES, "planes alias the work region");
+
+__device__ __forceinline__ void split(float x, uint16_t &hi, uint16_t &lo)
+{
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+}
+
+// Split 8 values and store the hi and lo halves as two 16-byte vectors.
+__device__ __forceinline__ void store8(unsigned char *hi_dst, unsigned char *lo_dst, const float *v)
+{
+    uint16_t h[8], l[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) split(v[j], h[j], l[j]);
+    uint4 H, L;
+    H.x = h[0] | ((uint32_t)h[1] << 16); H.y = h[2] | ((uint32_t)h[3] << 16);
+    H.z = h[4] | ((uint32_t)h[5] << 16); H.w = h[6] | ((uint32_t)h[7] << 16);
+    L.x = l[0] | ((uint32_t)l[1] << 16); L.y = l[2] | ((uint32_t)l[3] << 16);
+    L.z = l[4] | ((uint32_t)l[5] << 16); L.w = l[6] | ((uint32_t)l[7] << 16);
+    *reinterpret_cast<uint4 *>(hi_dst) = H;
+    *reinterpret_cast<uint4 *>(lo_dst) = L;
+}
+
+// One three-product GEMM: D (128 x n) (+)= A (128 x K) B (n x K)^T, K = 16*ksteps.
+__device__ __forceinline__ void gemm3(uint32_t d, uint32_t a_hi, uint32_t a_lo, uint32_t b_hi, uint32_t b_lo,
+                                      uint32_t n, int ksteps, bool a_mn)
+{
+    const uint32_t id = umma::idesc_bf16(128, n, a_mn);
+    for (int s = 0; s < ksteps; ++s) {
+        const uint64_t ah = umma::desc_tile(a_hi, 128, s), al = umma::desc_tile(a_lo, 128, s);
+        const uint64_t bh = umma::desc_tile(b_hi, n, s), bl = umma::desc_tile(b_lo, n, s);
+        umma::mma_bf16(d, ah, bh, id, s > 0 ? 1u : 0u);
+        umma::mma_bf16(d, ah, bl, id, 1u);
+        umma::mma_bf16(d, al, bh, id, 1u);
+    }
+}
+
+__device__ __forceinline__ void cta_sync_for_mma()
+{
+    umma::fence_smem_to_async();
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+}
+
+__global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *__restrict__ consts, int *status)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char *cst = sm;
+    unsigned char *wk = sm + CONST_BYTES;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + CONST_BYTES + WORK_BYTES);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 1);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+
+    for (int i = t; i < (int)(CONST_BYTES / 16); i += 128) reinterpret_cast<uint4 *>(cst)[i] = consts[i];
+    if (t == 0) umma::mbar_init(bar, 1);
+    if (warp == 0) umma::tmem_alloc(slot, TMEM_COLS);
+    cta_sync_for_mma();
+    const uint32_t tm = *slot;
+    const uint32_t lane_base = tm + ((uint32_t)(32 * warp) << 16);
+    const uint32_t cst_a = umma::smem_u32(cst), wk_a = umma::smem_u32(wk), bar_a = umma::smem_u32(bar);
+    uint32_t phase = 0;
+    bool ok = true;
+    const long long nwt = (long long)prm.nwy * prm.nwx;
+    const long long ngroups = (prm.total + G - 1) / G;
+    const float inv_numel = 1.0f / (float)(N * N);
+
+    for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
+        // ---- stage 0: gather, weight, mean, energy; warp w takes windows w and 4 + w,
+        //      lane = row y (PIV_2d_cross_correlate.c:299-353)
+        float enorm_h[2];
+        bool valid_h[2], inr_h[2];
+        long long idx_h[2];
+        int n_h[2], iw_h[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int wl = h * 4 + warp;
+            const long long idx = grp * G + wl;
+            const bool inrange = idx < prm.total;
+            bool valid = inrange;
+            int n = 0, iw = 0, r0 = 0, c0 = 0;
+            if (inrange) {
+                n = (int)(idx / nwt);
+                iw = (int)(idx - (long long)n * nwt);
+                const int ii = iw % prm.nwx, jj = iw / prm.nwx;
+                if (prm.mask && prm.mask[iw] == 1.0f) valid = false;
+                r0 = (int)floor((double)prm.ctr_y[jj] - ((double)N - 1.0) / 2.0 + 0.5);
+                c0 = (int)floor((double)prm.ctr_x[ii] - ((double)N - 1.0) / 2.0 + 0.5);
+                if (r0 < 0 || c0 < 0 || r0 + N > prm.H || c0 + N > prm.W) valid = false;
+            }
+            float a[N], b[N];
+            float sa = 0.0f, sb = 0.0f;
+            if (valid) {
+                const float *fa = prm.A + (long long)n * prm.img_stride + (long long)(r0 + lane) * prm.W + c0;
+                const float *fb = prm.B + (long long)n * prm.img_stride + (long long)(r0 + lane) * prm.W + c0;
+#pragma unroll
+                for (int x = 0; x < N; ++x) {
+                    a[x] = __ldg(fa + x) * __ldg(prm.wA + lane * N + x);
+                    b[x] = __ldg(fb + x) * __ldg(prm.wB + lane * N + x);
+                    sa += a[x];
+                    sb += b[x];
+                }
+            } else {
+#pragma unroll
+                for (int x = 0; x < N; ++x) { a[x] = 0.0f; b[x] = 0.0f; }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                sa += __shfl_xor_sync(0xffffffffu, sa, o);
+                sb += __shfl_xor_sync(0xffffffffu, sb, o);
+            }
+            const float ma = sa / (float)(N * N), mb = sb / (float)(N * N);
+            float ea = 0.0f, eb = 0.0f;
+#pragma unroll
+            for (int x = 0; x < N; ++x) {
+                if (valid && !prm.ensemble) { a[x] -= ma; b[x] -= mb; }
+                ea += a[x] * a[x];
+                eb += b[x] * b[x];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                ea += __shfl_xor_sync(0xffffffffu, ea, o);
+                eb += __shfl_xor_sync(0xffffffffu, eb, o);
+            }
+            enorm_h[h] = 1.0f / sqrtf(ea * eb);
+            valid_h[h] = valid;
+            inr_h[h] = inrange;
+            idx_h[h] = idx;
+            n_h[h] = n;
+            iw_h[h] = iw;
+            // A1 tiles (K-major, 8 KB hi + 8 KB lo each): h -> tile h (image A), 2 + h (image B)
+            const uint32_t r = (uint32_t)(warp * 32 + lane);
+#pragma unroll
+            for (int xb = 0; xb < 4; ++xb) {
+                unsigned char *ta = wk + h * 16384, *tb = wk + (2 + h) * 16384;
+                const uint32_t off = umma::kmajor_offset(128, r, 8 * xb);
+                store8(ta + off, ta + 8192 + off, a + 8 * xb);
+                store8(tb + off, tb + 8192 + off, b + 8 * xb);
+            }
+        }
+        cta_sync_for_mma();
+        // ---- stage 1: four tiles, N = 32, K = 32
+        if (t == 0) {
+            for (int tt = 0; tt < 4; ++tt)
+                gemm3(tm + 32 * tt, wk_a + tt * 16384, wk_a + tt * 16384 + 8192, cst_a + B1, cst_a + B1 + B1_BYTES,
+                      32, 2, false);
+            umma::commit(bar_a);
+        }
+        ok &= umma::mbar_wait(bar_a, phase);
+        phase ^= 1u;
+        umma::fence_after();
+        // ---- Y -> A2 (MN-major; image i: 16 KB hi + 16 KB lo at 32 KB * i).  Row
+        //      (window, kx) = wglob * 16 + kx; K: Re at y, Im at 32 + y.
+#pragma unroll 1
+        for (int tt = 0; tt < 4; ++tt) {
+            float v[32];
+            umma::tmem_ld32(lane_base + 32 * tt, v);
+            const int wglob = (tt & 1) * 4 + warp, img = tt >> 1;
+            unsigned char *hi = wk + img * 32768, *lo = hi + 16384;
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                const uint32_t o_re = umma::mnmajor_offset(128, wglob * 16 + half * 8, lane);
+                const uint32_t o_im = umma::mnmajor_offset(128, wglob * 16 + half * 8, 32 + lane);
+                store8(hi + o_re, lo + o_re, v + half * 8);
+                store8(hi + o_im, lo + o_im, v + 16 + half * 8);
+            }
+        }
+        cta_sync_for_mma();
+        // ---- stage 2: images A, B; N = 64, K = 64; D at columns 128 (A) and 192 (B)
+        if (t == 0) {
+            for (int img = 0; img < 2; ++img)
+                gemm3(tm + 128 + 64 * img, wk_a + img * 32768, wk_a + img * 32768 + 16384, cst_a + B2,
+                      cst_a + B2 + B2_BYTES, 64, 4, true);
+            umma::commit(bar_a);
+        }
+        ok &= umma::mbar_wait(bar_a, phase);
+        phase ^= 1u;
+        umma::fence_after();
+        // ---- spectrum product -> A3 (K-major, 16 KB hi + 16 KB lo); row r = (window, kx)
+        {
+            float fa[64], fb[64];
+            umma::tmem_ld32(lane_base + 128, *reinterpret_cast<float(*)[32]>(fa));
+            umma::tmem_ld32(lane_base + 160, *reinterpret_cast<float(*)[32]>(fa + 32));
+            umma::tmem_ld32(lane_base + 192, *reinterpret_cast<float(*)[32]>(fb));
+            umma::tmem_ld32(lane_base + 224, *reinterpret_cast<float(*)[32]>(fb + 32));
+            float cr[32], ci[32];
+            const int kx = lane & 15;
+            if (kx != 0) {
+#pragma unroll
+                for (int ky = 0; ky < 32; ++ky) {
+                    const float ar = fa[ky], ai = fa[32 + ky], br = fb[ky], bi = fb[32 + ky];
+                    cr[ky] = br * ar + bi * ai;
+                    ci[ky] = bi * ar - br * ai;
+                }
+            } else {
+                // P = F(.,0) + i F(.,16); F0 = (P + conj P(-ky)) / 2, F16 = (P - conj P(-ky)) / 2i
+#pragma unroll
+                for (int ky = 0; ky < 32; ++ky) {
+                    const int m = (32 - ky) & 31;
+                    const float a0r = 0.5f * (fa[ky] + fa[m]), a0i = 0.5f * (fa[32 + ky] - fa[32 + m]);
+                    const float a1r = 0.5f * (fa[32 + ky] + fa[32 + m]), a1i = -0.5f * (fa[ky] - fa[m]);
+                    const float b0r = 0.5f * (fb[ky] + fb[m]), b0i = 0.5f * (fb[32 + ky] - fb[32 + m]);
+                    const float b1r = 0.5f * (fb[32 + ky] + fb[32 + m]), b1i = -0.5f * (fb[ky] - fb[m]);
+                    const float c0r = b0r * a0r + b0i * a0i, c0i = b0i * a0r - b0r * a0i;
+                    const float c1r = b1r * a1r + b1i * a1i, c1i = b1i * a1r - b1r * a1i;
+                    cr[ky] = c0r - c1i;        // Q = C0 + i C16
+                    ci[ky] = c0i + c1r;
+                }
+            }
+            const uint32_t r = (uint32_t)(warp * 32 + lane);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const uint32_t o_re = umma::kmajor_offset(128, r, 8 * c);
+                const uint32_t o_im = umma::kmajor_offset(128, r, 32 + 8 * c);
+                store8(wk + o_re, wk + 16384 + o_re, cr + 8 * c);
+                store8(wk + o_im, wk + 16384 + o_im, ci + 8 * c);
+            }
+        }
+        cta_sync_for_mma();
+        // ---- stage 3: N = 64, K = 64, D at column 0
+        if (t == 0) {
+            gemm3(tm, wk_a, wk_a + 16384, cst_a + B3, cst_a + B3 + B3_BYTES, 64, 4, false);
+            umma::commit(bar_a);
+        }
+        ok &= umma::mbar_wait(bar_a, phase);
+        phase ^= 1u;
+        umma::fence_after();
+        // ---- G -> A4 (MN-major; tile t4 = window / 4: 8 KB hi + 8 KB lo at 16 KB * t4).
+        //      Row (window % 4) * 32 + y; K: Re at kx, Im at 16 + kx.
+        {
+            float gre[32], gim[32];
+            umma::tmem_ld32(lane_base + 0, gre);
+            umma::tmem_ld32(lane_base + 32, gim);
+            const int r = warp * 32 + lane, wglob = r >> 4, kx = r & 15;
+            unsigned char *hi = wk + (wglob >> 2) * 16384, *lo = hi + 8192;
+            const int rb = (wglob & 3) * 32;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t o_re = umma::mnmajor_offset(128, rb + 8 * q, kx);
+                const uint32_t o_im = umma::mnmajor_offset(128, rb + 8 * q, 16 + kx);
+                store8(hi + o_re, lo + o_re, gre + 8 * q);
+                store8(hi + o_im, lo + o_im, gim + 8 * q);
+            }
+        }
+        cta_sync_for_mma();
+        // ---- stage 4: two tiles, N = 32, K = 32, D at columns 64 and 96
+        if (t == 0) {
+            for (int t4 = 0; t4 < 2; ++t4)
+                gemm3(tm + 64 + 32 * t4, wk_a + t4 * 16384, wk_a + t4 * 16384 + 8192, cst_a + B4,
+                      cst_a + B4 + B4_BYTES, 32, 2, true);
+            umma::commit(bar_a);
+        }
+        ok &= umma::mbar_wait(bar_a, phase);
+        phase ^= 1u;
+        umma::fence_after();
+        // ---- planes: scale, fftshift into shared memory (aliases the work region)
+        float *planes = reinterpret_cast<float *>(wk);
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+            float c[32];
+            umma::tmem_ld32(lane_base + 64 + 32 * h, c);
+            float *pl = planes + (h * 4 + warp) * (N * PLANE_LD);
+            const int row = (lane + N / 2) & (N - 1);
+#pragma unroll
+            for (int x = 0; x < N; ++x) pl[row * PLANE_LD + ((x + N / 2) & (N - 1))] = c[x] * inv_numel;
+        }
+        umma::fence_before();
+        __syncwarp();
+        // ---- search, fit, outputs (the FFT path's code)
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+            float *pl = planes + (h * 4 + warp) * (N * PLANE_LD);
+            if (prm.planes && valid_h[h]) {
+                float *dst = prm.planes + idx_h[h] * (long long)(N * N);
+                for (int k = lane; k < N * N; k += 32) dst[k] = pl[(k / N) * PLANE_LD + (k % N)];
+            }
+            const Group<N> g{lane, nullptr};
+            PeakAcc acc;
+            bool has_nan;
+            search_plane<N>(g, pl, acc, has_nan);
+            if (lane == 0 && inr_h[h])
+                finish_window<N, false>(prm, pl, PLANE_LD, acc, has_nan, idx_h[h], n_h[h], iw_h[h], nwt, valid_h[h],
+                                        enorm_h[h]);
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+    if (!ok && lane == 0) atomicExch(status, 1);
+    umma::fence_before();
+    __syncthreads();
+    if (warp == 0) umma::tmem_free(tm, TMEM_COLS);
+}
+
+// ---- constant operands, built on the host in double precision and split to BF16
+inline uint16_t bf16_rn(float f)
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+inline float bf16_f(uint16_t h)
+{
+    uint32_t u = (uint32_t)h << 16;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+// K-major hi/lo images of a rows x K matrix given by coef(j, k).
+template <class F>
+void put(unsigned char *base, uint32_t off, uint32_t bytes, int rows, int K, F coef)
+{
+    for (int j = 0; j < rows; ++j)
+        for (int k = 0; k < K; ++k) {
+            const double v = coef(j, k);
+            const uint16_t h = bf16_rn((float)v);
+            const uint16_t l = bf16_rn((float)(v - (double)bf16_f(h)));
+            const uint32_t o = umma::kmajor_offset((uint32_t)rows, (uint32_t)j, (uint32_t)k);
+            memcpy(base + off + o, &h, 2);
+            memcpy(base + off + bytes + o, &l, 2);
+        }
+}
+
+void build_consts(unsigned char *c)
+{
+    const double tp = 2.0 * M_PI / N;
+    // W1: row j -> Re Y(j) (j < 16), Y(16) (j = 16), Im Y(j - 16) (j > 16); K = x
+    put(c, B1, B1_BYTES, 32, 32, [&](int j, int x) {
+        if (j < 16) return cos(tp * j * x);
+        if (j == 16) return (x & 1) ? -1.0 : 1.0;
+        return -sin(tp * (j - 16) * x);
+    });
+    // W2: row j -> Re F(ky = j) (j < 32), Im F(ky = j - 32); K: Re Y(y = k) (k < 32), Im Y(y = k - 32)
+    put(c, B2, B2_BYTES, 64, 64, [&](int j, int k) {
+        const int ky = j & 31, y = k & 31;
+        const double cs = cos(tp * ky * y), sn = sin(tp * ky * y);
+        if (j < 32) return k < 32 ? cs : sn;
+        return k < 32 ? -sn : cs;
+    });
+    // W3: row j -> Re G(y = j) (j < 32), Im G(y = j - 32); K: Re C(ky = k) (k < 32), Im C(ky = k - 32)
+    put(c, B3, B3_BYTES, 64, 64, [&](int j, int k) {
+        const int y = j & 31, ky = k & 31;
+        const double cs = cos(tp * ky * y), sn = sin(tp * ky * y);
+        if (j < 32) return k < 32 ? cs : -sn;
+        return k < 32 ? sn : cs;
+    });
+    // W4: row x -> c(x); K: Re G(kx = k) (k < 16), Im G(kx = k - 16); kx = 0 carries G(0) and G(16)
+    put(c, B4, B4_BYTES, 32, 32, [&](int x, int k) {
+        const int kx = k & 15;
+        if (k < 16) return kx == 0 ? 1.0 : 2.0 * cos(tp * kx * x);
+        return kx == 0 ? ((x & 1) ? -1.0 : 1.0) : -2.0 * sin(tp * kx * x);
+    });
+}
+
+std::mutex g_mu;
+void *g_consts[64] = {};
+
+const uint4 *consts_for_current_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_consts[dev]) {
+        static unsigned char host[CONST_BYTES];
+        memset(host, 0, sizeof(host));
+        build_consts(host);
+        void *d = nullptr;
+        if (cudaMalloc(&d, CONST_BYTES) != cudaSuccess) return nullptr;
+        if (cudaMemcpy(d, host, CONST_BYTES, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaFree(d);
+            return nullptr;
+        }
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) != cudaSuccess) {
+            cudaFree(d);
+            return nullptr;
+        }
+        g_consts[dev] = d;
+    }
+    return static_cast<const uint4 *>(g_consts[dev]);
+}
+
+}  // namespace dft32
+
 }  // namespace
 
 // Self-test of the tensor-core path: D (128 x N) = A (128 x K) B (N x K)^T with
@@ -83,4 +519,55 @@ PIV_EXPORT int pivb_umma_selftest(const void *d_A, const void *d_B, float *d_D, 
                                                                   static_cast<const uint16_t *>(d_B), d_D, N, K,
                                                                   a_mn, ncols, d_status);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Instantaneous correlation of 32 x 32 windows on the tensor core (DFT-as-GEMM,
+// split BF16, FP32 accumulation).  Arguments as pivb_xcorr_dev; supported:
+// win 32 x 32, ensemble 0, n_peaks 1, peak finders 3-6 (4-6 need the LM scratch
+// of pivb_xcorr_scratch_bytes).  *d_status (device int) is set to 1 if an MMA
+// completion was not observed.  The first call on a device builds the constant
+// DFT operands (a synchronous upload): make it before any stream capture.
+PIV_EXPORT int pivb_dft_xcorr_dev(const float *d_A, const float *d_B, long long img_stride, const float *d_mask,
+                                  int H, int W, int n_images, const float *d_ctr_x, const float *d_ctr_y,
+                                  int n_win_y, int n_win_x, const float *d_wA, const float *d_wB, const float *d_cw,
+                                  int win_h, int win_w, int ensemble, int n_peaks, int peak_finder,
+                                  int peakfit_impl, float *d_pk_x, float *d_pk_y, float *d_pk_h, float *d_sx,
+                                  float *d_sy, float *d_sxy, float *d_pk_ratio, float *d_planes, void *d_scratch,
+                                  size_t scratch_bytes, int *d_status, void *stream)
+{
+    using namespace piv;
+    if (win_h != 32 || win_w != 32) return PIV_ERROR_NOPLAN;
+    if (ensemble || n_peaks != 1 || peak_finder < 3 || peak_finder > 6 || n_images < 0 || !d_status)
+        return PIV_ERROR_OUT_OF_BOUNDS;
+    const long long total = (long long)n_images * n_win_y * n_win_x;
+    if (total == 0) return PIV_ERROR_NONE;
+    const bool lm = peak_finder >= 4;
+    if (lm && (d_scratch == nullptr || scratch_bytes < (size_t)total * sizeof(LmRecord))) return PIV_ERROR_NOMEM;
+    const uint4 *consts = dft32::consts_for_current_device();
+    if (!consts) return PIV_ERROR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    XcorrParams p{};
+    p.A = d_A; p.B = d_B; p.img_stride = img_stride; p.mask = d_mask;
+    p.H = H; p.W = W; p.n_img = n_images;
+    p.ctr_x = d_ctr_x; p.ctr_y = d_ctr_y; p.nwy = n_win_y; p.nwx = n_win_x;
+    p.wA = d_wA; p.wB = d_wB; p.cw = d_cw;
+    p.ensemble = 0; p.n_peaks = 1; p.finder = peak_finder;
+    p.pk_x = d_pk_x; p.pk_y = d_pk_y; p.pk_h = d_pk_h; p.sx = d_sx; p.sy = d_sy; p.sxy = d_sxy;
+    p.pk_ratio = d_pk_ratio; p.planes = d_planes;
+    p.lm = lm ? static_cast<LmRecord *>(d_scratch) : nullptr;
+    p.total = total;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long groups = (total + dft32::G - 1) / dft32::G;
+    const int grid = (int)(groups < 2LL * sms ? groups : 2LL * sms);
+    dft32::kernel<<<grid, 128, dft32::SMEM_BYTES, s>>>(p, consts, d_status);
+    if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
+    if (lm) {
+        const unsigned blocks = (unsigned)((total + 127) / 128);
+        if (peakfit_impl) lm_records_kernel<1><<<blocks, 128, 0, s>>>(p, 32);
+        else lm_records_kernel<0><<<blocks, 128, 0, s>>>(p, 32);
+        if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
+    }
+    return PIV_ERROR_NONE;
 }

@@ -33,7 +33,7 @@ struct WinGeo {
     static constexpr int WARPS_PER_CTA = (GW <= 32) ? 4 : GW / 32;
     static constexpr int CTA_THREADS = WARPS_PER_CTA * 32;
     // resident CTAs per SM the correlation kernel is compiled for (register cap)
-    static constexpr int MIN_CTAS = (N == 32) ? 5 : 1;
+    static constexpr int MIN_CTAS = (N == 32) ? 5 : (N <= 16 ? 8 : 1);
     static constexpr int GROUPS_PER_CTA = (GW <= 32) ? WARPS_PER_CTA * WPW : 1;
     static constexpr int PLANE_BYTES = N * ST * 8;
     static constexpr int RED_SLOTS = (GW > 32) ? GW / 32 : 1;

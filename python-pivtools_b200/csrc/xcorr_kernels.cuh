@@ -56,6 +56,99 @@ __device__ __forceinline__ void write_peak(const XcorrParams &p, long long o, in
     p.sxy[o] = sig[2];
 }
 
+// Group-leader finish of one window: peak choice and detectability (from the
+// parallel search, or an exact sequential scan when the plane holds NaN), the
+// height and border gates, the weighted 5x5 patch, the fit (or a deferred LM
+// record), and the outputs (PIV_2d_cross_correlate.c:80-125, peak_locate_lm.c:757-918).
+// pl: float plane of the window, row stride ld.
+template <int N, bool MULTI>
+__device__ __forceinline__ void finish_window(const XcorrParams &prm, float *pl, int ld, PeakAcc acc, bool has_nan,
+                                           long long idx, int n, int iw, long long nwt, bool valid, float enorm)
+{
+    LmRecord *rec = prm.lm ? prm.lm + idx : nullptr;
+    if (!valid) {
+        if (rec) rec->flag = 0;
+    } else {
+        PlaneView v{pl, ld};
+        int bi, bj;
+        float best, ratio;
+        if (has_nan) {
+            best = seq_search(v, N, N, &bi, &bj);
+            ratio = seq_detectability(v, N, N);
+        } else {
+            best = acc.best;
+            bi = (acc.idx == 0x7fffffff) ? 0 : acc.idx / N;
+            bj = (acc.idx == 0x7fffffff) ? 0 : acc.idx % N;
+            ratio = (acc.p2 > 0.0f) ? fdiv(acc.p1, acc.p2) : 0.0f;
+        }
+        prm.pk_ratio[(long long)n * nwt + iw] = ratio;
+        const int np = MULTI ? prm.n_peaks : 1;
+        for (int k = 0; k < np; ++k) {
+            if (k > 0) best = seq_search(v, N, N, &bi, &bj);
+            const long long o = (long long)n * np * nwt + (long long)k * nwt + iw;
+            if (!(best > 0.0f) && !(best != best)) {   // best <= 0
+                write_sentinel(prm, o, enorm);
+                if (rec) rec->flag = 0;
+                continue;
+            }
+            if (bi < 2 || bi >= N - 2 || bj < 2 || bj >= N - 2) {
+                write_sentinel(prm, o, enorm);
+                if (rec) rec->flag = 0;
+                continue;
+            }
+            float sub[PKN];
+#pragma unroll
+            for (int aa = 0; aa < PKW; ++aa)
+#pragma unroll
+                for (int bb = 0; bb < PKW; ++bb) {
+                    const int r = bi + aa - 2, c = bj + bb - 2;
+                    sub[aa * PKW + bb] = fmul(pl[r * ld + c], __ldg(prm.cw + r * N + c));
+                }
+            if (k == 0 && prm.finder >= 4 && prm.finder <= 6 && !MULTI) {
+                // deferred LM (single peak)
+#pragma unroll
+                for (int q = 0; q < PKN; ++q) rec->sub[q] = sub[q];
+                rec->best = best;
+                rec->enorm = enorm;
+                rec->ij = (bi << 16) | bj;
+                rec->flag = 1;
+                continue;
+            }
+            float off[2], sig[3], fv[PKN];
+            bool ok = true;
+            if constexpr (MULTI) {
+                if (k == 0 && prm.finder >= 4 && prm.finder <= 6) {
+                    ok = lm_fit_any<0>(prm.finder, sub, off, sig, fv);
+                } else {
+                    float A0, s0, s1;
+                    three_point(sub, PKW, PKW, PKW, off, &A0, &s0, &s1);
+                    sig[0] = s0; sig[1] = s1; sig[2] = 0.0f;
+                    for (int q = 0; q < PKN; ++q) {
+                        float di = fdiv(fsub((float)(q / PKW - 2), off[0]), s0);
+                        float dj = fdiv(fsub((float)(q % PKW - 2), off[1]), s1);
+                        fv[q] = fmul(A0, expf_cr(-fadd(fmul(di, di), fmul(dj, dj))));
+                    }
+                }
+            } else {
+                float A0, s0, s1;
+                three_point(sub, PKW, PKW, PKW, off, &A0, &s0, &s1);
+                sig[0] = s0; sig[1] = s1; sig[2] = 0.0f;
+            }
+            if (!ok) write_sentinel(prm, o, enorm);
+            else write_peak(prm, o, N, bi, bj, off, sig, best, enorm);
+            if constexpr (MULTI) {
+                float *mp = const_cast<float *>(pl);
+                for (int q = 0; q < PKN; ++q) {
+                    const int r = bi + q / PKW - 2, c = bj + q % PKW - 2;
+                    float f = fdiv(fv[q], __ldg(prm.cw + r * N + c));
+                    float d = fsub(mp[r * ld + c], f);
+                    mp[r * ld + c] = (0.0f > d) ? 0.0f : d;
+                }
+            }
+        }
+    }
+}
+
 // Fused correlation kernel (PIV_2d_cross_correlate.c:203-397): gather + weight +
 // mean/energy, packed forward FFT, conjugate product, inverse FFT, shift, peak
 // search, 3-point fit.  LM fits of single-peak calls are deferred to
@@ -150,90 +243,7 @@ xcorr_kernel(XcorrParams prm)
             PeakAcc acc;
             bool has_nan;
             search_plane<N>(g, pl, acc, has_nan);
-            if (t == 0 && inrange) {
-                LmRecord *rec = prm.lm ? prm.lm + idx : nullptr;
-                if (!valid) {
-                    if (rec) rec->flag = 0;
-                } else {
-                    PlaneView v{pl, G::STF};
-                    int bi, bj;
-                    float best, ratio;
-                    if (has_nan) {
-                        best = seq_search(v, N, N, &bi, &bj);
-                        ratio = seq_detectability(v, N, N);
-                    } else {
-                        best = acc.best;
-                        bi = (acc.idx == 0x7fffffff) ? 0 : acc.idx / N;
-                        bj = (acc.idx == 0x7fffffff) ? 0 : acc.idx % N;
-                        ratio = (acc.p2 > 0.0f) ? fdiv(acc.p1, acc.p2) : 0.0f;
-                    }
-                    prm.pk_ratio[(long long)n * nwt + iw] = ratio;
-                    const int np = MULTI ? prm.n_peaks : 1;
-                    for (int k = 0; k < np; ++k) {
-                        if (k > 0) best = seq_search(v, N, N, &bi, &bj);
-                        const long long o = (long long)n * np * nwt + (long long)k * nwt + iw;
-                        if (!(best > 0.0f) && !(best != best)) {   // best <= 0
-                            write_sentinel(prm, o, enorm);
-                            if (rec) rec->flag = 0;
-                            continue;
-                        }
-                        if (bi < 2 || bi >= N - 2 || bj < 2 || bj >= N - 2) {
-                            write_sentinel(prm, o, enorm);
-                            if (rec) rec->flag = 0;
-                            continue;
-                        }
-                        float sub[PKN];
-#pragma unroll
-                        for (int aa = 0; aa < PKW; ++aa)
-#pragma unroll
-                            for (int bb = 0; bb < PKW; ++bb) {
-                                const int r = bi + aa - 2, c = bj + bb - 2;
-                                sub[aa * PKW + bb] = fmul(pl[r * G::STF + c], __ldg(prm.cw + r * N + c));
-                            }
-                        if (k == 0 && prm.finder >= 4 && prm.finder <= 6 && !MULTI) {
-                            // deferred LM (single peak)
-#pragma unroll
-                            for (int q = 0; q < PKN; ++q) rec->sub[q] = sub[q];
-                            rec->best = best;
-                            rec->enorm = enorm;
-                            rec->ij = (bi << 16) | bj;
-                            rec->flag = 1;
-                            continue;
-                        }
-                        float off[2], sig[3], fv[PKN];
-                        bool ok = true;
-                        if constexpr (MULTI) {
-                            if (k == 0 && prm.finder >= 4 && prm.finder <= 6) {
-                                ok = lm_fit_any<0>(prm.finder, sub, off, sig, fv);
-                            } else {
-                                float A0, s0, s1;
-                                three_point(sub, PKW, PKW, PKW, off, &A0, &s0, &s1);
-                                sig[0] = s0; sig[1] = s1; sig[2] = 0.0f;
-                                for (int q = 0; q < PKN; ++q) {
-                                    float di = fdiv(fsub((float)(q / PKW - 2), off[0]), s0);
-                                    float dj = fdiv(fsub((float)(q % PKW - 2), off[1]), s1);
-                                    fv[q] = fmul(A0, expf_cr(-fadd(fmul(di, di), fmul(dj, dj))));
-                                }
-                            }
-                        } else {
-                            float A0, s0, s1;
-                            three_point(sub, PKW, PKW, PKW, off, &A0, &s0, &s1);
-                            sig[0] = s0; sig[1] = s1; sig[2] = 0.0f;
-                        }
-                        if (!ok) write_sentinel(prm, o, enorm);
-                        else write_peak(prm, o, N, bi, bj, off, sig, best, enorm);
-                        if constexpr (MULTI) {
-                            float *mp = const_cast<float *>(pl);
-                            for (int q = 0; q < PKN; ++q) {
-                                const int r = bi + q / PKW - 2, c = bj + q % PKW - 2;
-                                float f = fdiv(fv[q], __ldg(prm.cw + r * N + c));
-                                float d = fsub(mp[r * G::STF + c], f);
-                                mp[r * G::STF + c] = (0.0f > d) ? 0.0f : d;
-                            }
-                        }
-                    }
-                }
-            }
+            if (t == 0 && inrange) finish_window<N, MULTI>(prm, pl, G::STF, acc, has_nan, idx, n, iw, nwt, valid, enorm);
         }
         g.sync();
     }
