@@ -111,27 +111,21 @@ constexpr uint32_t SMEM_BYTES = CONST_BYTES + WORK_BYTES + 64;
 constexpr uint32_t TMEM_COLS = 256;
 static_assert(G * N * PLANE_LD * 4 <= WORK_BYTES, "planes alias the work region");
 
-__device__ __forceinline__ void split(float x, uint16_t &hi, uint16_t &lo)
-{
-    const __nv_bfloat16 h = __float2bfloat16_rn(x);
-    const __nv_bfloat16 l = __float2bfloat16_rn(x - __bfloat162float(h));
-    hi = __bfloat16_as_ushort(h);
-    lo = __bfloat16_as_ushort(l);
-}
-
-// Split 8 values and store the hi and lo halves as two 16-byte vectors.
+// Split 8 values into hi = bf16(x) and lo = bf16(x - hi) and store each half
+// as one 16-byte vector (paired conversions: cvt.rn.bf16x2 per two values).
 __device__ __forceinline__ void store8(unsigned char *hi_dst, unsigned char *lo_dst, const float *v)
 {
-    uint16_t h[8], l[8];
+    uint32_t H[4], L[4];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) split(v[j], h[j], l[j]);
-    uint4 H, L;
-    H.x = h[0] | ((uint32_t)h[1] << 16); H.y = h[2] | ((uint32_t)h[3] << 16);
-    H.z = h[4] | ((uint32_t)h[5] << 16); H.w = h[6] | ((uint32_t)h[7] << 16);
-    L.x = l[0] | ((uint32_t)l[1] << 16); L.y = l[2] | ((uint32_t)l[3] << 16);
-    L.z = l[4] | ((uint32_t)l[5] << 16); L.w = l[6] | ((uint32_t)l[7] << 16);
-    *reinterpret_cast<uint4 *>(hi_dst) = H;
-    *reinterpret_cast<uint4 *>(lo_dst) = L;
+    for (int j = 0; j < 4; ++j) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+        const float2 hf = __bfloat1622float2(h);
+        const __nv_bfloat162 l = __floats2bfloat162_rn(v[2 * j] - hf.x, v[2 * j + 1] - hf.y);
+        H[j] = *reinterpret_cast<const uint32_t *>(&h);
+        L[j] = *reinterpret_cast<const uint32_t *>(&l);
+    }
+    *reinterpret_cast<uint4 *>(hi_dst) = make_uint4(H[0], H[1], H[2], H[3]);
+    *reinterpret_cast<uint4 *>(lo_dst) = make_uint4(L[0], L[1], L[2], L[3]);
 }
 
 // One three-product GEMM: D (128 x n) (+)= A (128 x K) B (n x K)^T, K = 16*ksteps.
@@ -156,9 +150,18 @@ __device__ __forceinline__ void cta_sync_for_mma()
     umma::fence_after();
 }
 
+struct WinInfo {
+    long long idx;
+    int n, iw;
+    float enorm;
+    int flags;     // 1 valid, 2 in range, 4 plane holds NaN
+};
+
 __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *__restrict__ consts, int *status)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ WinInfo info[G];
+    __shared__ PeakAcc found[G];
     unsigned char *cst = sm;
     unsigned char *wk = sm + CONST_BYTES;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + CONST_BYTES + WORK_BYTES);
@@ -179,13 +182,10 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
     const float inv_numel = 1.0f / (float)(N * N);
 
     for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-        // ---- stage 0: gather, weight, mean, energy; warp w takes windows w and 4 + w,
-        //      lane = row y (PIV_2d_cross_correlate.c:299-353)
-        float enorm_h[2];
-        bool valid_h[2], inr_h[2];
-        long long idx_h[2];
-        int n_h[2], iw_h[2];
-#pragma unroll
+        // ---- stage 0: gather, weight, mean, energy (PIV_2d_cross_correlate.c:299-353).
+        //      Warp w takes windows w and 4 + w; lane = column x, so every load
+        //      instruction reads one 128-byte image row segment.
+#pragma unroll 1
         for (int h = 0; h < 2; ++h) {
             const int wl = h * 4 + warp;
             const long long idx = grp * G + wl;
@@ -204,18 +204,18 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
             float a[N], b[N];
             float sa = 0.0f, sb = 0.0f;
             if (valid) {
-                const float *fa = prm.A + (long long)n * prm.img_stride + (long long)(r0 + lane) * prm.W + c0;
-                const float *fb = prm.B + (long long)n * prm.img_stride + (long long)(r0 + lane) * prm.W + c0;
+                const float *fa = prm.A + (long long)n * prm.img_stride + (long long)r0 * prm.W + c0 + lane;
+                const float *fb = prm.B + (long long)n * prm.img_stride + (long long)r0 * prm.W + c0 + lane;
 #pragma unroll
-                for (int x = 0; x < N; ++x) {
-                    a[x] = __ldg(fa + x) * __ldg(prm.wA + lane * N + x);
-                    b[x] = __ldg(fb + x) * __ldg(prm.wB + lane * N + x);
-                    sa += a[x];
-                    sb += b[x];
+                for (int y = 0; y < N; ++y) {
+                    a[y] = __ldg(fa + y * prm.W) * __ldg(prm.wA + y * N + lane);
+                    b[y] = __ldg(fb + y * prm.W) * __ldg(prm.wB + y * N + lane);
+                    sa += a[y];
+                    sb += b[y];
                 }
             } else {
 #pragma unroll
-                for (int x = 0; x < N; ++x) { a[x] = 0.0f; b[x] = 0.0f; }
+                for (int y = 0; y < N; ++y) { a[y] = 0.0f; b[y] = 0.0f; }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -225,30 +225,31 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
             const float ma = sa / (float)(N * N), mb = sb / (float)(N * N);
             float ea = 0.0f, eb = 0.0f;
 #pragma unroll
-            for (int x = 0; x < N; ++x) {
-                if (valid && !prm.ensemble) { a[x] -= ma; b[x] -= mb; }
-                ea += a[x] * a[x];
-                eb += b[x] * b[x];
+            for (int y = 0; y < N; ++y) {
+                if (valid && !prm.ensemble) { a[y] -= ma; b[y] -= mb; }
+                ea += a[y] * a[y];
+                eb += b[y] * b[y];
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 ea += __shfl_xor_sync(0xffffffffu, ea, o);
                 eb += __shfl_xor_sync(0xffffffffu, eb, o);
             }
-            enorm_h[h] = 1.0f / sqrtf(ea * eb);
-            valid_h[h] = valid;
-            inr_h[h] = inrange;
-            idx_h[h] = idx;
-            n_h[h] = n;
-            iw_h[h] = iw;
-            // A1 tiles (K-major, 8 KB hi + 8 KB lo each): h -> tile h (image A), 2 + h (image B)
-            const uint32_t r = (uint32_t)(warp * 32 + lane);
+            if (lane == 0) {
+                info[wl].idx = idx;
+                info[wl].n = n;
+                info[wl].iw = iw;
+                info[wl].enorm = 1.0f / sqrtf(ea * eb);
+                info[wl].flags = (valid ? 1 : 0) | (inrange ? 2 : 0);
+            }
+            // A1 tiles (MN-major, 8 KB hi + 8 KB lo each): h -> tile h (image A), 2 + h (image B);
+            // row (window % 4) * 32 + y, K = x
+            unsigned char *ta = wk + h * 16384, *tb = wk + (2 + h) * 16384;
 #pragma unroll
-            for (int xb = 0; xb < 4; ++xb) {
-                unsigned char *ta = wk + h * 16384, *tb = wk + (2 + h) * 16384;
-                const uint32_t off = umma::kmajor_offset(128, r, 8 * xb);
-                store8(ta + off, ta + 8192 + off, a + 8 * xb);
-                store8(tb + off, tb + 8192 + off, b + 8 * xb);
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t off = umma::mnmajor_offset(128, warp * 32 + 8 * q, lane);
+                store8(ta + off, ta + 8192 + off, a + 8 * q);
+                store8(tb + off, tb + 8192 + off, b + 8 * q);
             }
         }
         cta_sync_for_mma();
@@ -256,7 +257,7 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
         if (t == 0) {
             for (int tt = 0; tt < 4; ++tt)
                 gemm3(tm + 32 * tt, wk_a + tt * 16384, wk_a + tt * 16384 + 8192, cst_a + B1, cst_a + B1 + B1_BYTES,
-                      32, 2, false);
+                      32, 2, true);
             umma::commit(bar_a);
         }
         ok &= umma::mbar_wait(bar_a, phase);
@@ -379,22 +380,31 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
         }
         umma::fence_before();
         __syncwarp();
-        // ---- search, fit, outputs (the FFT path's code)
+        // ---- search (warp per window), then the fits of all eight windows in
+        //      parallel on the lanes of warp 0 (the FFT path's code)
 #pragma unroll 1
         for (int h = 0; h < 2; ++h) {
-            float *pl = planes + (h * 4 + warp) * (N * PLANE_LD);
-            if (prm.planes && valid_h[h]) {
-                float *dst = prm.planes + idx_h[h] * (long long)(N * N);
+            const int wl = h * 4 + warp;
+            float *pl = planes + wl * (N * PLANE_LD);
+            if (prm.planes && (info[wl].flags & 1)) {
+                float *dst = prm.planes + info[wl].idx * (long long)(N * N);
                 for (int k = lane; k < N * N; k += 32) dst[k] = pl[(k / N) * PLANE_LD + (k % N)];
             }
             const Group<N> g{lane, nullptr};
             PeakAcc acc;
             bool has_nan;
             search_plane<N>(g, pl, acc, has_nan);
-            if (lane == 0 && inr_h[h])
-                finish_window<N, false>(prm, pl, PLANE_LD, acc, has_nan, idx_h[h], n_h[h], iw_h[h], nwt, valid_h[h],
-                                        enorm_h[h]);
-            __syncwarp();
+            if (lane == 0) {
+                found[wl] = acc;
+                if (has_nan) info[wl].flags |= 4;
+            }
+        }
+        __syncthreads();
+        if (warp == 0 && lane < G) {
+            const WinInfo wi = info[lane];
+            if (wi.flags & 2)
+                finish_window<N, false>(prm, planes + lane * (N * PLANE_LD), PLANE_LD, found[lane],
+                                        (wi.flags & 4) != 0, wi.idx, wi.n, wi.iw, nwt, (wi.flags & 1) != 0, wi.enorm);
         }
         __syncthreads();
     }
