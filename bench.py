@@ -33,6 +33,8 @@ sys.path.insert(0, os.path.join(ROOT, "python-pivtools_b200"))
 METRIC = "vectors/s and p50/p99 pair latency on 1 B200 at ≤0.01 px RMS vs FP64 oracle"
 WORKLOAD = "multipass window-deformation PIV, 64 pairs 2048x2048, passes 128/64/32/32 px at 50/50/50/75%"
 HW = (2048, 2048)
+# FP32 CUDA-core peak, nominal: 148 SMs x 128 lanes x 2 flops x 1.965 GHz (no measured figure)
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 def _args():
@@ -271,12 +273,11 @@ def run_b200(args):
     hbm_peak, bf16_peak, peak_kind = _peaks()
     achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
     fp32_flops = windows * 80.1e3
-    traffic = None
-    try:
-        with open(os.path.join(ROOT, "profiles", "xcorr32_traffic.json")) as f:
-            traffic = json.load(f).get("bytes_per_launch")
-    except Exception:
-        pass
+    # DRAM traffic of one launch: dram__bytes_read.sum + dram__bytes_write.sum of the
+    # same kernel and pass captured by ncu on 8 pairs (305.0 MB + 16.2 MB for 512,072
+    # windows, profiles/xcorr_kernel32_pass4_8pairs.md), scaled by windows processed
+    # (frames and outputs both grow with the pair count).
+    traffic = (304.946688e6 + 16.182016e6) / 512072 * windows
 
     # ---- end to end through host buffers: every step copies its 64 pairs of
     # uint16 frames from pinned memory (chunked, overlapped with compute), converts
@@ -336,7 +337,8 @@ def run_b200(args):
                          "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "xcorr_kernel<32> (final pass, 4.1M windows)", "kernel_ms": kern_ms,
                          "algorithmic_bytes": alg_bytes,
-                         "fp32_view": {"flops_per_launch": fp32_flops,
+                         "fp32_view": {"flops_per_launch": fp32_flops, "peak_tflops_nominal": FP32_NOMINAL_TFLOPS,
+                                       "frac_of_nominal": fp32_flops / (kern_ms * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS,
                                        "achieved_tflops": fp32_flops / (kern_ms * 1e-3) / 1e12}},
             "e2e": {"value": e2e_val, "unit": "vectors/s", "h2d_bytes_per_step": 2 * N * HW[0] * HW[1] * 2,
                     "d2h_bytes_per_step": 2 * N * p["ny"] * p["nx"] * 4, "frames": "uint16",
