@@ -42,6 +42,28 @@ int pivb_remap_dev(const float *pdy, const float *pdx, int N, int nyp, int nxp, 
  * pivtools_core/image_handling/load_images.py:594,625).  in 8-byte, out 16-byte aligned. */
 int pivb_u16_to_f32_dev(const unsigned short *in, float *out, long long n, void *stream);
 
+/* Ensemble pass on the GPU (the reference does these steps in NumPy:
+ * pivtools_cli/piv/piv_backend/single_pass_accumulator.py:292-320, 508-800). */
+
+/* sum (+)= the n_frames frames (stride elements apart, npix pixels each), Kahan-
+ * compensated through comp (zero both before the first call). */
+int pivb_frame_sum_dev(const float *frames, long long stride, int n_frames, long long npix, float *sum,
+                       float *comp, void *stream);
+
+/* out = sum / n: the mean frame of n accumulated pairs. */
+int pivb_frame_mean_dev(const float *sum, long long npix, int n, float *out, void *stream);
+
+/* Finalise of one ensemble pass (std mode): average the accumulated AB/AA/BB sums
+ * of n_win windows of h x w over n_pairs, subtract the background planes (all three
+ * or none), optionally zero each plane's mean (the '+dc_zero' methods), divide by
+ * the pair-count envelopes (nullable; env_ab defaults to env_auto), normalise by
+ * sqrt(max(AA_c BB_c, 1e-12)) at the centre bin and write FP64 planes for
+ * pivb_kspace_fit_dev.  norm (nullable) receives the per-window factors. */
+int pivb_ensemble_finalize_dev(const float *sum_ab, const float *sum_aa, const float *sum_bb, const float *bg_ab,
+                               const float *bg_aa, const float *bg_bb, int n_pairs, int n_win, int h, int w,
+                               int dc_zero, const float *env_auto, const float *env_ab, double *out_ab,
+                               double *out_aa, double *out_bb, float *norm, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -236,3 +236,57 @@ def kspace_fit(R_AA, R_BB, R_AB, mask, corr_size, use_kx4=0, use_ky4=0, P_win=No
                                       o["n_valid"], o["iters"], o["conv"], n_threads)
     o["ret"] = int(r)
     return o
+
+
+# ---------------------------------------------------------------------------
+# Ensemble finalise (pivtools_cli/piv/piv_backend/single_pass_accumulator.py)
+# ---------------------------------------------------------------------------
+
+def pair_envelope(wa, wb, corr_size):
+    """Linear pair-count envelope E(s) = sum_x wa(x + s) wb(x), centre-cropped to
+    corr_size with zero lag at corr_size // 2 and normalised to 1 there
+    (single_pass_accumulator.py:52-102), by direct summation in FP64."""
+    wa = np.asarray(wa, np.float64)
+    wb = np.asarray(wb, np.float64)
+    h, w = wa.shape
+    ch, cw = corr_size
+    env = np.zeros((ch, cw))
+    for i in range(ch):
+        for j in range(cw):
+            sy, sx = i - ch // 2, j - cw // 2
+            y0, y1 = max(0, -sy), min(h, h - sy)
+            x0, x1 = max(0, -sx), min(w, w - sx)
+            if y1 > y0 and x1 > x0:
+                env[i, j] = np.sum(wa[y0 + sy:y1 + sy, x0 + sx:x1 + sx] * wb[y0:y1, x0:x1])
+    return env / env[ch // 2, cw // 2]
+
+
+def zero_plane_means(planes):
+    """Subtract each window's plane mean (single_pass_accumulator.py:105-123);
+    planes (n, h, w) float32."""
+    p = np.asarray(planes, np.float32)
+    return p - p.mean(axis=(1, 2), keepdims=True, dtype=np.float64).astype(np.float32)
+
+
+def ensemble_finalize(sum_ab, sum_aa, sum_bb, n_pairs, bg=None, dc_zero=False, env_auto=None, env_ab=None):
+    """Averaged, background-subtracted, optionally DC-zeroed and envelope-divided,
+    normalised ensemble planes, in float32 as the reference computes them
+    (single_pass_accumulator.py:564-800, std mode): R = sum / N - bg; R -= mean;
+    R /= E; R /= sqrt(max(AA_c * BB_c, 1e-12)).  Inputs (n, h, w); returns
+    (R_AA, R_BB, R_AB, norm)."""
+    n = np.float32(n_pairs)
+    R = [np.asarray(s, np.float32) / n for s in (sum_aa, sum_bb, sum_ab)]
+    if bg is not None:
+        bg_aa, bg_bb, bg_ab = bg
+        R = [r - np.asarray(b, np.float32) for r, b in zip(R, (bg_aa, bg_bb, bg_ab))]
+    if dc_zero:
+        R = [zero_plane_means(r) for r in R]
+    if env_auto is not None:
+        ea = np.asarray(env_auto, np.float32)[None]
+        eb = np.asarray(env_ab if env_ab is not None else env_auto, np.float32)[None]
+        R = [R[0] / ea, R[1] / ea, R[2] / eb]
+    h, w = R[0].shape[1:]
+    c = (h // 2, w // 2)
+    norm = np.sqrt(np.maximum(R[0][:, c[0], c[1]] * R[1][:, c[0], c[1]], np.float32(1e-12)))
+    R = [r / norm[:, None, None] for r in R]
+    return R[0], R[1], R[2], norm

@@ -407,3 +407,132 @@ PIV_EXPORT int pivb_u16_to_f32_dev(const unsigned short *in, float *out, long lo
     u16_to_f32_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(in, out, n);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
+
+// ---------------------------------------------------------------------------
+// Ensemble pass: frame sums and the finalise of the accumulated planes
+// (pivtools_cli/piv/piv_backend/single_pass_accumulator.py:292-320, 508-800)
+// ---------------------------------------------------------------------------
+namespace {
+
+// sum[p] += sum_k frames[k][p] with a Kahan compensation term per pixel.
+__global__ void frame_sum_kernel(const float *__restrict__ frames, long long stride, int n_frames, long long npix,
+                                 float *__restrict__ sum, float *__restrict__ comp)
+{
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npix;
+         p += (long long)gridDim.x * blockDim.x) {
+        float s = sum[p], c = comp[p];
+        for (int k = 0; k < n_frames; ++k) {
+            const float y = __ldg(frames + (long long)k * stride + p) - c;
+            const float t = s + y;
+            c = (t - s) - y;
+            s = t;
+        }
+        sum[p] = s;
+        comp[p] = c;
+    }
+}
+
+__global__ void frame_mean_kernel(const float *__restrict__ sum, long long npix, float n, float *__restrict__ out)
+{
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npix;
+         p += (long long)gridDim.x * blockDim.x)
+        out[p] = sum[p] / n;
+}
+
+struct FinParams {
+    const float *sum_ab, *sum_aa, *sum_bb;     // (n_win, h, w) accumulated sums
+    const float *bg_ab, *bg_aa, *bg_bb;        // background planes or null
+    const float *env_auto, *env_ab;            // (h, w) envelopes or null
+    float n_pairs;
+    int n_win, hw, centre, dc_zero;
+    double *out_aa, *out_bb, *out_ab;          // normalised planes for the k-space fit
+    float *norm;                               // (n_win) normalisation factors, nullable
+};
+
+// One warp per window; float32 arithmetic in the reference's order.
+__global__ void ensemble_finalize_kernel(FinParams p)
+{
+    const int warp = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (warp >= p.n_win) return;
+    const long long base = (long long)warp * p.hw;
+    const float *sums[3] = {p.sum_aa, p.sum_bb, p.sum_ab};
+    const float *bgs[3] = {p.bg_aa, p.bg_bb, p.bg_ab};
+    double *outs[3] = {p.out_aa, p.out_bb, p.out_ab};
+    float centre[3] = {0.0f, 0.0f, 0.0f};
+    // pass 1: mean of each plane (after averaging and background), and its centre value
+    float mean[3] = {0.0f, 0.0f, 0.0f};
+    for (int q = 0; q < 3; ++q) {
+        float acc = 0.0f;
+        for (int k = lane; k < p.hw; k += 32) {
+            float v = sums[q][base + k] / p.n_pairs;
+            if (bgs[q]) v = v - bgs[q][base + k];
+            acc += v;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        mean[q] = p.dc_zero ? acc / (float)p.hw : 0.0f;
+        float c = sums[q][base + p.centre] / p.n_pairs;
+        if (bgs[q]) c = c - bgs[q][base + p.centre];
+        if (p.dc_zero) c = c - mean[q];
+        const float *env = q < 2 ? p.env_auto : p.env_ab;
+        if (env) c = c / env[p.centre];
+        centre[q] = c;
+    }
+    const float nf = sqrtf(fmaxf(centre[0] * centre[1], 1e-12f));
+    if (p.norm && lane == 0) p.norm[warp] = nf;
+    for (int q = 0; q < 3; ++q) {
+        const float *env = q < 2 ? p.env_auto : p.env_ab;
+        for (int k = lane; k < p.hw; k += 32) {
+            float v = sums[q][base + k] / p.n_pairs;
+            if (bgs[q]) v = v - bgs[q][base + k];
+            if (p.dc_zero) v = v - mean[q];
+            if (env) v = v / env[k];
+            outs[q][base + k] = (double)(v / nf);
+        }
+    }
+}
+
+}  // namespace
+
+// sum (+)= the n_frames frames (stride elements apart) of npix pixels, with a
+// Kahan compensation array comp (zero it with sum).
+PIV_EXPORT int pivb_frame_sum_dev(const float *frames, long long stride, int n_frames, long long npix, float *sum,
+                                  float *comp, void *stream)
+{
+    if (n_frames <= 0 || npix <= 0 || stride < npix || !frames || !sum || !comp) return 1;
+    const long long want = (npix + 255) / 256;
+    const unsigned grid = (unsigned)(want < 148 * 16 ? want : 148 * 16);
+    frame_sum_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(frames, stride, n_frames, npix, sum, comp);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// out = sum / n (the mean frame of n accumulated pairs).
+PIV_EXPORT int pivb_frame_mean_dev(const float *sum, long long npix, int n, float *out, void *stream)
+{
+    if (n <= 0 || npix <= 0 || !sum || !out) return 1;
+    const long long want = (npix + 255) / 256;
+    const unsigned grid = (unsigned)(want < 148 * 16 ? want : 148 * 16);
+    frame_mean_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(sum, npix, (float)n, out);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Finalise of one ensemble pass for n_win windows of h x w planes: average the
+// sums over n_pairs, subtract the background planes (nullable), optionally zero
+// each plane's mean, divide by the envelopes (nullable), normalise by
+// sqrt(max(AA_c BB_c, 1e-12)) at the centre (h/2, w/2), and write the planes in
+// FP64 for the k-space fit.  norm (nullable) receives the factors.
+PIV_EXPORT int pivb_ensemble_finalize_dev(const float *sum_ab, const float *sum_aa, const float *sum_bb,
+                                          const float *bg_ab, const float *bg_aa, const float *bg_bb, int n_pairs,
+                                          int n_win, int h, int w, int dc_zero, const float *env_auto,
+                                          const float *env_ab, double *out_ab, double *out_aa, double *out_bb,
+                                          float *norm, void *stream)
+{
+    if (n_pairs <= 0 || n_win <= 0 || h <= 0 || w <= 0) return 1;
+    if (!sum_ab || !sum_aa || !sum_bb || !out_ab || !out_aa || !out_bb) return 1;
+    if ((bg_ab == nullptr) != (bg_aa == nullptr) || (bg_aa == nullptr) != (bg_bb == nullptr)) return 1;
+    FinParams p{sum_ab, sum_aa, sum_bb, bg_ab, bg_aa, bg_bb, env_auto, env_ab ? env_ab : env_auto,
+                (float)n_pairs, n_win, h * w, (h / 2) * w + w / 2, dc_zero ? 1 : 0, out_aa, out_bb, out_ab, norm};
+    const long long threads = (long long)n_win * 32;
+    ensemble_finalize_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}

@@ -171,6 +171,12 @@ def pass_lib() -> ctypes.CDLL:
     L.pivb_remap_dev.restype = ci
     L.pivb_u16_to_f32_dev.argtypes = [vp, vp, cll, vp]
     L.pivb_u16_to_f32_dev.restype = ci
+    L.pivb_frame_sum_dev.argtypes = [vp, cll, ci, cll, vp, vp, vp]
+    L.pivb_frame_sum_dev.restype = ci
+    L.pivb_frame_mean_dev.argtypes = [vp, cll, ci, vp, vp]
+    L.pivb_frame_mean_dev.restype = ci
+    L.pivb_ensemble_finalize_dev.argtypes = [vp, vp, vp, vp, vp, vp, ci, ci, ci, ci, ci, vp, vp, vp, vp, vp, vp, vp]
+    L.pivb_ensemble_finalize_dev.restype = ci
     L._pivb_bound = True
     return L
 

@@ -1,0 +1,186 @@
+"""GPU-resident ensemble PIV pass: accumulate, finalise, k-space fit.
+
+Follows the reference's single-pass ensemble (std mode) for one pass
+(pivtools_cli/piv/piv_backend/cpu_ensemble.py:590-676,
+single_pass_accumulator.py:292-320, 352-506, 508-800,
+kspace_lm_fitting.py:804-961):
+
+  accumulate  per batch of pairs: the AB, AA and BB correlation sums of every
+              window (bulkxcorr2d_accumulate_triple, Kahan-compensated FP32 across
+              batches) and the frame sums for the mean images;
+  finalise    mean images, their correlation as the background term ('correlation'
+              methods), the per-window plane-mean removal ('+dc_zero'), the
+              optional pair-count envelope divide, the normalisation by the auto
+              peaks, FP64 planes;
+  fit         the k-space LM fit of every window (libkspacefit).
+
+All sums, planes and fit outputs stay on the device; every step is a kernel of
+the repo's libraries launched on the caller's stream.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib, geometry
+
+_METHODS = {
+    # method: (per-pair window-mean removal in the correlator, subtract the
+    #          mean-image correlation at finalise, zero the plane means)
+    "correlation": (0, True, False),
+    "correlation+dc_zero": (0, True, True),
+    "window_mean": (1, False, False),
+    "correlation+window_mean": (1, True, False),
+}
+
+
+def pair_envelope(wa, wb, corr_size):
+    """Linear pair-count envelope E(s) = (wa * wb)(s) of two window weights,
+    centre-cropped to corr_size (zero lag at corr_size // 2) and normalised to 1
+    there (single_pass_accumulator.py:52-102): FP64, zero-padded FFT."""
+    wa = np.asarray(wa, np.float64)
+    wb = np.asarray(wb, np.float64)
+    h, w = wa.shape
+    ch, cw = corr_size
+    full = np.fft.fftshift(np.fft.ifft2(np.fft.fft2(wa, s=(2 * h, 2 * w)) *
+                                        np.conj(np.fft.fft2(wb, s=(2 * h, 2 * w)))).real)
+    env = full[h - ch // 2:h - ch // 2 + ch, w - cw // 2:w - cw // 2 + cw]
+    env = env / env[ch // 2, cw // 2]
+    if np.any(env <= 0.0):
+        raise ValueError("pair-count envelope has non-positive entries inside the plane")
+    return env
+
+
+class EnsemblePIV:
+    """One std-mode ensemble pass over frames of one size on one GPU."""
+
+    def __init__(self, image_shape, window=(16, 16), overlap=75, window_type="square",
+                 background="correlation+dc_zero", envelope_divide=False, device=None):
+        import torch
+
+        if background not in _METHODS:
+            raise ValueError(f"background method {background!r} not supported on the GPU path "
+                             f"(supported: {sorted(_METHODS)})")
+        self.torch = torch
+        self.device = torch.device("cuda" if device is None else device)
+        self.H, self.W = image_shape
+        self.win = tuple(window)
+        self.mean_subtract, self.use_bg, self.dc_zero = _METHODS[background]
+        self.grid = geometry.compute_window_centers(image_shape, self.win, overlap)
+        g = self.grid
+        self.n_win = g.n_win_y * g.n_win_x
+        h, w = self.win
+        dev, f32 = self.device, torch.float32
+        wt = geometry.window_weight(self.win, window_type)
+        self.weight = torch.tensor(wt, dtype=f32, device=dev)
+        self.cx = torch.tensor(g.win_ctrs_x, dtype=f32, device=dev)
+        self.cy = torch.tensor(g.win_ctrs_y, dtype=f32, device=dev)
+        self.env = (torch.tensor(pair_envelope(wt, wt, self.win), dtype=f32, device=dev)
+                    if envelope_divide else None)
+        plane = self.n_win * h * w
+        self.sums = torch.zeros((3, plane), dtype=f32, device=dev)       # AB, AA, BB
+        self.comp = torch.zeros((3, plane), dtype=f32, device=dev)
+        self.bg = torch.zeros((3, plane), dtype=f32, device=dev)
+        self.fsum = torch.zeros((2, self.H * self.W), dtype=f32, device=dev)   # frame sums A, B
+        self.fcomp = torch.zeros_like(self.fsum)
+        self.fmean = torch.zeros_like(self.fsum)
+        self.planes = torch.zeros((3, self.n_win, h, w), dtype=torch.float64, device=dev)  # AA, BB, AB
+        self.norm = torch.zeros(self.n_win, dtype=f32, device=dev)
+        self.Lx = _lib.bulkxcorr2d_lib()
+        self.Lp = _lib.pass_lib()
+        self.Lk = _lib.kspacefit_lib()
+        sb = int(self.Lx.pivb_accumulate_scratch_bytes(h, self.n_win))
+        self.scratch = torch.empty(max(sb, 256), dtype=torch.uint8, device=dev)
+        self.n_pairs = 0
+
+    def _stream(self):
+        return ctypes.c_void_p(self.torch.cuda.current_stream(self.device).cuda_stream)
+
+    @staticmethod
+    def _ok(code, what):
+        if code != 0:
+            raise RuntimeError(f"{what} failed with code {code}")
+
+    def reset(self):
+        for t in (self.sums, self.comp, self.fsum, self.fcomp):
+            t.zero_()
+        self.n_pairs = 0
+
+    def _triple(self, A, B, n, mean_subtract, out, comp, s):
+        g = self.grid
+        h, w = self.win
+        wp = self.weight.data_ptr()
+        self._ok(self.Lx.pivb_accumulate_triple_dev(
+            A.data_ptr(), B.data_ptr(), self.H * self.W, None, self.H, self.W, n, self.cx.data_ptr(),
+            self.cy.data_ptr(), g.n_win_y, g.n_win_x, wp, wp, wp, wp, h, w, h, w, mean_subtract, 0,
+            out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(),
+            None if comp is None else comp.data_ptr(), self.scratch.data_ptr(), self.scratch.numel(), s),
+            "accumulate_triple")
+
+    def accumulate(self, A, B):
+        """Add a batch of pairs: A, B (n, H, W) float32 CUDA tensors."""
+        n = int(A.shape[0])
+        s = self._stream()
+        self._triple(A, B, n, self.mean_subtract, self.sums, self.comp, s)
+        npix = self.H * self.W
+        for k, F in enumerate((A, B)):
+            self._ok(self.Lp.pivb_frame_sum_dev(F.data_ptr(), npix, n, npix, self.fsum[k].data_ptr(),
+                                                self.fcomp[k].data_ptr(), s), "frame sum")
+        self.n_pairs += n
+
+    def finalize(self):
+        """Background, DC zero, envelope, normalisation -> FP64 planes (AA, BB, AB)
+        of shape (n_win, h, w) on the device, and the normalisation factors."""
+        if self.n_pairs == 0:
+            raise RuntimeError("finalize before any accumulate")
+        s = self._stream()
+        h, w = self.win
+        bg = None
+        if self.use_bg:
+            npix = self.H * self.W
+            for k in range(2):
+                self._ok(self.Lp.pivb_frame_mean_dev(self.fsum[k].data_ptr(), npix, self.n_pairs,
+                                                     self.fmean[k].data_ptr(), s), "frame mean")
+            self.bg.zero_()
+            MA, MB = self.fmean[0].view(1, self.H, self.W), self.fmean[1].view(1, self.H, self.W)
+            self._triple(MA, MB, 1, self.mean_subtract, self.bg, None, s)
+            bg = self.bg
+        env = None if self.env is None else self.env.data_ptr()
+        self._ok(self.Lp.pivb_ensemble_finalize_dev(
+            self.sums[0].data_ptr(), self.sums[1].data_ptr(), self.sums[2].data_ptr(),
+            None if bg is None else bg[0].data_ptr(), None if bg is None else bg[1].data_ptr(),
+            None if bg is None else bg[2].data_ptr(), self.n_pairs, self.n_win, h, w, int(self.dc_zero), env, env,
+            self.planes[2].data_ptr(), self.planes[0].data_ptr(), self.planes[1].data_ptr(),
+            self.norm.data_ptr(), s), "ensemble finalize")
+        return {"R_AA": self.planes[0], "R_BB": self.planes[1], "R_AB": self.planes[2], "norm": self.norm}
+
+    def fit(self, mask=None, use_kx4=0, use_ky4=0):
+        """k-space LM fit of the finalised planes (flat floor).  Returns device
+        tensors: gauss (n_win, 16) and status (n_win,), plus diagnostics."""
+        torch = self.torch
+        dev = self.device
+        h, w = self.win
+        n = self.n_win
+        m = (torch.zeros(n, dtype=torch.uint8, device=dev) if mask is None
+             else torch.as_tensor(mask, dtype=torch.uint8, device=dev).reshape(n))
+        o = {
+            "gauss": torch.zeros((n, 16), dtype=torch.float64, device=dev),
+            "status": torch.zeros(n, dtype=torch.int32, device=dev),
+            "init": torch.zeros((n, 16), dtype=torch.float64, device=dev),
+        }
+        for k in ("gain", "N0", "b4x", "b4y", "cost_per_pt"):
+            o[k] = torch.zeros(n, dtype=torch.float64, device=dev)
+        o["n_valid"] = torch.zeros(n, dtype=torch.int32, device=dev)
+        o["iters"] = torch.zeros(n, dtype=torch.int32, device=dev)
+        o["conv"] = torch.zeros(n, dtype=torch.uint8, device=dev)
+        sb = int(self.Lk.pivb_kspace_scratch_bytes(n, h, w))
+        scratch = torch.empty(max(sb, 256), dtype=torch.uint8, device=dev)
+        self._ok(self.Lk.pivb_kspace_fit_dev(
+            self.planes[0].data_ptr(), self.planes[1].data_ptr(), self.planes[2].data_ptr(), m.data_ptr(), None,
+            n, h, w, use_kx4, use_ky4, o["gauss"].data_ptr(), o["status"].data_ptr(), o["init"].data_ptr(),
+            o["gain"].data_ptr(), o["N0"].data_ptr(), o["b4x"].data_ptr(), o["b4y"].data_ptr(),
+            o["cost_per_pt"].data_ptr(), o["n_valid"].data_ptr(), o["iters"].data_ptr(), o["conv"].data_ptr(),
+            scratch.data_ptr(), scratch.numel(), self._stream()), "kspace fit")
+        return o

@@ -86,6 +86,31 @@ def channel_flow(rng, shape, peak=12.0, re_tau=1000.0, rms_frac=0.08, corr_len=2
     return u, v
 
 
+def ensemble_row_statistics(yn, peak=4.0, uu_max=0.6, vv_max=0.3, rho=-0.4):
+    """Prescribed per-row statistics of the ensemble flow at normalised height yn:
+    mean streamwise displacement (parabolic profile, `peak` px at the centre),
+    variances <u'u'>, <v'v'> (largest near the walls) and covariance <u'v'> with
+    correlation coefficient rho.  Returns (mean_u, (uu, vv, uv))."""
+    yn = np.asarray(yn, np.float64)
+    mean_u = peak * 4.0 * yn * (1.0 - yn)
+    shape_ = 0.35 + 0.65 * (1.0 - 4.0 * yn * (1.0 - yn))
+    uu = uu_max * shape_
+    vv = vv_max * shape_
+    uv = rho * np.sqrt(uu * vv)
+    return mean_u, (uu, vv, uv)
+
+
+def ensemble_row_displacements(rng, yn, **kw):
+    """Per-particle (u, v) drawn from the row's joint Gaussian."""
+    mean_u, (uu, vv, uv) = ensemble_row_statistics(yn, **kw)
+    z1, z2 = rng.standard_normal((2, len(yn)))
+    su = np.sqrt(uu)
+    rho_ = uv / np.maximum(su * np.sqrt(vv), 1e-30)
+    du = mean_u + su * z1
+    dv = np.sqrt(vv) * (rho_ * z1 + np.sqrt(1.0 - rho_ ** 2) * z2)
+    return du, dv
+
+
 def particle_pair(shape, seed, density=0.05, sigma=0.6, i_range=(1000.0, 4000.0), background=100.0,
                   flow="uniform_grf", device=None, flow_kwargs=None):
     """One image pair (A, B) as float32 arrays (numpy, or torch tensors on `device`)
@@ -105,12 +130,20 @@ def particle_pair(shape, seed, density=0.05, sigma=0.6, i_range=(1000.0, 4000.0)
     elif flow == "uniform":
         u = np.full(shape, kw.get("u", 0.0))
         v = np.full(shape, kw.get("v", 0.0))
+    elif flow == "ensemble_rows":
+        u = v = None
     else:
         raise ValueError(flow)
     xi = np.clip(np.round(xs).astype(np.int64), 0, w - 1)
     yi = np.clip(np.round(ys).astype(np.int64), 0, h - 1)
-    xb = xs + u[yi, xi]
-    yb = ys + v[yi, xi]
+    if flow == "ensemble_rows":
+        # every particle draws its own displacement from the row's joint Gaussian
+        du, dv = ensemble_row_displacements(rng, ys / h, **kw)
+        xb, yb = xs + du, ys + dv
+        u, v = ensemble_row_statistics(np.linspace(0.0, 1.0, h), **kw)
+    else:
+        xb = xs + u[yi, xi]
+        yb = ys + v[yi, xi]
     seed_a, seed_b = rng.integers(0, 2**62, 2)
     if device is None:
         ia = _render_np(shape, xs, ys, amp, sigma)

@@ -7,6 +7,7 @@ Python package).  The fixtures are committed; tests never need the reference.
 
     python tests/golden/make_golden.py            # peakfit_ref.npz, warp_ref.npz
     python tests/golden/make_golden.py kspace     # kspace_ref.npz
+    python tests/golden/make_golden.py ensemble   # ensemble_ref.npz
 """
 
 from __future__ import annotations
@@ -232,6 +233,43 @@ def make_kspace():
     print("kspace_ref.npz written")
 
 
+def _reference_functions(path, names):
+    """Compile the named module-level functions of a reference source file on
+    their own (they need only NumPy; the module's other imports are not
+    available here)."""
+    import ast
+
+    tree = ast.parse(open(path).read())
+    body = [n for n in tree.body if isinstance(n, ast.FunctionDef) and n.name in names]
+    ns = {"np": np}
+    exec(compile(ast.Module(body=body, type_ignores=[]), path, "exec"), ns)
+    return [ns[n] for n in names]
+
+
+def make_ensemble():
+    """Fixtures for the ensemble finalise steps, from the reference's own
+    functions (pivtools_cli/piv/piv_backend/single_pass_accumulator.py:52-125):
+    the linear pair-count envelope and the per-window plane-mean removal."""
+    sys.path.insert(0, os.path.join(ROOT, "python-pivtools_b200"))
+    from pivtools_b200 import geometry
+
+    env_fn, dc_fn = _reference_functions(
+        os.path.join(REF_ROOT, "pivtools_cli/piv/piv_backend/single_pass_accumulator.py"),
+        ["_linear_pair_envelope", "_zero_plane_means"])
+    out = {}
+    for wtype in ("square", "gaussian", "blackman"):
+        for n in (16, 32):
+            w = geometry.window_weight((n, n), wtype).astype(np.float64)
+            out[f"w_{wtype}_{n}"] = w
+            out[f"env_{wtype}_{n}"] = env_fn(w, w, (n, n))
+    rng = np.random.default_rng(11)
+    planes = rng.standard_normal(7 * 16 * 16).astype(np.float32) + 3.0
+    out["dc_in"] = planes
+    out["dc_out"] = dc_fn(planes.copy(), 7, (16, 16))
+    np.savez_compressed(os.path.join(HERE, "ensemble_ref.npz"), **out)
+    print("ensemble_ref.npz written")
+
+
 if __name__ == "__main__":
     what = sys.argv[1:] or ["peakfit", "warp"]
     if "peakfit" in what:
@@ -240,3 +278,5 @@ if __name__ == "__main__":
         make_warp()
     if "kspace" in what:
         make_kspace()
+    if "ensemble" in what:
+        make_ensemble()

@@ -1,0 +1,70 @@
+"""The GPU-resident ensemble pass (pivtools_b200.ensemble.EnsemblePIV):
+accumulate in batches, finalise (background of the mean images, plane-mean
+removal, envelope divide, normalisation) and k-space fit, against the oracle's
+restatement of the same steps (oracle accumulate_triple, ensemble_finalize,
+kspace_fit) on the same seeded pairs."""
+
+import numpy as np
+import pytest
+
+from pivtools_b200 import ensemble, geometry, synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _pairs(n, shape, seed):
+    out = [synthetic.particle_pair(shape, seed=seed + k, flow="uniform_grf")[:2] for k in range(n)]
+    return np.stack([p[0] for p in out]).astype(np.float32), np.stack([p[1] for p in out]).astype(np.float32)
+
+
+@pytest.mark.parametrize("method,env", [("correlation+dc_zero", False), ("correlation", True), ("window_mean", False)])
+def test_ensemble_pass_matches_oracle(oracle, cuda, method, env):
+    import torch
+
+    shape, win = (128, 160), (16, 16)
+    A, B = _pairs(10, shape, 700)
+    ep = ensemble.EnsemblePIV(shape, win, 75, "square", background=method, envelope_divide=env, device=cuda)
+    for sl in (slice(0, 4), slice(4, 10)):                      # two batches
+        ep.accumulate(torch.tensor(A[sl], device=cuda), torch.tensor(B[sl], device=cuda))
+    fin = ep.finalize()
+    fit = ep.fit()
+    torch.cuda.synchronize()
+
+    g = ep.grid
+    w = geometry.window_weight(win, "square")
+    mask = np.zeros((g.n_win_y, g.n_win_x), np.float32)
+    ms, use_bg, dc = ensemble._METHODS[method]
+    s_ab, s_aa, s_bb = oracle.accumulate_triple(A, B, mask, g.win_ctrs_x, g.win_ctrs_y, win, w, w, w, w,
+                                                mean_subtract=ms)
+    n_win = g.n_win_y * g.n_win_x
+    bg = None
+    if use_bg:
+        mA = (A.astype(np.float64).sum(0) / 10).astype(np.float32)
+        mB = (B.astype(np.float64).sum(0) / 10).astype(np.float32)
+        b_ab, b_aa, b_bb = oracle.accumulate_triple(mA[None], mB[None], mask, g.win_ctrs_x, g.win_ctrs_y, win,
+                                                    w, w, w, w, mean_subtract=ms)
+        bg = [x.reshape(n_win, *win) for x in (b_aa, b_bb, b_ab)]
+    e = oracle.pair_envelope(w, w, win) if env else None
+    R_AA, R_BB, R_AB, norm = oracle.ensemble_finalize(s_ab.reshape(n_win, *win), s_aa.reshape(n_win, *win),
+                                                      s_bb.reshape(n_win, *win), 10, bg=bg, dc_zero=dc,
+                                                      env_auto=e)
+    for got, ref in ((fin["R_AA"], R_AA), (fin["R_BB"], R_BB), (fin["R_AB"], R_AB)):
+        got = got.cpu().numpy()
+        scale = np.abs(ref).reshape(n_win, -1).max(axis=1)[:, None, None]
+        assert np.all(np.abs(got - ref) <= 2e-4 * scale + 1e-7), float(np.max(np.abs(got - ref) / scale))
+    np.testing.assert_allclose(fin["norm"].cpu().numpy(), norm, rtol=2e-4)
+
+    ref_fit = oracle.kspace_fit(R_AA, R_BB, R_AB, np.zeros(n_win, np.uint8), win)
+    st_g, st_o = fit["status"].cpu().numpy(), ref_fit["status"]
+    assert (st_g == st_o).mean() >= 0.95
+    both = (st_g == 0) & (st_o == 0)
+    assert both.sum() >= 0.5 * n_win
+    gg, go = fit["gauss"].cpu().numpy()[both], ref_fit["gauss_flat"][both]
+    # fitted displacement (cols 14-15) and Reynolds stresses (cols 9-11)
+    assert np.max(np.abs(gg[:, 14:16] - go[:, 14:16])) < 2e-3
+    np.testing.assert_allclose(gg[:, 9:12], go[:, 9:12], rtol=5e-3, atol=1e-4)
+
+
+def test_ensemble_rejects_two_sweep_methods(cuda):
+    with pytest.raises(ValueError):
+        ensemble.EnsemblePIV((64, 64), (16, 16), 75, "square", background="image", device=cuda)

@@ -117,3 +117,15 @@ def test_oracle_matches_live_reference_fitter(oracle):
         s2 = np.zeros(3, np.float32)
         R.lsqpeaklocate_lm(p, np.array([33, 33], np.int32), l2, 1, t, s2, None)
         assert _eq(loc, l2) and _eq(sd, s2)
+
+
+def test_ensemble_finalise_restatement_matches_reference_fixture(oracle):
+    """Pair-count envelope and plane-mean removal against the reference's own
+    functions (fixture from tests/golden/make_golden.py ensemble)."""
+    g = np.load(os.path.join(GOLD, "ensemble_ref.npz"))
+    for wtype in ("square", "gaussian", "blackman"):
+        for n in (16, 32):
+            env = oracle.pair_envelope(g[f"w_{wtype}_{n}"], g[f"w_{wtype}_{n}"], (n, n))
+            np.testing.assert_allclose(env, g[f"env_{wtype}_{n}"], rtol=1e-12, atol=1e-14)
+    got = oracle.zero_plane_means(g["dc_in"].reshape(7, 16, 16)).ravel()
+    np.testing.assert_allclose(got, g["dc_out"], rtol=0, atol=2e-6)
