@@ -46,8 +46,11 @@ def _args():
     ap.add_argument("--pairs", type=int, default=64)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--cpu-pairs", type=int, default=1)
-    ap.add_argument("--workload", default="multipass", choices=["multipass", "ensemble"],
-                    help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass")
+    ap.add_argument("--workload", default="multipass", choices=["multipass", "ensemble", "serve"],
+                    help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
+                         "serve: Poisson request stream with continuous batching")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: offered pairs/s")
+    ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
     return ap.parse_args()
 
 
@@ -472,12 +475,110 @@ def run_ensemble(args):
         torch.distributed.destroy_process_group()
 
 
+def run_serve(args):
+    """Serving mix: Poisson arrivals at --rate pairs/s for --duration s; each
+    request is one uint16 pair of a size drawn from {512^2, 1024^2, 2048^2,
+    2048x4096} with a schedule drawn from {32; 64-32; 128-64-32-16 px} at 50%
+    overlap, channel-flow particle images (a small pool per size, cycled), frames
+    in pinned host memory, a 120 GB device budget.  Reports vectors/s over the run
+    and p50/p99 request latency (arrival to result in host memory)."""
+    import numpy as np
+    import torch
+
+    from pivtools_b200 import serving, synthetic
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    sizes = [(512, 512), (1024, 1024), (2048, 2048), (2048, 4096)]
+    scheds = [(32,), (64, 32), (128, 64, 32, 16)]
+    pool = {}
+    for si, shp in enumerate(sizes):
+        pool[shp] = []
+        for k in range(2):
+            A, B, _ = synthetic.particle_pair(shp, seed=7000 + 10 * si + k + 1000 * rank, flow="channel",
+                                              device=dev, flow_kwargs={"peak": 12.0})
+            pool[shp].append((A.to(torch.int32).to(torch.uint16).cpu().pin_memory(),
+                              B.to(torch.int32).to(torch.uint16).cpu().pin_memory()))
+    srv = serving.PivServer(device=dev, max_batch=4, hbm_budget_bytes=120e9)
+    for shp in sizes:                           # build every engine, warm it, pin output buffers
+        for sch in scheds:
+            srv.reserve_outputs(shp, sch, 64)
+            for _ in range(2):
+                srv.submit(*pool[shp][0], sch)
+            for r in srv.drain():
+                srv.release(r)
+    torch.cuda.synchronize()
+    arr = serving.poisson_arrivals(args.rate, args.duration, seed=11 + rank)
+    rng = np.random.default_rng(12 + rank)
+    picks = [(sizes[rng.integers(4)], scheds[rng.integers(3)], int(rng.integers(2))) for _ in arr]
+    reqs = []
+    vec = 0
+    d2h = []
+    if ws > 1:
+        torch.distributed.barrier()
+    import gc
+
+    gc.disable()                                # no collector pauses inside the served window
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(arr) or not srv.idle():
+            now = time.perf_counter() - t0
+            while i < len(arr) and arr[i] <= now:
+                shp, sch, k = picks[i]
+                reqs.append(srv.submit(*pool[shp][k], sch, arrival=t0 + arr[i]))
+                i += 1
+            for r in srv.poll():
+                vec += int(r.ux.numel())
+                d2h.append(r.ux.numel() * 8)
+                srv.release(r)
+            time.sleep(5e-5)
+        t1 = time.perf_counter()
+    gc.enable()
+    lat = np.array([r.done - r.arrival for r in reqs]) * 1e3
+    wall = t1 - t0
+    by_sched = {}
+    for (shp, sch, _), l in zip(picks, lat):
+        by_sched.setdefault("-".join(map(str, sch)), []).append(l)
+    if ws > 1:
+        t = torch.tensor([wall], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        wall = float(t.item())
+    if rank == 0:
+        line = {
+            "metric": "served vectors/s with p50/p99 pair latency on 1 B200", "value": vec * ws / wall,
+            "unit": "vectors/s", "n_gpus": ws, "steps": len(reqs), "warmup": 2 * len(sizes) * len(scheds),
+            "ms_per_step": wall * 1e3 / max(len(reqs), 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"Poisson {args.rate:g} pairs/s for {args.duration:g} s; sizes 512^2, 1024^2, "
+                                   "2048^2, 2048x4096 uint16; schedules 32 / 64-32 / 128-64-32-16 px at 50%",
+                       "max_batch": srv.max_batch, "hbm_budget_gb": 120, "engines": len(srv.engines),
+                       "engine_bytes_gb": srv.used_bytes / 1e9},
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(lat.max()),
+                           "by_schedule": {k: {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),
+                                               "n": len(v)} for k, v in sorted(by_sched.items())}},
+            "offered_pairs_per_s": args.rate, "served_pairs_per_s": len(reqs) / wall,
+            "e2e": {"value": vec * ws / wall, "unit": "vectors/s",
+                    "h2d_bytes_per_step": float(np.mean([2 * p[0][0] * p[0][1] * 2 for p in picks])),
+                    "d2h_bytes_per_step": float(np.mean(d2h))},
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
 def main():
     args = _args()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "ensemble":
         run_ensemble(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_b200(args)
 

@@ -152,12 +152,16 @@ class MultipassPIV:
                 n += 2                                    # remap, warp
         return n
 
-    def run(self, A, B):
+    def run(self, A, B, n=None):
         """A, B: (N, H, W) float32 CUDA tensors.  Returns (ux, uy) of the final pass
-        (device tensors, views into internal buffers)."""
+        (device tensors, views into internal buffers).  n (<= N) processes only the
+        first n pairs (a partly filled batch); every pair's result is independent of
+        the others in the batch."""
         cfg = self.cfg
         s = self._stream()
-        N, H, W = self.N, self.H, self.W
+        N, H, W = (self.N if n is None else int(n)), self.H, self.W
+        if not 1 <= N <= self.N:
+            raise ValueError(f"n = {N} outside 1..{self.N}")
         scr = self.scratch
         for k, p in enumerate(self.passes):
             if k == 0:
