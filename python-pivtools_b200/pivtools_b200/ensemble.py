@@ -135,26 +135,58 @@ class EnsemblePIV:
         of shape (n_win, h, w) on the device, and the normalisation factors."""
         if self.n_pairs == 0:
             raise RuntimeError("finalize before any accumulate")
+        self._finalize(self.sums, self.n_pairs, self.fsum, 0, self.n_win, self.planes, self.norm)
+        return {"R_AA": self.planes[0], "R_BB": self.planes[1], "R_AB": self.planes[2], "norm": self.norm}
+
+    def finalize_distributed(self, group=None):
+        """Finalise across the ranks of `group` (one GPU each, pairs sharded):
+        one exchange combines the sums (ensemble_dist.exchange_sums), then this
+        rank finalises its block of windows.  Returns the block's planes and
+        (start, stop); `fit` then fits the block and `gather_fit` joins them."""
+        from . import ensemble_dist as ed
+
+        h, w = self.win
+        block, fsum, n_tot, (a, b) = ed.exchange_sums(self.sums, self.comp, self.fsum, self.fcomp, self.n_pairs,
+                                                      self.n_win, h * w, group)
+        torch = self.torch
+        nb = b - a
+        self.block = (a, b)
+        self.planes = torch.zeros((3, nb, h, w), dtype=torch.float64, device=self.device)
+        self.norm = torch.zeros(max(nb, 1), dtype=torch.float32, device=self.device)
+        if nb > 0:
+            self._finalize(block.reshape(3, -1), n_tot, fsum, a, b, self.planes, self.norm)
+        return {"R_AA": self.planes[0], "R_BB": self.planes[1], "R_AB": self.planes[2], "norm": self.norm,
+                "windows": (a, b), "n_pairs": n_tot}
+
+    def _finalize(self, sums, n_pairs, fsum, w0, w1, planes, norm):
+        """Finalise windows [w0, w1): sums (3, (w1 - w0) * h * w) for those windows,
+        fsum (2, H * W) frame sums over n_pairs pairs."""
         s = self._stream()
         h, w = self.win
+        hw = h * w
         bg = None
         if self.use_bg:
             npix = self.H * self.W
             for k in range(2):
-                self._ok(self.Lp.pivb_frame_mean_dev(self.fsum[k].data_ptr(), npix, self.n_pairs,
-                                                     self.fmean[k].data_ptr(), s), "frame mean")
+                self._ok(self.Lp.pivb_frame_mean_dev(fsum[k].data_ptr(), npix, n_pairs, self.fmean[k].data_ptr(), s),
+                         "frame mean")
             self.bg.zero_()
             MA, MB = self.fmean[0].view(1, self.H, self.W), self.fmean[1].view(1, self.H, self.W)
             self._triple(MA, MB, 1, self.mean_subtract, self.bg, None, s)
-            bg = self.bg
+            bg = self.bg[:, w0 * hw:w1 * hw]
         env = None if self.env is None else self.env.data_ptr()
         self._ok(self.Lp.pivb_ensemble_finalize_dev(
-            self.sums[0].data_ptr(), self.sums[1].data_ptr(), self.sums[2].data_ptr(),
+            sums[0].data_ptr(), sums[1].data_ptr(), sums[2].data_ptr(),
             None if bg is None else bg[0].data_ptr(), None if bg is None else bg[1].data_ptr(),
-            None if bg is None else bg[2].data_ptr(), self.n_pairs, self.n_win, h, w, int(self.dc_zero), env, env,
-            self.planes[2].data_ptr(), self.planes[0].data_ptr(), self.planes[1].data_ptr(),
-            self.norm.data_ptr(), s), "ensemble finalize")
-        return {"R_AA": self.planes[0], "R_BB": self.planes[1], "R_AB": self.planes[2], "norm": self.norm}
+            None if bg is None else bg[2].data_ptr(), n_pairs, w1 - w0, h, w, int(self.dc_zero), env, env,
+            planes[2].data_ptr(), planes[0].data_ptr(), planes[1].data_ptr(), norm.data_ptr(), s),
+            "ensemble finalize")
+
+    def gather_fit(self, fit, group=None):
+        """All-gather the per-window fit outputs of every rank's block."""
+        from . import ensemble_dist as ed
+
+        return {k: ed.gather_rows(v, self.n_win, group) for k, v in fit.items()}
 
     def fit(self, mask=None, use_kx4=0, use_ky4=0):
         """k-space LM fit of the finalised planes (flat floor).  Returns device
@@ -162,7 +194,7 @@ class EnsemblePIV:
         torch = self.torch
         dev = self.device
         h, w = self.win
-        n = self.n_win
+        n = int(self.planes.shape[1])
         m = (torch.zeros(n, dtype=torch.uint8, device=dev) if mask is None
              else torch.as_tensor(mask, dtype=torch.uint8, device=dev).reshape(n))
         o = {

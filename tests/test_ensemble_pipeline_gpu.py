@@ -68,3 +68,43 @@ def test_ensemble_pass_matches_oracle(oracle, cuda, method, env):
 def test_ensemble_rejects_two_sweep_methods(cuda):
     with pytest.raises(ValueError):
         ensemble.EnsemblePIV((64, 64), (16, 16), 75, "square", background="image", device=cuda)
+
+
+def test_distributed_finalise_single_rank_equals_local(cuda):
+    """The multi-GPU finalise path on a one-rank group (GPU tensors through gloo)
+    gives the local finalise's planes and fits."""
+    import datetime
+    import os
+    import socket
+
+    import torch
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.distributed.init_process_group("gloo", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        shape, win = (128, 128), (16, 16)
+        A, B = _pairs(6, shape, 760)
+        ep = ensemble.EnsemblePIV(shape, win, 75, "square", device=cuda)
+        ep.accumulate(torch.tensor(A, device=cuda), torch.tensor(B, device=cuda))
+        loc = {k: v.clone() for k, v in ep.finalize().items()}
+        fit_loc = ep.fit()
+        dist = ep.finalize_distributed()
+        assert dist["windows"] == (0, ep.n_win) and dist["n_pairs"] == 6
+        for k in ("R_AA", "R_BB", "R_AB"):
+            ref = loc[k].cpu().numpy()
+            scale = np.abs(ref).reshape(ref.shape[0], -1).max(axis=1)[:, None, None]
+            assert np.all(np.abs(dist[k].cpu().numpy() - ref) <= 1e-5 * scale)
+        fit = ep.gather_fit(ep.fit())
+        torch.cuda.synchronize()
+        st_l, st_d = fit_loc["status"].cpu().numpy(), fit["status"].cpu().numpy()
+        assert (st_l == st_d).mean() > 0.95
+        ok = (st_l == 0) & (st_d == 0)
+        np.testing.assert_allclose(fit["gauss"].cpu().numpy()[ok][:, 14:16],
+                                   fit_loc["gauss"].cpu().numpy()[ok][:, 14:16], atol=1e-3)
+    finally:
+        torch.distributed.destroy_process_group()
