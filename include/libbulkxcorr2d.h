@@ -96,6 +96,12 @@ int codelet_lanes(void);
 /* Scratch bytes pivb_xcorr_dev needs (deferred LM fit records). */
 size_t pivb_xcorr_scratch_bytes(long long n_windows_total, int n_peaks, int peak_finder);
 
+/* Bytes of per-window records (128 B each) with which pivb_xcorr_dev defers every
+ * single-peak fit, the 3-point Gaussian included, to a thread-per-window kernel.
+ * Optional for peak finder 3 (passing less scratch keeps the fit in the
+ * correlation kernel, with identical results); no counterpart in the reference. */
+size_t pivb_xcorr_record_bytes(long long n_windows_total);
+
 /* numel / (wB (*) wB) into d_out [h*w] (the fit patch's loss-of-correlation weight). */
 int pivb_correl_weight_dev(const float *d_wB, int h, int w, float *d_out, void *stream);
 

@@ -155,6 +155,13 @@ PIV_EXPORT size_t pivb_xcorr_scratch_bytes(long long n_windows_total, int n_peak
     return 0;
 }
 
+// Bytes of the per-window records with which pivb_xcorr_dev defers every
+// single-peak fit (3-point included) to a thread-per-window kernel.
+PIV_EXPORT size_t pivb_xcorr_record_bytes(long long n_windows_total)
+{
+    return pad256((size_t)n_windows_total * sizeof(LmRecord));
+}
+
 // Loss-of-correlation weight numel / (wB (*) wB) on the device.
 PIV_EXPORT int pivb_correl_weight_dev(const float *d_wB, int h, int w, float *d_out, void *stream)
 {
@@ -186,6 +193,11 @@ PIV_EXPORT int pivb_xcorr_dev(const float *d_A, const float *d_B, long long img_
     const bool lm = !ensemble && n_peaks == 1 && peak_finder >= 4 && peak_finder <= 6;
     if (lm && (d_scratch == nullptr || scratch_bytes < pivb_xcorr_scratch_bytes(total, n_peaks, peak_finder)))
         return PIV_ERROR_NOMEM;
+    // 3-point fits also move to the per-window record kernel when the caller's
+    // scratch holds the records (pivb_xcorr_record_bytes): the correlation kernel's
+    // group leader then only extracts the patch; results are the same either way
+    const bool defer = lm || (!ensemble && n_peaks == 1 && peak_finder == 3 && d_scratch != nullptr &&
+                              scratch_bytes >= pivb_xcorr_record_bytes(total));
     cudaStream_t s = (cudaStream_t)stream;
     XcorrParams p{};
     p.A = d_A; p.B = d_B; p.img_stride = img_stride; p.mask = d_mask;
@@ -195,14 +207,14 @@ PIV_EXPORT int pivb_xcorr_dev(const float *d_A, const float *d_B, long long img_
     p.ensemble = ensemble; p.n_peaks = n_peaks; p.finder = peak_finder;
     p.pk_x = d_pk_x; p.pk_y = d_pk_y; p.pk_h = d_pk_h; p.sx = d_sx; p.sy = d_sy; p.sxy = d_sxy;
     p.pk_ratio = d_pk_ratio; p.planes = d_planes;
-    p.lm = lm ? static_cast<LmRecord *>(d_scratch) : nullptr;
+    p.lm = defer ? static_cast<LmRecord *>(d_scratch) : nullptr;
     p.total = total;
     const bool timing = g_timing != 0;
     if (timing) cudaEventRecord(g_ws.ev[0], s);
     int e = (n_peaks > 1 && !ensemble) ? launch_xcorr<true>(win_h, p, s) : launch_xcorr<false>(win_h, p, s);
     if (e) return e;
     if (timing) cudaEventRecord(g_ws.ev[1], s);
-    if (lm) {
+    if (defer) {
         const unsigned blocks = (unsigned)((total + 127) / 128);
         if (peakfit_impl) lm_records_kernel<1><<<blocks, 128, 0, s>>>(p, win_h);
         else lm_records_kernel<0><<<blocks, 128, 0, s>>>(p, win_h);

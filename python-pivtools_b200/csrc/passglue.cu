@@ -152,7 +152,33 @@ __global__ void median_kernel(ValParams p, const float *gx, const float *gy)
 // Weights 1/dx^2 (x neighbours) and 1/dy^2 (y neighbours); neighbours outside
 // the grid or masked drop out (zero flux).  Cells start from the mean of the
 // pair's valid vectors; iteration stops at max_iter or when the largest update
-// is below tol (px).
+// is below tol (px).  The invalid cells are listed once in shared memory (any
+// order: a Jacobi sweep's updates are independent) so that a sweep touches only
+// them; grids with more invalid cells than the list holds sweep the whole grid.
+constexpr int kInfillList = 6144;
+
+__device__ __forceinline__ void infill_cell(int w, int ny, int nx, float wy, float wx, const float *mask,
+                                            const float *sx, const float *sy, float *dx, float *dy, float &local)
+{
+    const int r = w / nx, c = w % nx;
+    float su = 0.0f, sv = 0.0f, sw = 0.0f;
+    const int nr[4] = {r - 1, r + 1, r, r};
+    const int nc[4] = {c, c, c - 1, c + 1};
+    const float ww[4] = {wy, wy, wx, wx};
+    for (int k = 0; k < 4; ++k) {
+        if (nr[k] < 0 || nr[k] >= ny || nc[k] < 0 || nc[k] >= nx) continue;
+        const int q = nr[k] * nx + nc[k];
+        if (mask && mask[q] != 0.0f) continue;
+        su += ww[k] * sx[q];
+        sv += ww[k] * sy[q];
+        sw += ww[k];
+    }
+    const float nu = sw > 0.0f ? su / sw : sx[w], nv = sw > 0.0f ? sv / sw : sy[w];
+    local = fmaxf(local, fmaxf(fabsf(nu - sx[w]), fabsf(nv - sy[w])));
+    dx[w] = nu;
+    dy[w] = nv;
+}
+
 __global__ void __launch_bounds__(512) infill_kernel(float *ux, float *uy, const unsigned char *invalid,
                                                      const float *mask, int ny, int nx, float wy, float wx,
                                                      int max_iter, float tol, float *work)
@@ -163,13 +189,19 @@ __global__ void __launch_bounds__(512) infill_kernel(float *ux, float *uy, const
     const unsigned char *bad = invalid + (long long)n * plane;
     float *X2 = work + (long long)n * 2 * plane, *Y2 = X2 + plane;
     __shared__ float s_max;
-    __shared__ int s_any;
-    if (threadIdx.x == 0) s_any = 0;
+    __shared__ int s_cnt;
+    __shared__ int s_list[kInfillList];
+    if (threadIdx.x == 0) s_cnt = 0;
     __syncthreads();
     for (int w = threadIdx.x; w < plane; w += blockDim.x)
-        if (bad[w]) s_any = 1;
+        if (bad[w]) {
+            const int k = atomicAdd(&s_cnt, 1);
+            if (k < kInfillList) s_list[k] = w;
+        }
     __syncthreads();
-    if (!s_any) return;
+    const int n_bad = s_cnt;
+    if (n_bad == 0) return;
+    const bool listed = n_bad <= kInfillList;
     // initial guess: mean of the valid vectors (the iteration converges to the
     // unique harmonic solution from any start; a good start shortens it)
     // deterministic block reduction (fixed order), so repeated runs agree bit for bit
@@ -209,27 +241,15 @@ __global__ void __launch_bounds__(512) infill_kernel(float *ux, float *uy, const
         if (threadIdx.x == 0) s_max = 0.0f;
         __syncthreads();
         float local = 0.0f;
+        // valid cells are equal in both buffers and never change
         const float *sx = (it & 1) ? X2 : X, *sy = (it & 1) ? Y2 : Y;
         float *dx = (it & 1) ? X : X2, *dy = (it & 1) ? Y : Y2;
-        for (int w = threadIdx.x; w < plane; w += blockDim.x) {
-            if (!bad[w]) { dx[w] = sx[w]; dy[w] = sy[w]; continue; }
-            const int r = w / nx, c = w % nx;
-            float su = 0.0f, sv = 0.0f, sw = 0.0f;
-            const int nr[4] = {r - 1, r + 1, r, r};
-            const int nc[4] = {c, c, c - 1, c + 1};
-            const float ww[4] = {wy, wy, wx, wx};
-            for (int k = 0; k < 4; ++k) {
-                if (nr[k] < 0 || nr[k] >= ny || nc[k] < 0 || nc[k] >= nx) continue;
-                const int q = nr[k] * nx + nc[k];
-                if (mask && mask[q] != 0.0f) continue;
-                su += ww[k] * sx[q];
-                sv += ww[k] * sy[q];
-                sw += ww[k];
-            }
-            const float nu = sw > 0.0f ? su / sw : sx[w], nv = sw > 0.0f ? sv / sw : sy[w];
-            local = fmaxf(local, fmaxf(fabsf(nu - sx[w]), fabsf(nv - sy[w])));
-            dx[w] = nu;
-            dy[w] = nv;
+        if (listed) {
+            for (int i = threadIdx.x; i < n_bad; i += blockDim.x)
+                infill_cell(s_list[i], ny, nx, wy, wx, mask, sx, sy, dx, dy, local);
+        } else {
+            for (int w = threadIdx.x; w < plane; w += blockDim.x)
+                if (bad[w]) infill_cell(w, ny, nx, wy, wx, mask, sx, sy, dx, dy, local);
         }
         atomicMax(reinterpret_cast<int *>(&s_max), __float_as_int(local));   // local >= 0
         __syncthreads();
@@ -237,7 +257,15 @@ __global__ void __launch_bounds__(512) infill_kernel(float *ux, float *uy, const
         __syncthreads();
         if (done || it == max_iter - 1) {
             if (!(it & 1)) {   // result is in X2/Y2
-                for (int w = threadIdx.x; w < plane; w += blockDim.x) { X[w] = X2[w]; Y[w] = Y2[w]; }
+                if (listed) {
+                    for (int i = threadIdx.x; i < n_bad; i += blockDim.x) {
+                        const int w = s_list[i];
+                        X[w] = X2[w];
+                        Y[w] = Y2[w];
+                    }
+                } else {
+                    for (int w = threadIdx.x; w < plane; w += blockDim.x) { X[w] = X2[w]; Y[w] = Y2[w]; }
+                }
             }
             break;
         }

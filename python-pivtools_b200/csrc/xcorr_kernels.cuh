@@ -104,8 +104,8 @@ __device__ __forceinline__ void finish_window(const XcorrParams &prm, float *pl,
                     const int r = bi + aa - 2, c = bj + bb - 2;
                     sub[aa * PKW + bb] = fmul(pl[r * ld + c], __ldg(prm.cw + r * N + c));
                 }
-            if (k == 0 && prm.finder >= 4 && prm.finder <= 6 && !MULTI) {
-                // deferred LM (single peak)
+            if (k == 0 && rec && !MULTI) {
+                // deferred fit (single peak): the patch goes to the window's record
 #pragma unroll
                 for (int q = 0; q < PKN; ++q) rec->sub[q] = sub[q];
                 rec->best = best;
@@ -249,7 +249,7 @@ xcorr_kernel(XcorrParams prm)
     }
 }
 
-// Deferred single-peak LM fits: one thread per window record.
+// Deferred single-peak fits (3-point or LM): one thread per window record.
 template <int MODE>
 __global__ void __launch_bounds__(128) lm_records_kernel(XcorrParams prm, int N)
 {
@@ -266,7 +266,14 @@ __global__ void __launch_bounds__(128) lm_records_kernel(XcorrParams prm, int N)
     }
     sub[24] = rec.sub[24];
     float off[2], sig[3];
-    const bool ok = lm_fit_any<MODE>(prm.finder, sub, off, sig, nullptr);
+    bool ok = true;
+    if (prm.finder == 3) {
+        float A0, s0, s1;
+        three_point(sub, PKW, PKW, PKW, off, &A0, &s0, &s1);
+        sig[0] = s0; sig[1] = s1; sig[2] = 0.0f;
+    } else {
+        ok = lm_fit_any<MODE>(prm.finder, sub, off, sig, nullptr);
+    }
     if (!ok) write_sentinel(prm, idx, rec.enorm);
     else write_peak(prm, idx, N, rec.ij >> 16, rec.ij & 0xffff, off, sig, rec.best, rec.enorm);
 }

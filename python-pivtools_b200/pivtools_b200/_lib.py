@@ -80,6 +80,8 @@ def bulkxcorr2d_lib() -> ctypes.CDLL:
     L.pivb_xcorr_scratch_bytes.restype = csz
     L.pivb_correl_weight_dev.argtypes = [vp, ci, ci, vp, vp]
     L.pivb_correl_weight_dev.restype = ci
+    L.pivb_xcorr_record_bytes.argtypes = [cll]
+    L.pivb_xcorr_record_bytes.restype = csz
     L.pivb_xcorr_dev.argtypes = [vp, vp, cll, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, vp, ci, ci, ci, ci,
                                  ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, vp, csz, vp]
     L.pivb_xcorr_dev.restype = ci

@@ -110,7 +110,10 @@ class MultipassPIV:
                                         self.geo[k + 1].ksize_filt[0])
                 p["taps"] = torch.tensor(taps, device=dev)
                 p["radius"] = rad
-            max_scratch = max(max_scratch, int(self.Lx.pivb_xcorr_scratch_bytes(N * ny * nx, 1, self.cfg.peak_finder)))
+            # room for the per-window records, so every single-peak fit (3-point
+            # included) runs in the thread-per-window record kernel
+            max_scratch = max(max_scratch, int(self.Lx.pivb_xcorr_scratch_bytes(N * ny * nx, 1, self.cfg.peak_finder)),
+                              int(self.Lx.pivb_xcorr_record_bytes(N * ny * nx)))
             max_vec = max(max_vec, N * ny * nx)
             max_pad = max(max_pad, N * nyp * nxp)
             self.passes.append(p)
@@ -142,7 +145,7 @@ class MultipassPIV:
         n = 0
         for k in range(len(self.geo)):
             n += 1                                        # correlation
-            n += 1 if (self.cfg.peak_finder >= 4) else 0  # deferred LM
+            n += 1 if (3 <= self.cfg.peak_finder <= 6) else 0  # deferred fit (record kernel)
             n += 2 if self.cfg.median_threshold > 0 else 1  # validate (+ median)
             if k + 1 < len(self.geo) or self.cfg.final_infill:
                 n += 1                                    # infill
@@ -179,7 +182,7 @@ class MultipassPIV:
                                                cfg.warp_impl, s), "warp")
                 pred_dy, pred_dx = p["pred_dy"], p["pred_dx"]
             o = p["out"]
-            nbytes = int(self.Lx.pivb_xcorr_scratch_bytes(N * p["ny"] * p["nx"], 1, cfg.peak_finder))
+            nbytes = scr.numel()
             self._ok(self.Lx.pivb_xcorr_dev(
                 fa.data_ptr(), fb.data_ptr(), H * W, None, H, W, N, p["cx"].data_ptr(), p["cy"].data_ptr(),
                 p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win"],

@@ -234,3 +234,37 @@ def test_utilities(cuda, oracle):
     assert L.xcorr(a, b, c, np.array([16, 16], np.int32)) == 0
     np.testing.assert_allclose(c, oracle.xcorr_plane(a, b), rtol=0, atol=1e-5)
     assert L.pivtools_cpu_supported() == 1 and L.peakfit_batch_available() == 1
+
+
+@pytest.mark.parametrize("n", [16, 32, 64])
+def test_deferred_three_point_equals_in_kernel(cuda, n):
+    """With record scratch the 3-point fits run in the thread-per-window record
+    kernel; without it, in the correlation kernel.  Same outputs, bit for bit."""
+    import ctypes
+
+    import torch
+
+    L = _lib.bulkxcorr2d_lib()
+    A, B, _ = _pair(n, 500 + n)
+    g = geometry.compute_window_centers(A.shape, (n, n), 50)
+    w = torch.tensor(geometry.window_weight((n, n), "gaussian"), device=cuda)
+    cw = torch.empty_like(w)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert L.pivb_correl_weight_dev(w.data_ptr(), n, n, cw.data_ptr(), s) == 0
+    tA, tB = torch.tensor(A[None], device=cuda), torch.tensor(B[None], device=cuda)
+    cx, cy = torch.tensor(g.win_ctrs_x, device=cuda), torch.tensor(g.win_ctrs_y, device=cuda)
+    total = g.n_win_y * g.n_win_x
+    nb = int(L.pivb_xcorr_record_bytes(total))
+    scratch = torch.empty(nb, dtype=torch.uint8, device=cuda)
+    res = []
+    for sb in (0, nb):
+        out = [torch.full((1, 1, g.n_win_y, g.n_win_x), -3.0, device=cuda) for _ in range(7)]
+        assert L.pivb_xcorr_dev(tA.data_ptr(), tB.data_ptr(), tA.stride(0), None, A.shape[0], A.shape[1], 1,
+                                cx.data_ptr(), cy.data_ptr(), g.n_win_y, g.n_win_x, w.data_ptr(), w.data_ptr(),
+                                cw.data_ptr(), n, n, 0, 1, 3, 0, *[o.data_ptr() for o in out], None,
+                                scratch.data_ptr() if sb else None, sb, s) == 0
+        torch.cuda.synchronize()
+        res.append([o.cpu().numpy() for o in out])
+    for a, b in zip(*res):
+        assert np.array_equal(a, b, equal_nan=True)
+    assert np.isfinite(res[0][0]).mean() > 0.5
