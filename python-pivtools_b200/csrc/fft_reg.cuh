@@ -158,4 +158,31 @@ __device__ __forceinline__ void lane_combine(float2 (&y)[M], int p)
     }
 }
 
+// Forward (SIGN = -1) four-lane combine with the lane twiddles W_N^{p k} read from
+// a table tw[p * M + k] instead of being selected among compile-time candidates:
+// one complex product per sample, the same arithmetic as c_twiddle's.
+template <int P, int M>
+__device__ __forceinline__ void lane_combine_fwd_tab(float2 (&y)[M], int p, const float2 *__restrict__ tw)
+{
+    static_assert(P == 4, "table combine is the four-lane form");
+#pragma unroll
+    for (int k = 1; k < M; ++k) {
+        const float2 w = tw[p * M + k];
+        const float2 v = y[k];
+        y[k] = make_float2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
+    }
+    const int p1 = p >> 1, p0 = p & 1;
+#pragma unroll
+    for (int k = 0; k < M; ++k) {
+        float2 o;
+        o.x = __shfl_xor_sync(0xffffffffu, y[k].x, 2);
+        o.y = __shfl_xor_sync(0xffffffffu, y[k].y, 2);
+        float2 u = p1 ? c_sub(o, y[k]) : c_add(y[k], o);
+        if (p == 3) u = make_float2(u.y, -u.x);          // W4^1 = -i
+        o.x = __shfl_xor_sync(0xffffffffu, u.x, 1);
+        o.y = __shfl_xor_sync(0xffffffffu, u.y, 1);
+        y[k] = p0 ? c_sub(o, u) : c_add(u, o);
+    }
+}
+
 }  // namespace piv

@@ -37,7 +37,10 @@ struct WinGeo {
     static constexpr int GROUPS_PER_CTA = (GW <= 32) ? WARPS_PER_CTA * WPW : 1;
     static constexpr int PLANE_BYTES = N * ST * 8;
     static constexpr int RED_SLOTS = (GW > 32) ? GW / 32 : 1;
-    static constexpr int SMEM_BYTES = GROUPS_PER_CTA * PLANE_BYTES + 64 * RED_SLOTS * 4 + 64;
+    static constexpr int RED_BYTES = 64 * RED_SLOTS * 4 + 64;
+    // lane twiddles W_N^{p k} for the four-lane combine (forward sign), float2 [P][M]
+    static constexpr int TW_BYTES = (P == 4) ? P * M * 8 : 0;
+    static constexpr int SMEM_BYTES = GROUPS_PER_CTA * PLANE_BYTES + RED_BYTES + TW_BYTES;
     static_assert(N * STF * 4 <= PLANE_BYTES, "float plane must alias the complex plane");
 };
 
@@ -252,9 +255,26 @@ __device__ __forceinline__ void fft2_inverse(const Group<N> &g, float2 *S, float
 // taken as conj(FFT(conj(C'))): the product stage emits conj(C') directly, and
 // only the real part of the result is used, which the final conjugation leaves
 // unchanged.  Negation is exact, so this equals the inverse transform bit for bit.
+// Fill the lane-twiddle table of the four-lane combine: tw[p][k] = W_N^{p k}
+// (forward sign), once per CTA.
+template <int N>
+__device__ __forceinline__ void fill_lane_twiddles(float2 *tw, int tid, int nthreads)
+{
+    using G = WinGeo<N>;
+    if constexpr (G::TW_BYTES > 0) {
+        for (int i = tid; i < G::P * G::M; i += nthreads) {
+            const int pp = i / G::M, k = i % G::M;
+            double sn, cs;
+            sincospi(2.0 * (double)(pp * k) / (double)N, &sn, &cs);
+            tw[i] = make_float2((float)cs, (float)(-sn));
+        }
+    }
+}
+
 template <int N>
 __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, const float (&a)[WinGeo<N>::M],
-                                                const float (&b)[WinGeo<N>::M], float scale)
+                                                const float (&b)[WinGeo<N>::M], float scale,
+                                                const float2 *tw = nullptr)
 {
     using G = WinGeo<N>;
     constexpr int M = G::M, P = G::P, ST = G::ST;
@@ -269,7 +289,8 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
 #pragma unroll 1
     for (int pass = 0;; ++pass) {
         RegFFT<M, -1>::run(z);
-        lane_combine<P, M, -1>(z, p);
+        if constexpr (G::TW_BYTES > 0) lane_combine_fwd_tab<P, M>(z, p, tw);
+        else lane_combine<P, M, -1>(z, p);
         if (pass == 3) break;
         g.sync();
         if (active) {

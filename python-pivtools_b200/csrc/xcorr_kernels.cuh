@@ -172,6 +172,9 @@ xcorr_kernel(XcorrParams prm)
     }
     float2 *S = reinterpret_cast<float2 *>(smem + gi * G::PLANE_BYTES);
     float *red = reinterpret_cast<float *>(smem + G::GROUPS_PER_CTA * G::PLANE_BYTES);
+    float2 *tw = reinterpret_cast<float2 *>(smem + G::GROUPS_PER_CTA * G::PLANE_BYTES + G::RED_BYTES);
+    fill_lane_twiddles<N>(tw, threadIdx.x, G::CTA_THREADS);
+    if constexpr (G::TW_BYTES > 0) __syncthreads();
     const Group<N> g{t, red};
     const bool active = t < G::T;
     int line, p;
@@ -231,7 +234,7 @@ xcorr_kernel(XcorrParams prm)
         eb = g.sum(eb);
         const float enorm = 1.0f / sqrtf(ea * eb);
 
-        correlate_plane<N>(g, S, a, b, inv_numel);
+        correlate_plane<N>(g, S, a, b, inv_numel, tw);
         float *pl = reinterpret_cast<float *>(S);
 
         if (prm.planes && valid) {
