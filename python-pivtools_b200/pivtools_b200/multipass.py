@@ -247,6 +247,8 @@ class HostPipeline:
         """Ah, Bh: pinned uint16 (N, H, W) host tensors, N a multiple of the chunk;
         ux_out, uy_out: pinned float32 (N, ny, nx) host tensors."""
         torch = self.torch
+        if not all(t.is_pinned() for t in (Ah, Bh, ux_out, uy_out)):
+            raise ValueError("HostPipeline.run needs page-locked host tensors (use .pin_memory())")
         comp = torch.cuda.current_stream(self.mp.device)
         C = self.C
         n_chunks = Ah.shape[0] // C
