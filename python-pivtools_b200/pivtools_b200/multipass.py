@@ -241,6 +241,7 @@ class HostPipeline:
         self.copy_stream = torch.cuda.Stream(device=dev)
         self.ev_h2d = [torch.cuda.Event() for _ in range(2)]
         self.ev_conv = [torch.cuda.Event() for _ in range(2)]
+        self._slot = 0
         self.Lp = _lib.pass_lib()
 
     def run(self, Ah, Bh, ux_out, uy_out):
@@ -252,10 +253,12 @@ class HostPipeline:
         comp = torch.cuda.current_stream(self.mp.device)
         C = self.C
         n_chunks = Ah.shape[0] // C
-        for s in range(2):
-            self.ev_conv[s].record(comp)
         for c in range(n_chunks):
-            s = c % 2
+            # staging slots alternate across calls too, so the next call's first
+            # chunk crosses PCIe while this call's last chunk computes; a slot is
+            # refilled only after its previous frames were converted
+            s = self._slot
+            self._slot ^= 1
             sl = slice(c * C, (c + 1) * C)
             self.copy_stream.wait_event(self.ev_conv[s])
             with torch.cuda.stream(self.copy_stream):
