@@ -19,6 +19,16 @@
 #include "fft_reg.cuh"
 #include "peakfit_dev.cuh"
 
+// Resident correlation CTAs per SM that the register allocation is capped for
+// (measured on B200: 32 px 5, 64 px 4; more CTAs spill or lose to the smaller
+// register budget).
+#ifndef PIVB_MIN_CTAS_32
+#define PIVB_MIN_CTAS_32 5
+#endif
+#ifndef PIVB_MIN_CTAS_64
+#define PIVB_MIN_CTAS_64 4
+#endif
+
 namespace piv {
 
 template <int N>
@@ -33,7 +43,7 @@ struct WinGeo {
     static constexpr int WARPS_PER_CTA = (GW <= 32) ? 4 : GW / 32;
     static constexpr int CTA_THREADS = WARPS_PER_CTA * 32;
     // resident CTAs per SM the correlation kernel is compiled for (register cap)
-    static constexpr int MIN_CTAS = (N == 32) ? 5 : (N <= 16 ? 8 : 1);
+    static constexpr int MIN_CTAS = (N == 32) ? PIVB_MIN_CTAS_32 : (N <= 16 ? 8 : (N == 64 ? PIVB_MIN_CTAS_64 : 1));
     static constexpr int GROUPS_PER_CTA = (GW <= 32) ? WARPS_PER_CTA * WPW : 1;
     static constexpr int PLANE_BYTES = N * ST * 8;
     static constexpr int RED_SLOTS = (GW > 32) ? GW / 32 : 1;

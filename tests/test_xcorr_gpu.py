@@ -268,3 +268,36 @@ def test_deferred_three_point_equals_in_kernel(cuda, n):
     for a, b in zip(*res):
         assert np.array_equal(a, b, equal_nan=True)
     assert np.isfinite(res[0][0]).mean() > 0.5
+
+
+def test_config1_workload_against_oracle(oracle, cuda):
+    """The CPU-runnable reference workload at full size: one 1024x1024 pair
+    (0.05 ppp, sigma 0.6 px, uniform (3.3, -1.7) px + GRF 0.5 px, corr. length
+    40 px), 32 px Gaussian windows at 50% (63 x 63 vectors), gauss3, through
+    the host-pointer C-ABI entry point against the oracle: identical NaN
+    sentinels, integer peaks identical except near-ties, displacements within
+    0.005 px, and both within 0.1 px (median) of the true field."""
+    A, B, (u, v) = synthetic.particle_pair((1024, 1024), seed=1, flow="uniform_grf")
+    g = geometry.compute_window_centers(A.shape, (32, 32), 50)
+    assert (g.n_win_y, g.n_win_x) == (63, 63)
+    w = geometry.window_weight((32, 32), "gaussian")
+    mask = np.zeros((63, 63), np.float32)
+    gpu = correlator.bulkxcorr2d(A, B, g.win_ctrs_x, g.win_ctrs_y, (32, 32), w, w, mask=mask, peak_finder=3,
+                                 dump_planes=True)
+    orc = oracle.bulkxcorr2d(A, B, mask, g.win_ctrs_x, g.win_ctrs_y, (32, 32), w, w, peak_finder=3,
+                             want_planes=True)
+    gx, ox = gpu["pk_loc_x"].ravel(), orc["pk_x"].ravel()
+    gy, oy = gpu["pk_loc_y"].ravel(), orc["pk_y"].ravel()
+    assert np.array_equal(np.isnan(gx), np.isnan(ox))
+    ok = ~np.isnan(gx)
+    d = np.maximum(np.abs(gx - ox), np.abs(gy - oy))
+    bad = ok & (d > 0.005)
+    planes = orc["planes"].reshape(-1, 32, 32)
+    for k in np.nonzero(bad)[0]:
+        assert _near_tie(planes[k]), k
+    iy = np.clip(np.round(g.win_ctrs_y).astype(int), 0, 1023)
+    ix = np.clip(np.round(g.win_ctrs_x).astype(int), 0, 1023)
+    tu, tv = u[np.ix_(iy, ix)].ravel(), v[np.ix_(iy, ix)].ravel()
+    for X, Y in ((gx, gy), (ox, oy)):
+        e = np.hypot(X - tu, Y - tv)[ok]
+        assert np.median(e) < 0.1
