@@ -274,15 +274,17 @@ def run_b200(args):
     stream.synchronize()
     kern_ms = k0.elapsed_time(k1) / R
     windows = N * p["ny"] * p["nx"]
-    alg_bytes = 2 * N * HW[0] * HW[1] * 4 + 7 * windows * 4
+    alg_bytes = 2 * N * HW[0] * HW[1] * 4 + 7 * windows * 4 + 2 * 128 * windows   # frames, outputs, records
     hbm_peak, bf16_peak, peak_kind = _peaks()
     achieved = alg_bytes / (kern_ms * 1e-3) / 1e9
     fp32_flops = windows * 80.1e3
-    # DRAM traffic of one launch: dram__bytes_read.sum + dram__bytes_write.sum of the
-    # same kernel and pass captured by ncu on 8 pairs (305.0 MB + 16.2 MB for 512,072
-    # windows, profiles/xcorr_kernel32_pass4_8pairs.md), scaled by windows processed
-    # (frames and outputs both grow with the pair count).
-    traffic = (304.946688e6 + 16.182016e6) / 512072 * windows
+    # DRAM traffic of one launch pair (correlation + deferred fits): dram__bytes_read.sum
+    # + dram__bytes_write.sum of the same kernels and pass captured by ncu on 8 pairs
+    # (xcorr_kernel<32>: 351.3 + 61.1 MB, lm_records_kernel: 65.6 + 4.8 MB, for
+    # 512,072 windows; profiles/xcorr_kernel32_pass4_8pairs.md,
+    # profiles/lm_records_gauss3_8pairs.md), scaled by windows processed (frames,
+    # records and outputs all grow with the pair count).
+    traffic = (351.2768e6 + 61.10976e6 + 65.61664e6 + 4.807424e6) / 512072 * windows
 
     # ---- end to end through host buffers: every step copies its 64 pairs of
     # uint16 frames from pinned memory (chunked, overlapped with compute), converts
