@@ -49,6 +49,8 @@ def _args():
     ap.add_argument("--workload", default="multipass", choices=["multipass", "ensemble", "serve"],
                     help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
                          "serve: Poisson request stream with continuous batching")
+    ap.add_argument("--engine32", default="fft", choices=["fft", "dft"],
+                    help="32 px passes on the FP32 FFT path or the tensor-core DFT-as-GEMM path")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: offered pairs/s")
     ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
     return ap.parse_args()
@@ -199,7 +201,7 @@ def run_b200(args):
     dev = torch.device("cuda", local)
     N = args.pairs
     A, B = synthetic.channel_batch_torch(N, HW, seed=2026 + rank, device=dev)
-    mp = multipass.MultipassPIV(HW, N, device=dev)
+    mp = multipass.MultipassPIV(HW, N, multipass.MultipassConfig(engine_32=args.engine32), device=dev)
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
@@ -256,11 +258,15 @@ def run_b200(args):
 
     def corr_launch():
         s = ctypes.c_void_p(stream.cuda_stream)
-        Lx.pivb_xcorr_dev(mp.warped[0].data_ptr(), mp.warped[1].data_ptr(), HW[0] * HW[1], None, HW[0], HW[1], N,
-                          p["cx"].data_ptr(), p["cy"].data_ptr(), p["ny"], p["nx"], p["weight"].data_ptr(),
-                          p["weight"].data_ptr(), p["cw"].data_ptr(), 32, 32, 0, 1, 3, 0, o["pk_loc_x"].data_ptr(),
-                          o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(),
-                          o["sxy"].data_ptr(), p["ratio"].data_ptr(), None, mp.scratch.data_ptr(), nbytes, s)
+        a = (mp.warped[0].data_ptr(), mp.warped[1].data_ptr(), HW[0] * HW[1], None, HW[0], HW[1], N,
+             p["cx"].data_ptr(), p["cy"].data_ptr(), p["ny"], p["nx"], p["weight"].data_ptr(),
+             p["weight"].data_ptr(), p["cw"].data_ptr(), 32, 32, 0, 1, 3, 0, o["pk_loc_x"].data_ptr(),
+             o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(),
+             o["sxy"].data_ptr(), p["ratio"].data_ptr(), None, mp.scratch.data_ptr(), nbytes)
+        if mp.Ld is not None:
+            mp.Ld.pivb_dft_xcorr_dev(*a, mp.dft_status.data_ptr(), s)
+        else:
+            Lx.pivb_xcorr_dev(*a, s)
 
     with torch.cuda.stream(stream):
         for _ in range(3):
@@ -292,7 +298,7 @@ def run_b200(args):
     from pivtools_b200.multipass import HostPipeline
 
     chunk = 16 if N % 16 == 0 else N
-    pipe = HostPipeline(HW, chunk, device=dev)
+    pipe = HostPipeline(HW, chunk, multipass.MultipassConfig(engine_32=args.engine32), device=dev)
     # frames are integer counts in [0, 65535]; every host buffer is page-locked with
     # .pin_memory() (torch.empty_like of a pinned tensor is pageable, which turns the
     # copies synchronous and serialises them with the compute)
@@ -340,16 +346,24 @@ def run_b200(args):
                        "passes": "128/64/32/32 px, 50/50/50/75%", "peak_finder": "gauss3", "warp": "bicubic",
                        "vectors_per_step_per_gpu": vec_step, "windows_per_step_per_gpu": mp.windows_per_step(),
                        "cuda_graph": graph is not None, "l2": "inputs 4.3 GB > L2, no flush",
+                       "engine_32px": "tensor-core DFT-as-GEMM (split BF16 x3)" if args.engine32 == "dft" else "FP32 FFT",
                        "parallelism": f"dp{ws} (pairs)"},
             "pair_latency_ms": {"p50": step_ms[len(step_ms) // 2] / N, "p99": step_ms[-1] / N,
                                 "note": "per-pair share of a batched step; served latency comes from the serving loop"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "xcorr_kernel<32> + lm_records_kernel (final pass, 4.1M windows)", "kernel_ms": kern_ms,
-                         "algorithmic_bytes": alg_bytes,
-                         "fp32_view": {"flops_per_launch": fp32_flops, "peak_tflops_nominal": FP32_NOMINAL_TFLOPS,
-                                       "frac_of_nominal": fp32_flops / (kern_ms * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS,
-                                       "achieved_tflops": fp32_flops / (kern_ms * 1e-3) / 1e12}},
+            "roofline": ({"bound": "tensor", "achieved": windows * 1.769e6 / (kern_ms * 1e-3) / 1e12,
+                          "peak": bf16_peak, "unit": "TFLOP/s",
+                          "frac": windows * 1.769e6 / (kern_ms * 1e-3) / 1e12 / bf16_peak, "traffic": None,
+                          "peak_kind": peak_kind, "tensor_flops_per_window": 1.769e6,
+                          "kernel": "dft32 tcgen05 kernel + lm_records_kernel (final pass, 4.1M windows)",
+                          "kernel_ms": kern_ms, "hbm_view": {"achieved_gbs": achieved, "frac": achieved / hbm_peak}}
+                         if mp.Ld is not None else
+                         {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                          "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
+                          "kernel": "xcorr_kernel<32> + lm_records_kernel (final pass, 4.1M windows)", "kernel_ms": kern_ms,
+                          "algorithmic_bytes": alg_bytes,
+                          "fp32_view": {"flops_per_launch": fp32_flops, "peak_tflops_nominal": FP32_NOMINAL_TFLOPS,
+                                        "frac_of_nominal": fp32_flops / (kern_ms * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS,
+                                        "achieved_tflops": fp32_flops / (kern_ms * 1e-3) / 1e12}}),
             "e2e": {"value": e2e_val, "unit": "vectors/s", "h2d_bytes_per_step": 2 * N * HW[0] * HW[1] * 2,
                     "d2h_bytes_per_step": 2 * N * p["ny"] * p["nx"] * 4, "frames": "uint16",
                     "chunk_pairs": chunk, "gpu_launches_per_step": e2e_launches, "host_frames_pinned": True,

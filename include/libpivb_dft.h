@@ -15,6 +15,12 @@ extern "C" {
 int pivb_umma_selftest(const void *d_A, const void *d_B, float *d_D, int N, int K, int a_mn, int *d_status,
                        void *stream);
 
+/* The timeout path of the kernels' bounded mbarrier waits: one CTA allocates
+ * tensor memory, waits `limit` polls on a phase that nothing completes, adds 1
+ * per warp to *d_status (device int), frees the tensor memory and returns.  No
+ * counterpart in the reference. */
+int pivb_wait_timeout_selftest(int *d_status, int limit, void *stream);
+
 /* Instantaneous correlation of 32 x 32 windows as DFT-as-GEMM on the tensor core:
  * four chained GEMMs (real row DFT, complex column DFT, inverse column DFT,
  * Hermitian inverse row DFT) with every operand split into BF16 hi + lo and three

@@ -90,6 +90,29 @@ __global__ void __launch_bounds__(128) umma_selftest_kernel(const uint16_t *__re
     if (warp == 0) umma::tmem_free(tbase, ncols);
 }
 
+// The failure path of the bounded waits: allocate tensor memory, wait on an
+// mbarrier phase that nothing completes (no MMA is issued, nothing arrives) with a
+// short poll limit, record the timeout in *status, free the tensor memory and
+// return.  The correlation kernels take the same path if an MMA completion is
+// ever not observed.
+__global__ void __launch_bounds__(128) wait_timeout_kernel(int *status, uint32_t limit)
+{
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t slot;
+    const int t = threadIdx.x, warp = t >> 5;
+    if (t == 0) umma::mbar_init(&bar, 1);
+    if (warp == 0) umma::tmem_alloc(&slot, 32);
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+    const uint32_t tbase = slot;
+    const bool ok = umma::mbar_wait(umma::smem_u32(&bar), 0, limit);
+    if (!ok && (t & 31) == 0) atomicAdd(status, 1);
+    umma::fence_before();
+    __syncthreads();
+    if (warp == 0) umma::tmem_free(tbase, 32);
+}
+
 // ---------------------------------------------------------------------------
 // DFT-as-GEMM correlation, 32 x 32 windows
 // ---------------------------------------------------------------------------
@@ -157,7 +180,14 @@ struct WinInfo {
     int flags;     // 1 valid, 2 in range, 4 plane holds NaN
 };
 
-__global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *__restrict__ consts, int *status)
+// Two warpgroups: warp w (w = 4 wg + q) owns tensor-memory lanes 32 q .. 32 q + 31
+// like warp q of the other group; the groups split each stage's columns (the
+// two images, the two halves of ky or y, the two plane tiles) and each warp
+// gathers, searches and fits one window of the eight.
+constexpr int THREADS = 256;
+constexpr uint32_t XCHG = 48 * 1024;      // kx = 0 exchange area inside the work region
+
+__global__ void __launch_bounds__(THREADS, 2) kernel(XcorrParams prm, const uint4 *__restrict__ consts, int *status)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ WinInfo info[G];
@@ -167,27 +197,28 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + CONST_BYTES + WORK_BYTES);
     uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 1);
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int wg = warp >> 2, wq = warp & 3;
 
-    for (int i = t; i < (int)(CONST_BYTES / 16); i += 128) reinterpret_cast<uint4 *>(cst)[i] = consts[i];
+    for (int i = t; i < (int)(CONST_BYTES / 16); i += THREADS) reinterpret_cast<uint4 *>(cst)[i] = consts[i];
     if (t == 0) umma::mbar_init(bar, 1);
     if (warp == 0) umma::tmem_alloc(slot, TMEM_COLS);
     cta_sync_for_mma();
     const uint32_t tm = *slot;
-    const uint32_t lane_base = tm + ((uint32_t)(32 * warp) << 16);
+    const uint32_t lane_base = tm + ((uint32_t)(32 * wq) << 16);
     const uint32_t cst_a = umma::smem_u32(cst), wk_a = umma::smem_u32(wk), bar_a = umma::smem_u32(bar);
     uint32_t phase = 0;
     bool ok = true;
     const long long nwt = (long long)prm.nwy * prm.nwx;
     const long long ngroups = (prm.total + G - 1) / G;
     const float inv_numel = 1.0f / (float)(N * N);
+    float *xchg = reinterpret_cast<float *>(wk + XCHG);   // [wg][wq][2 rows][4][16]
 
     for (long long grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
         // ---- stage 0: gather, weight, mean, energy (PIV_2d_cross_correlate.c:299-353).
-        //      Warp w takes windows w and 4 + w; lane = column x, so every load
-        //      instruction reads one 128-byte image row segment.
-#pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-            const int wl = h * 4 + warp;
+        //      Warp w takes window w; lane = column x, so every load instruction reads
+        //      one 128-byte image row segment.
+        {
+            const int wl = warp;
             const long long idx = grp * G + wl;
             const bool inrange = idx < prm.total;
             bool valid = inrange;
@@ -242,12 +273,12 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
                 info[wl].enorm = 1.0f / sqrtf(ea * eb);
                 info[wl].flags = (valid ? 1 : 0) | (inrange ? 2 : 0);
             }
-            // A1 tiles (MN-major, 8 KB hi + 8 KB lo each): h -> tile h (image A), 2 + h (image B);
-            // row (window % 4) * 32 + y, K = x
-            unsigned char *ta = wk + h * 16384, *tb = wk + (2 + h) * 16384;
+            // A1 tiles (MN-major, 8 KB hi + 8 KB lo each): tile wg (image A) and 2 + wg
+            // (image B) hold windows 4 wg .. 4 wg + 3; row (window % 4) * 32 + y, K = x
+            unsigned char *ta = wk + wg * 16384, *tb = wk + (2 + wg) * 16384;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const uint32_t off = umma::mnmajor_offset(128, warp * 32 + 8 * q, lane);
+                const uint32_t off = umma::mnmajor_offset(128, wq * 32 + 8 * q, lane);
                 store8(ta + off, ta + 8192 + off, a + 8 * q);
                 store8(tb + off, tb + 8192 + off, b + 8 * q);
             }
@@ -264,12 +295,14 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
         phase ^= 1u;
         umma::fence_after();
         // ---- Y -> A2 (MN-major; image i: 16 KB hi + 16 KB lo at 32 KB * i).  Row
-        //      (window, kx) = wglob * 16 + kx; K: Re at y, Im at 32 + y.
+        //      (window, kx) = wglob * 16 + kx; K: Re at y, Im at 32 + y.  Group wg
+        //      takes tiles wg (image A) and 2 + wg (image B): its own windows.
 #pragma unroll 1
-        for (int tt = 0; tt < 4; ++tt) {
+        for (int img = 0; img < 2; ++img) {
+            const int tt = 2 * img + wg;
             float v[32];
             umma::tmem_ld32(lane_base + 32 * tt, v);
-            const int wglob = (tt & 1) * 4 + warp, img = tt >> 1;
+            const int wglob = wg * 4 + wq;
             unsigned char *hi = wk + img * 32768, *lo = hi + 16384;
 #pragma unroll
             for (int half = 0; half < 2; ++half) {
@@ -290,42 +323,58 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
         ok &= umma::mbar_wait(bar_a, phase);
         phase ^= 1u;
         umma::fence_after();
-        // ---- spectrum product -> A3 (K-major, 16 KB hi + 16 KB lo); row r = (window, kx)
+        // ---- spectrum product -> A3 (K-major, 16 KB hi + 16 KB lo); row r = (window, kx);
+        //      group wg takes ky in [16 wg, 16 wg + 16)
         {
-            float fa[64], fb[64];
-            umma::tmem_ld32(lane_base + 128, *reinterpret_cast<float(*)[32]>(fa));
-            umma::tmem_ld32(lane_base + 160, *reinterpret_cast<float(*)[32]>(fa + 32));
-            umma::tmem_ld32(lane_base + 192, *reinterpret_cast<float(*)[32]>(fb));
-            umma::tmem_ld32(lane_base + 224, *reinterpret_cast<float(*)[32]>(fb + 32));
-            float cr[32], ci[32];
+            const int k0 = 16 * wg;
+            float ar[16], ai[16], br[16], bi[16];
+            umma::tmem_ld16(lane_base + 128 + k0, ar);
+            umma::tmem_ld16(lane_base + 160 + k0, ai);
+            umma::tmem_ld16(lane_base + 192 + k0, br);
+            umma::tmem_ld16(lane_base + 224 + k0, bi);
             const int kx = lane & 15;
-            if (kx != 0) {
+            // rows kx = 0 (lanes 0, 16) need F(-ky), held by the other group: exchange
+            float *mine = xchg + ((wg * 4 + wq) * 2 + (lane >> 4)) * 64;
+            if (kx == 0) {
 #pragma unroll
-                for (int ky = 0; ky < 32; ++ky) {
-                    const float ar = fa[ky], ai = fa[32 + ky], br = fb[ky], bi = fb[32 + ky];
-                    cr[ky] = br * ar + bi * ai;
-                    ci[ky] = bi * ar - br * ai;
-                }
-            } else {
-                // P = F(.,0) + i F(.,16); F0 = (P + conj P(-ky)) / 2, F16 = (P - conj P(-ky)) / 2i
-#pragma unroll
-                for (int ky = 0; ky < 32; ++ky) {
-                    const int m = (32 - ky) & 31;
-                    const float a0r = 0.5f * (fa[ky] + fa[m]), a0i = 0.5f * (fa[32 + ky] - fa[32 + m]);
-                    const float a1r = 0.5f * (fa[32 + ky] + fa[32 + m]), a1i = -0.5f * (fa[ky] - fa[m]);
-                    const float b0r = 0.5f * (fb[ky] + fb[m]), b0i = 0.5f * (fb[32 + ky] - fb[32 + m]);
-                    const float b1r = 0.5f * (fb[32 + ky] + fb[32 + m]), b1i = -0.5f * (fb[ky] - fb[m]);
-                    const float c0r = b0r * a0r + b0i * a0i, c0i = b0i * a0r - b0r * a0i;
-                    const float c1r = b1r * a1r + b1i * a1i, c1i = b1i * a1r - b1r * a1i;
-                    cr[ky] = c0r - c1i;        // Q = C0 + i C16
-                    ci[ky] = c0i + c1r;
+                for (int j = 0; j < 16; ++j) {
+                    mine[j] = ar[j]; mine[16 + j] = ai[j]; mine[32 + j] = br[j]; mine[48 + j] = bi[j];
                 }
             }
-            const uint32_t r = (uint32_t)(warp * 32 + lane);
+            __syncthreads();
+            float cr[16], ci[16];
+            if (kx != 0) {
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const uint32_t o_re = umma::kmajor_offset(128, r, 8 * c);
-                const uint32_t o_im = umma::kmajor_offset(128, r, 32 + 8 * c);
+                for (int j = 0; j < 16; ++j) {
+                    cr[j] = br[j] * ar[j] + bi[j] * ai[j];
+                    ci[j] = bi[j] * ar[j] - br[j] * ai[j];
+                }
+            } else {
+                // P = F(., 0) + i F(., 16); F0 = (P + conj P(-ky)) / 2, F16 = (P - conj P(-ky)) / 2i
+                const float *other = xchg + (((wg ^ 1) * 4 + wq) * 2 + (lane >> 4)) * 64;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int ky = k0 + j, m = (32 - ky) & 31;
+                    // F(m) lives with this group when m is in [k0, k0 + 16), else with the other
+                    const bool own = (m >> 4) == wg;
+                    const int jm = m & 15;
+                    const float amr = own ? ar[jm] : other[jm], ami = own ? ai[jm] : other[16 + jm];
+                    const float bmr = own ? br[jm] : other[32 + jm], bmi = own ? bi[jm] : other[48 + jm];
+                    const float a0r = 0.5f * (ar[j] + amr), a0i = 0.5f * (ai[j] - ami);
+                    const float a1r = 0.5f * (ai[j] + ami), a1i = -0.5f * (ar[j] - amr);
+                    const float b0r = 0.5f * (br[j] + bmr), b0i = 0.5f * (bi[j] - bmi);
+                    const float b1r = 0.5f * (bi[j] + bmi), b1i = -0.5f * (br[j] - bmr);
+                    const float c0r = b0r * a0r + b0i * a0i, c0i = b0i * a0r - b0r * a0i;
+                    const float c1r = b1r * a1r + b1i * a1i, c1i = b1i * a1r - b1r * a1i;
+                    cr[j] = c0r - c1i;        // Q = C0 + i C16
+                    ci[j] = c0i + c1r;
+                }
+            }
+            const uint32_t r = (uint32_t)(wq * 32 + lane);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const uint32_t o_re = umma::kmajor_offset(128, r, k0 + 8 * c);
+                const uint32_t o_im = umma::kmajor_offset(128, r, 32 + k0 + 8 * c);
                 store8(wk + o_re, wk + 16384 + o_re, cr + 8 * c);
                 store8(wk + o_im, wk + 16384 + o_im, ci + 8 * c);
             }
@@ -340,16 +389,18 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
         phase ^= 1u;
         umma::fence_after();
         // ---- G -> A4 (MN-major; tile t4 = window / 4: 8 KB hi + 8 KB lo at 16 KB * t4).
-        //      Row (window % 4) * 32 + y; K: Re at kx, Im at 16 + kx.
+        //      Row (window % 4) * 32 + y; K: Re at kx, Im at 16 + kx.  Group wg takes
+        //      y in [16 wg, 16 wg + 16).
         {
-            float gre[32], gim[32];
-            umma::tmem_ld32(lane_base + 0, gre);
-            umma::tmem_ld32(lane_base + 32, gim);
-            const int r = warp * 32 + lane, wglob = r >> 4, kx = r & 15;
+            const int y0 = 16 * wg;
+            float gre[16], gim[16];
+            umma::tmem_ld16(lane_base + y0, gre);
+            umma::tmem_ld16(lane_base + 32 + y0, gim);
+            const int r = wq * 32 + lane, wglob = r >> 4, kx = r & 15;
             unsigned char *hi = wk + (wglob >> 2) * 16384, *lo = hi + 8192;
-            const int rb = (wglob & 3) * 32;
+            const int rb = (wglob & 3) * 32 + y0;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < 2; ++q) {
                 const uint32_t o_re = umma::mnmajor_offset(128, rb + 8 * q, kx);
                 const uint32_t o_im = umma::mnmajor_offset(128, rb + 8 * q, 16 + kx);
                 store8(hi + o_re, lo + o_re, gre + 8 * q);
@@ -367,24 +418,24 @@ __global__ void __launch_bounds__(128, 2) kernel(XcorrParams prm, const uint4 *_
         ok &= umma::mbar_wait(bar_a, phase);
         phase ^= 1u;
         umma::fence_after();
-        // ---- planes: scale, fftshift into shared memory (aliases the work region)
+        // ---- plane of this warp's window: scale, fftshift into shared memory (aliases
+        //      the work region; tile wg holds windows 4 wg .. 4 wg + 3)
         float *planes = reinterpret_cast<float *>(wk);
-#pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
+        {
             float c[32];
-            umma::tmem_ld32(lane_base + 64 + 32 * h, c);
-            float *pl = planes + (h * 4 + warp) * (N * PLANE_LD);
+            umma::tmem_ld32(lane_base + 64 + 32 * wg, c);
+            umma::fence_before();
+            __syncthreads();              // every group has finished reading the work region
+            float *pl = planes + warp * (N * PLANE_LD);
             const int row = (lane + N / 2) & (N - 1);
 #pragma unroll
             for (int x = 0; x < N; ++x) pl[row * PLANE_LD + ((x + N / 2) & (N - 1))] = c[x] * inv_numel;
         }
-        umma::fence_before();
         __syncwarp();
         // ---- search (warp per window), then the fits of all eight windows in
         //      parallel on the lanes of warp 0 (the FFT path's code)
-#pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-            const int wl = h * 4 + warp;
+        {
+            const int wl = warp;
             float *pl = planes + wl * (N * PLANE_LD);
             if (prm.planes && (info[wl].flags & 1)) {
                 float *dst = prm.planes + info[wl].idx * (long long)(N * N);
@@ -531,6 +582,16 @@ PIV_EXPORT int pivb_umma_selftest(const void *d_A, const void *d_B, float *d_D, 
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
+// Exercise the timeout path of the bounded mbarrier wait: each of the 4 warps of
+// one CTA adds 1 to *d_status when its wait (limit polls) runs out.  Returns 0, or
+// 1 for bad arguments / launch failure.
+PIV_EXPORT int pivb_wait_timeout_selftest(int *d_status, int limit, void *stream)
+{
+    if (!d_status || limit <= 0) return 1;
+    wait_timeout_kernel<<<1, 128, 0, (cudaStream_t)stream>>>(d_status, (uint32_t)limit);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
 // Instantaneous correlation of 32 x 32 windows on the tensor core (DFT-as-GEMM,
 // split BF16, FP32 accumulation).  Arguments as pivb_xcorr_dev; supported:
 // win 32 x 32, ensemble 0, n_peaks 1, peak finders 3-6 (4-6 need the LM scratch
@@ -553,6 +614,8 @@ PIV_EXPORT int pivb_dft_xcorr_dev(const float *d_A, const float *d_B, long long 
     if (total == 0) return PIV_ERROR_NONE;
     const bool lm = peak_finder >= 4;
     if (lm && (d_scratch == nullptr || scratch_bytes < (size_t)total * sizeof(LmRecord))) return PIV_ERROR_NOMEM;
+    // with record scratch the 3-point fits also run in the thread-per-window record kernel
+    const bool defer = lm || (d_scratch != nullptr && scratch_bytes >= (size_t)total * sizeof(LmRecord));
     const uint4 *consts = dft32::consts_for_current_device();
     if (!consts) return PIV_ERROR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
@@ -564,16 +627,16 @@ PIV_EXPORT int pivb_dft_xcorr_dev(const float *d_A, const float *d_B, long long 
     p.ensemble = 0; p.n_peaks = 1; p.finder = peak_finder;
     p.pk_x = d_pk_x; p.pk_y = d_pk_y; p.pk_h = d_pk_h; p.sx = d_sx; p.sy = d_sy; p.sxy = d_sxy;
     p.pk_ratio = d_pk_ratio; p.planes = d_planes;
-    p.lm = lm ? static_cast<LmRecord *>(d_scratch) : nullptr;
+    p.lm = defer ? static_cast<LmRecord *>(d_scratch) : nullptr;
     p.total = total;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long groups = (total + dft32::G - 1) / dft32::G;
     const int grid = (int)(groups < 2LL * sms ? groups : 2LL * sms);
-    dft32::kernel<<<grid, 128, dft32::SMEM_BYTES, s>>>(p, consts, d_status);
+    dft32::kernel<<<grid, dft32::THREADS, dft32::SMEM_BYTES, s>>>(p, consts, d_status);
     if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
-    if (lm) {
+    if (defer) {
         const unsigned blocks = (unsigned)((total + 127) / 128);
         if (peakfit_impl) lm_records_kernel<1><<<blocks, 128, 0, s>>>(p, 32);
         else lm_records_kernel<0><<<blocks, 128, 0, s>>>(p, 32);

@@ -189,6 +189,8 @@ def dft_lib() -> ctypes.CDLL:
         return L
     L.pivb_umma_selftest.argtypes = [vp, vp, vp, ci, ci, ci, vp, vp]
     L.pivb_umma_selftest.restype = ci
+    L.pivb_wait_timeout_selftest.argtypes = [vp, ci, vp]
+    L.pivb_wait_timeout_selftest.restype = ci
     L.pivb_dft_xcorr_dev.argtypes = [vp, vp, cll, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, vp, ci, ci, ci, ci,
                                      ci, ci, vp, vp, vp, vp, vp, vp, vp, vp, vp, csz, vp, vp]
     L.pivb_dft_xcorr_dev.restype = ci

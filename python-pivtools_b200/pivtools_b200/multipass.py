@@ -43,6 +43,7 @@ class MultipassConfig:
     infill_iters: int = 400
     infill_tol: float = 1e-3
     final_infill: bool = True
+    engine_32: str = "fft"          # 32 px passes: "fft" (FP32 FFT) or "dft" (tensor-core DFT-as-GEMM)
 
 
 def _gauss_taps(sigma: float, ksize: int):
@@ -73,7 +74,12 @@ class MultipassPIV:
         self.Lx = _lib.bulkxcorr2d_lib()
         self.Lw = _lib.fusedwarp_lib()
         self.Lp = _lib.pass_lib()
+        if self.cfg.engine_32 not in ("fft", "dft"):
+            raise ValueError(f"engine_32 {self.cfg.engine_32!r}")
+        self.Ld = _lib.dft_lib() if self.cfg.engine_32 == "dft" else None
         dev, f32 = self.device, torch.float32
+        # device status word of the tensor-core engine (1 = an MMA completion was not observed)
+        self.dft_status = torch.zeros(1, dtype=torch.int32, device=dev)
         N, H, W = self.N, self.H, self.W
         self.warped = [torch.empty((N, H, W), dtype=f32, device=dev) for _ in range(2)]
         self.passes = []
@@ -183,12 +189,15 @@ class MultipassPIV:
                 pred_dy, pred_dx = p["pred_dy"], p["pred_dx"]
             o = p["out"]
             nbytes = scr.numel()
-            self._ok(self.Lx.pivb_xcorr_dev(
-                fa.data_ptr(), fb.data_ptr(), H * W, None, H, W, N, p["cx"].data_ptr(), p["cy"].data_ptr(),
-                p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win"],
-                p["win"], 0, 1, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(),
-                o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(), o["sxy"].data_ptr(),
-                p["ratio"].data_ptr(), None, scr.data_ptr(), nbytes, s), "correlation")
+            args = (fa.data_ptr(), fb.data_ptr(), H * W, None, H, W, N, p["cx"].data_ptr(), p["cy"].data_ptr(),
+                    p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win"],
+                    p["win"], 0, 1, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(),
+                    o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(),
+                    o["sxy"].data_ptr(), p["ratio"].data_ptr(), None, scr.data_ptr(), nbytes)
+            if self.Ld is not None and p["win"] == 32:
+                self._ok(self.Ld.pivb_dft_xcorr_dev(*args, self.dft_status.data_ptr(), s), "correlation (tensor core)")
+            else:
+                self._ok(self.Lx.pivb_xcorr_dev(*args, s), "correlation")
             thr = p["win"] / 2.0 if k == 0 else p["win"] / 4.0
             self._ok(self.Lp.pivb_validate_dev(
                 o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(),

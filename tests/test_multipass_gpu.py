@@ -271,3 +271,28 @@ def test_host_pipeline_matches_resident_batch(cuda):
         pipe.run(Ah, Bh, oux, ouy)
         torch.cuda.synchronize()
         assert torch.equal(oux, ux.cpu()) and torch.equal(ouy, uy.cpu())
+
+
+def test_multipass_tensor_core_engine_tracks_fft(cuda):
+    """The 32 px passes on the tensor-core DFT-as-GEMM engine give the FFT
+    engine's field within the split-BF16 precision (planes 1e-4 of the peak)."""
+    import torch
+
+    H = W = 384
+    N = 2
+    pairs = [synthetic.particle_pair((H, W), seed=70 + k, flow="channel", flow_kwargs={"peak": 6.0})
+             for k in range(N)]
+    A = torch.tensor(np.stack([p[0] for p in pairs]), device=cuda)
+    B = torch.tensor(np.stack([p[1] for p in pairs]), device=cuda)
+    res = []
+    for eng in ("fft", "dft"):
+        cfg = multipass.MultipassConfig(window_sizes=[(64, 64), (32, 32), (32, 32)], overlaps=[50, 50, 75],
+                                        engine_32=eng)
+        mp = multipass.MultipassPIV((H, W), N, cfg, device=cuda)
+        ux, uy = mp.run(A, B)
+        torch.cuda.synchronize()
+        assert mp.dft_status.item() == 0
+        res.append((ux.cpu().numpy().copy(), uy.cpu().numpy().copy()))
+    d = np.hypot(res[0][0] - res[1][0], res[0][1] - res[1][1])
+    assert np.isfinite(d).all()
+    assert np.median(d) < 1e-3 and np.percentile(d, 99) < 0.05

@@ -46,3 +46,20 @@ def test_umma_rejects_bad_shapes(cuda):
     L = _lib.dft_lib()
     assert L.pivb_umma_selftest(1, 1, 1, 24, 32, 0, 1, None) == 1
     assert L.pivb_umma_selftest(1, 1, 1, 32, 8, 0, 1, None) == 1
+
+
+def test_bounded_wait_times_out_and_context_survives(cuda):
+    """A wait that nothing completes ends after its poll limit, reports through
+    the status word, frees its tensor memory, and the context stays usable."""
+    import ctypes
+
+    import torch
+
+    L = _lib.dft_lib()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    st = torch.zeros(1, dtype=torch.int32, device=cuda)
+    assert L.pivb_wait_timeout_selftest(st.data_ptr(), 2048, s) == 0
+    torch.cuda.synchronize()
+    assert st.item() == 4                       # every warp saw its wait run out
+    test_umma_product(cuda, 32, 32, 0)          # tensor memory was released
+    assert L.pivb_wait_timeout_selftest(None, 10, s) == 1
