@@ -293,6 +293,20 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
     lane_slot<N>(active ? g.t : 0, line, p);
     const int q = out_block<P>(p);
     const int rm = (N - line) % N;
+    // Complex plane element (row, col) lives at row * ST + (col + rot(row)) % N: with
+    // four lanes per column each block of M rows is rotated by SH = 4 columns, so
+    // that the column-phase stores of one half-warp (4 lines from each of the 4
+    // blocks) fall on distinct banks instead of all blocks on the same ones.  (With
+    // two lanes the extra address registers cost more than the conflicts: measured.)
+    constexpr int SH = (P == 4) ? 4 : 0;
+    constexpr bool POW2 = (N & (N - 1)) == 0;
+    // blk = row / M, known at each call site
+    auto at = [&](int row, int blk, int col) {
+        if constexpr (SH == 0) return row * ST + col;
+        else if constexpr (POW2) return row * ST + ((col + SH * blk) & (N - 1));
+        else return row * ST + (col + SH * blk) % N;
+    };
+    const int lb = line / M, rb = rm / M;
     float2 z[M];
 #pragma unroll
     for (int n = 0; n < M; ++n) z[n] = make_float2(a[n], b[n]);
@@ -306,10 +320,10 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
         if (active) {
             if (pass == 0) {
 #pragma unroll
-                for (int k = 0; k < M; ++k) S[(M * q + k) * ST + line] = z[k];
+                for (int k = 0; k < M; ++k) S[at(M * q + k, q, line)] = z[k];
             } else {
 #pragma unroll
-                for (int k = 0; k < M; ++k) S[line * ST + M * q + k] = z[k];
+                for (int k = 0; k < M; ++k) S[at(line, lb, M * q + k)] = z[k];
             }
         }
         g.sync();
@@ -319,8 +333,8 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
 #pragma unroll
                 for (int n = 0; n < M; ++n) {
                     const int kx = P * n + p;
-                    const float2 zk = S[line * ST + kx];
-                    const float2 zn = S[rm * ST + (N - kx) % N];
+                    const float2 zk = S[at(line, lb, kx)];
+                    const float2 zn = S[at(rm, rb, (N - kx) % N)];
                     const float2 d = make_float2(zk.x - zn.x, zk.y + zn.y);   // Z - Zm
                     const float2 sm = make_float2(zk.x + zn.x, zk.y - zn.y);  // Z + Zm
                     const float re = d.x * sm.x + d.y * sm.y;
@@ -334,10 +348,10 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
         } else if (active) {
             if (pass == 0) {
 #pragma unroll
-                for (int n = 0; n < M; ++n) z[n] = S[line * ST + P * n + p];
+                for (int n = 0; n < M; ++n) z[n] = S[at(line, lb, P * n + p)];
             } else {
 #pragma unroll
-                for (int n = 0; n < M; ++n) z[n] = S[(P * n + p) * ST + line];
+                for (int n = 0; n < M; ++n) z[n] = S[at(P * n + p, (P * n) / M, line)];
             }
         }
     }
