@@ -64,6 +64,20 @@ int pivb_ensemble_finalize_dev(const float *sum_ab, const float *sum_aa, const f
                                int dc_zero, const float *env_auto, const float *env_ab, double *out_ab,
                                double *out_aa, double *out_bb, float *norm, void *stream);
 
+/* Decode n_frames camera payloads (frame k at raw + k * stride bytes) into float32
+ * frames, as the reference's PIVTOOLs Acquisition reader does on the host
+ * (pivtools_core/image_handling/readers/pivraw_reader.py:896-960,
+ * set_reader.py:1296-1345): format 0 Mono12p (two pixels in three bytes, LSB
+ * first), 1 BayerRG8 (2x2 superpixel sum R+G+G+B at half resolution); optional
+ * in-run dark (same format, dark_frames 1 or 2: odd 1-based file indices, counted
+ * from first_index, take dark frame A) subtracted as max(frame, dark) - dark per
+ * photosite before the sum; view rotation as rot = np.rot90 turns (0..3; the
+ * reader's cw90 is 3).  out_stride: floats between output frames.  Returns 0, or
+ * 1 for bad arguments. */
+int pivb_decode_frames_dev(const unsigned char *raw, long long stride, int n_frames, int first_index, int width,
+                           int height, int format, const unsigned char *dark, long long dark_stride, int dark_frames,
+                           int rot, float *out, long long out_stride, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -290,3 +290,40 @@ def ensemble_finalize(sum_ab, sum_aa, sum_bb, n_pairs, bg=None, dc_zero=False, e
     norm = np.sqrt(np.maximum(R[0][:, c[0], c[1]] * R[1][:, c[0], c[1]], np.float32(1e-12)))
     R = [r / norm[:, None, None] for r in R]
     return R[0], R[1], R[2], norm
+
+
+# ---------------------------------------------------------------------------
+# Camera payload decode (pivtools_core/image_handling/readers/pivraw_reader.py:896-960,
+# set_reader.py:1296-1345)
+# ---------------------------------------------------------------------------
+
+def decode_frames(raw, stride, n_frames, first_index, width, height, fmt, dark=None, dark_frames=2, rot=0):
+    """Payloads (uint8, frame k at k * stride) -> float32 frames: Mono12p unpack
+    (fmt 0) or the BayerRG8 mosaic (fmt 1), optional dark max(f, d) - d in the
+    sensor type (odd 1-based indices take dark A, even dark B when dark_frames is
+    2), the Bayer 2x2 superpixel sum, then np.rot90(., rot)."""
+    raw = np.asarray(raw, np.uint8)
+    npx = width * height
+
+    def sensor(buf, k):
+        if fmt == 0:
+            b = buf[k * stride:k * stride + npx // 2 * 3].reshape(-1, 3).astype(np.uint16)
+            p = np.empty((b.shape[0], 2), np.uint16)
+            p[:, 0] = b[:, 0] | ((b[:, 1] & 0x0F) << 8)
+            p[:, 1] = (b[:, 1] >> 4) | (b[:, 2] << 4)
+            return p.reshape(height, width)
+        return buf[k * stride:k * stride + npx].reshape(height, width).copy()
+
+    out = []
+    for k in range(n_frames):
+        f = sensor(raw, k)
+        if dark is not None:
+            role = (first_index + k - 1) % 2 if dark_frames == 2 else 0
+            d = sensor(np.asarray(dark, np.uint8), role)
+            f = np.maximum(f, d) - d
+        if fmt == 0:
+            img = f.astype(np.float32)
+        else:
+            img = f.reshape(height // 2, 2, width // 2, 2).astype(np.float32).sum(axis=(1, 3))
+        out.append(np.rot90(img, rot).astype(np.float32))
+    return np.stack(out)

@@ -564,3 +564,117 @@ PIV_EXPORT int pivb_ensemble_finalize_dev(const float *sum_ab, const float *sum_
     ensemble_finalize_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
+
+// ---------------------------------------------------------------------------
+// Ingest: camera payloads -> float32 frames
+// (pivtools_core/image_handling/readers/pivraw_reader.py:896-960,
+//  set_reader.py:1296-1345)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct DecodeParams {
+    const unsigned char *raw;     // frames back to back, frame k at k * stride
+    long long stride;
+    int n_frames, first_index;    // 1-based file index of frame 0 (its A/B role)
+    int width, height;            // sensor photosites
+    int format;                   // 0 Mono12p, 1 BayerRG8
+    const unsigned char *dark;    // dark frames (same format), or null
+    long long dark_stride;
+    int dark_frames;              // 1 (time-resolved) or 2 (A, B roles)
+    int rot;                      // np.rot90 turns, 0..3
+    int out_h, out_w;             // output frame shape (after the rotation)
+    float *out;
+    long long out_stride;
+};
+
+// Photosite (y, x) of a Mono12p payload: two pixels in three bytes, LSB first.
+__device__ __forceinline__ unsigned mono12p_at(const unsigned char *f, int width, int y, int x)
+{
+    const long long p = (long long)y * width + x;
+    const unsigned char *b = f + 3 * (p >> 1);
+    return (p & 1) ? ((unsigned)(b[1] >> 4) | ((unsigned)b[2] << 4)) : ((unsigned)b[0] | ((unsigned)(b[1] & 0x0F) << 8));
+}
+
+__global__ void decode_kernel(DecodeParams p)
+{
+    const long long npix = (long long)p.out_h * p.out_w;
+    const long long total = npix * p.n_frames;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(i / npix);
+        const long long o = i - (long long)k * npix;
+        const int oy = (int)(o / p.out_w), ox = (int)(o - (long long)oy * p.out_w);
+        // decoded image (before rotation) is dh x dw
+        const int dh = p.format == 1 ? p.height / 2 : p.height, dw = p.format == 1 ? p.width / 2 : p.width;
+        int sy, sx;                               // np.rot90(m, rot)[oy, ox] = m[sy, sx]
+        switch (p.rot) {
+        case 1: sy = ox; sx = dw - 1 - oy; break;
+        case 2: sy = dh - 1 - oy; sx = dw - 1 - ox; break;
+        case 3: sy = dh - 1 - ox; sx = oy; break;
+        default: sy = oy; sx = ox; break;
+        }
+        const unsigned char *f = p.raw + (long long)k * p.stride;
+        const unsigned char *d = nullptr;
+        if (p.dark) {
+            const int role = p.dark_frames == 2 ? (p.first_index + k - 1) % 2 : 0;
+            d = p.dark + (long long)role * p.dark_stride;
+        }
+        float v;
+        if (p.format == 0) {
+            unsigned a = mono12p_at(f, p.width, sy, sx);
+            if (d) {
+                const unsigned dd = mono12p_at(d, p.width, sy, sx);
+                a = (a > dd ? a : dd) - dd;
+            }
+            v = (float)a;
+        } else {
+            unsigned s = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const long long at = (long long)(2 * sy + (q >> 1)) * p.width + 2 * sx + (q & 1);
+                unsigned a = f[at];
+                if (d) {
+                    const unsigned dd = d[at];
+                    a = (a > dd ? a : dd) - dd;
+                }
+                s += a;
+            }
+            v = (float)s;                          // at most 1020: exact
+        }
+        p.out[(long long)k * p.out_stride + o] = v;
+    }
+}
+
+}  // namespace
+
+// Decode n_frames camera payloads (Mono12p = format 0, BayerRG8 = format 1, as the
+// PIVTOOLs Acquisition containers store them) into float32 frames: optional
+// in-run dark subtraction max(frame, dark) - dark per photosite in the sensor's
+// type (dark_frames 2: odd 1-based file indices take dark frame A, even ones B),
+// the BayerRG8 2x2 superpixel sum R+G+G+B, and the view rotation as np.rot90 turns
+// (0..3).  out_stride: elements between output frames.  Returns 0, or 1 for bad
+// arguments (odd Mono12p pixel count, odd Bayer geometry, short strides).
+PIV_EXPORT int pivb_decode_frames_dev(const unsigned char *raw, long long stride, int n_frames, int first_index,
+                                      int width, int height, int format, const unsigned char *dark,
+                                      long long dark_stride, int dark_frames, int rot, float *out,
+                                      long long out_stride, void *stream)
+{
+    if (!raw || !out || n_frames <= 0 || width <= 0 || height <= 0 || first_index < 1) return 1;
+    if (format != 0 && format != 1) return 1;
+    if (rot < 0 || rot > 3) return 1;
+    const long long npx = (long long)width * height;
+    const long long bytes = format == 0 ? npx / 2 * 3 : npx;
+    if (format == 0 && (npx & 1)) return 1;
+    if (format == 1 && ((width | height) & 1)) return 1;
+    if (stride < bytes) return 1;
+    if (dark && (dark_stride < bytes || (dark_frames != 1 && dark_frames != 2))) return 1;
+    const int dh = format == 1 ? height / 2 : height, dw = format == 1 ? width / 2 : width;
+    DecodeParams p{raw, stride, n_frames, first_index, width, height, format, dark, dark_stride, dark_frames, rot,
+                   (rot & 1) ? dw : dh, (rot & 1) ? dh : dw, out, out_stride};
+    if (out_stride < (long long)dh * dw) return 1;
+    const long long total = (long long)dh * dw * n_frames;
+    const long long want = (total + 255) / 256;
+    const unsigned grid = (unsigned)(want < 148 * 32 ? want : 148 * 32);
+    decode_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}

@@ -8,6 +8,7 @@ Python package).  The fixtures are committed; tests never need the reference.
     python tests/golden/make_golden.py            # peakfit_ref.npz, warp_ref.npz
     python tests/golden/make_golden.py kspace     # kspace_ref.npz
     python tests/golden/make_golden.py ensemble   # ensemble_ref.npz
+    python tests/golden/make_golden.py ingest     # ingest_ref.npz
 """
 
 from __future__ import annotations
@@ -270,6 +271,102 @@ def make_ensemble():
     print("ensemble_ref.npz written")
 
 
+def _load_reference_readers():
+    """The reference's readers package without its __init__ (which imports camera
+    SDKs absent here) and with the LZ4 binding stubbed (only the IM7 path uses it)."""
+    import importlib.util
+    import types
+
+    R = os.path.join(REF_ROOT, "pivtools_core/image_handling/readers")
+    for name, path in (("pivtools_core", os.path.join(REF_ROOT, "pivtools_core")),
+                       ("pivtools_core.image_handling", os.path.join(REF_ROOT, "pivtools_core/image_handling")),
+                       ("pivtools_core.image_handling.readers", R)):
+        m = types.ModuleType(name)
+        m.__path__ = [path]
+        sys.modules[name] = m
+    lz4 = types.ModuleType("lz4")
+    lz4b = types.ModuleType("lz4.block")
+    lz4.block = lz4b
+    sys.modules.setdefault("lz4", lz4)
+    sys.modules.setdefault("lz4.block", lz4b)
+    spec = importlib.util.spec_from_file_location("pivtools_core.image_handling.readers.pivraw_reader",
+                                                  os.path.join(R, "pivraw_reader.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _pack_mono12p(pix):
+    p = pix.reshape(-1, 2).astype(np.uint16)
+    b = np.empty((p.shape[0], 3), np.uint8)
+    b[:, 0] = p[:, 0] & 0xFF
+    b[:, 1] = ((p[:, 0] >> 8) & 0x0F) | ((p[:, 1] & 0x0F) << 4)
+    b[:, 2] = p[:, 1] >> 4
+    return b.ravel()
+
+
+def make_ingest():
+    """Fixtures for the payload decode of PIVTOOLs Acquisition containers, from
+    the reference's own _decode_into (pivraw_reader.py:938-960, which uses
+    set_reader.decode_mono12p), driven with minimal header objects over
+    temporary container files."""
+    import tempfile
+    from pathlib import Path
+    from types import SimpleNamespace
+
+    pr = _load_reference_readers()
+    rng = np.random.default_rng(21)
+    W, H, n = 20, 12, 4
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for fmt in ("Mono12p", "BayerRG8"):
+            if fmt == "Mono12p":
+                frames = rng.integers(0, 4096, (n, H, W))
+                dark = rng.integers(0, 300, (2, H, W))
+                pay = [_pack_mono12p(f) for f in frames]
+                dpay = [_pack_mono12p(d) for d in dark]
+            else:
+                frames = rng.integers(0, 256, (n, H, W))
+                dark = rng.integers(0, 40, (2, H, W))
+                pay = [f.astype(np.uint8).ravel() for f in frames]
+                dpay = [d.astype(np.uint8).ravel() for d in dark]
+            nbytes = pay[0].size
+            stride = -(-nbytes // 4096) * 4096
+            blob = np.zeros(n * stride, np.uint8)
+            dblob = np.zeros(2 * stride, np.uint8)
+            for k in range(n):
+                blob[k * stride:k * stride + nbytes] = pay[k]
+            for k in range(2):
+                dblob[k * stride:k * stride + nbytes] = dpay[k]
+            fpath = Path(tmp) / f"Camera1_{fmt}.pivraw"
+            dpath = Path(tmp) / f"dark_{fmt}.pivraw"
+            blob.tofile(fpath)
+            dblob.tofile(dpath)
+            for q in (fpath, dpath):
+                for ext in (".json", ".idx"):
+                    Path(str(q) + ext).write_text("{}")
+            shape = (H // 2, W // 2) if fmt == "BayerRG8" else (H, W)
+            hdr = SimpleNamespace(path=fpath, frame_stride=stride, bytes_per_frame=nbytes, pixel_format=fmt,
+                                  width=W, height=H, image_shape=shape, n_frames=n, mode="double_frame")
+            dhdr = SimpleNamespace(path=dpath, frame_stride=stride, bytes_per_frame=nbytes, pixel_format=fmt,
+                                   width=W, height=H, image_shape=shape, n_frames=2, mode="double_frame")
+            out[f"{fmt}_raw"] = blob
+            out[f"{fmt}_dark"] = dblob
+            out[f"{fmt}_stride"] = np.array(stride)
+            for view, k in pr.VIEW_ROTATIONS.items():
+                for with_dark in (0, 1):
+                    cam = SimpleNamespace(header=hdr, dark=dhdr if with_dark else None, view_rotation=view)
+                    oshape = (shape[1], shape[0]) if k % 2 else shape
+                    res = np.stack([np.empty(oshape, np.float32) for _ in range(n)])
+                    for idx in range(1, n + 1):
+                        pr._decode_into(cam, idx, res[idx - 1])
+                    out[f"{fmt}_{view}_{with_dark}"] = res
+    out["W"], out["H"], out["n"] = np.array(W), np.array(H), np.array(n)
+    np.savez_compressed(os.path.join(HERE, "ingest_ref.npz"), **out)
+    print("ingest_ref.npz written")
+
+
 if __name__ == "__main__":
     what = sys.argv[1:] or ["peakfit", "warp"]
     if "peakfit" in what:
@@ -280,3 +377,5 @@ if __name__ == "__main__":
         make_kspace()
     if "ensemble" in what:
         make_ensemble()
+    if "ingest" in what:
+        make_ingest()

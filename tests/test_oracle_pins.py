@@ -129,3 +129,20 @@ def test_ensemble_finalise_restatement_matches_reference_fixture(oracle):
             np.testing.assert_allclose(env, g[f"env_{wtype}_{n}"], rtol=1e-12, atol=1e-14)
     got = oracle.zero_plane_means(g["dc_in"].reshape(7, 16, 16)).ravel()
     np.testing.assert_allclose(got, g["dc_out"], rtol=0, atol=2e-6)
+
+
+ROTS = {"none": 0, "cw90": 3, "ccw90": 1, "180": 2}
+
+
+def test_ingest_decode_restatement_matches_reference_fixture(oracle):
+    """Mono12p / BayerRG8 payload decode with and without the in-run dark, every
+    view rotation, against the reference's own decode (fixture from
+    tests/golden/make_golden.py ingest)."""
+    g = np.load(os.path.join(GOLD, "ingest_ref.npz"))
+    W, H, n = int(g["W"]), int(g["H"]), int(g["n"])
+    for fi, fmt in enumerate(("Mono12p", "BayerRG8")):
+        for view, rot in ROTS.items():
+            for with_dark in (0, 1):
+                got = oracle.decode_frames(g[f"{fmt}_raw"], int(g[f"{fmt}_stride"]), n, 1, W, H, fi,
+                                           g[f"{fmt}_dark"] if with_dark else None, 2, rot)
+                assert np.array_equal(got, g[f"{fmt}_{view}_{with_dark}"]), (fmt, view, with_dark)
