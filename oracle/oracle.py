@@ -327,3 +327,52 @@ def decode_frames(raw, stride, n_frames, first_index, width, height, fmt, dark=N
             img = f.reshape(height // 2, 2, width // 2, 2).astype(np.float32).sum(axis=(1, 3))
         out.append(np.rot90(img, rot).astype(np.float32))
     return np.stack(out)
+
+
+# ---------------------------------------------------------------------------
+# Inter-pass outlier tests (pivtools_cli/piv/piv_backend/outlier_detection.py)
+# ---------------------------------------------------------------------------
+
+def median_outlier(ux, uy, eps=0.1, thr=2.0, size=5, masked=None):
+    """Normalised median, vector-norm form (outlier_detection.py:87-243): the
+    size x size neighbourhood without the node (grid edge and masked nodes
+    excluded), residual norm over the median of the neighbour residual norms plus
+    eps, non-finite residual flagged; 3x3 guard counting finite or masked cells
+    (fewer than 6 flags); masked nodes never flagged."""
+    ux = np.asarray(ux, np.float32)
+    uy = np.asarray(uy, np.float32)
+    ny, nx = ux.shape
+    if masked is not None:
+        masked = np.asarray(masked, bool)
+        ux = np.where(masked, np.float32(np.nan), ux)
+        uy = np.where(masked, np.float32(np.nan), uy)
+    h = size // 2
+    pu = np.pad(ux, h, constant_values=np.nan)
+    pv = np.pad(uy, h, constant_values=np.nan)
+    out = np.zeros((ny, nx), bool)
+    with np.errstate(all="ignore"):
+        for r in range(ny):
+            for c in range(nx):
+                wu = pu[r:r + size, c:c + size].ravel()
+                wv = pv[r:r + size, c:c + size].ravel()
+                k = size * size // 2
+                nu = np.delete(wu, k)
+                nv = np.delete(wv, k)
+                if np.all(np.isnan(nu)):
+                    mu = mv = np.nan
+                else:
+                    mu, mv = np.float32(np.nanmedian(nu)), np.float32(np.nanmedian(nv))
+                r0 = np.sqrt((ux[r, c] - mu) ** 2 + (uy[r, c] - mv) ** 2)
+                ri = np.sqrt((nu - mu) ** 2 + (nv - mv) ** 2)
+                rm = np.float32(np.nanmedian(ri)) if np.any(np.isfinite(ri)) else np.nan
+                nr = r0 / (rm + np.float32(eps))
+                out[r, c] = (not np.isfinite(nr)) or nr > thr
+        present = np.isfinite(ux) & np.isfinite(uy)
+        if masked is not None:
+            present |= masked
+        pp = np.pad(present.astype(np.int32), 1)
+        n_present = sum(pp[1 + dr:1 + dr + ny, 1 + dc:1 + dc + nx] for dr in (-1, 0, 1) for dc in (-1, 0, 1))
+        out |= n_present < 6
+        if masked is not None:
+            out &= ~masked
+    return out

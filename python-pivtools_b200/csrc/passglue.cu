@@ -102,9 +102,11 @@ __global__ void gate_kernel(ValParams p, int apply)
     p.invalid[i] = bad ? 1 : 0;
 }
 
-// Stage 2: normalised-median test on the gated field gx/gy (vector-norm
-// residual over the size x size neighbourhood without the node, 3x3 presence
-// guard), OR-ed with the stage-1 flags; invalid vectors become NaN.
+// Stage 2: normalised-median test (outlier_detection.py:87-243) on the gated
+// field gx/gy (vector-norm residual over the size x size neighbourhood without
+// the node, 3x3 presence guard), OR-ed with the stage-1 flags; invalid vectors
+// become NaN.  As in the reference, vectors that failed before the test enter it
+// as zeros, masked windows drop out of the medians and count as present.
 __global__ void median_kernel(ValParams p, const float *gx, const float *gy)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -126,15 +128,22 @@ __global__ void median_kernel(ValParams p, const float *gx, const float *gy)
         float a = qnanf(), b = qnanf();
         if (inside) {
             const bool mk = p.mask && p.mask[rr * p.nx + cc] != 0.0f;
-            if (!mk) { a = X[rr * p.nx + cc]; b = Y[rr * p.nx + cc]; }
-            if (abs(dr) <= 1 && abs(dc) <= 1 && (mk || a == a)) ++present;
+            if (!mk) {
+                a = X[rr * p.nx + cc];
+                b = Y[rr * p.nx + cc];
+                // the reference zeroes failed vectors before its outlier tests
+                // (cpu_instantaneous.py:627-629): they enter as 0, and are present
+                if (a != a || b != b) { a = 0.0f; b = 0.0f; }
+            }
+            if (abs(dr) <= 1 && abs(dc) <= 1) ++present;     // finite or masked
         }
         if (t == 12) continue;
         nu[t < 12 ? t : t - 1] = a;
         nvv[t < 12 ? t : t - 1] = b;
     }
     const float mu = median24(nu), mv = median24(nvv);
-    const float u0 = X[w], v0 = Y[w];
+    float u0 = X[w], v0 = Y[w];
+    if (u0 != u0 || v0 != v0) { u0 = 0.0f; v0 = 0.0f; }
     const float r0 = sqrtf((u0 - mu) * (u0 - mu) + (v0 - mv) * (v0 - mv));
     float ri[24];
 #pragma unroll
@@ -144,8 +153,8 @@ __global__ void median_kernel(ValParams p, const float *gx, const float *gy)
     const float nr = r0 / (rm + p.med_eps);
     const bool bad = p.invalid[i] || (nr > p.med_thr) || !isfinite(nr) || present < 6;
     p.invalid[i] = bad ? 1 : 0;
-    p.ux[i] = bad ? qnanf() : u0;
-    p.uy[i] = bad ? qnanf() : v0;
+    p.ux[i] = bad ? qnanf() : X[w];
+    p.uy[i] = bad ? qnanf() : Y[w];
 }
 
 // Harmonic inpainting: one CTA per pair, Jacobi sweeps over the invalid cells.

@@ -9,6 +9,7 @@ Python package).  The fixtures are committed; tests never need the reference.
     python tests/golden/make_golden.py kspace     # kspace_ref.npz
     python tests/golden/make_golden.py ensemble   # ensemble_ref.npz
     python tests/golden/make_golden.py ingest     # ingest_ref.npz
+    python tests/golden/make_golden.py validate   # validate_ref.npz
 """
 
 from __future__ import annotations
@@ -367,6 +368,49 @@ def make_ingest():
     print("ingest_ref.npz written")
 
 
+def make_validate():
+    """Fixtures for the inter-pass outlier tests from the reference's own
+    median_outlier_detection and peak_magnitude_detection
+    (pivtools_cli/piv/piv_backend/outlier_detection.py:62-243); its NaN-aware
+    median binding (bottleneck, absent here) is given NumPy's nanmedian, the
+    same statistic."""
+    import importlib.util
+    import types
+
+    bn = types.ModuleType("bottleneck")
+    bn.nanmedian = np.nanmedian
+    sys.modules.setdefault("bottleneck", bn)
+    path = os.path.join(REF_ROOT, "pivtools_cli/piv/piv_backend/outlier_detection.py")
+    spec = importlib.util.spec_from_file_location("ref_outlier_detection", path)
+    od = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(od)
+    rng = np.random.default_rng(17)
+    out = {}
+    for case in range(4):
+        ny, nx = 19, 27
+        ux = rng.normal(3.0, 0.3, (ny, nx)).astype(np.float32)
+        uy = rng.normal(-1.0, 0.3, (ny, nx)).astype(np.float32)
+        fail = rng.random((ny, nx)) < 0.04            # failed vectors, zeroed as the driver does
+        ux[fail] = 0.0
+        uy[fail] = 0.0
+        out_idx = rng.integers(0, ny * nx, 6)
+        ux.ravel()[out_idx] += rng.normal(0, 4, 6).astype(np.float32)
+        masked = np.zeros((ny, nx), bool)
+        if case >= 2:
+            masked[:, :3] = True
+            masked[8:11, 10:14] = True
+            ux[masked] = 0.0
+            uy[masked] = 0.0
+        pk = rng.uniform(0.05, 0.9, (ny, nx)).astype(np.float32)
+        for size in (3, 5):
+            out[f"c{case}_s{size}_median"] = od.median_outlier_detection(ux, uy, 0.1, 2.0, size,
+                                                                         masked=masked if case >= 2 else None)
+        out[f"c{case}_ux"], out[f"c{case}_uy"], out[f"c{case}_masked"], out[f"c{case}_pk"] = ux, uy, masked, pk
+        out[f"c{case}_peakmag"] = od.peak_magnitude_detection(pk, 0.25)
+    np.savez_compressed(os.path.join(HERE, "validate_ref.npz"), **out)
+    print("validate_ref.npz written")
+
+
 if __name__ == "__main__":
     what = sys.argv[1:] or ["peakfit", "warp"]
     if "peakfit" in what:
@@ -379,3 +423,5 @@ if __name__ == "__main__":
         make_ensemble()
     if "ingest" in what:
         make_ingest()
+    if "validate" in what:
+        make_validate()

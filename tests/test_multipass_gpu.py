@@ -24,42 +24,43 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-def _median_ref(ux, uy, eps, thr, size):
-    """Normalised median (vector norm, size x size without the node, 3x3 guard)."""
-    ny, nx = ux.shape
-    h = size // 2
-    out = np.zeros((ny, nx), bool)
-    for r in range(ny):
-        for c in range(nx):
-            nu, nv, present = [], [], 0
-            for dr in range(-h, h + 1):
-                for dc in range(-h, h + 1):
-                    rr, cc = r + dr, c + dc
-                    a = b = np.nan
-                    if 0 <= rr < ny and 0 <= cc < nx:
-                        a, b = ux[rr, cc], uy[rr, cc]
-                        if abs(dr) <= 1 and abs(dc) <= 1 and not np.isnan(a):
-                            present += 1
-                    if dr == 0 and dc == 0:
-                        continue
-                    nu.append(a)
-                    nv.append(b)
-            nu, nv = np.array(nu, np.float32), np.array(nv, np.float32)
-            if np.all(np.isnan(nu)):
-                out[r, c] = True
-                continue
-            mu, mv = np.nanmedian(nu), np.nanmedian(nv)
-            r0 = np.sqrt((ux[r, c] - mu) ** 2 + (uy[r, c] - mv) ** 2)
-            ri = np.sqrt((nu - mu) ** 2 + (nv - mv) ** 2)
-            rm = np.nanmedian(ri) if np.any(~np.isnan(ri)) else np.nan
-            nr = r0 / (rm + eps)
-            out[r, c] = (not np.isfinite(nr)) or nr > thr or present < 6
-    return out
-
-
-def test_validate_matches_restatement(cuda):
+def _validate(L, cuda, pk_x, pk_y, pk_h, pdy, pdx, mask, thr, size):
     import torch
 
+    N, ny, nx = pk_x.shape
+    ux = torch.empty((N, ny, nx), device=cuda)
+    uy = torch.empty_like(ux)
+    inv = torch.empty((N, ny, nx), dtype=torch.uint8, device=cuda)
+    work = torch.empty(2 * N * ny * nx, device=cuda)
+    T = [_t(a, cuda) for a in (pk_x, pk_y, pk_h)]
+    P = [None if a is None else _t(a, cuda) for a in (pdy, pdx, mask)]
+    assert L.pivb_validate_dev(T[0].data_ptr(), T[1].data_ptr(), T[2].data_ptr(),
+                               *[None if t is None else t.data_ptr() for t in P], N, ny, nx, thr, thr, 0.25, 0.1,
+                               2.0, size, ux.data_ptr(), uy.data_ptr(), inv.data_ptr(), work.data_ptr(),
+                               _stream()) == 0
+    torch.cuda.synchronize()
+    return inv.cpu().numpy().astype(bool), ux.cpu().numpy(), uy.cpu().numpy()
+
+
+def test_median_matches_reference_fixture(cuda):
+    """The GPU normalised-median test on the reference's own fixture fields
+    (outlier_detection.median_outlier_detection, tests/golden/validate_ref.npz)."""
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "validate_ref.npz"))
+    L = _lib.pass_lib()
+    for case in range(4):
+        ux, uy = g[f"c{case}_ux"][None], g[f"c{case}_uy"][None]
+        mask = g[f"c{case}_masked"].astype(np.float32) if case >= 2 else None
+        for size in (3, 5):
+            inv, _, _ = _validate(L, cuda, ux, uy, np.ones_like(ux), None, None, mask, 1e6, size)
+            assert np.array_equal(inv[0], g[f"c{case}_s{size}_median"]), (case, size)
+
+
+def test_validate_matches_restatement(oracle, cuda):
+    """Gate, predictor, peak magnitude and the median test on a field with failed
+    fits: failed and gated vectors enter the median test as zeros, as the
+    reference driver passes them (cpu_instantaneous.py:592-674)."""
     L = _lib.pass_lib()
     rng = np.random.default_rng(3)
     N, ny, nx = 2, 23, 31
@@ -68,24 +69,21 @@ def test_validate_matches_restatement(cuda):
     pk_h = rng.uniform(0.1, 0.9, (N, ny, nx)).astype(np.float32)
     pk_x[0, 5, 5] = 9.0            # gate
     pk_x[1, 7, 8] = np.nan          # failed fit
+    pk_x[1, 7, 9] = np.nan
     pk_x[0, 10, 10] += 3.0          # outlier
     pdx = rng.normal(4.0, 0.1, (N, ny, nx)).astype(np.float32)
     pdy = rng.normal(1.0, 0.1, (N, ny, nx)).astype(np.float32)
-    ux = torch.empty((N, ny, nx), device=cuda)
-    uy = torch.empty_like(ux)
-    inv = torch.empty((N, ny, nx), dtype=torch.uint8, device=cuda)
-    work = torch.empty(2 * N * ny * nx, device=cuda)
-    T = [_t(a, cuda) for a in (pk_x, pk_y, pk_h, pdy, pdx)]
-    assert L.pivb_validate_dev(T[0].data_ptr(), T[1].data_ptr(), T[2].data_ptr(), T[3].data_ptr(), T[4].data_ptr(),
-                               None, N, ny, nx, 8.0, 8.0, 0.25, 0.1, 2.0, 5, ux.data_ptr(), uy.data_ptr(),
-                               inv.data_ptr(), work.data_ptr(), _stream()) == 0
-    torch.cuda.synchronize()
-    gx = np.where((np.abs(pk_x) > 8) | (np.abs(pk_y) > 8), np.nan, pk_x) + pdx
-    gy = np.where((np.abs(pk_x) > 8) | (np.abs(pk_y) > 8), np.nan, pk_y) + pdy
+    inv, ux, uy = _validate(L, cuda, pk_x, pk_y, pk_h, pdy, pdx, None, 8.0, 5)
+    gate = (np.abs(pk_x) > 8) | (np.abs(pk_y) > 8)
+    gx = np.where(gate, np.nan, pk_x) + pdx
+    gy = np.where(gate, np.nan, pk_y) + pdy
     for n in range(N):
-        bad = np.isnan(gx[n]) | np.isnan(gy[n]) | (pk_h[n] < 0.25)
-        bad |= _median_ref(gx[n], gy[n], 0.1, 2.0, 5)
-        assert np.array_equal(inv[n].cpu().numpy().astype(bool), bad)
+        failed = np.isnan(gx[n]) | np.isnan(gy[n])
+        zx, zy = np.where(failed, 0.0, gx[n]), np.where(failed, 0.0, gy[n])
+        bad = failed | (pk_h[n] < 0.25) | oracle.median_outlier(zx, zy, 0.1, 2.0, 5)
+        assert np.array_equal(inv[n], bad)
+        ok = ~bad
+        assert np.array_equal(ux[n][ok], gx[n][ok]) and np.all(np.isnan(ux[n][bad]))
     assert inv[0, 5, 5] and inv[1, 7, 8] and inv[0, 10, 10]
 
 

@@ -146,3 +146,17 @@ def test_ingest_decode_restatement_matches_reference_fixture(oracle):
                 got = oracle.decode_frames(g[f"{fmt}_raw"], int(g[f"{fmt}_stride"]), n, 1, W, H, fi,
                                            g[f"{fmt}_dark"] if with_dark else None, 2, rot)
                 assert np.array_equal(got, g[f"{fmt}_{view}_{with_dark}"]), (fmt, view, with_dark)
+
+
+def test_median_outlier_restatement_matches_reference_fixture(oracle):
+    """Normalised-median outlier test against the reference's own function
+    (fixture from tests/golden/make_golden.py validate): zeroed failed vectors,
+    masked windows, sizes 3 and 5."""
+    g = np.load(os.path.join(GOLD, "validate_ref.npz"))
+    for case in range(4):
+        m = g[f"c{case}_masked"] if case >= 2 else None
+        for size in (3, 5):
+            got = oracle.median_outlier(g[f"c{case}_ux"], g[f"c{case}_uy"], 0.1, 2.0, size, masked=m)
+            assert np.array_equal(got, g[f"c{case}_s{size}_median"]), (case, size)
+        assert np.array_equal(g[f"c{case}_pk"] < 0.25, g[f"c{case}_peakmag"]) or \
+            np.array_equal((g[f"c{case}_pk"] < 0.25) | np.isnan(g[f"c{case}_pk"]), g[f"c{case}_peakmag"])
