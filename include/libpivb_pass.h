@@ -15,12 +15,17 @@ extern "C" {
 
 /* Gate (|d| > thresh), add the window-grid predictor (nullable), peak-magnitude
  * (peak_thr < 0 disables) and normalised-median (med_thr <= 0 disables;
- * med_size 3 or 5) tests.  ux/uy: NaN where invalid, 0 at masked windows.
+ * med_size 3 or 5) tests (cpu_instantaneous.py:575-760 with one peak,
+ * outlier_detection.py:56-243).  ux/uy: NaN where invalid, 0 at masked windows;
+ * invalid: 1 where the vector is to be infilled; nan_reason (nullable): int8
+ * codes of nan_reason_codes.py:18-25 (-1 masked, 0 valid, 1 fit failure,
+ * 6 large displacement, 9 unclassified, 10 outlier, 13 NaN peak height).
  * work: 2*N*ny*nx floats. */
 int pivb_validate_dev(const float *pk_x, const float *pk_y, const float *pk_h, const float *pred_dy,
                       const float *pred_dx, const float *mask, int N, int ny, int nx, float thresh_x,
                       float thresh_y, float peak_thr, float med_eps, float med_thr, int med_size,
-                      float *ux, float *uy, unsigned char *invalid, float *work, void *stream);
+                      float *ux, float *uy, unsigned char *invalid, signed char *nan_reason,
+                      float *work, void *stream);
 
 /* Harmonic inpainting of the invalid vectors in place (infilling.py:336-376).
  * work: 2*N*ny*nx floats. */

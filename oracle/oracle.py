@@ -376,3 +376,57 @@ def median_outlier(ux, uy, eps=0.1, thr=2.0, size=5, masked=None):
         if masked is not None:
             out &= ~masked
     return out
+
+
+NAN_MASKED, NAN_VALID, NAN_FIT_FAIL, NAN_LARGE_DISP = -1, 0, 1, 6
+NAN_UNCLASSIFIED, NAN_OUTLIER, NAN_PEAK_MAG_NAN = 9, 10, 13
+
+
+def pass_validation(pk_x, pk_y, pk_h, pred_dy, pred_dx, masked, thresh_x, thresh_y, peak_thr=0.25,
+                    med_eps=0.1, med_thr=2.0, med_size=5):
+    """One pass's validation of the primary peak for one pair, as the reference
+    driver runs it (cpu_instantaneous.py:575-760; single peak, no secondary-peak
+    substitution): masked windows and displacements beyond the gate are NaN-ed,
+    the predictor is added, the failed vectors enter the peak-magnitude and
+    normalised-median tests as zeros (outlier_detection.py:56-85, :87-243), NaN
+    peak heights fail, and each invalid vector gets the reason code of the first
+    stage that claimed it (nan_reason_codes.py:18-25).
+    Returns (ux, uy, nan_mask, nan_reason): ux/uy NaN where invalid, 0 at masked."""
+    x = np.asarray(pk_x, np.float32).copy()
+    y = np.asarray(pk_y, np.float32).copy()
+    h = np.asarray(pk_h, np.float32).copy()
+    ny, nx = x.shape
+    m = np.zeros((ny, nx), bool) if masked is None else np.asarray(masked, bool)
+    with np.errstate(invalid="ignore"):
+        large = (np.abs(x) > thresh_x) | (np.abs(y) > thresh_y)
+    fit_fail = np.isnan(x) | np.isnan(y)
+    gone = m | large
+    x[gone] = np.nan
+    y[gone] = np.nan
+    h[gone] = np.nan
+    if pred_dx is not None:
+        x = x + np.asarray(pred_dx, np.float32)
+        y = y + np.asarray(pred_dy, np.float32)
+    nan_mask = np.isnan(x) | np.isnan(y) | m
+    zx, zy = np.where(nan_mask, np.float32(0), x), np.where(nan_mask, np.float32(0), y)
+    reason = np.zeros((ny, nx), np.int8)
+    reason[fit_fail] = NAN_FIT_FAIL
+    reason[large] = NAN_LARGE_DISP
+    outlier = np.zeros((ny, nx), bool)
+    with np.errstate(invalid="ignore"):
+        if peak_thr >= 0:
+            outlier |= (h < peak_thr) | np.isnan(h)
+    if med_thr > 0:
+        outlier |= median_outlier(zx, zy, med_eps, med_thr, med_size, masked=m if masked is not None else None)
+    outlier &= ~m
+    nan_mask |= outlier
+    reason[outlier & (reason == NAN_VALID)] = NAN_OUTLIER
+    nan_mask |= np.isnan(h)
+    reason[np.isnan(h) & (reason == NAN_VALID)] = NAN_PEAK_MAG_NAN
+    reason[nan_mask & (reason == NAN_VALID)] = NAN_UNCLASSIFIED
+    reason[m] = NAN_MASKED
+    ux = np.where(nan_mask, np.float32(np.nan), zx).astype(np.float32)
+    uy = np.where(nan_mask, np.float32(np.nan), zy).astype(np.float32)
+    ux[m] = 0.0
+    uy[m] = 0.0
+    return ux, uy, nan_mask, reason

@@ -77,12 +77,21 @@ struct ValParams {
     int med_size;
     float *ux, *uy;                       // out: displacement, NaN where invalid, 0 at masked
     unsigned char *invalid;               // out: 1 where the vector must be infilled
+    signed char *reason;                  // out (nullable): why the vector is invalid (codes below)
+};
+
+// Invalid-vector reason codes (pivtools_cli/piv/piv_backend/nan_reason_codes.py:18-25).
+// The first stage that claims a vector keeps it; masked windows always read -1.
+enum : signed char {
+    kMasked = -1, kValid = 0, kFitFail = 1, kLargeDisp = 6, kUnclassified = 9, kOutlier = 10, kPeakMagNaN = 13
 };
 
 // Stage 1: gate + predictor.  ux/uy receive the gated field (NaN where the
 // correlation failed or the displacement gate fired, 0 at masked windows);
-// invalid additionally marks peak-magnitude failures.  With the median test off
-// the invalid vectors are NaN-ed here, otherwise by median_kernel.
+// invalid additionally marks peak-magnitude failures and NaN peak heights
+// (cpu_instantaneous.py:589-631, :728-732).  With the median test off the
+// invalid vectors are NaN-ed and their reasons completed here, otherwise by
+// median_kernel.
 __global__ void gate_kernel(ValParams p, int apply)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -91,15 +100,23 @@ __global__ void gate_kernel(ValParams p, int apply)
     const int w = (int)(i % ((long long)p.ny * p.nx));
     const bool masked = p.mask && p.mask[w] != 0.0f;
     float x = p.pk_x[i], y = p.pk_y[i], h = p.pk_h[i];
-    if (masked || fabsf(x) > p.thresh_x || fabsf(y) > p.thresh_y) { x = qnanf(); y = qnanf(); h = qnanf(); }
+    const bool fit_fail = (x != x) || (y != y);
+    const bool large = fabsf(x) > p.thresh_x || fabsf(y) > p.thresh_y;   // false for NaN
+    if (masked || large) { x = qnanf(); y = qnanf(); h = qnanf(); }
     if (p.pred_dx) { x += p.pred_dx[i]; y += p.pred_dy[i]; }
-    bool bad = (x != x) || (y != y);
-    if (p.peak_thr >= 0.0f && ((h < p.peak_thr) || (h != h))) bad = true;
+    const bool pk_fail = p.peak_thr >= 0.0f && ((h < p.peak_thr) || (h != h));
+    bool bad = (x != x) || (y != y) || pk_fail || (h != h);
     bad = bad && !masked;
     if (apply && bad) { x = qnanf(); y = qnanf(); }
     p.ux[i] = masked ? 0.0f : x;
     p.uy[i] = masked ? 0.0f : y;
     p.invalid[i] = bad ? 1 : 0;
+    if (p.reason) {
+        signed char rc = masked ? kMasked : fit_fail ? kFitFail : large ? kLargeDisp : kValid;
+        if (rc == kValid && pk_fail) rc = kOutlier;
+        if (apply && rc == kValid && bad) rc = (h != h) ? kPeakMagNaN : kUnclassified;
+        p.reason[i] = rc;
+    }
 }
 
 // Stage 2: normalised-median test (outlier_detection.py:87-243) on the gated
@@ -151,10 +168,17 @@ __global__ void median_kernel(ValParams p, const float *gx, const float *gy)
         ri[j] = sqrtf((nu[j] - mu) * (nu[j] - mu) + (nvv[j] - mv) * (nvv[j] - mv));
     const float rm = median24(ri);
     const float nr = r0 / (rm + p.med_eps);
-    const bool bad = p.invalid[i] || (nr > p.med_thr) || !isfinite(nr) || present < 6;
+    const bool outlier = (nr > p.med_thr) || !isfinite(nr) || present < 6;
+    const bool bad = p.invalid[i] || outlier;
     p.invalid[i] = bad ? 1 : 0;
     p.ux[i] = bad ? qnanf() : X[w];
     p.uy[i] = bad ? qnanf() : Y[w];
+    if (p.reason) {
+        signed char rc = p.reason[i];
+        if (rc == kValid && outlier) rc = kOutlier;
+        if (rc == kValid && bad) rc = (p.pk_h[i] != p.pk_h[i]) ? kPeakMagNaN : kUnclassified;
+        p.reason[i] = rc;
+    }
 }
 
 // Harmonic inpainting: one CTA per pair, Jacobi sweeps over the invalid cells.
@@ -355,16 +379,18 @@ inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t);
 
 // Validation of one pass for N pairs.  pred_* (nullable) is the window-grid
 // predictor added to the correlation result.  Outputs ux, uy (NaN = to infill,
-// 0 at masked windows) and invalid flags.  work: 2*N*ny*nx floats.
+// 0 at masked windows), invalid flags and (nullable) int8 reason codes.
+// work: 2*N*ny*nx floats.
 PIV_EXPORT int pivb_validate_dev(const float *pk_x, const float *pk_y, const float *pk_h, const float *pred_dy,
                                  const float *pred_dx, const float *mask, int N, int ny, int nx, float thresh_x,
                                  float thresh_y, float peak_thr, float med_eps, float med_thr, int med_size,
-                                 float *ux, float *uy, unsigned char *invalid, float *work, void *stream)
+                                 float *ux, float *uy, unsigned char *invalid, signed char *nan_reason,
+                                 float *work, void *stream)
 {
     if (N <= 0 || ny <= 0 || nx <= 0 || med_size < 3 || med_size > 5 || !(med_size & 1)) return 1;
     cudaStream_t s = (cudaStream_t)stream;
     ValParams p{pk_x, pk_y, pk_h, pred_dy, pred_dx, mask, N, ny, nx, thresh_x, thresh_y, peak_thr, med_eps,
-                med_thr, med_size, ux, uy, invalid};
+                med_thr, med_size, ux, uy, invalid, nan_reason};
     const long long nv = (long long)N * ny * nx;
     gate_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, med_thr > 0.0f ? 0 : 1);
     if (med_thr > 0.0f) {

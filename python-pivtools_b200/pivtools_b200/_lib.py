@@ -163,7 +163,7 @@ def pass_lib() -> ctypes.CDLL:
         return L
     fl = ctypes.c_float
     L.pivb_validate_dev.argtypes = [vp, vp, vp, vp, vp, vp, ci, ci, ci, fl, fl, fl, fl, fl, ci, vp, vp, vp, vp,
-                                    vp]
+                                    vp, vp]
     L.pivb_validate_dev.restype = ci
     L.pivb_infill_dev.argtypes = [vp, vp, vp, vp, ci, ci, ci, fl, fl, ci, fl, vp, vp]
     L.pivb_infill_dev.restype = ci

@@ -101,6 +101,7 @@ class MultipassPIV:
                 ux=torch.empty((N, ny, nx), dtype=f32, device=dev),
                 uy=torch.empty((N, ny, nx), dtype=f32, device=dev),
                 invalid=torch.empty((N, ny, nx), dtype=torch.uint8, device=dev),
+                reason=torch.empty((N, ny, nx), dtype=torch.int8, device=dev),
                 pdy=torch.empty((N, nyp, nxp), dtype=f32, device=dev),
                 pdx=torch.empty((N, nyp, nxp), dtype=f32, device=dev),
                 spacing=(float(g.grid.win_spacing_y), float(g.grid.win_spacing_x)),
@@ -137,6 +138,18 @@ class MultipassPIV:
             self._ok(self.Lx.pivb_correl_weight_dev(p["weight"].data_ptr(), p["win"], p["win"], p["cw"].data_ptr(), s),
                      "correlation weight")
         self.launches_per_step = self._count_launches()
+        self.planes = None
+        self._last_n = self.N
+
+    def keep_planes(self, on: bool = True):
+        """Keep every window's correlation plane of every pass on the device (the
+        reference's dump_correlation_planes, cpu_instantaneous.py:425-432):
+        N x n_windows x win^2 floats per pass, for save_corr_plane_dump."""
+        torch = self.torch
+        self.planes = None
+        if on:
+            self.planes = [torch.zeros((self.N, p["ny"], p["nx"], p["win"], p["win"]), dtype=torch.float32,
+                                       device=self.device) for p in self.passes]
 
     # ------------------------------------------------------------------ #
     def _stream(self):
@@ -193,7 +206,8 @@ class MultipassPIV:
                     p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win"],
                     p["win"], 0, 1, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(),
                     o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(),
-                    o["sxy"].data_ptr(), p["ratio"].data_ptr(), None, scr.data_ptr(), nbytes)
+                    o["sxy"].data_ptr(), p["ratio"].data_ptr(),
+                    None if self.planes is None else self.planes[k].data_ptr(), scr.data_ptr(), nbytes)
             if self.Ld is not None and p["win"] == 32:
                 self._ok(self.Ld.pivb_dft_xcorr_dev(*args, self.dft_status.data_ptr(), s), "correlation (tensor core)")
             else:
@@ -204,7 +218,7 @@ class MultipassPIV:
                 None if pred_dy is None else pred_dy.data_ptr(), None if pred_dx is None else pred_dx.data_ptr(),
                 None, N, p["ny"], p["nx"], thr, thr, cfg.peak_mag_threshold, cfg.median_epsilon,
                 cfg.median_threshold, cfg.median_size, p["ux"].data_ptr(), p["uy"].data_ptr(),
-                p["invalid"].data_ptr(), self.work.data_ptr(), s), "validate")
+                p["invalid"].data_ptr(), p["reason"].data_ptr(), self.work.data_ptr(), s), "validate")
             last = k + 1 == len(self.passes)
             if not last or cfg.final_infill:
                 self._ok(self.Lp.pivb_infill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), None,
@@ -215,8 +229,52 @@ class MultipassPIV:
                                                      p["nyp"], p["nxp"], p["pre"][0], p["pre"][1],
                                                      p["taps"].data_ptr(), p["radius"], p["pdy"].data_ptr(),
                                                      p["pdx"].data_ptr(), self.work.data_ptr(), s), "pad/smooth")
+        self._last_n = N
         last = self.passes[-1]
         return last["ux"], last["uy"]
+
+    def collect(self, n=None):
+        """Per-pair results of the last run, every pass, as host PIVResult objects
+        (the reference's PIVPassResult fields, cpu_instantaneous.py:875-910):
+        infilled ux/uy, nan_mask, nan_reason, peak_mag (NaN where gated),
+        peak_ratio, peak_choice, the predictor added on this pass, window grid.
+        With keep_planes on, each pass carries the correlation-plane payload."""
+        from .results import PIVPassResult, PIVResult
+
+        torch = self.torch
+        n = self._last_n if n is None else int(n)
+        torch.cuda.current_stream(self.device).synchronize()
+        out = [PIVResult() for _ in range(n)]
+        for k, (p, g) in enumerate(zip(self.passes, self.geo)):
+            ny, nx = p["ny"], p["nx"]
+            o = {key: v[:n].cpu().numpy() for key, v in p["out"].items()}
+            ux, uy = p["ux"][:n].cpu().numpy(), p["uy"][:n].cpu().numpy()
+            reason = p["reason"][:n].cpu().numpy()
+            nan_mask = p["invalid"][:n].cpu().numpy().astype(bool) | (reason == -1)
+            ratio = p["ratio"][:n].cpu().numpy()
+            if k > 0:
+                pred = torch.stack((p["pred_dy"][:n], p["pred_dx"][:n]), dim=-1).cpu().numpy()
+            else:
+                pred = np.zeros((n, ny, nx, 2), np.float32)
+            gone = (reason == -1) | (reason == 6)           # masked or gated: the reference NaNs their peaks
+            peak_mag = np.where(gone[:, None], np.float32(np.nan), o["pk_height"])
+            planes = None if self.planes is None else self.planes[k][:n].cpu().numpy()
+            for i in range(n):
+                pr = PIVPassResult(
+                    n_windows=np.array([ny, nx], dtype=np.int32), ux_mat=ux[i].copy(), uy_mat=uy[i].copy(),
+                    nan_mask=nan_mask[i].copy(), nan_reason=reason[i].copy(), peak_mag=peak_mag[i].copy(),
+                    peak_ratio=ratio[i].copy(), peak_choice=np.where(nan_mask[i], 0, 1).astype(np.intp),
+                    predictor_field=pred[i].copy(), b_mask=np.zeros((ny, nx), bool),
+                    window_size=tuple(self.cfg.window_sizes[k]), win_ctrs_x=g.grid.win_ctrs_x,
+                    win_ctrs_y=g.grid.win_ctrs_y)
+                if planes is not None:
+                    pr.debug_dump = {
+                        "planes": planes[i], "peak_finder": int(self.cfg.peak_finder),
+                        "pk_loc_x_raw": o["pk_loc_x"][i], "pk_loc_y_raw": o["pk_loc_y"][i],
+                        "pk_height_raw": o["pk_height"][i], "pk_ratio_raw": ratio[i], "sx": o["sx"][i],
+                        "sy": o["sy"][i], "sxy": o["sxy"][i]}
+                out[i].add_pass(pr)
+        return out
 
     def vectors_per_step(self) -> int:
         p = self.passes[-1]

@@ -10,6 +10,7 @@ Python package).  The fixtures are committed; tests never need the reference.
     python tests/golden/make_golden.py ensemble   # ensemble_ref.npz
     python tests/golden/make_golden.py ingest     # ingest_ref.npz
     python tests/golden/make_golden.py validate   # validate_ref.npz
+    python tests/golden/make_golden.py results    # results_in.npz, results_ref/
 """
 
 from __future__ import annotations
@@ -411,6 +412,86 @@ def make_validate():
     print("validate_ref.npz written")
 
 
+def results_inputs():
+    """Seeded per-pass fields of one pair over three passes (NaNs, masked windows,
+    values beyond the float16 range, every reason code)."""
+    rng = np.random.default_rng(23)
+    out = {}
+    for k, (ny, nx, win) in enumerate(((3, 4, 16), (4, 5, 8), (6, 7, 8))):
+        pre = f"p{k}_"
+        ux = rng.normal(2.0, 1.0, (ny, nx)).astype(np.float32)
+        uy = rng.normal(-1.0, 1.0, (ny, nx)).astype(np.float32)
+        ux[0, 0] = 7.0e4
+        uy[-1, -1] = -9.0e4
+        b_mask = np.zeros((ny, nx), bool)
+        b_mask[0, 1] = True
+        reason = rng.choice(np.array([0, 0, 0, 1, 6, 9, 10, 12, 13], np.int8), (ny, nx)).astype(np.int8)
+        reason[b_mask] = -1
+        nan_mask = reason != 0
+        ux[b_mask] = 0.0
+        uy[b_mask] = 0.0
+        pk_h = rng.uniform(0.0, 2.0, (1, ny, nx)).astype(np.float32)
+        pk_h[0][reason == 6] = np.nan
+        out.update({
+            pre + "ux": ux, pre + "uy": uy, pre + "b_mask": b_mask, pre + "nan_mask": nan_mask,
+            pre + "nan_reason": reason, pre + "peak_mag": pk_h,
+            pre + "peak_ratio": rng.uniform(1.0, 1.0e5, (ny, nx)).astype(np.float32),
+            pre + "peak_choice": np.where(nan_mask, 0, 1).astype(np.intp),
+            pre + "predictor": rng.normal(0, 3, (ny, nx, 2)).astype(np.float32),
+            pre + "win_ctrs_x": np.linspace(8, 8 + 16 * (nx - 1), nx, dtype=np.float32),
+            pre + "win_ctrs_y": np.linspace(8, 8 + 16 * (ny - 1), ny, dtype=np.float32),
+            pre + "window_size": np.array([win, win]),
+            pre + "planes": rng.normal(0, 1, (ny, nx, win, win)).astype(np.float32),
+            pre + "pk_loc_x_raw": rng.normal(0, 1, (1, ny, nx)).astype(np.float32),
+            pre + "pk_loc_y_raw": rng.normal(0, 1, (1, ny, nx)).astype(np.float32),
+            pre + "sx": rng.uniform(1, 2, (1, ny, nx)).astype(np.float32),
+            pre + "sy": rng.uniform(1, 2, (1, ny, nx)).astype(np.float32),
+            pre + "sxy": rng.normal(0, 0.1, (1, ny, nx)).astype(np.float32),
+        })
+    return out
+
+
+def make_results():
+    """Result files written by the reference's own writers
+    (pivtools_cli/piv/save_results.py:23-172) from seeded per-pass fields:
+    B00007.mat (full), B00008.mat (minimal, passes 1-2 only), B00007's
+    correlation-plane npz.  The inputs go to results_in.npz."""
+    import shutil
+
+    sys.path.insert(0, REF_ROOT)
+    from pivtools_cli.piv import save_results as sr
+    from pivtools_cli.piv.piv_result import PIVPassResult, PIVResult
+
+    d = results_inputs()
+    res = PIVResult()
+    for k in range(3):
+        g = lambda key: d[f"p{k}_{key}"]
+        ny, nx = g("ux").shape
+        res.add_pass(PIVPassResult(
+            n_windows=np.array([ny, nx], dtype=np.int32), ux_mat=g("ux"), uy_mat=g("uy"), nan_mask=g("nan_mask"),
+            nan_reason=g("nan_reason"), peak_mag=g("peak_mag"), peak_ratio=g("peak_ratio"),
+            peak_choice=g("peak_choice"), predictor_field=g("predictor"), b_mask=g("b_mask"),
+            window_size=[int(v) for v in g("window_size")], win_ctrs_x=g("win_ctrs_x"),
+            win_ctrs_y=g("win_ctrs_y"),
+            debug_dump={"planes": g("planes"), "peak_finder": 3, "pk_loc_x_raw": g("pk_loc_x_raw"),
+                        "pk_loc_y_raw": g("pk_loc_y_raw"), "pk_height_raw": g("peak_mag"),
+                        "pk_ratio_raw": g("peak_ratio"), "sx": g("sx"), "sy": g("sy"), "sxy": g("sxy")}))
+    out = os.path.join(HERE, "results_ref")
+    if os.path.isdir(out):
+        shutil.rmtree(out)
+    sr.save_piv_result_distributed(res, out, 7)
+    sr.save_piv_result_distributed(res, out, 8, runs_to_save=[1, 2], save_mode="minimal")
+    dump = sr.save_corr_plane_dump(res, out, 7)
+    # keep the arrays; of the two text entries keep only the label codes
+    z = dict(np.load(dump))
+    codes = sorted(int(c) for c in __import__("json").loads(str(z.pop("nan_reason_labels"))))
+    z.pop("pk_origin_note")
+    z["nan_reason_label_codes"] = np.array(codes, np.int64)
+    np.savez_compressed(dump, **z)
+    np.savez_compressed(os.path.join(HERE, "results_in.npz"), **d)
+    print("results_ref/ and results_in.npz written")
+
+
 if __name__ == "__main__":
     what = sys.argv[1:] or ["peakfit", "warp"]
     if "peakfit" in what:
@@ -425,3 +506,5 @@ if __name__ == "__main__":
         make_ingest()
     if "validate" in what:
         make_validate()
+    if "results" in what:
+        make_results()

@@ -24,22 +24,24 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
-def _validate(L, cuda, pk_x, pk_y, pk_h, pdy, pdx, mask, thr, size):
+def _validate(L, cuda, pk_x, pk_y, pk_h, pdy, pdx, mask, thr, size, peak_thr=0.25, med_thr=2.0, reasons=False):
     import torch
 
     N, ny, nx = pk_x.shape
     ux = torch.empty((N, ny, nx), device=cuda)
     uy = torch.empty_like(ux)
     inv = torch.empty((N, ny, nx), dtype=torch.uint8, device=cuda)
+    rc = torch.full((N, ny, nx), 99, dtype=torch.int8, device=cuda)
     work = torch.empty(2 * N * ny * nx, device=cuda)
     T = [_t(a, cuda) for a in (pk_x, pk_y, pk_h)]
     P = [None if a is None else _t(a, cuda) for a in (pdy, pdx, mask)]
     assert L.pivb_validate_dev(T[0].data_ptr(), T[1].data_ptr(), T[2].data_ptr(),
-                               *[None if t is None else t.data_ptr() for t in P], N, ny, nx, thr, thr, 0.25, 0.1,
-                               2.0, size, ux.data_ptr(), uy.data_ptr(), inv.data_ptr(), work.data_ptr(),
-                               _stream()) == 0
+                               *[None if t is None else t.data_ptr() for t in P], N, ny, nx, thr, thr, peak_thr, 0.1,
+                               med_thr, size, ux.data_ptr(), uy.data_ptr(), inv.data_ptr(),
+                               rc.data_ptr() if reasons else None, work.data_ptr(), _stream()) == 0
     torch.cuda.synchronize()
-    return inv.cpu().numpy().astype(bool), ux.cpu().numpy(), uy.cpu().numpy()
+    out = (inv.cpu().numpy().astype(bool), ux.cpu().numpy(), uy.cpu().numpy())
+    return out + (rc.cpu().numpy(),) if reasons else out
 
 
 def test_median_matches_reference_fixture(cuda):
@@ -85,6 +87,47 @@ def test_validate_matches_restatement(oracle, cuda):
         ok = ~bad
         assert np.array_equal(ux[n][ok], gx[n][ok]) and np.all(np.isnan(ux[n][bad]))
     assert inv[0, 5, 5] and inv[1, 7, 8] and inv[0, 10, 10]
+
+
+@pytest.mark.parametrize("peak_thr", [0.25, -1.0])
+@pytest.mark.parametrize("med_thr", [2.0, 0.0])
+@pytest.mark.parametrize("masked", [False, True])
+def test_validation_reason_codes(oracle, cuda, med_thr, masked, peak_thr):
+    """ux/uy, the invalid flags and the int8 reason codes of every stage against
+    the restatement of the reference driver's validation (fit failure, large
+    displacement, masked window, peak magnitude, median outlier, NaN peak height)."""
+    L = _lib.pass_lib()
+    rng = np.random.default_rng(11)
+    N, ny, nx = 3, 21, 26
+    pk_x = rng.normal(0.5, 0.3, (N, ny, nx)).astype(np.float32)
+    pk_y = rng.normal(-0.2, 0.3, (N, ny, nx)).astype(np.float32)
+    pk_h = rng.uniform(0.1, 0.9, (N, ny, nx)).astype(np.float32)
+    sel = lambda f: rng.random((N, ny, nx)) < f
+    pk_x[sel(0.03)] = np.nan                         # fit failures
+    pk_y[sel(0.02)] = 11.0                           # large displacement
+    pk_x[sel(0.03)] += 4.0                           # outliers
+    nanh = sel(0.02)
+    pk_h[nanh] = np.nan                              # NaN height with a finite location
+    pdx = rng.normal(2.0, 0.1, (N, ny, nx)).astype(np.float32)
+    pdy = rng.normal(-1.0, 0.1, (N, ny, nx)).astype(np.float32)
+    mask = None
+    if masked:
+        mask = np.zeros((ny, nx), np.float32)
+        mask[:, :2] = 1.0
+        mask[9:12, 12:15] = 1.0
+    inv, ux, uy, rc = _validate(L, cuda, pk_x, pk_y, pk_h, pdy, pdx, mask, 8.0, 5, peak_thr=peak_thr,
+                                med_thr=med_thr, reasons=True)
+    for n in range(N):
+        ox, oy, onan, orc = oracle.pass_validation(pk_x[n], pk_y[n], pk_h[n], pdy[n], pdx[n],
+                                                   None if mask is None else mask.astype(bool), 8.0, 8.0,
+                                                   peak_thr, 0.1, med_thr, 5)
+        m = np.zeros((ny, nx), bool) if mask is None else mask.astype(bool)
+        assert np.array_equal(rc[n], orc), (n, np.argwhere(rc[n] != orc)[:5])
+        assert np.array_equal(inv[n] | m, onan)
+        assert np.array_equal(ux[n], ox, equal_nan=True) and np.array_equal(uy[n], oy, equal_nan=True)
+    codes = set(np.unique(rc).tolist())
+    assert {0, 1, 6}.issubset(codes) and ((-1 in codes) == masked)
+    assert (10 in codes) == (peak_thr >= 0 or med_thr > 0) and (13 in codes) == (peak_thr < 0)
 
 
 def test_infill_harmonic_matches_sparse_solve(cuda):
@@ -219,6 +262,77 @@ def test_multipass_recovers_displacement(cuda, flow):
     gph.replay()
     torch.cuda.synchronize()
     assert torch.equal(ux, ref[0]) and torch.equal(uy, ref[1])
+
+
+@pytest.mark.parametrize("engine", ["fft", "dft"])
+def test_collect_and_result_files(cuda, oracle, tmp_path, engine):
+    """Per-pass results of a step: every pass's validation (reason codes, invalid
+    flags) against the restatement applied to that pass's raw peaks and predictor,
+    the kept planes against the raw peak positions, and the .mat / plane-dump
+    files read back."""
+    import scipy.io
+    import torch
+
+    from pivtools_b200 import results
+
+    H = W = 256
+    N = 2
+    pairs = [synthetic.particle_pair((H, W), seed=80 + k, flow="channel", flow_kwargs={"peak": 6.0})
+             for k in range(N)]
+    A = np.stack([p[0] for p in pairs])
+    B = np.stack([p[1] for p in pairs])
+    B[1, 96:160, 96:160] = np.random.default_rng(0).uniform(0, 1, (64, 64)).astype(np.float32)   # decorrelated patch
+    cfg = multipass.MultipassConfig(window_sizes=[(64, 64), (32, 32), (32, 32)], overlaps=[50, 50, 75],
+                                    engine_32=engine)
+    mp = multipass.MultipassPIV((H, W), N, cfg, device=cuda)
+    mp.keep_planes()
+    mp.run(torch.tensor(A, device=cuda), torch.tensor(B, device=cuda))
+    res = mp.collect()
+    assert len(res) == N and all(len(r.passes) == 3 for r in res)
+    n_invalid = 0
+    for n, r in enumerate(res):
+        for k, pr in enumerate(r.passes):
+            dd = pr.debug_dump
+            win = pr.window_size[0]
+            thr = win / 2.0 if k == 0 else win / 4.0
+            pred = pr.predictor_field
+            assert k > 0 or not pred.any()
+            _, _, onan, orc = oracle.pass_validation(dd["pk_loc_x_raw"][0], dd["pk_loc_y_raw"][0],
+                                                     dd["pk_height_raw"][0], pred[..., 0], pred[..., 1], None,
+                                                     thr, thr, cfg.peak_mag_threshold, cfg.median_epsilon,
+                                                     cfg.median_threshold, cfg.median_size)
+            assert np.array_equal(pr.nan_reason, orc), (n, k)
+            assert np.array_equal(pr.nan_mask, onan) and np.array_equal(pr.nan_mask, pr.nan_reason != 0)
+            assert np.array_equal(pr.peak_choice, (~pr.nan_mask).astype(np.intp))
+            assert np.isfinite(pr.ux_mat).all() and np.isfinite(pr.uy_mat).all()
+            assert np.array_equal(np.isnan(pr.peak_mag[0]), (pr.nan_reason == 6) | np.isnan(dd["pk_height_raw"][0]))
+            n_invalid += int(pr.nan_mask.sum())
+            # on valid windows the raw peak sits at the kept plane's largest 3x3
+            # local maximum inside the central half (the correlator's peak search);
+            # on failed ones a 3-point estimate over a flat peak can land far away
+            ok = pr.nan_reason == 0
+            P = dd["planes"]
+            q, h2 = win // 4, win // 2
+            core = P[..., q:q + h2, q:q + h2]
+            locmax = np.ones(core.shape, bool)
+            for a in (-1, 0, 1):
+                for b in (-1, 0, 1):
+                    locmax &= ~(P[..., q + a:q + a + h2, q + b:q + b + h2] > core)
+            cand = np.where(locmax & (core > 0), core, -1.0).reshape(core.shape[:2] + (h2 * h2,))
+            am = cand.argmax(axis=-1)
+            py, px = am // h2 + q - h2, am % h2 + q - h2
+            assert np.abs(px - dd["pk_loc_x_raw"][0])[ok].max() <= 1.0
+            assert np.abs(py - dd["pk_loc_y_raw"][0])[ok].max() <= 1.0
+    assert n_invalid > 0
+    path = results.save_piv_result_distributed(res[1], tmp_path, 2)
+    st = scipy.io.loadmat(path)["piv_result"]
+    assert st.shape == (1, 3)
+    for k, pr in enumerate(res[1].passes):
+        assert np.array_equal(st["ux"][0, k], results.to_half(pr.ux_mat))
+        assert np.array_equal(st["nan_reason"][0, k], pr.nan_reason)
+        assert np.array_equal(st["n_windows"][0, k].ravel(), pr.n_windows)
+    dump = np.load(results.save_corr_plane_dump(res[1], tmp_path, 2))
+    assert dump["pass2_planes"].shape == (res[1].passes[2].n_windows[0], res[1].passes[2].n_windows[1], 32, 32)
 
 
 def test_u16_to_f32_conversion(cuda):

@@ -160,3 +160,19 @@ def test_median_outlier_restatement_matches_reference_fixture(oracle):
             assert np.array_equal(got, g[f"c{case}_s{size}_median"]), (case, size)
         assert np.array_equal(g[f"c{case}_pk"] < 0.25, g[f"c{case}_peakmag"]) or \
             np.array_equal((g[f"c{case}_pk"] < 0.25) | np.isnan(g[f"c{case}_pk"]), g[f"c{case}_peakmag"])
+
+
+def test_pass_validation_outlier_stage_matches_reference_fixture(oracle):
+    """The outlier stage of the pass-validation restatement is the OR of the
+    reference's peak-magnitude and median tests with masked windows exempt, and
+    the reason codes follow the first claiming stage (fixture fields, no gate)."""
+    g = np.load(os.path.join(GOLD, "validate_ref.npz"))
+    for case in range(4):
+        m = g[f"c{case}_masked"] if case >= 2 else None
+        ux, uy, pk = g[f"c{case}_ux"], g[f"c{case}_uy"], g[f"c{case}_pk"]
+        _, _, nan_mask, reason = oracle.pass_validation(ux, uy, pk, None, None, m, 1e6, 1e6, 0.25, 0.1, 2.0, 5)
+        mk = np.zeros(ux.shape, bool) if m is None else m
+        flagged = (g[f"c{case}_s5_median"] | g[f"c{case}_peakmag"]) & ~mk
+        assert np.array_equal(nan_mask, flagged | mk)
+        assert np.array_equal(reason == 10, flagged) and np.array_equal(reason == -1, mk)
+        assert np.all(reason[~(flagged | mk)] == 0)
