@@ -83,6 +83,16 @@ int pivb_decode_frames_dev(const unsigned char *raw, long long stride, int n_fra
                            int height, int format, const unsigned char *dark, long long dark_stride, int dark_frames,
                            int rot, float *out, long long out_stride, void *stream);
 
+/* Coloured-floor regressor for the k-space fit (kspace_floor_psd.py:241-275 and
+ * single_pass_accumulator.py:836-880): P_win (n_win, hw) FP64 from the fraction
+ * grid P_grid (n_fracs, n_fracs, hw) FP64 indexed [fy][fx], fs (n_fracs) the
+ * ascending grid fractions, pred_dy / pred_dx (nullable together) the pass
+ * predictor on the window grid (float32; fractions |x - rint(x)| of x = pred / 2);
+ * bilinear, rounded through float32.  The caller rejects non-finite predictors. */
+int pivb_floor_interp_dev(const double *fs, int n_fracs, const double *P_grid, int hw,
+                          const float *pred_dy, const float *pred_dx, int n_win, double *P_win,
+                          void *stream);
+
 #ifdef __cplusplus
 }
 #endif

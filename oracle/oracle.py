@@ -430,3 +430,30 @@ def pass_validation(pk_x, pk_y, pk_h, pred_dy, pred_dx, masked, thresh_x, thresh
     ux[m] = 0.0
     uy[m] = 0.0
     return ux, uy, nan_mask, reason
+
+
+# ---------------------------------------------------------------------------
+# Coloured-floor lookup (pivtools_cli/piv/piv_backend/kspace_floor_psd.py:241-275)
+# ---------------------------------------------------------------------------
+
+def floor_fractions(pred):
+    """|x - round(x)| of x = pred / 2 in float32 (interpolation_noise_psd.py:191-204,
+    single_pass_accumulator.py:852-853)."""
+    x = np.asarray(pred, np.float32) / np.float32(2.0)
+    return np.abs(x - np.round(x))
+
+
+def floor_interp(fs, P_grid, fx, fy):
+    """Bilinear lookup of P_grid (nf, nf, h, w) [iy, ix] at per-window fractions,
+    rounded through float32 as the driver stores it: (n, h*w)."""
+    fx = np.asarray(fx, np.float64).ravel()
+    fy = np.asarray(fy, np.float64).ravel()
+    nf = len(fs)
+    ix = np.clip(np.searchsorted(fs, fx) - 1, 0, nf - 2)
+    iy = np.clip(np.searchsorted(fs, fy) - 1, 0, nf - 2)
+    tx = np.clip((fx - fs[ix]) / (fs[ix + 1] - fs[ix]), 0.0, 1.0)
+    ty = np.clip((fy - fs[iy]) / (fs[iy + 1] - fs[iy]), 0.0, 1.0)
+    Pf = np.asarray(P_grid, np.float64).reshape(nf, nf, -1)
+    out = (((1.0 - ty) * (1.0 - tx))[:, None] * Pf[iy, ix] + ((1.0 - ty) * tx)[:, None] * Pf[iy, ix + 1]
+           + (ty * (1.0 - tx))[:, None] * Pf[iy + 1, ix] + (ty * tx)[:, None] * Pf[iy + 1, ix + 1])
+    return out.astype(np.float32)

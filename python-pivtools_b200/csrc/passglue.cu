@@ -20,6 +20,8 @@
 // small vector grids, one launch per step for the whole batch of pairs.
 #include <math.h>
 
+#include <algorithm>
+
 #include "piv_common.cuh"
 
 namespace {
@@ -597,6 +599,61 @@ PIV_EXPORT int pivb_ensemble_finalize_dev(const float *sum_ab, const float *sum_
                 (float)n_pairs, n_win, h * w, (h / 2) * w + w / 2, dc_zero ? 1 : 0, out_aa, out_bb, out_ab, norm};
     const long long threads = (long long)n_win * 32;
     ensemble_finalize_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(p);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Coloured-floor regressor: per window the fractions fx = |x - rint(x)| of
+// x = pred_dx / 2 (float32; fy likewise), the grid cell by a left search of fs,
+// bilinear weights and the four-corner sum in FP64 without contraction, rounded
+// through float32 (kspace_floor_psd.py:241-275, single_pass_accumulator.py:852-880).
+__global__ void floor_interp_kernel(const double *fs, int nf, const double *grid, int hw, const float *pdy,
+                                    const float *pdx, long long n, double *out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long wdx = i / hw;
+        const int k = (int)(i - wdx * hw);
+        double f[2] = {0.0, 0.0};                 // fx, fy
+        if (pdx) {
+            const float xs = pdx[wdx] * 0.5f, ys = pdy[wdx] * 0.5f;
+            f[0] = (double)fabsf(xs - rintf(xs));
+            f[1] = (double)fabsf(ys - rintf(ys));
+        }
+        int c[2];
+        double t[2];
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+            int j = 0;
+            while (j < nf && fs[j] < f[a]) ++j;   // first fs[j] >= f
+            c[a] = min(max(j - 1, 0), nf - 2);
+            const double tt = (f[a] - fs[c[a]]) / (fs[c[a] + 1] - fs[c[a]]);
+            t[a] = fmin(fmax(tt, 0.0), 1.0);
+        }
+        const double ux = __dadd_rn(1.0, -t[0]), uy = __dadd_rn(1.0, -t[1]);
+        const double *g = grid + ((long long)c[1] * nf + c[0]) * hw + k;
+        const long long dx = hw, dy = (long long)nf * hw;
+        double s = __dmul_rn(__dmul_rn(uy, ux), g[0]);
+        s = __dadd_rn(s, __dmul_rn(__dmul_rn(uy, t[0]), g[dx]));
+        s = __dadd_rn(s, __dmul_rn(__dmul_rn(t[1], ux), g[dy]));
+        s = __dadd_rn(s, __dmul_rn(__dmul_rn(t[1], t[0]), g[dy + dx]));
+        out[i] = (double)__double2float_rn(s);
+    }
+}
+
+// P_win (n_win, hw) for the k-space fit's coloured floor from the fraction grid
+// P_grid (n_fracs, n_fracs, hw) [fy, fx] and the ascending fractions fs
+// (n_fracs >= 2); pred_dy / pred_dx (nullable together): the pass predictor on
+// the window grid, float32.  The fractions must lie in [fs[0], fs[n_fracs-1]].
+PIV_EXPORT int pivb_floor_interp_dev(const double *fs, int n_fracs, const double *P_grid, int hw,
+                                     const float *pred_dy, const float *pred_dx, int n_win, double *P_win,
+                                     void *stream)
+{
+    if (!fs || !P_grid || !P_win || n_fracs < 2 || hw <= 0 || n_win <= 0) return 1;
+    if ((pred_dy == nullptr) != (pred_dx == nullptr)) return 1;
+    const long long n = (long long)n_win * hw;
+    const unsigned nb = (unsigned)std::min<long long>((n + 255) / 256, 148LL * 16);
+    floor_interp_kernel<<<nb, 256, 0, (cudaStream_t)stream>>>(fs, n_fracs, P_grid, hw, pred_dy, pred_dx, n,
+                                                              P_win);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

@@ -188,13 +188,60 @@ class EnsemblePIV:
 
         return {k: ed.gather_rows(v, self.n_win, group) for k, v in fit.items()}
 
-    def fit(self, mask=None, use_kx4=0, use_ky4=0):
-        """k-space LM fit of the finalised planes (flat floor).  Returns device
-        tensors: gauss (n_win, 16) and status (n_win,), plus diagnostics."""
+    def floor_regressor(self, predictor=None, warp_kernel="lanczos"):
+        """Coloured-floor regressor P_win (n, h*w) FP64 on the device for the windows
+        of the finalised planes (kspace_floor_psd.py, single_pass_accumulator.py:814-887):
+        the P grid of this pass's chain (window weight, envelope when divided,
+        window-mean hole when the method removes window means) looked up per window
+        at the fractions of predictor / 2.  predictor: (n_win_y, n_win_x, 2) [dy, dx]
+        on the full window grid (None on a first pass: zero shift everywhere)."""
+        from . import floor_psd
+
+        torch = self.torch
+        dev = self.device
+        h, w = self.win
+        a, b = getattr(self, "block", (0, self.n_win))
+        n = b - a
+        pdy = pdx = None
+        nf = 2
+        if predictor is not None:
+            pr = torch.as_tensor(predictor, dtype=torch.float32, device=dev).reshape(self.n_win, 2)
+            if not bool(torch.isfinite(pr).all()):
+                raise ValueError("non-finite predictor: the coloured-floor fractions are undefined")
+            pdy, pdx = pr[a:b, 0].contiguous(), pr[a:b, 1].contiguous()
+            half = pr[a:b] * 0.5
+            if float((half - torch.round(half)).abs().max()) > 0.0:
+                nf = floor_psd.N_FRACS
+        hole = self.mean_subtract == 1
+        key = (nf, warp_kernel, hole)
+        cache = self.__dict__.setdefault("_p_grids", {})
+        if key not in cache:
+            env = self.env.cpu().numpy().astype(np.float64) if self.env is not None else np.ones((h, w))
+            fs, P = floor_psd.build_p_grid(env, warp_kernel, hole, self.weight.cpu().numpy(), n_fracs=nf)
+            cache[key] = (torch.tensor(fs, dtype=torch.float64, device=dev),
+                          torch.tensor(P, dtype=torch.float64, device=dev).contiguous())
+        fs_d, P_d = cache[key]
+        out = torch.empty((max(n, 1), h * w), dtype=torch.float64, device=dev)
+        if n > 0:
+            self._ok(self.Lp.pivb_floor_interp_dev(fs_d.data_ptr(), nf, P_d.data_ptr(), h * w,
+                                                   None if pdy is None else pdy.data_ptr(),
+                                                   None if pdx is None else pdx.data_ptr(), n, out.data_ptr(),
+                                                   self._stream()), "floor regressor")
+        return out[:n]
+
+    def fit(self, mask=None, use_kx4=0, use_ky4=0, floor="flat", predictor=None, warp_kernel="lanczos"):
+        """k-space LM fit of the finalised planes, flat or coloured noise floor
+        (`floor_regressor`).  Returns device tensors: gauss (n_win, 16) and status
+        (n_win,), plus diagnostics."""
         torch = self.torch
         dev = self.device
         h, w = self.win
         n = int(self.planes.shape[1])
+        if floor not in ("flat", "coloured"):
+            raise ValueError(f"kspace floor {floor!r} (valid: 'flat', 'coloured')")
+        if floor == "flat" and predictor is not None:
+            raise ValueError("a predictor only enters the coloured floor")
+        p_win = self.floor_regressor(predictor, warp_kernel) if floor == "coloured" else None
         m = (torch.zeros(n, dtype=torch.uint8, device=dev) if mask is None
              else torch.as_tensor(mask, dtype=torch.uint8, device=dev).reshape(n))
         o = {
@@ -210,7 +257,8 @@ class EnsemblePIV:
         sb = int(self.Lk.pivb_kspace_scratch_bytes(n, h, w))
         scratch = torch.empty(max(sb, 256), dtype=torch.uint8, device=dev)
         self._ok(self.Lk.pivb_kspace_fit_dev(
-            self.planes[0].data_ptr(), self.planes[1].data_ptr(), self.planes[2].data_ptr(), m.data_ptr(), None,
+            self.planes[0].data_ptr(), self.planes[1].data_ptr(), self.planes[2].data_ptr(), m.data_ptr(),
+            None if p_win is None else p_win.data_ptr(),
             n, h, w, use_kx4, use_ky4, o["gauss"].data_ptr(), o["status"].data_ptr(), o["init"].data_ptr(),
             o["gain"].data_ptr(), o["N0"].data_ptr(), o["b4x"].data_ptr(), o["b4y"].data_ptr(),
             o["cost_per_pt"].data_ptr(), o["n_valid"].data_ptr(), o["iters"].data_ptr(), o["conv"].data_ptr(),

@@ -11,6 +11,7 @@ Python package).  The fixtures are committed; tests never need the reference.
     python tests/golden/make_golden.py ingest     # ingest_ref.npz
     python tests/golden/make_golden.py validate   # validate_ref.npz
     python tests/golden/make_golden.py results    # results_in.npz, results_ref/
+    python tests/golden/make_golden.py floor      # floor_ref.npz
 """
 
 from __future__ import annotations
@@ -492,6 +493,38 @@ def make_results():
     print("results_ref/ and results_in.npz written")
 
 
+def make_floor():
+    """Coloured-floor P grids and the per-window lookup from the reference's own
+    build_P_grid / interp_P (pivtools_cli/piv/piv_backend/kspace_floor_psd.py:206-275)
+    on 16 x 16 windows, with the fractions the ensemble driver derives from a
+    float32 predictor (single_pass_accumulator.py:852-853)."""
+    sys.path.insert(0, REF_ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "python-pivtools_b200"))
+    from pivtools_cli.piv.piv_backend import kspace_floor_psd as K
+    from pivtools_cli.piv.piv_backend.interpolation_noise_psd import frac_distance
+    from pivtools_b200 import geometry
+    from pivtools_b200.ensemble import pair_envelope
+
+    rng = np.random.default_rng(31)
+    out = {}
+    cases = [("lanczos", True, "square"), ("lanczos", False, "gaussian"), ("cubic", True, "gaussian"),
+             ("cubic", False, "square")]
+    for ci, (kernel, hole, wt) in enumerate(cases):
+        w = geometry.window_weight((16, 16), wt).astype(np.float32)
+        env = pair_envelope(w, w, (16, 16)) if wt == "gaussian" else np.ones((16, 16))
+        fs, P = K.build_P_grid(env, kernel, hole, w, n_fracs=5)
+        out[f"c{ci}_w"], out[f"c{ci}_env"], out[f"c{ci}_fs"], out[f"c{ci}_P"] = w, env, fs, P
+    pdy = rng.normal(0.0, 3.0, 64).astype(np.float32)
+    pdx = rng.normal(0.0, 3.0, 64).astype(np.float32)
+    pdx[:8] = np.array([0.0, 1.0, -1.0, 0.5, -0.5, 0.25, 2.0, 3.0], np.float32)   # nodes and half steps
+    fx, fy = frac_distance(pdx / 2.0), frac_distance(pdy / 2.0)
+    out["pred_dy"], out["pred_dx"] = pdy, pdx
+    for ci in range(len(cases)):
+        out[f"c{ci}_Pwin"] = K.interp_P(out[f"c{ci}_fs"], out[f"c{ci}_P"], fx, fy).astype(np.float32)
+    np.savez_compressed(os.path.join(HERE, "floor_ref.npz"), **out)
+    print("floor_ref.npz written")
+
+
 if __name__ == "__main__":
     what = sys.argv[1:] or ["peakfit", "warp"]
     if "peakfit" in what:
@@ -508,3 +541,5 @@ if __name__ == "__main__":
         make_validate()
     if "results" in what:
         make_results()
+    if "floor" in what:
+        make_floor()

@@ -176,3 +176,20 @@ def test_pass_validation_outlier_stage_matches_reference_fixture(oracle):
         assert np.array_equal(nan_mask, flagged | mk)
         assert np.array_equal(reason == 10, flagged) and np.array_equal(reason == -1, mk)
         assert np.all(reason[~(flagged | mk)] == 0)
+
+
+def test_floor_grid_and_lookup_match_reference_fixture(oracle):
+    """Coloured-floor P grid (package builder) and per-window lookup (oracle
+    restatement) against the reference's build_P_grid / interp_P
+    (fixture from tests/golden/make_golden.py floor)."""
+    from pivtools_b200 import floor_psd
+
+    g = np.load(os.path.join(GOLD, "floor_ref.npz"))
+    cases = [("lanczos", True), ("lanczos", False), ("cubic", True), ("cubic", False)]
+    fx, fy = oracle.floor_fractions(g["pred_dx"]), oracle.floor_fractions(g["pred_dy"])
+    for ci, (kernel, hole) in enumerate(cases):
+        fs, P = floor_psd.build_p_grid(g[f"c{ci}_env"], kernel, hole, g[f"c{ci}_w"], n_fracs=5)
+        assert np.array_equal(fs, g[f"c{ci}_fs"])
+        np.testing.assert_allclose(P, g[f"c{ci}_P"], rtol=1e-13, atol=1e-13 * np.abs(P).max())
+        got = oracle.floor_interp(g[f"c{ci}_fs"], g[f"c{ci}_P"], fx, fy)
+        assert np.array_equal(got, g[f"c{ci}_Pwin"]), ci
