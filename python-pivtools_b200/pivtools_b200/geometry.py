@@ -52,6 +52,35 @@ def compute_window_centers(image_shape, window_size, overlap) -> WindowGrid:
     return WindowGrid(cx, cy, nx, ny, sx, sy)
 
 
+def compute_vector_masks(pixel_mask, image_shape, window_sizes, overlaps, threshold=0.5):
+    """Per-pass masked-window flags (n_win_y, n_win_x) from a boolean pixel mask
+    (H, W) (load_images.py:827-990, standard passes): a window is masked when the
+    masked pixels inside its footprint [floor(c - (w-1)/2 + 0.5),
+    floor(c + (w-1)/2 + 0.5)], clipped to the image, exceed threshold * h * w.
+    Counts come from an integral image (exact integers)."""
+    H, W = image_shape
+    m = np.asarray(pixel_mask, bool)
+    if m.shape != (H, W):
+        raise ValueError(f"pixel mask shape {m.shape} is not the image shape {(H, W)}")
+    S = np.zeros((H + 1, W + 1), np.int64)
+    S[1:, 1:] = np.cumsum(np.cumsum(m, axis=0, dtype=np.int64), axis=1)
+    out = []
+    for (wy, wx), ov in zip(window_sizes, overlaps):
+        g = compute_window_centers(image_shape, (wy, wx), ov)
+        hy, hx = (wy - 1) / 2.0, (wx - 1) / 2.0
+        cy = g.win_ctrs_y.astype(np.float64)
+        cx = g.win_ctrs_x.astype(np.float64)
+        y0 = np.clip(np.floor(cy - hy + 0.5).astype(np.int64), 0, H)
+        y1 = np.clip(np.floor(cy + hy + 0.5).astype(np.int64) + 1, 0, H)
+        x0 = np.clip(np.floor(cx - hx + 0.5).astype(np.int64), 0, W)
+        x1 = np.clip(np.floor(cx + hx + 0.5).astype(np.int64) + 1, 0, W)
+        cnt = (S[y1[:, None], x1[None, :]] - S[y0[:, None], x1[None, :]] - S[y1[:, None], x0[None, :]]
+               + S[y0[:, None], x0[None, :]])
+        ok = (y1 > y0)[:, None] & (x1 > x0)[None, :]
+        out.append(ok & (cnt / (wy * wx) > threshold))
+    return out
+
+
 def window_weight(wsize, window_type: str, sum_window=None) -> np.ndarray:
     """2-D correlation weighting window (base.py:52-134), float32."""
     m, n = wsize

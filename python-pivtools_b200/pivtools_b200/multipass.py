@@ -43,6 +43,8 @@ class MultipassConfig:
     infill_iters: int = 400
     infill_tol: float = 1e-3
     final_infill: bool = True
+    predictor_fill: str = "harmonic"  # masked windows in the predictor: "harmonic" or "none" (kept at 0)
+    predictor_fill_iters: int = 2000
     engine_32: str = "fft"          # 32 px passes: "fft" (FP32 FFT) or "dft" (tensor-core DFT-as-GEMM)
 
 
@@ -61,7 +63,12 @@ def _gauss_taps(sigma: float, ksize: int):
 class MultipassPIV:
     """Multipass PIV for batches of N pairs of one image size on one GPU."""
 
-    def __init__(self, image_shape, n_pairs: int, cfg: MultipassConfig | None = None, device=None):
+    def __init__(self, image_shape, n_pairs: int, cfg: MultipassConfig | None = None, device=None,
+                 vector_masks=None):
+        """vector_masks: per-pass boolean (n_win_y, n_win_x) masked-window flags
+        (geometry.compute_vector_masks), or None: masked windows are skipped by the
+        correlator, stored as 0 with reason -1, never infill donors, and filled in
+        the predictor (cpu_instantaneous.py:586-600, :836-850)."""
         import torch
 
         self.torch = torch
@@ -76,6 +83,10 @@ class MultipassPIV:
         self.Lp = _lib.pass_lib()
         if self.cfg.engine_32 not in ("fft", "dft"):
             raise ValueError(f"engine_32 {self.cfg.engine_32!r}")
+        if self.cfg.predictor_fill not in ("harmonic", "none"):
+            raise ValueError(f"predictor_fill {self.cfg.predictor_fill!r} (valid: 'harmonic', 'none')")
+        if vector_masks is not None and len(vector_masks) != len(self.geo):
+            raise ValueError(f"{len(vector_masks)} vector masks for {len(self.geo)} passes")
         self.Ld = _lib.dft_lib() if self.cfg.engine_32 == "dft" else None
         dev, f32 = self.device, torch.float32
         # device status word of the tensor-core engine (1 = an MMA completion was not observed)
@@ -95,9 +106,10 @@ class MultipassPIV:
                 ny=ny, nx=nx, nyp=nyp, nxp=nxp, win=g.window_size[0], weight=w, cw=cw,
                 cx=torch.tensor(g.grid.win_ctrs_x, device=dev), cy=torch.tensor(g.grid.win_ctrs_y, device=dev),
                 cx_all=torch.tensor(g.ctrs_x_all, device=dev), cy_all=torch.tensor(g.ctrs_y_all, device=dev),
-                out={k2: torch.empty((N, 1, ny, nx), dtype=f32, device=dev)
+                # zero-filled once: skipped (masked) windows are never written
+                out={k2: torch.zeros((N, 1, ny, nx), dtype=f32, device=dev)
                      for k2 in ("pk_loc_x", "pk_loc_y", "pk_height", "sx", "sy", "sxy")},
-                ratio=torch.empty((N, ny, nx), dtype=f32, device=dev),
+                ratio=torch.zeros((N, ny, nx), dtype=f32, device=dev),
                 ux=torch.empty((N, ny, nx), dtype=f32, device=dev),
                 uy=torch.empty((N, ny, nx), dtype=f32, device=dev),
                 invalid=torch.empty((N, ny, nx), dtype=torch.uint8, device=dev),
@@ -107,6 +119,18 @@ class MultipassPIV:
                 spacing=(float(g.grid.win_spacing_y), float(g.grid.win_spacing_x)),
                 pre=g.n_pre,
             )
+            bm = None if vector_masks is None else np.asarray(vector_masks[k], bool)
+            if bm is not None and bm.shape != (ny, nx):
+                raise ValueError(f"pass {k}: vector mask shape {bm.shape} != window grid {(ny, nx)}")
+            p["b_mask"] = np.zeros((ny, nx), bool) if bm is None else bm
+            p["mask"] = None
+            if bm is not None and bm.any():
+                if bm.all():
+                    raise ValueError(f"pass {k}: every window is masked")
+                p["mask"] = torch.tensor(bm.astype(np.float32), device=dev)
+                # (a broadcast view's astype keeps its odd strides: materialise C order)
+                p["mask_u8"] = torch.tensor(np.ascontiguousarray(np.broadcast_to(bm, (N, ny, nx)), dtype=np.uint8),
+                                            device=dev).contiguous()
             if k > 0:
                 p["map_x"] = torch.tensor(g.pred_map_x, device=dev)
                 p["map_y"] = torch.tensor(g.pred_map_y, device=dev)
@@ -126,6 +150,9 @@ class MultipassPIV:
             self.passes.append(p)
         self.scratch = torch.empty(max(max_scratch, 256), dtype=torch.uint8, device=dev)
         self.work = torch.empty(max(2 * max_vec, max_pad), dtype=f32, device=dev)
+        # predictor copies with the masked windows filled (the stored field keeps 0 there)
+        self.fill = (torch.empty((2, max_vec), dtype=f32, device=dev)
+                     if any(self._fills(k) for k in range(len(self.passes))) else None)
         # warp tables per pass (centres of the previous pass's padded grid)
         tb = int(self.Lw.pivb_warp_table_bytes(H, W))
         self.tables = [None] + [torch.empty(tb, dtype=torch.uint8, device=dev) for _ in self.geo[1:]]
@@ -160,9 +187,14 @@ class MultipassPIV:
         if code != 0:
             raise RuntimeError(f"{what} failed with code {code}")
 
+    def _fills(self, k):
+        return (k + 1 < len(self.passes) and self.passes[k]["mask"] is not None
+                and self.cfg.predictor_fill == "harmonic")
+
     def _count_launches(self):
         n = 0
         for k in range(len(self.geo)):
+            n += 1 if self._fills(k) else 0                  # predictor fill of masked windows
             n += 1                                        # correlation
             n += 1 if (3 <= self.cfg.peak_finder <= 6) else 0  # deferred fit (record kernel)
             n += 2 if self.cfg.median_threshold > 0 else 1  # validate (+ median)
@@ -202,7 +234,8 @@ class MultipassPIV:
                 pred_dy, pred_dx = p["pred_dy"], p["pred_dx"]
             o = p["out"]
             nbytes = scr.numel()
-            args = (fa.data_ptr(), fb.data_ptr(), H * W, None, H, W, N, p["cx"].data_ptr(), p["cy"].data_ptr(),
+            mptr = None if p["mask"] is None else p["mask"].data_ptr()
+            args = (fa.data_ptr(), fb.data_ptr(), H * W, mptr, H, W, N, p["cx"].data_ptr(), p["cy"].data_ptr(),
                     p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win"],
                     p["win"], 0, 1, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(),
                     o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(),
@@ -216,16 +249,28 @@ class MultipassPIV:
             self._ok(self.Lp.pivb_validate_dev(
                 o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(),
                 None if pred_dy is None else pred_dy.data_ptr(), None if pred_dx is None else pred_dx.data_ptr(),
-                None, N, p["ny"], p["nx"], thr, thr, cfg.peak_mag_threshold, cfg.median_epsilon,
+                mptr, N, p["ny"], p["nx"], thr, thr, cfg.peak_mag_threshold, cfg.median_epsilon,
                 cfg.median_threshold, cfg.median_size, p["ux"].data_ptr(), p["uy"].data_ptr(),
                 p["invalid"].data_ptr(), p["reason"].data_ptr(), self.work.data_ptr(), s), "validate")
             last = k + 1 == len(self.passes)
             if not last or cfg.final_infill:
-                self._ok(self.Lp.pivb_infill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), None,
+                self._ok(self.Lp.pivb_infill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), mptr,
                                                  N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
                                                  cfg.infill_iters, cfg.infill_tol, self.work.data_ptr(), s), "infill")
             if not last:
-                self._ok(self.Lp.pivb_pad_smooth_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), N, p["ny"], p["nx"],
+                src_x, src_y = p["ux"], p["uy"]
+                if self._fills(k):
+                    # harmonic fill of the masked windows, every other window fixed
+                    # (infilling.py:808-874 with the harmonic least-squares fill)
+                    nv = N * p["ny"] * p["nx"]
+                    src_x, src_y = self.fill[0, :nv], self.fill[1, :nv]
+                    src_x.copy_(p["ux"].reshape(-1)[:nv])
+                    src_y.copy_(p["uy"].reshape(-1)[:nv])
+                    self._ok(self.Lp.pivb_infill_dev(src_x.data_ptr(), src_y.data_ptr(), p["mask_u8"].data_ptr(),
+                                                     None, N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
+                                                     cfg.predictor_fill_iters, cfg.infill_tol, self.work.data_ptr(),
+                                                     s), "predictor fill")
+                self._ok(self.Lp.pivb_pad_smooth_dev(src_x.data_ptr(), src_y.data_ptr(), N, p["ny"], p["nx"],
                                                      p["nyp"], p["nxp"], p["pre"][0], p["pre"][1],
                                                      p["taps"].data_ptr(), p["radius"], p["pdy"].data_ptr(),
                                                      p["pdx"].data_ptr(), self.work.data_ptr(), s), "pad/smooth")
@@ -264,7 +309,7 @@ class MultipassPIV:
                     n_windows=np.array([ny, nx], dtype=np.int32), ux_mat=ux[i].copy(), uy_mat=uy[i].copy(),
                     nan_mask=nan_mask[i].copy(), nan_reason=reason[i].copy(), peak_mag=peak_mag[i].copy(),
                     peak_ratio=ratio[i].copy(), peak_choice=np.where(nan_mask[i], 0, 1).astype(np.intp),
-                    predictor_field=pred[i].copy(), b_mask=np.zeros((ny, nx), bool),
+                    predictor_field=pred[i].copy(), b_mask=p["b_mask"].copy(),
                     window_size=tuple(self.cfg.window_sizes[k]), win_ctrs_x=g.grid.win_ctrs_x,
                     win_ctrs_y=g.grid.win_ctrs_y)
                 if planes is not None:
@@ -295,11 +340,12 @@ class HostPipeline:
     chunk's final field is read back right after its last pass.
     """
 
-    def __init__(self, image_shape, chunk: int, cfg: MultipassConfig | None = None, device=None):
+    def __init__(self, image_shape, chunk: int, cfg: MultipassConfig | None = None, device=None,
+                 vector_masks=None):
         import torch
 
         self.torch = torch
-        self.mp = MultipassPIV(image_shape, chunk, cfg, device)
+        self.mp = MultipassPIV(image_shape, chunk, cfg, device, vector_masks)
         dev = self.mp.device
         H, W = image_shape
         self.C = chunk

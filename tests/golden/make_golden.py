@@ -12,6 +12,7 @@ Python package).  The fixtures are committed; tests never need the reference.
     python tests/golden/make_golden.py validate   # validate_ref.npz
     python tests/golden/make_golden.py results    # results_in.npz, results_ref/
     python tests/golden/make_golden.py floor      # floor_ref.npz
+    python tests/golden/make_golden.py vmask      # vmask_ref.npz
 """
 
 from __future__ import annotations
@@ -525,6 +526,41 @@ def make_floor():
     print("floor_ref.npz written")
 
 
+def make_vmask():
+    """Per-pass vector masks from the reference's own compute_vector_mask
+    (pivtools_core/image_handling/load_images.py:827-990), compiled on its own
+    with the reference's window_utils; its image-shape guard is skipped (the
+    fixture masks have the image shape)."""
+    import logging
+    from types import SimpleNamespace
+
+    sys.path.insert(0, REF_ROOT)
+    from pivtools_core import window_utils as wu
+
+    (cvm,) = _reference_functions(os.path.join(REF_ROOT, "pivtools_core/image_handling/load_images.py"),
+                                  ["compute_vector_mask"])
+    cvm.__globals__.update(logging=logging, compute_window_centers=wu.compute_window_centers,
+                           compute_window_centers_single_mode=wu.compute_window_centers_single_mode,
+                           require_mask_fits_camera=lambda *a, **k: None, List=list)
+    rng = np.random.default_rng(41)
+    out = {}
+    ws, ov = [(64, 64), (32, 32), (16, 16)], [50, 50, 75]
+    for ci, (H, W) in enumerate(((512, 384), (300, 257))):
+        pm = np.zeros((H, W), bool)
+        pm[100:180, 50:200] = True
+        yy, xx = np.mgrid[:H, :W]
+        pm |= (yy - 0.6 * H) ** 2 + (xx - 0.3 * W) ** 2 < 40 ** 2
+        pm[rng.random((H, W)) < 0.02] = True
+        out[f"c{ci}_pixel_mask"] = pm
+        for ti, thr in enumerate((0.0, 0.5, 0.9)):
+            cfg = SimpleNamespace(image_shape_for=lambda cam, H=H, W=W: (H, W), mask_threshold=thr, num_passes=3,
+                                  window_sizes=ws, overlap=ov, ensemble_piv=False)
+            for k, vm in enumerate(cvm(pm, cfg, 1, ensemble=False)):
+                out[f"c{ci}_t{ti}_p{k}"] = vm
+    np.savez_compressed(os.path.join(HERE, "vmask_ref.npz"), **out)
+    print("vmask_ref.npz written")
+
+
 if __name__ == "__main__":
     what = sys.argv[1:] or ["peakfit", "warp"]
     if "peakfit" in what:
@@ -543,3 +579,5 @@ if __name__ == "__main__":
         make_results()
     if "floor" in what:
         make_floor()
+    if "vmask" in what:
+        make_vmask()

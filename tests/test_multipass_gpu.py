@@ -335,6 +335,54 @@ def test_collect_and_result_files(cuda, oracle, tmp_path, engine):
     assert dump["pass2_planes"].shape == (res[1].passes[2].n_windows[0], res[1].passes[2].n_windows[1], 32, 32)
 
 
+@pytest.mark.parametrize("engine", ["fft", "dft"])
+def test_multipass_with_vector_masks(cuda, oracle, engine):
+    """Masked windows (from a pixel mask, geometry.compute_vector_masks) are
+    skipped, stored as 0 with reason -1 and kept out of the infill; the
+    predictor is filled across them, so the next pass's predictor there follows
+    the flow instead of the stored zeros; every pass's reason codes equal the
+    restatement given the mask."""
+    import torch
+
+    H = W = 384
+    N = 2
+    pairs = [synthetic.particle_pair((H, W), seed=120 + k, flow="uniform", flow_kwargs={"u": 3.3, "v": -1.7})
+             for k in range(N)]
+    A = torch.tensor(np.stack([p[0] for p in pairs]), device=cuda)
+    B = torch.tensor(np.stack([p[1] for p in pairs]), device=cuda)
+    pm = np.zeros((H, W), bool)
+    pm[140:250, 100:210] = True
+    cfg = multipass.MultipassConfig(window_sizes=[(64, 64), (32, 32), (32, 32)], overlaps=[50, 50, 75],
+                                    engine_32=engine)
+    vm = geometry.compute_vector_masks(pm, (H, W), cfg.window_sizes, cfg.overlaps, 0.5)
+    assert all(m.any() for m in vm)
+    mp = multipass.MultipassPIV((H, W), N, cfg, device=cuda, vector_masks=vm)
+    ux, uy = mp.run(A, B)
+    res = mp.collect()
+    for n, r in enumerate(res):
+        for k, pr in enumerate(r.passes):
+            m = vm[k]
+            assert np.array_equal(pr.b_mask, m)
+            assert np.all(pr.nan_reason[m] == -1) and np.all(pr.nan_reason[~m] != -1)
+            assert np.all(pr.ux_mat[m] == 0) and np.all(pr.uy_mat[m] == 0)
+            assert np.isfinite(pr.ux_mat).all()
+            thr = pr.window_size[0] / 2.0 if k == 0 else pr.window_size[0] / 4.0
+            pred = pr.predictor_field
+            raw = mp.passes[k]["out"]
+            _, _, onan, orc = oracle.pass_validation(
+                raw["pk_loc_x"][n, 0].cpu().numpy(), raw["pk_loc_y"][n, 0].cpu().numpy(),
+                raw["pk_height"][n, 0].cpu().numpy(), pred[..., 0], pred[..., 1], m, thr, thr,
+                cfg.peak_mag_threshold, cfg.median_epsilon, cfg.median_threshold, cfg.median_size)
+            assert np.array_equal(pr.nan_reason, orc), (n, k)
+            if k > 0:
+                # the predictor under the mask follows the flow (filled), not 0
+                assert np.abs(pred[m][:, 1] - 3.3).max() < 0.3 and np.abs(pred[m][:, 0] + 1.7).max() < 0.3
+        fin = r.passes[-1]
+        ok = ~vm[-1]
+        err = np.hypot(fin.ux_mat[ok] - 3.3, fin.uy_mat[ok] + 1.7)
+        assert np.sqrt(np.mean(err ** 2)) < 0.1
+
+
 def test_u16_to_f32_conversion(cuda):
     import torch
 

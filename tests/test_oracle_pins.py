@@ -193,3 +193,18 @@ def test_floor_grid_and_lookup_match_reference_fixture(oracle):
         np.testing.assert_allclose(P, g[f"c{ci}_P"], rtol=1e-13, atol=1e-13 * np.abs(P).max())
         got = oracle.floor_interp(g[f"c{ci}_fs"], g[f"c{ci}_P"], fx, fy)
         assert np.array_equal(got, g[f"c{ci}_Pwin"]), ci
+
+
+def test_vector_masks_match_reference_fixture():
+    """Per-pass masked-window flags from a pixel mask against the reference's
+    compute_vector_mask (fixture from tests/golden/make_golden.py vmask)."""
+    from pivtools_b200 import geometry
+
+    g = np.load(os.path.join(GOLD, "vmask_ref.npz"))
+    for ci in range(2):
+        pm = g[f"c{ci}_pixel_mask"]
+        for ti, thr in enumerate((0.0, 0.5, 0.9)):
+            got = geometry.compute_vector_masks(pm, pm.shape, [(64, 64), (32, 32), (16, 16)], [50, 50, 75], thr)
+            for k in range(3):
+                ref = g[f"c{ci}_t{ti}_p{k}"]
+                assert ref.any() and np.array_equal(got[k], ref), (ci, thr, k)
