@@ -167,7 +167,7 @@ __device__ __forceinline__ void lane_combine_fwd_tab(float2 (&y)[M], int p, cons
     static_assert(P == 4, "table combine is the four-lane form");
 #pragma unroll
     for (int k = 1; k < M; ++k) {
-        const float2 w = tw[p * M + k];
+        const float2 w = tw[p * (M + 1) + k];     // rows padded to M + 1 entries
         const float2 v = y[k];
         y[k] = make_float2(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
     }

@@ -38,7 +38,11 @@ struct WinGeo {
     static constexpr int T = N * P;                                     // active threads per window
     static constexpr int GW = (T <= 8) ? 8 : (T <= 16) ? 16 : (T <= 32) ? 32 : T;  // lanes per group
     static constexpr int WPW = (GW <= 32) ? 32 / GW : 1;                // windows per warp
-    static constexpr int ST = N + ((P == 1) ? 1 : (P == 2 ? 2 : 4));    // complex row stride
+    // complex row stride.  Four lanes add one slot per 32-column block (the skew
+    // in correlate_plane) plus a margin that keeps rows 8 banks apart.  (An odd
+    // stride would also clear the row-phase conflicts of two lanes, but costs the
+    // 64 px kernel registers and 6% time: measured.)
+    static constexpr int ST = N + ((P == 1) ? 1 : (P == 2 ? 2 : (N == 128 ? 4 : 6)));
     static constexpr int STF = N + 1;                                   // float row stride
     static constexpr int WARPS_PER_CTA = (GW <= 32) ? 4 : GW / 32;
     static constexpr int CTA_THREADS = WARPS_PER_CTA * 32;
@@ -48,8 +52,10 @@ struct WinGeo {
     static constexpr int PLANE_BYTES = N * ST * 8;
     static constexpr int RED_SLOTS = (GW > 32) ? GW / 32 : 1;
     static constexpr int RED_BYTES = 64 * RED_SLOTS * 4 + 64;
-    // lane twiddles W_N^{p k} for the four-lane combine (forward sign), float2 [P][M]
-    static constexpr int TW_BYTES = (P == 4) ? P * M * 8 : 0;
+    // lane twiddles W_N^{p k} for the four-lane combine (forward sign), float2
+    // [P][M + 1]: the padded row puts the four lanes' entries on distinct banks
+    static constexpr int TW_LD = M + 1;
+    static constexpr int TW_BYTES = (P == 4) ? P * TW_LD * 8 : 0;
     static constexpr int SMEM_BYTES = GROUPS_PER_CTA * PLANE_BYTES + RED_BYTES + TW_BYTES;
     static_assert(N * STF * 4 <= PLANE_BYTES, "float plane must alias the complex plane");
 };
@@ -276,7 +282,7 @@ __device__ __forceinline__ void fill_lane_twiddles(float2 *tw, int tid, int nthr
             const int pp = i / G::M, k = i % G::M;
             double sn, cs;
             sincospi(2.0 * (double)(pp * k) / (double)N, &sn, &cs);
-            tw[i] = make_float2((float)cs, (float)(-sn));
+            tw[pp * G::TW_LD + k] = make_float2((float)cs, (float)(-sn));
         }
     }
 }
@@ -293,18 +299,21 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
     lane_slot<N>(active ? g.t : 0, line, p);
     const int q = out_block<P>(p);
     const int rm = (N - line) % N;
-    // Complex plane element (row, col) lives at row * ST + (col + rot(row)) % N: with
-    // four lanes per column each block of M rows is rotated by SH = 4 columns, so
-    // that the column-phase stores of one half-warp (4 lines from each of the 4
-    // blocks) fall on distinct banks instead of all blocks on the same ones.  (With
-    // two lanes the extra address registers cost more than the conflicts: measured.)
+    // Complex plane element (row, col) lives at row * ST + c + c / 32 with
+    // c = (col + rot(row)) % N: with four lanes per column each block of M rows is
+    // rotated by SH = 4 columns, so that the column-phase stores of one half-warp
+    // (4 lines from each of the 4 blocks) fall on distinct banks, and each block of
+    // 32 columns is skewed by one slot, so that the row-phase stores (the 4 lanes of
+    // a line write columns 32 apart) do too.
     constexpr int SH = (P == 4) ? 4 : 0;
     constexpr bool POW2 = (N & (N - 1)) == 0;
     // blk = row / M, known at each call site
     auto at = [&](int row, int blk, int col) {
         if constexpr (SH == 0) return row * ST + col;
-        else if constexpr (POW2) return row * ST + ((col + SH * blk) & (N - 1));
-        else return row * ST + (col + SH * blk) % N;
+        else {
+            const int c = POW2 ? ((col + SH * blk) & (N - 1)) : (col + SH * blk) % N;
+            return row * ST + c + (c >> 5);
+        }
     };
     const int lb = line / M, rb = rm / M;
     float2 z[M];
