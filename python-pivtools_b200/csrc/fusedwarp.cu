@@ -187,7 +187,7 @@ struct WarpParams {
 // Output rows per thread.  The rows of one thread share the column-side work
 // (predictor column weights and indices) and, while they fall in the same
 // predictor cell row, the 4x4 predictor patch, which stays in registers.
-constexpr int kWarpRows = 4;
+constexpr int kWarpRows = 8;
 
 template <int MODE, int IMPL>
 __global__ void __launch_bounds__(256) warp_kernel(WarpParams p)
