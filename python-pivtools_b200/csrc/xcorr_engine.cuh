@@ -379,20 +379,45 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
 
 // Parallel Westerweel search + detectability over the plane in shared memory.
 // Returns, in every lane, the accumulator and whether a NaN was seen.
+// The candidates (rows and columns [N/4, 3N/4); a value above zero that no
+// neighbour of its 3x3 block exceeds) are taken in vertical strips of up to 8
+// rows of one column, rolling the maxima of three consecutive 3-wide rows: 3
+// loads per row of the strip instead of 9 per candidate.  PeakAcc's result
+// does not depend on the order in which candidates arrive.  A plane holding
+// NaN sets the flag (over the same neighbourhoods) and is searched again by
+// the caller's exact sequential scan, so only NaN-free planes rely on the
+// maximum form of the test.
 template <int N>
 __device__ __forceinline__ void search_plane(const Group<N> &g, const float *pl, PeakAcc &acc, bool &has_nan)
 {
     using G = WinGeo<N>;
-    constexpr int H2 = N / 2, NC = H2 * H2;
-    PlaneView v{pl, G::STF};
+    constexpr int H2 = N / 2, Q = N / 4, S = (H2 < 8) ? H2 : 8;
+    constexpr int NS = (H2 + S - 1) / S, U = H2 * NS;
     acc.init();
     bool nan = false;
     if (g.t < G::T) {
 #pragma unroll 1
-        for (int c = g.t; c < NC; c += G::T) {
-            const int i = N / 4 + c / H2, j = N / 4 + c % H2;
-            float val = candidate(v, i, j, &nan);
-            acc.add(val, i * N + j);
+        for (int u = g.t; u < U; u += G::T) {
+            const int j = Q + u % H2, r0 = Q + (u / H2) * S;
+            const int rows = min(S, Q + H2 - r0);
+            const float *c0 = pl + (r0 - 1) * G::STF + j;
+            float m0 = 0.0f, m1 = 0.0f, c1 = 0.0f;      // row maxima k-2, k-1; centre value k-1
+#pragma unroll
+            for (int k = 0; k < S + 2; ++k) {
+                if (k < rows + 2) {
+                    const float l = c0[k * G::STF - 1], c = c0[k * G::STF], r = c0[k * G::STF + 1];
+                    nan |= (l != l) | (c != c) | (r != r);
+                    const float m2 = fmaxf(l, fmaxf(c, r));
+                    if (k >= 2) {
+                        const float v = c1;                 // candidate row r0 + k - 2
+                        const bool mx = v >= fmaxf(m0, fmaxf(m1, m2));
+                        acc.add((mx && v > 0.0f) ? v : -1.0f, (r0 + k - 2) * N + j);
+                    }
+                    m0 = m1;
+                    m1 = m2;
+                    c1 = c;
+                }
+            }
         }
     }
     has_nan = g.any(nan);

@@ -149,6 +149,50 @@ __device__ __forceinline__ void finish_window(const XcorrParams &prm, float *pl,
     }
 }
 
+// finish_window for a single-peak call with deferred fits, spread over the
+// window's group: every thread holds the same search result, so the gates are
+// uniform and the 128-byte record (compensated 5x5 patch, peak, norm, position,
+// flag) is written by up to 32 threads at once instead of element by element.
+// Invalid windows and planes holding NaN take the leader's finish_window.
+template <int N>
+__device__ __forceinline__ void finish_window_rec(int t, int gw, const XcorrParams &prm, float *pl, int ld,
+                                                  const PeakAcc &acc, bool has_nan, long long idx, int n, int iw,
+                                                  long long nwt, bool valid, float enorm)
+{
+    if (!valid || has_nan) {
+        if (t == 0) finish_window<N, false>(prm, pl, ld, acc, has_nan, idx, n, iw, nwt, valid, enorm);
+        return;
+    }
+    const float best = acc.best;
+    const int bi = (acc.idx == 0x7fffffff) ? 0 : acc.idx / N;
+    const int bj = (acc.idx == 0x7fffffff) ? 0 : acc.idx % N;
+    const long long o = (long long)n * nwt + iw;
+    const bool gated = !(best > 0.0f) || bi < 2 || bi >= N - 2 || bj < 2 || bj >= N - 2;
+    if (t == 0) prm.pk_ratio[o] = (acc.p2 > 0.0f) ? fdiv(acc.p1, acc.p2) : 0.0f;
+    if (gated) {
+        if (t == 0) {
+            write_sentinel(prm, o, enorm);
+            prm.lm[idx].flag = 0;
+        }
+        return;
+    }
+    float *rec = reinterpret_cast<float *>(prm.lm + idx);      // sub[25], best, enorm, ij, flag
+    for (int q = t; q < PKN + 4; q += gw) {
+        float val;
+        if (q < PKN) {
+            const int r = bi + q / PKW - 2, c = bj + q % PKW - 2;
+            val = fmul(pl[r * ld + c], __ldg(prm.cw + r * N + c));
+        } else if (q == PKN) {
+            val = best;
+        } else if (q == PKN + 1) {
+            val = enorm;
+        } else {
+            val = __int_as_float(q == PKN + 2 ? ((bi << 16) | bj) : 1);
+        }
+        rec[q] = val;
+    }
+}
+
 // Fused correlation kernel (PIV_2d_cross_correlate.c:203-397): gather + weight +
 // mean/energy, packed forward FFT, conjugate product, inverse FFT, shift, peak
 // search, 3-point fit.  LM fits of single-peak calls are deferred to
@@ -246,7 +290,16 @@ xcorr_kernel(XcorrParams prm)
             PeakAcc acc;
             bool has_nan;
             search_plane<N>(g, pl, acc, has_nan);
-            if (t == 0 && inrange) finish_window<N, MULTI>(prm, pl, G::STF, acc, has_nan, idx, n, iw, nwt, valid, enorm);
+            if constexpr (!MULTI) {
+                if (prm.lm) {
+                    if (inrange && active)
+                        finish_window_rec<N>(t, G::T, prm, pl, G::STF, acc, has_nan, idx, n, iw, nwt, valid, enorm);
+                } else if (t == 0 && inrange) {
+                    finish_window<N, false>(prm, pl, G::STF, acc, has_nan, idx, n, iw, nwt, valid, enorm);
+                }
+            } else if (t == 0 && inrange) {
+                finish_window<N, MULTI>(prm, pl, G::STF, acc, has_nan, idx, n, iw, nwt, valid, enorm);
+            }
         }
         g.sync();
     }
