@@ -301,3 +301,35 @@ def test_config1_workload_against_oracle(oracle, cuda):
     for X, Y in ((gx, gy), (ox, oy)):
         e = np.hypot(X - tu, Y - tv)[ok]
         assert np.median(e) < 0.1
+
+
+def test_host_calls_from_concurrent_threads(cuda):
+    """The host-pointer entry points are re-entrant across host threads (ctypes
+    releases the GIL; the library serialises its host staging): results of
+    concurrent calls equal the same calls made in turn."""
+    import threading
+
+    g = geometry.compute_window_centers((192, 160), (32, 32), 50)
+    w = geometry.window_weight((32, 32), "gaussian")
+    pairs = [synthetic.particle_pair((192, 160), seed=300 + k, flow="uniform_grf")[:2] for k in range(6)]
+    ref = [correlator.bulkxcorr2d(A, B, g.win_ctrs_x, g.win_ctrs_y, (32, 32), w, w) for A, B in pairs]
+    got = [None] * len(pairs)
+    errs = []
+
+    def work(k):
+        try:
+            for _ in range(3):
+                A, B = pairs[k]
+                got[k] = correlator.bulkxcorr2d(A, B, g.win_ctrs_x, g.win_ctrs_y, (32, 32), w, w)
+        except Exception as e:          # surfaced below
+            errs.append(e)
+
+    th = [threading.Thread(target=work, args=(k,)) for k in range(len(pairs))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs, errs
+    for r, o in zip(ref, got):
+        for key in r:
+            assert np.array_equal(r[key], o[key], equal_nan=True), key
