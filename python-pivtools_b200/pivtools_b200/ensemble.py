@@ -94,6 +94,9 @@ class EnsemblePIV:
         sb = int(self.Lx.pivb_accumulate_scratch_bytes(h, self.n_win))
         self.scratch = torch.empty(max(sb, 256), dtype=torch.uint8, device=dev)
         self.n_pairs = 0
+        # zero fills above ran on the construction stream: finish them before use
+        # from another stream
+        torch.cuda.current_stream(self.device).synchronize()
 
     def _stream(self):
         return ctypes.c_void_p(self.torch.cuda.current_stream(self.device).cuda_stream)

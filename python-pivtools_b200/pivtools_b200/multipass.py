@@ -167,6 +167,10 @@ class MultipassPIV:
         self.launches_per_step = self._count_launches()
         self.planes = None
         self._last_n = self.N
+        # the set-up above (zero fills, correlation weights, warp tables) ran on the
+        # stream current at construction; finish it before run() is called from
+        # any other stream (a serving engine runs on its own)
+        torch.cuda.current_stream(self.device).synchronize()
 
     def keep_planes(self, on: bool = True):
         """Keep every window's correlation plane of every pass on the device (the
@@ -177,6 +181,7 @@ class MultipassPIV:
         if on:
             self.planes = [torch.zeros((self.N, p["ny"], p["nx"], p["win"], p["win"]), dtype=torch.float32,
                                        device=self.device) for p in self.passes]
+            torch.cuda.current_stream(self.device).synchronize()
 
     # ------------------------------------------------------------------ #
     def _stream(self):
