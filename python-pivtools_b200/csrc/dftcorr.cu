@@ -177,7 +177,7 @@ struct WinInfo {
     long long idx;
     int n, iw;
     float enorm;
-    int flags;     // 1 valid, 2 in range, 4 plane holds NaN
+    int flags;     // 1 valid, 2 in range
 };
 
 // Two warpgroups: warp w (w = 4 wg + q) owns tensor-memory lanes 32 q .. 32 q + 31
@@ -191,7 +191,6 @@ __global__ void __launch_bounds__(THREADS, 2) kernel(XcorrParams prm, const uint
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ WinInfo info[G];
-    __shared__ PeakAcc found[G];
     unsigned char *cst = sm;
     unsigned char *wk = sm + CONST_BYTES;
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + CONST_BYTES + WORK_BYTES);
@@ -432,30 +431,29 @@ __global__ void __launch_bounds__(THREADS, 2) kernel(XcorrParams prm, const uint
             for (int x = 0; x < N; ++x) pl[row * PLANE_LD + ((x + N / 2) & (N - 1))] = c[x] * inv_numel;
         }
         __syncwarp();
-        // ---- search (warp per window), then the fits of all eight windows in
-        //      parallel on the lanes of warp 0 (the FFT path's code)
+        // ---- search and finish, warp per window (the FFT path's code): with
+        //      record scratch the warp writes its window's record line at once,
+        //      otherwise its lane 0 fits in place
         {
             const int wl = warp;
             float *pl = planes + wl * (N * PLANE_LD);
-            if (prm.planes && (info[wl].flags & 1)) {
-                float *dst = prm.planes + info[wl].idx * (long long)(N * N);
+            const WinInfo wi = info[wl];
+            if (prm.planes && (wi.flags & 1)) {
+                float *dst = prm.planes + wi.idx * (long long)(N * N);
                 for (int k = lane; k < N * N; k += 32) dst[k] = pl[(k / N) * PLANE_LD + (k % N)];
             }
             const Group<N> g{lane, nullptr};
             PeakAcc acc;
             bool has_nan;
             search_plane<N>(g, pl, acc, has_nan);
-            if (lane == 0) {
-                found[wl] = acc;
-                if (has_nan) info[wl].flags |= 4;
+            if (wi.flags & 2) {
+                if (prm.lm)
+                    finish_window_rec<N>(lane, 32, prm, pl, PLANE_LD, acc, has_nan, wi.idx, wi.n, wi.iw, nwt,
+                                         (wi.flags & 1) != 0, wi.enorm);
+                else if (lane == 0)
+                    finish_window<N, false>(prm, pl, PLANE_LD, acc, has_nan, wi.idx, wi.n, wi.iw, nwt,
+                                            (wi.flags & 1) != 0, wi.enorm);
             }
-        }
-        __syncthreads();
-        if (warp == 0 && lane < G) {
-            const WinInfo wi = info[lane];
-            if (wi.flags & 2)
-                finish_window<N, false>(prm, planes + lane * (N * PLANE_LD), PLANE_LD, found[lane],
-                                        (wi.flags & 4) != 0, wi.idx, wi.n, wi.iw, nwt, (wi.flags & 1) != 0, wi.enorm);
         }
         __syncthreads();
     }
