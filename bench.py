@@ -49,6 +49,7 @@ def _args():
     ap.add_argument("--workload", default="multipass", choices=["multipass", "ensemble", "serve"],
                     help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
                          "serve: Poisson request stream with continuous batching")
+    ap.add_argument("--chunk", type=int, default=16, help="e2e: pairs per host-to-device chunk")
     ap.add_argument("--engine32", default="fft", choices=["fft", "dft"],
                     help="32 px passes on the FP32 FFT path or the tensor-core DFT-as-GEMM path")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: offered pairs/s")
@@ -297,7 +298,7 @@ def run_b200(args):
     # them on the GPU, runs the passes and reads the final vector fields back
     from pivtools_b200.multipass import HostPipeline
 
-    chunk = 16 if N % 16 == 0 else N
+    chunk = args.chunk if (args.chunk > 0 and N % args.chunk == 0) else N
     pipe = HostPipeline(HW, chunk, multipass.MultipassConfig(engine_32=args.engine32), device=dev)
     # frames are integer counts in [0, 65535]; every host buffer is page-locked with
     # .pin_memory() (torch.empty_like of a pinned tensor is pageable, which turns the
