@@ -506,7 +506,9 @@ def run_serve(args):
     """Serving mix: Poisson arrivals at --rate pairs/s for --duration s; each
     request is one uint16 pair of a size drawn from {512^2, 1024^2, 2048^2,
     2048x4096} with a schedule drawn from {32; 64-32; 128-64-32-16 px} at 50%
-    overlap, channel-flow particle images (a small pool per size, cycled), frames
+    overlap, particle images of the single-pair workload's particle and flow model
+    (uniform (3.3, -1.7) px plus a Gaussian random field of 0.5 px std and 40 px
+    correlation length; a small pool per size, cycled), frames
     in pinned host memory, a 120 GB device budget.  Reports vectors/s over the run
     and p50/p99 request latency (arrival to result in host memory)."""
     import numpy as np
@@ -523,8 +525,8 @@ def run_serve(args):
     for si, shp in enumerate(sizes):
         pool[shp] = []
         for k in range(2):
-            A, B, _ = synthetic.particle_pair(shp, seed=7000 + 10 * si + k + 1000 * rank, flow="channel",
-                                              device=dev, flow_kwargs={"peak": 12.0})
+            A, B, _ = synthetic.particle_pair(shp, seed=7000 + 10 * si + k + 1000 * rank, flow="uniform_grf",
+                                              device=dev)
             pool[shp].append((A.to(torch.int32).to(torch.uint16).cpu().pin_memory(),
                               B.to(torch.int32).to(torch.uint16).cpu().pin_memory()))
     srv = serving.PivServer(device=dev, max_batch=4, hbm_budget_bytes=120e9)
@@ -579,7 +581,8 @@ def run_serve(args):
             "ms_per_step": wall * 1e3 / max(len(reqs), 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"Poisson {args.rate:g} pairs/s for {args.duration:g} s; sizes 512^2, 1024^2, "
-                                   "2048^2, 2048x4096 uint16; schedules 32 / 64-32 / 128-64-32-16 px at 50%",
+                                   "2048^2, 2048x4096 uint16; schedules 32 / 64-32 / 128-64-32-16 px at 50%; "
+                                   "flow (3.3, -1.7) px + GRF 0.5 px",
                        "max_batch": srv.max_batch, "hbm_budget_gb": 120, "engines": len(srv.engines),
                        "engine_bytes_gb": srv.used_bytes / 1e9},
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
