@@ -1,6 +1,6 @@
 """GPU parity of libbulkxcorr2d (through its C-ABI) against the oracle.
 
-Bars (north-star parity contract): correlation planes within 1e-5 of the plane's
+Bars (the parity contract of this path): correlation planes within 1e-5 of the plane's
 peak magnitude; integer peak locations identical except documented near-ties
 (two candidate maxima within 1e-5 relative); displacements within 0.005 px;
 identical NaN sentinels.  The fitter entry points, which see identical input
