@@ -20,10 +20,10 @@
 #include "peakfit_dev.cuh"
 
 // Resident correlation CTAs per SM that the register allocation is capped for
-// (measured on B200: 32 px 5, 64 px 4; more CTAs spill or lose to the smaller
-// register budget).
+// (measured on B200: 32 px 4, 64 px 4; 3 or 5 at 32 px and 3 or 5 at 64 px are
+// slower, 6 at 32 px spills).
 #ifndef PIVB_MIN_CTAS_32
-#define PIVB_MIN_CTAS_32 5
+#define PIVB_MIN_CTAS_32 4
 #endif
 #ifndef PIVB_MIN_CTAS_64
 #define PIVB_MIN_CTAS_64 4
