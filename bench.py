@@ -49,7 +49,7 @@ def _args():
     ap.add_argument("--workload", default="multipass", choices=["multipass", "ensemble", "serve"],
                     help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
                          "serve: Poisson request stream with continuous batching")
-    ap.add_argument("--chunk", type=int, default=16, help="e2e: pairs per host-to-device chunk")
+    ap.add_argument("--chunk", type=int, default=32, help="e2e: pairs per host-to-device chunk")
     ap.add_argument("--engine32", default="fft", choices=["fft", "dft"],
                     help="32 px passes on the FP32 FFT path or the tensor-core DFT-as-GEMM path")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: offered pairs/s")

@@ -346,11 +346,15 @@ class HostPipeline:
     """
 
     def __init__(self, image_shape, chunk: int, cfg: MultipassConfig | None = None, device=None,
-                 vector_masks=None):
+                 vector_masks=None, graph: bool = True):
+        """graph: after the first chunk, replay the chunk's passes as one captured
+        CUDA graph (the conversions and copies stay stream operations)."""
         import torch
 
         self.torch = torch
         self.mp = MultipassPIV(image_shape, chunk, cfg, device, vector_masks)
+        self.use_graph = graph
+        self._graph = None
         dev = self.mp.device
         H, W = image_shape
         self.C = chunk
@@ -390,7 +394,21 @@ class HostPipeline:
                 if self.Lp.pivb_u16_to_f32_dev(src.data_ptr(), dst.data_ptr(), src.numel(), st) != 0:
                     raise RuntimeError("u16 -> f32 conversion failed")
             self.ev_conv[s].record(comp)
-            ux, uy = self.mp.run(self.f32[0], self.f32[1])
+            if self._graph is not None:
+                self._graph.replay()
+                last = self.mp.passes[-1]
+                ux, uy = last["ux"], last["uy"]
+            else:
+                ux, uy = self.mp.run(self.f32[0], self.f32[1])
             ux_out[sl].copy_(ux, non_blocking=True)
             uy_out[sl].copy_(uy, non_blocking=True)
+        if self.use_graph and self._graph is None:
+            # every lazy set-up has run once: capture the chunk's passes (capture
+            # records, it does not execute)
+            comp.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self.mp.run(self.f32[0], self.f32[1])
+            torch.cuda.current_stream(self.mp.device).synchronize()
+            self._graph = g
         return ux_out, uy_out
