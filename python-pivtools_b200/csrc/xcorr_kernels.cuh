@@ -248,13 +248,29 @@ xcorr_kernel(XcorrParams prm)
         if (active && valid) {
             const float *fa = prm.A + (long long)n * prm.img_stride + (long long)r0 * prm.W + c0 + line;
             const float *fb = prm.B + (long long)n * prm.img_stride + (long long)r0 * prm.W + c0 + line;
+            if constexpr (P == 4) {
+                // one weight for both frames: load it once (measured slower at one
+                // and two lanes per column, so those keep the plain loop)
+                const bool same_w = prm.wA == prm.wB;
 #pragma unroll
-            for (int k = 0; k < M; ++k) {
-                const int r = P * k + p;
-                a[k] = __ldg(fa + (long long)r * prm.W) * __ldg(prm.wA + r * N + line);
-                b[k] = __ldg(fb + (long long)r * prm.W) * __ldg(prm.wB + r * N + line);
-                sa += a[k];
-                sb += b[k];
+                for (int k = 0; k < M; ++k) {
+                    const int r = P * k + p;
+                    const float wa = __ldg(prm.wA + r * N + line);
+                    const float wb = same_w ? wa : __ldg(prm.wB + r * N + line);
+                    a[k] = __ldg(fa + (long long)r * prm.W) * wa;
+                    b[k] = __ldg(fb + (long long)r * prm.W) * wb;
+                    sa += a[k];
+                    sb += b[k];
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < M; ++k) {
+                    const int r = P * k + p;
+                    a[k] = __ldg(fa + (long long)r * prm.W) * __ldg(prm.wA + r * N + line);
+                    b[k] = __ldg(fb + (long long)r * prm.W) * __ldg(prm.wB + r * N + line);
+                    sa += a[k];
+                    sb += b[k];
+                }
             }
         } else {
 #pragma unroll
