@@ -304,12 +304,14 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
     // rotated by SH = 4 columns, so that the column-phase stores of one half-warp
     // (4 lines from each of the 4 blocks) fall on distinct banks, and each block of
     // 32 columns is skewed by one slot, so that the row-phase stores (the 4 lanes of
-    // a line write columns 32 apart) do too.
+    // a line write columns 32 apart) do too.  With two lanes the skew alone clears
+    // the row-phase conflicts of the pair of lanes of a line.
     constexpr int SH = (P == 4) ? 4 : 0;
     constexpr bool POW2 = (N & (N - 1)) == 0;
     // blk = row / M, known at each call site
     auto at = [&](int row, int blk, int col) {
-        if constexpr (SH == 0) return row * ST + col;
+        if constexpr (P == 1) return row * ST + col;
+        else if constexpr (SH == 0) return row * ST + col + (col >> 5);   // two lanes: skew only
         else {
             const int c = POW2 ? ((col + SH * blk) & (N - 1)) : (col + SH * blk) % N;
             return row * ST + c + (c >> 5);
