@@ -133,6 +133,49 @@ class EnsemblePIV:
                                                 self.fcomp[k].data_ptr(), s), "frame sum")
         self.n_pairs += n
 
+    def accumulate_host(self, Ah, Bh, chunk: int = 16):
+        """Add pairs from page-locked uint16 host frames Ah, Bh (n, H, W): chunks
+        cross PCIe on a copy stream into two alternating staging slots while the
+        previous chunk is converted to float32 on the GPU and accumulated on the
+        caller's stream.  Equal, bit for bit, to accumulate() called on the same
+        frames in float32, chunk by chunk."""
+        import ctypes as C
+
+        torch = self.torch
+        if not (Ah.is_pinned() and Bh.is_pinned()):
+            raise ValueError("accumulate_host needs page-locked host frames (use .pin_memory())")
+        if Ah.dtype != torch.uint16 or Bh.dtype != torch.uint16 or Ah.shape != Bh.shape:
+            raise ValueError("accumulate_host takes two uint16 frame stacks of one shape")
+        n, H, W = Ah.shape
+        if (H, W) != (self.H, self.W):
+            raise ValueError(f"frames {H}x{W} do not match the pass's {self.H}x{self.W}")
+        st = self.__dict__.get("_stage")
+        if st is None or st["chunk"] != chunk:
+            dev = self.device
+            st = dict(chunk=chunk, slot=0, copy=torch.cuda.Stream(device=dev),
+                      u16=[[torch.empty((chunk, H, W), dtype=torch.uint16, device=dev) for _ in range(2)]
+                           for _ in range(2)],
+                      f32=[torch.empty((chunk, H, W), dtype=torch.float32, device=dev) for _ in range(2)],
+                      ev_h2d=[torch.cuda.Event() for _ in range(2)], ev_conv=[torch.cuda.Event() for _ in range(2)])
+            self._stage = st
+        comp = torch.cuda.current_stream(self.device)
+        cs = C.c_void_p(comp.cuda_stream)
+        for c0 in range(0, n, chunk):
+            k = min(chunk, n - c0)
+            sl = st["slot"]
+            st["slot"] ^= 1
+            st["copy"].wait_event(st["ev_conv"][sl])
+            with torch.cuda.stream(st["copy"]):
+                st["u16"][sl][0][:k].copy_(Ah[c0:c0 + k], non_blocking=True)
+                st["u16"][sl][1][:k].copy_(Bh[c0:c0 + k], non_blocking=True)
+                st["ev_h2d"][sl].record(st["copy"])
+            comp.wait_event(st["ev_h2d"][sl])
+            for j in range(2):
+                self._ok(self.Lp.pivb_u16_to_f32_dev(st["u16"][sl][j].data_ptr(), st["f32"][j].data_ptr(), k * H * W,
+                                                     cs), "u16 -> f32")
+            st["ev_conv"][sl].record(comp)
+            self.accumulate(st["f32"][0][:k], st["f32"][1][:k])
+
     def finalize(self):
         """Background, DC zero, envelope, normalisation -> FP64 planes (AA, BB, AB)
         of shape (n_win, h, w) on the device, and the normalisation factors."""

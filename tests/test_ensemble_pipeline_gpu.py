@@ -108,3 +108,33 @@ def test_distributed_finalise_single_rank_equals_local(cuda):
                                    fit_loc["gauss"].cpu().numpy()[ok][:, 14:16], atol=1e-3)
     finally:
         torch.distributed.destroy_process_group()
+
+
+def test_accumulate_from_uint16_host_frames(cuda):
+    """Pairs streamed from page-locked uint16 host frames (chunked, staged on a
+    copy stream) accumulate exactly as the same frames in float32, chunk by chunk."""
+    import torch
+
+    shape, win = (128, 160), (16, 16)
+    A, B = _pairs(7, shape, 730)
+    A16 = np.clip(np.round(A), 0, 65535).astype(np.int32)
+    B16 = np.clip(np.round(B), 0, 65535).astype(np.int32)
+    host = ensemble.EnsemblePIV(shape, win, 75, "square", device=cuda)
+    dev = ensemble.EnsemblePIV(shape, win, 75, "square", device=cuda)
+    Ah = torch.tensor(A16).to(torch.uint16).pin_memory()
+    Bh = torch.tensor(B16).to(torch.uint16).pin_memory()
+    for _ in range(2):                                   # staging slots and events reused
+        host.accumulate_host(Ah, Bh, chunk=3)
+    for _ in range(2):
+        for c0 in range(0, 7, 3):
+            dev.accumulate(torch.tensor(A16[c0:c0 + 3], dtype=torch.float32, device=cuda),
+                           torch.tensor(B16[c0:c0 + 3], dtype=torch.float32, device=cuda))
+    torch.cuda.synchronize()
+    assert host.n_pairs == dev.n_pairs == 14
+    for a, b in ((host.sums, dev.sums), (host.comp, dev.comp), (host.fsum, dev.fsum)):
+        assert torch.equal(a, b)
+    fa, fb = host.finalize(), dev.finalize()
+    torch.cuda.synchronize()
+    assert torch.equal(fa["R_AB"], fb["R_AB"]) and torch.equal(fa["R_AA"], fb["R_AA"])
+    with pytest.raises(ValueError):
+        host.accumulate_host(torch.tensor(A16).to(torch.uint16), Bh)          # pageable
