@@ -129,7 +129,7 @@ constexpr uint32_t B3 = B2 + 2 * B2_BYTES, B3_BYTES = 64 * 64 * 2;
 constexpr uint32_t B4 = B3 + 2 * B3_BYTES, B4_BYTES = 32 * 32 * 2;
 constexpr uint32_t CONST_BYTES = B4 + 2 * B4_BYTES;          // 40 KB
 constexpr uint32_t WORK_BYTES = 64 * 1024;
-constexpr uint32_t PLANE_LD = N + 1;
+constexpr uint32_t PLANE_LD = WinGeo<N>::STF;   // the search reads with this stride
 constexpr uint32_t SMEM_BYTES = CONST_BYTES + WORK_BYTES + 64;
 constexpr uint32_t TMEM_COLS = 256;
 static_assert(G * N * PLANE_LD * 4 <= WORK_BYTES, "planes alias the work region");

@@ -43,7 +43,9 @@ struct WinGeo {
     // stride would also clear the row-phase conflicts of two lanes, but costs the
     // 64 px kernel registers and 6% time: measured.)
     static constexpr int ST = N + ((P == 1) ? 1 : (P == 2 ? 2 : (N == 128 ? 4 : 6)));
-    static constexpr int STF = N + 1;                                   // float row stride
+    // float row stride; at 32 px rows 8 apart (the two halves of a warp in the
+    // peak search) then fall 16 banks apart
+    static constexpr int STF = (N == 32) ? N + 2 : N + 1;
     static constexpr int WARPS_PER_CTA = (GW <= 32) ? 4 : GW / 32;
     static constexpr int CTA_THREADS = WARPS_PER_CTA * 32;
     // resident CTAs per SM the correlation kernel is compiled for (register cap)
