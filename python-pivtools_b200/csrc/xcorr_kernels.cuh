@@ -219,6 +219,15 @@ xcorr_kernel(XcorrParams prm)
     float2 *tw = reinterpret_cast<float2 *>(smem + G::GROUPS_PER_CTA * G::PLANE_BYTES + G::RED_BYTES);
     fill_lane_twiddles<N>(tw, threadIdx.x, G::CTA_THREADS);
     if constexpr (G::TW_BYTES > 0) __syncthreads();
+    // 32 px: both window weights staged once per CTA (shared loads in the gather)
+    float *swt = reinterpret_cast<float *>(smem + G::GROUPS_PER_CTA * G::PLANE_BYTES + G::RED_BYTES + G::TW_BYTES);
+    if constexpr (G::WT_BYTES > 0) {
+        for (int i = threadIdx.x; i < N * N; i += G::CTA_THREADS) {
+            swt[i] = prm.wA[i];
+            swt[N * N + i] = prm.wB[i];
+        }
+        __syncthreads();
+    }
     const Group<N> g{t, red};
     const bool active = t < G::T;
     int line, p;
@@ -259,6 +268,15 @@ xcorr_kernel(XcorrParams prm)
                     const float wb = same_w ? wa : __ldg(prm.wB + r * N + line);
                     a[k] = __ldg(fa + (long long)r * prm.W) * wa;
                     b[k] = __ldg(fb + (long long)r * prm.W) * wb;
+                    sa += a[k];
+                    sb += b[k];
+                }
+            } else if constexpr (G::WT_BYTES > 0) {
+#pragma unroll
+                for (int k = 0; k < M; ++k) {
+                    const int r = P * k + p;
+                    a[k] = __ldg(fa + (long long)r * prm.W) * swt[r * N + line];
+                    b[k] = __ldg(fb + (long long)r * prm.W) * swt[N * N + r * N + line];
                     sa += a[k];
                     sb += b[k];
                 }
