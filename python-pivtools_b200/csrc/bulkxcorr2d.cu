@@ -238,7 +238,8 @@ namespace {
 template <int N>
 constexpr size_t accum_smem_bytes()
 {
-    return (size_t)WinGeo<N>::SMEM_BYTES + (size_t)WinGeo<N>::GROUPS_PER_CTA * 6 * N * N * 4;
+    // the accumulation kernel has no use for the correlator's staged weights
+    return (size_t)(WinGeo<N>::SMEM_BYTES - WinGeo<N>::WT_BYTES) + (size_t)WinGeo<N>::GROUPS_PER_CTA * 6 * N * N * 4;
 }
 template <int N>
 constexpr bool accum_in_smem()
@@ -253,7 +254,7 @@ int accum_grid(long long nwt)
     constexpr bool SM = accum_in_smem<N>();
     static int per_sm = -1;
     auto kern = accum_kernel<N, SM>;
-    const size_t smem = SM ? accum_smem_bytes<N>() : (size_t)G::SMEM_BYTES;
+    const size_t smem = SM ? accum_smem_bytes<N>() : (size_t)(G::SMEM_BYTES - G::WT_BYTES);
     if (per_sm < 0) {
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
         int nb = 0;
@@ -285,7 +286,7 @@ int accum_launch_n(AccumParams p, char *scratch, cudaStream_t s)
     const int grid = accum_grid<N>(p.nwt);
     if (grid < 0) return PIV_ERROR_CUDA;
     p.gacc = SM ? nullptr : reinterpret_cast<float *>(scratch + 256);
-    const size_t smem = SM ? accum_smem_bytes<N>() : (size_t)G::SMEM_BYTES;
+    const size_t smem = SM ? accum_smem_bytes<N>() : (size_t)(G::SMEM_BYTES - G::WT_BYTES);
     accum_kernel<N, SM><<<grid, G::CTA_THREADS, smem, s>>>(p);
     return cudaGetLastError() == cudaSuccess ? PIV_ERROR_NONE : PIV_ERROR_CUDA;
 }
