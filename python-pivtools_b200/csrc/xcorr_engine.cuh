@@ -33,16 +33,18 @@ namespace piv {
 
 template <int N>
 struct WinGeo {
-    static constexpr int P = (N <= 32) ? 1 : ((N <= 64) ? 2 : 4);
+    // lanes per column (measured on B200 with the deferred fits: one lane at 64 px
+    // is 20% faster than two; two at 128 px 1% faster than four; 96 px keeps four)
+    static constexpr int P = (N <= 32 || N == 64) ? 1 : ((N == 48 || N == 128) ? 2 : 4);
     static constexpr int M = N / P;
     static constexpr int T = N * P;                                     // active threads per window
     static constexpr int GW = (T <= 8) ? 8 : (T <= 16) ? 16 : (T <= 32) ? 32 : T;  // lanes per group
     static constexpr int WPW = (GW <= 32) ? 32 / GW : 1;                // windows per warp
-    // complex row stride.  Four lanes add one slot per 32-column block (the skew
-    // in correlate_plane) plus a margin that keeps rows 8 banks apart.  (An odd
-    // stride would also clear the row-phase conflicts of two lanes, but costs the
-    // 64 px kernel registers and 6% time: measured.)
-    static constexpr int ST = N + ((P == 1) ? 1 : (P == 2 ? 2 : (N == 128 ? 4 : 6)));
+    // complex row stride: N + 1 at one lane; two and four lanes add one slot per
+    // 32-column block (the skew in correlate_plane) plus a margin chosen so that
+    // every store and load phase of a warp falls on distinct banks (simulated
+    // per size: 48 -> 50, 128 at two lanes -> 133, 96 -> 102, 128 at four -> 132)
+    static constexpr int ST = N + ((P == 1) ? 1 : (P == 2 ? (N == 128 ? 5 : 2) : (N == 128 ? 4 : 6)));
     // float row stride; at 32 px rows 8 apart (the two halves of a warp in the
     // peak search) then fall 16 banks apart
     static constexpr int STF = (N == 32) ? N + 2 : N + 1;
