@@ -263,9 +263,9 @@ xcorr_kernel(XcorrParams prm)
         if (active && valid) {
             const float *fa = prm.A + (long long)n * prm.img_stride + (long long)r0 * prm.W + c0 + line;
             const float *fb = prm.B + (long long)n * prm.img_stride + (long long)r0 * prm.W + c0 + line;
-            if constexpr (P == 4) {
-                // one weight for both frames: load it once (measured slower at one
-                // and two lanes per column, so those keep the plain loop)
+            if constexpr (P == 4 || N == 128) {
+                // one weight for both frames: load it once (measured faster at 96
+                // and 128 px only; the other sizes keep the plain loop)
                 const bool same_w = prm.wA == prm.wB;
 #pragma unroll
                 for (int k = 0; k < M; ++k) {
