@@ -60,8 +60,9 @@ struct WinGeo {
     // [P][M + 1]: the padded row puts the four lanes' entries on distinct banks
     static constexpr int TW_LD = M + 1;
     static constexpr int TW_BYTES = (P == 4) ? P * TW_LD * 8 : 0;
-    // window weights staged in shared memory: both at 32 px, the shared one at 64 px
-    static constexpr int WT_BYTES = (N == 32) ? 2 * N * N * 4 : (N == 64 ? N * N * 4 : 0);
+    // window weights staged in shared memory at 32 px (measured slower at 64 px
+    // with one lane per column and at 128 px)
+    static constexpr int WT_BYTES = (N == 32) ? 2 * N * N * 4 : 0;
     static constexpr int SMEM_BYTES = GROUPS_PER_CTA * PLANE_BYTES + RED_BYTES + TW_BYTES + WT_BYTES;
     static_assert(N * STF * 4 <= PLANE_BYTES, "float plane must alias the complex plane");
 };

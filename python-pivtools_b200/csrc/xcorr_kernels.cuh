@@ -219,18 +219,12 @@ xcorr_kernel(XcorrParams prm)
     float2 *tw = reinterpret_cast<float2 *>(smem + G::GROUPS_PER_CTA * G::PLANE_BYTES + G::RED_BYTES);
     fill_lane_twiddles<N>(tw, threadIdx.x, G::CTA_THREADS);
     if constexpr (G::TW_BYTES > 0) __syncthreads();
-    // window weights staged once per CTA (shared loads in the gather): both at
-    // 32 px; at 64 px the one weight of both frames, when the call has one
+    // 32 px: both window weights staged once per CTA (shared loads in the gather)
     float *swt = reinterpret_cast<float *>(smem + G::GROUPS_PER_CTA * G::PLANE_BYTES + G::RED_BYTES + G::TW_BYTES);
     if constexpr (N == 32) {
         for (int i = threadIdx.x; i < N * N; i += G::CTA_THREADS) {
             swt[i] = prm.wA[i];
             swt[N * N + i] = prm.wB[i];
-        }
-        __syncthreads();
-    } else if constexpr (N == 64) {
-        if (prm.wA == prm.wB) {
-            for (int i = threadIdx.x; i < N * N; i += G::CTA_THREADS) swt[i] = prm.wA[i];
         }
         __syncthreads();
     }
@@ -276,27 +270,6 @@ xcorr_kernel(XcorrParams prm)
                     b[k] = __ldg(fb + (long long)r * prm.W) * wb;
                     sa += a[k];
                     sb += b[k];
-                }
-            } else if constexpr (N == 64) {
-                if (prm.wA == prm.wB) {
-#pragma unroll
-                    for (int k = 0; k < M; ++k) {
-                        const int r = P * k + p;
-                        const float wv = swt[r * N + line];
-                        a[k] = __ldg(fa + (long long)r * prm.W) * wv;
-                        b[k] = __ldg(fb + (long long)r * prm.W) * wv;
-                        sa += a[k];
-                        sb += b[k];
-                    }
-                } else {
-#pragma unroll
-                    for (int k = 0; k < M; ++k) {
-                        const int r = P * k + p;
-                        a[k] = __ldg(fa + (long long)r * prm.W) * __ldg(prm.wA + r * N + line);
-                        b[k] = __ldg(fb + (long long)r * prm.W) * __ldg(prm.wB + r * N + line);
-                        sa += a[k];
-                        sb += b[k];
-                    }
                 }
             } else if constexpr (G::WT_BYTES > 0) {
 #pragma unroll
