@@ -190,7 +190,7 @@ struct WarpParams {
 constexpr int kWarpRows = 8;
 
 template <int MODE, int IMPL>
-__global__ void __launch_bounds__(256) warp_kernel(WarpParams p)
+__global__ void __launch_bounds__(128) warp_kernel(WarpParams p)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * kWarpRows;
@@ -327,7 +327,7 @@ PIV_EXPORT int pivb_warp_dev(const float *d_ia, const float *d_ib, float *d_oa, 
     p.lx = reinterpret_cast<const float *>(t + pad256((size_t)H * 4));
     p.lut = reinterpret_cast<const float *>(t + pad256((size_t)H * 4) + pad256((size_t)W * 4));
     p.round_shifts = round_shifts;
-    dim3 blk(32, 8), grd((W + 31) / 32, (H + 8 * kWarpRows - 1) / (8 * kWarpRows), N);
+    dim3 blk(32, 4), grd((W + 31) / 32, (H + 4 * kWarpRows - 1) / (4 * kWarpRows), N);   // 32 x 4 measured best
     cudaStream_t s = (cudaStream_t)stream;
     if (interp_mode == 0) {
         if (impl) warp_kernel<0, 1><<<grd, blk, 0, s>>>(p);
