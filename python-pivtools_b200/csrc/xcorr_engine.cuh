@@ -40,11 +40,23 @@ struct WinGeo {
     static constexpr int T = N * P;                                     // active threads per window
     static constexpr int GW = (T <= 8) ? 8 : (T <= 16) ? 16 : (T <= 32) ? 32 : T;  // lanes per group
     static constexpr int WPW = (GW <= 32) ? 32 / GW : 1;                // windows per warp
-    // complex row stride: N + 1 at one lane; two and four lanes add one slot per
-    // 32-column block (the skew in correlate_plane) plus a margin chosen so that
-    // every store and load phase of a warp falls on distinct banks (simulated
-    // per size: 48 -> 50, 128 at two lanes -> 133, 96 -> 102, 128 at four -> 132)
-    static constexpr int ST = N + ((P == 1) ? 1 : (P == 2 ? (N == 128 ? 5 : 2) : (N == 128 ? 4 : 6)));
+    // Plane layout of correlate_plane: complex element (row, col) at
+    // row * ST + c + SKEW * (c >> SKB), c = (col + ROT * (row / M)) % N.  ST, the
+    // rotation of each block of M rows and the skew per 2^SKB columns come from
+    // simulating the banks of every store and load phase: a 64-bit access is
+    // served per half-warp, so the cost of a phase is the largest number of
+    // distinct words one bank holds among 16 lanes, summed over the two halves.
+    // Chosen per size (cost summed over the phases, 14 = no conflict): 48 ->
+    // ST 50, skew per 32 columns (19.5); 96 -> 100, rotation 4, skew per 32
+    // (20.0; the former 102 ran 6% longer); 128 at two lanes -> 134 without
+    // rotation or skew (22; the skewed 133 scored 28 and ran 6% longer).  At 128
+    // px rotation 8 with a skew per 64 columns scores 16.6 but measured no faster:
+    // its index arithmetic costs what the conflicts did.
+    static constexpr int ST = N + ((P == 1) ? 1 : (P == 2 ? (N == 128 ? 6 : 2) : 4));
+    static constexpr int SKEW = (P == 1 || (P == 2 && N == 128)) ? 0 : 1;
+    static constexpr int SKB = 5;
+    static constexpr int ROT = (P == 4) ? 4 : 0;
+    static_assert(N - 1 + SKEW * ((N - 1) >> SKB) < ST, "a skewed plane row must fit its stride");
     // float row stride; at 32 px rows 8 apart (the two halves of a warp in the
     // peak search) then fall 16 banks apart
     static constexpr int STF = (N == 32) ? N + 2 : N + 1;
@@ -306,22 +318,19 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
     lane_slot<N>(active ? g.t : 0, line, p);
     const int q = out_block<P>(p);
     const int rm = (N - line) % N;
-    // Complex plane element (row, col) lives at row * ST + c + c / 32 with
-    // c = (col + rot(row)) % N: with four lanes per column each block of M rows is
-    // rotated by SH = 4 columns, so that the column-phase stores of one half-warp
-    // (4 lines from each of the 4 blocks) fall on distinct banks, and each block of
-    // 32 columns is skewed by one slot, so that the row-phase stores (the 4 lanes of
-    // a line write columns 32 apart) do too.  With two lanes the skew alone clears
-    // the row-phase conflicts of the pair of lanes of a line.
-    constexpr int SH = (P == 4) ? 4 : 0;
+    // Complex plane element (row, col) lives at row * ST + c + SKEW * (c >> SKB)
+    // with c = (col + ROT * blk) % N, blk = row / M (known at each call site).
+    // The rotation of each block of M rows separates the column-phase stores of
+    // the lanes of one half-warp that write different blocks; the skew separates
+    // the row-phase stores of the lanes of one line, which write columns M apart.
+    constexpr int ROT = G::ROT, SKB = G::SKB;
     constexpr bool POW2 = (N & (N - 1)) == 0;
-    // blk = row / M, known at each call site
     auto at = [&](int row, int blk, int col) {
         if constexpr (P == 1) return row * ST + col;
-        else if constexpr (SH == 0) return row * ST + col + (col >> 5);   // two lanes: skew only
         else {
-            const int c = POW2 ? ((col + SH * blk) & (N - 1)) : (col + SH * blk) % N;
-            return row * ST + c + (c >> 5);
+            int c = col;
+            if constexpr (ROT != 0) c = POW2 ? ((col + ROT * blk) & (N - 1)) : (col + ROT * blk) % N;
+            return row * ST + c + G::SKEW * (c >> SKB);
         }
     };
     const int lb = line / M, rb = rm / M;
