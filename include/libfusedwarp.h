@@ -36,7 +36,8 @@ int fused_symmetric_warp_batch(const float *imgs_a, const float *imgs_b, float *
 
 /* ---- device-pointer API (no counterpart in the reference; resident callers) ---- */
 
-/* Bytes of the per-geometry tables (pixel -> predictor index maps, Lanczos weights). */
+/* Bytes of the per-geometry tables (pixel -> predictor index maps, Lanczos weights,
+   per-row predictor weights). */
 size_t pivb_warp_table_bytes(int H, int W);
 
 /* Build the tables for predictor centres d_ctrs_y [nPY], d_ctrs_x [nPX] (ascending). */

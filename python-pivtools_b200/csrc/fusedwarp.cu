@@ -19,6 +19,7 @@
 
 #include <mutex>
 
+#include "f32x2.cuh"
 #include "piv_common.cuh"
 
 namespace {
@@ -39,6 +40,21 @@ __device__ __forceinline__ void keys4(float d, float *w)
     w[3] = fa(fm(fs(fm(fa(fm(-0.75f, s3), 3.75f), s3), 6.0f), s3), 3.0f);
 }
 
+// keys4 on two independent offsets at once (.x and .y), the same operations in
+// the same order, so each half is bit-identical to keys4 of that offset.
+// nz = {-0, -0} from a run-time value: the products are mulz2, never contracted.
+__device__ __forceinline__ void keys4_x2(float2 d, float2 (&w)[4], float2 nz)
+{
+    using namespace piv;
+    const float2 one = dup2(1.0f);
+    auto mu = [&](float2 a, float2 b) { return mulz2(a, b, nz); };
+    const float2 s0 = add2(one, d), q2 = sub2(one, d), s3 = sub2(dup2(2.0f), d);
+    w[1] = add2(mu(mu(sub2(mu(dup2(1.25f), d), dup2(2.25f)), d), d), one);
+    w[2] = add2(mu(mu(sub2(mu(dup2(1.25f), q2), dup2(2.25f)), q2), q2), one);
+    w[0] = add2(mu(sub2(mu(add2(mu(dup2(-0.75f), s0), dup2(3.75f)), s0), dup2(6.0f)), s0), dup2(3.0f));
+    w[3] = add2(mu(sub2(mu(add2(mu(dup2(-0.75f), s3), dup2(3.75f)), s3), dup2(6.0f)), s3), dup2(3.0f));
+}
+
 __device__ __forceinline__ void lanczos_w(float d, const float *lut, float *w)
 {
     const float pos = fm(d, (float)kLutN);
@@ -50,6 +66,38 @@ __device__ __forceinline__ void lanczos_w(float d, const float *lut, float *w)
         const float a = lut[k * 6 + q], b = lut[(k + 1) * 6 + q];
         w[q] = fa(a, fm(fr, fs(b, a)));
     }
+}
+
+// One bicubic sample from precomputed weights and stencil origin (iy, ix):
+// sample_bicubic<1> after its weight step.
+__device__ __forceinline__ float bicubic_from_weights(const float *__restrict__ img, int iy, int ix, const float *wy,
+                                                      const float *wx, int H, int W)
+{
+    if (iy >= 0 && iy + 3 < H && ix >= 0 && ix + 3 < W) {
+        const float *r = img + (iy * W + ix);
+        float c[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) c[n] = fm(__ldg(r + n), wy[0]);
+#pragma unroll
+        for (int m = 1; m < 4; ++m)
+#pragma unroll
+            for (int n = 0; n < 4; ++n) c[n] = __fmaf_rn(__ldg(r + m * W + n), wy[m], c[n]);
+        const float p0 = fm(c[0], wx[0]), p1 = fm(c[1], wx[1]), p2 = fm(c[2], wx[2]), p3 = fm(c[3], wx[3]);
+        return fa(fa(p0, p1), fa(p2, p3));
+    }
+    float v = 0.0f;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        const int row = iy + m;
+        if (row < 0 || row >= H) continue;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const int col = ix + n;
+            if (col < 0 || col >= W) continue;
+            v = fa(v, fm(fm(wy[m], wx[n]), __ldg(img + (long long)row * W + col)));
+        }
+    }
+    return v;
 }
 
 template <int IMPL>
@@ -181,8 +229,26 @@ struct WarpParams {
     int N, H, W, nPY, nPX;
     const float *ly, *lx;      // pixel -> fractional predictor index
     const float *lut;          // Lanczos table or null
+    const float4 *wyb;         // per row: predictor row weights as pairs {w0,w0,w1,w1}, {w2,w2,w3,w3}
+    const int *byr;            // per row: first predictor row of the 4x4 stencil
     int round_shifts;
+    float neg_zero;            // -0.0f, passed at run time (see mulz2)
 };
+
+// Per-row side of the bicubic predictor (fused_warp.c:224-250): the Keys weights
+// of each output row's fractional predictor index, stored twice each so that the
+// warp kernel reads them as ready-made f32x2 operands, and the stencil's first row.
+__global__ void row_weights_kernel(const float *ly, int H, float4 *wyb, int *byr)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= H) return;
+    const float f = ly[i], ff = floorf(f);
+    float w[4];
+    keys4(fs(f, ff), w);
+    wyb[2 * i] = make_float4(w[0], w[0], w[1], w[1]);
+    wyb[2 * i + 1] = make_float4(w[2], w[2], w[3], w[3]);
+    byr[i] = (int)ff - 1;
+}
 
 // Output rows per thread.  The rows of one thread share the column-side work
 // (predictor column weights and indices) and, while they fall in the same
@@ -254,6 +320,94 @@ __global__ void __launch_bounds__(128) warp_kernel(WarpParams p)
     }
 }
 
+// warp_kernel<0, 1> with paired arithmetic: the predictor's dy and dx sums run
+// as one f32x2 chain, and the samples of frame A (.x) and frame B (.y) share
+// every weight, gather and combine instruction.  Each half performs the scalar
+// kernel's operations in its order, so the output is bit-identical to it.  When
+// either stencil touches the border both samples take the scalar routines.
+// (96 registers, 5 CTAs per SM; capping them for 6 or 8 spills and ran 5% slower)
+__global__ void __launch_bounds__(128) warp_bicubic_x2_kernel(WarpParams p)
+{
+    using namespace piv;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * kWarpRows;
+    const int n = blockIdx.z;
+    if (j >= p.W || i0 >= p.H) return;
+    const float2 nz = dup2(p.neg_zero);
+    const float *dy = p.pdy + n * p.pred_stride, *dx = p.pdx + n * p.pred_stride;
+    const float fx = p.lx[j], fxf = floorf(fx);
+    const int bx = (int)fxf - 1;
+    float wx[4];
+    keys4(fs(fx, fxf), wx);
+    float2 wxb[4];
+    int cq[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        wxb[q] = dup2(wx[q]);
+        cq[q] = min(max(bx + q, 0), p.nPX - 1);
+    }
+    float2 pyx[4][4];      // {dy, dx} at the 4x4 predictor stencil
+    int cur_by = -0x7fffffff;
+    const float *a = p.ia + n * p.img_stride, *b = p.ib + n * p.img_stride;
+    const int H = p.H, W = p.W;
+    const float fj = (float)j;
+    const int i_end = min(i0 + kWarpRows, H);
+#pragma unroll 1
+    for (int i = i0; i < i_end; ++i) {
+        const int by = p.byr[i];
+        const float4 w01 = p.wyb[2 * i], w23 = p.wyb[2 * i + 1];
+        const float2 wyb[4] = {make_float2(w01.x, w01.y), make_float2(w01.z, w01.w), make_float2(w23.x, w23.y),
+                               make_float2(w23.z, w23.w)};
+        if (by != cur_by) {          // warp-uniform: all lanes share row i
+            cur_by = by;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                const int r = min(max(by + m, 0), p.nPY - 1) * p.nPX;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) pyx[m][q] = make_float2(__ldg(dy + r + cq[q]), __ldg(dx + r + cq[q]));
+            }
+        }
+        float2 v = make_float2(0.0f, 0.0f);
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v = add2(v, mulz2(mulz2(wyb[m], wxb[q], nz), pyx[m][q], nz));
+        float2 h = mulz2(dup2(0.5f), v, nz);     // {hy, hx}
+        if (p.round_shifts) { h.x = roundf(h.x); h.y = roundf(h.y); }
+        const float fi = (float)i;
+        const float2 Y = make_float2(fs(fi, h.x), fa(fi, h.x));     // {frame A, frame B}
+        const float2 X = make_float2(fs(fj, h.y), fa(fj, h.y));
+        const float2 FY = make_float2(floorf(Y.x), floorf(Y.y)), FX = make_float2(floorf(X.x), floorf(X.y));
+        float2 wy2[4], wx2[4];
+        keys4_x2(sub2(Y, FY), wy2, nz);
+        keys4_x2(sub2(X, FX), wx2, nz);
+        const int iya = (int)FY.x - 1, iyb = (int)FY.y - 1, ixa = (int)FX.x - 1, ixb = (int)FX.y - 1;
+        const long long o = n * p.img_stride + (long long)i * W + j;
+        const bool inside = iya >= 0 && iya + 3 < H && ixa >= 0 && ixa + 3 < W && iyb >= 0 && iyb + 3 < H &&
+                            ixb >= 0 && ixb + 3 < W;
+        if (inside) {
+            const float *ra = a + (iya * W + ixa), *rb = b + (iyb * W + ixb);
+            float2 c[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) c[q] = mulz2(make_float2(__ldg(ra + q), __ldg(rb + q)), wy2[0], nz);
+#pragma unroll
+            for (int m = 1; m < 4; ++m)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    c[q] = fma2(make_float2(__ldg(ra + m * W + q), __ldg(rb + m * W + q)), wy2[m], c[q]);
+            const float2 r = add2(add2(mulz2(c[0], wx2[0], nz), mulz2(c[1], wx2[1], nz)),
+                                  add2(mulz2(c[2], wx2[2], nz), mulz2(c[3], wx2[3], nz)));
+            p.oa[o] = r.x;
+            p.ob[o] = r.y;
+        } else {
+            const float wya[4] = {wy2[0].x, wy2[1].x, wy2[2].x, wy2[3].x}, wyb_[4] = {wy2[0].y, wy2[1].y, wy2[2].y, wy2[3].y};
+            const float wxa[4] = {wx2[0].x, wx2[1].x, wx2[2].x, wx2[3].x}, wxb_[4] = {wx2[0].y, wx2[1].y, wx2[2].y, wx2[3].y};
+            p.oa[o] = bicubic_from_weights(a, iya, ixa, wya, wxa, H, W);
+            p.ob[o] = bicubic_from_weights(b, iyb, ixb, wyb_, wxb_, H, W);
+        }
+    }
+}
+
 std::mutex g_mu;
 volatile int g_impl = 1;
 struct Ws {
@@ -282,11 +436,33 @@ inline size_t pad256(size_t b) { return (b + 255) & ~size_t(255); }
 PIV_EXPORT void fused_warp_set_impl(int impl) { g_impl = impl ? 1 : 0; }
 PIV_EXPORT int fused_warp_get_impl(void) { return g_impl; }
 
-// Bytes of device tables pivb_warp_dev needs: lut_y [H], lut_x [W], Lanczos [4097*6].
+// Bytes of device tables pivb_warp_dev needs: lut_y [H], lut_x [W], Lanczos
+// [4097*6], predictor row weight pairs [H*8], predictor stencil rows [H].
 PIV_EXPORT size_t pivb_warp_table_bytes(int H, int W)
 {
-    return pad256((size_t)H * 4) + pad256((size_t)W * 4) + pad256((size_t)(kLutN + 1) * 6 * 4);
+    return pad256((size_t)H * 4) + pad256((size_t)W * 4) + pad256((size_t)(kLutN + 1) * 6 * 4) +
+           pad256((size_t)H * 32) + pad256((size_t)H * 4);
 }
+
+namespace {
+struct WarpTables {
+    float *ly, *lx, *lut;
+    float4 *wyb;
+    int *byr;
+};
+WarpTables warp_tables(void *t_, int H, int W)
+{
+    char *t = static_cast<char *>(t_);
+    WarpTables r;
+    size_t off = 0;
+    r.ly = reinterpret_cast<float *>(t + off); off += pad256((size_t)H * 4);
+    r.lx = reinterpret_cast<float *>(t + off); off += pad256((size_t)W * 4);
+    r.lut = reinterpret_cast<float *>(t + off); off += pad256((size_t)(kLutN + 1) * 6 * 4);
+    r.wyb = reinterpret_cast<float4 *>(t + off); off += pad256((size_t)H * 32);
+    r.byr = reinterpret_cast<int *>(t + off);
+    return r;
+}
+}  // namespace
 
 // Build the per-call tables on the device (pixel -> predictor index, Lanczos weights).
 PIV_EXPORT int pivb_warp_setup_dev(const float *d_ctrs_y, int nPY, const float *d_ctrs_x, int nPX, int H,
@@ -294,14 +470,12 @@ PIV_EXPORT int pivb_warp_setup_dev(const float *d_ctrs_y, int nPY, const float *
 {
     if (H <= 0 || W <= 0 || nPY <= 0 || nPX <= 0 || !d_ctrs_y || !d_ctrs_x || !d_tables) return 1;
     cudaStream_t s = (cudaStream_t)stream;
-    char *t = static_cast<char *>(d_tables);
-    float *ly = reinterpret_cast<float *>(t);
-    float *lx = reinterpret_cast<float *>(t + pad256((size_t)H * 4));
-    float *lut = reinterpret_cast<float *>(t + pad256((size_t)H * 4) + pad256((size_t)W * 4));
-    pred_index_kernel<<<(H + 255) / 256, 256, 0, s>>>(d_ctrs_y, nPY, ly, H);
-    pred_index_kernel<<<(W + 255) / 256, 256, 0, s>>>(d_ctrs_x, nPX, lx, W);
+    const WarpTables t = warp_tables(d_tables, H, W);
+    pred_index_kernel<<<(H + 255) / 256, 256, 0, s>>>(d_ctrs_y, nPY, t.ly, H);
+    pred_index_kernel<<<(W + 255) / 256, 256, 0, s>>>(d_ctrs_x, nPX, t.lx, W);
+    row_weights_kernel<<<(H + 255) / 256, 256, 0, s>>>(t.ly, H, t.wyb, t.byr);
     std::call_once(g_lut_once, build_lut_host);
-    if (cudaMemcpyAsync(lut, g_lut_host, sizeof(g_lut_host), cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(t.lut, g_lut_host, sizeof(g_lut_host), cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
@@ -317,20 +491,19 @@ PIV_EXPORT int pivb_warp_dev(const float *d_ia, const float *d_ib, float *d_oa, 
     if (!d_ia || !d_ib || !d_oa || !d_ob || !d_pdy || !d_pdx || !d_tables) return 1;
     if ((long long)H * W >= (1LL << 31) - 64 || (long long)nPY * nPX >= (1LL << 31)) return 1;  // 32-bit offsets
     if (img_stride < (long long)H * W) return 1;
-    const char *t = static_cast<const char *>(d_tables);
+    const WarpTables t = warp_tables(const_cast<void *>(d_tables), H, W);
     WarpParams p;
     p.ia = d_ia; p.ib = d_ib; p.oa = d_oa; p.ob = d_ob; p.pdy = d_pdy; p.pdx = d_pdx;
     p.pred_stride = shared_predictor ? 0 : (long long)nPY * nPX;
     p.img_stride = img_stride;
     p.N = N; p.H = H; p.W = W; p.nPY = nPY; p.nPX = nPX;
-    p.ly = reinterpret_cast<const float *>(t);
-    p.lx = reinterpret_cast<const float *>(t + pad256((size_t)H * 4));
-    p.lut = reinterpret_cast<const float *>(t + pad256((size_t)H * 4) + pad256((size_t)W * 4));
+    p.ly = t.ly; p.lx = t.lx; p.lut = t.lut; p.wyb = t.wyb; p.byr = t.byr;
     p.round_shifts = round_shifts;
+    p.neg_zero = -0.0f;
     dim3 blk(32, 4), grd((W + 31) / 32, (H + 4 * kWarpRows - 1) / (4 * kWarpRows), N);   // 32 x 4 measured best
     cudaStream_t s = (cudaStream_t)stream;
     if (interp_mode == 0) {
-        if (impl) warp_kernel<0, 1><<<grd, blk, 0, s>>>(p);
+        if (impl) warp_bicubic_x2_kernel<<<grd, blk, 0, s>>>(p);
         else warp_kernel<0, 0><<<grd, blk, 0, s>>>(p);
     } else {
         if (impl) warp_kernel<1, 1><<<grd, blk, 0, s>>>(p);
