@@ -9,12 +9,15 @@
 // exp(-2*pi*i*k*n/N), SIGN = +1 the inverse; neither is normalised.
 #pragma once
 
+#include "f32x2.cuh"
 #include "piv_common.cuh"
 
 namespace piv {
 
-__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// Complex sums as one paired FP32 instruction each (f32x2): the same two IEEE
+// additions, half the issue slots (measured +9% at 32 px, +6% at 64 px).
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) { return add2(a, b); }
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) { return sub2(a, b); }
 
 // v * exp(SIGN * 2*pi*i * m / N), constant twiddle.
 template <int N, int m, int SIGN>
@@ -47,12 +50,12 @@ __device__ __forceinline__ void butterfly(float2 (&t)[R])
     } else if constexpr (R == 3) {
         constexpr float k = 0.866025403784438646763723170752936f;   // sqrt(3)/2
         float2 s = c_add(t[1], t[2]), d = c_sub(t[1], t[2]);
-        float2 m = make_float2(t[0].x - 0.5f * s.x, t[0].y - 0.5f * s.y);
+        const float2 m = fma2(dup2(-0.5f), s, t[0]);           // t0 - s/2, one rounding
         t[0] = c_add(t[0], s);
-        // y1 = m + SIGN*i*k*d, y2 = m - SIGN*i*k*d
-        float2 r = make_float2(-(float)SIGN * k * d.y, (float)SIGN * k * d.x);
-        t[1] = c_add(m, r);
-        t[2] = c_sub(m, r);
+        // y1 = m + SIGN*i*k*d, y2 = m - SIGN*i*k*d (scalar: each a fused multiply-add)
+        constexpr float sk = (float)SIGN * k;
+        t[1] = make_float2(m.x - sk * d.y, m.y + sk * d.x);
+        t[2] = make_float2(m.x + sk * d.y, m.y - sk * d.x);
     } else {  // R == 4
         float2 a = c_add(t[0], t[2]), b = c_sub(t[0], t[2]);
         float2 c = c_add(t[1], t[3]), d = c_sub(t[1], t[3]);
