@@ -209,6 +209,7 @@ PIV_EXPORT int pivb_xcorr_dev(const float *d_A, const float *d_B, long long img_
     p.pk_ratio = d_pk_ratio; p.planes = d_planes;
     p.lm = defer ? static_cast<LmRecord *>(d_scratch) : nullptr;
     p.total = total;
+    p.neg_zero = -0.0f;
     const bool timing = g_timing != 0;
     if (timing) cudaEventRecord(g_ws.ev[0], s);
     int e = (n_peaks > 1 && !ensemble) ? launch_xcorr<true>(win_h, p, s) : launch_xcorr<false>(win_h, p, s);
@@ -828,6 +829,7 @@ PIV_EXPORT int pivb_xcorr_dev_noalloc(const float *d_A, const float *d_B, long l
     p.pk_ratio = d_pk_ratio; p.planes = d_planes;
     p.lm = records;
     p.total = total;
+    p.neg_zero = -0.0f;
     const int e = (n_peaks > 1 && !ensemble) ? launch_xcorr<true>(win_h, p, s) : launch_xcorr<false>(win_h, p, s);
     if (e) return e;
     if (lm) {

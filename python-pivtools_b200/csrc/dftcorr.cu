@@ -627,6 +627,7 @@ PIV_EXPORT int pivb_dft_xcorr_dev(const float *d_A, const float *d_B, long long 
     p.pk_ratio = d_pk_ratio; p.planes = d_planes;
     p.lm = defer ? static_cast<LmRecord *>(d_scratch) : nullptr;
     p.total = total;
+    p.neg_zero = -0.0f;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -307,9 +307,8 @@ __device__ __forceinline__ void fill_lane_twiddles(float2 *tw, int tid, int nthr
 }
 
 template <int N>
-__device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, const float (&a)[WinGeo<N>::M],
-                                                const float (&b)[WinGeo<N>::M], float scale,
-                                                const float2 *tw = nullptr)
+__device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, const float2 (&zab)[WinGeo<N>::M],
+                                                float scale, const float2 *tw = nullptr)
 {
     using G = WinGeo<N>;
     constexpr int M = G::M, P = G::P, ST = G::ST;
@@ -336,7 +335,7 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
     const int lb = line / M, rb = rm / M;
     float2 z[M];
 #pragma unroll
-    for (int n = 0; n < M; ++n) z[n] = make_float2(a[n], b[n]);
+    for (int n = 0; n < M; ++n) z[n] = zab[n];
 #pragma unroll 1
     for (int pass = 0;; ++pass) {
         RegFFT<M, -1>::run(z);
