@@ -20,13 +20,14 @@
 #include "peakfit_dev.cuh"
 
 // Resident correlation CTAs per SM that the register allocation is capped for
-// (measured on B200: 32 px 4, 64 px 4; 3 or 5 at 32 px and 3 or 5 at 64 px are
-// slower, 6 at 32 px spills).
+// (measured on B200 with the paired FP32 FFT: 32 px 5 (96 registers, +1% over
+// 4), 64 px 6 (168 registers, +0.6% over 4); before the pairing, 5 at 32 px was
+// slower and 6 spilled).
 #ifndef PIVB_MIN_CTAS_32
-#define PIVB_MIN_CTAS_32 4
+#define PIVB_MIN_CTAS_32 5
 #endif
 #ifndef PIVB_MIN_CTAS_64
-#define PIVB_MIN_CTAS_64 4
+#define PIVB_MIN_CTAS_64 6
 #endif
 
 namespace piv {
