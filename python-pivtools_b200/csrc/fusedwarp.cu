@@ -252,8 +252,9 @@ __global__ void row_weights_kernel(const float *ly, int H, float4 *wyb, int *byr
 
 // Output rows per thread.  The rows of one thread share the column-side work
 // (predictor column weights and indices) and, while they fall in the same
-// predictor cell row, the 4x4 predictor patch, which stays in registers.
-constexpr int kWarpRows = 8;
+// predictor cell row, the 4x4 predictor patch, which stays in registers
+// (measured with the paired kernel: 16 rows 3% faster than 8, 4 rows 7% slower).
+constexpr int kWarpRows = 16;
 
 template <int MODE, int IMPL>
 __global__ void __launch_bounds__(128) warp_kernel(WarpParams p)
