@@ -1,9 +1,11 @@
 """ctypes bindings for the CPU oracle (TEST INFRASTRUCTURE ONLY).
 
 `lib/libpivoracle.so` is the project's C restatement of the reference path;
-`_ref/libpeakfit_ref.so` and `_ref/libfusedwarp_ref.so` are the reference's own
-peak fitter and warp compiled from its sources by `make -C oracle ref`.  Only the
-tests, the smoke check and bench.py's CPU-baseline leg import this module.
+`_ref/libpeakfit_ref.so`, `_ref/libfusedwarp_ref.so`, `_ref/libbulkxcorr2d_ref.so`
+and `_ref/libkspacefit_ref.so` are the reference's own fitter, warp, correlator and
+k-space fitter compiled from its sources by `make -C oracle ref
+PIVTOOLS_REF=<reference checkout>`.  Only the tests, the smoke check and bench.py's
+CPU legs import this module.
 """
 
 from __future__ import annotations
@@ -18,7 +20,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libpivoracle.so")
 REF_PEAKFIT = os.path.join(HERE, "_ref", "libpeakfit_ref.so")
 REF_WARP = os.path.join(HERE, "_ref", "libfusedwarp_ref.so")
-REF_SRC = "/root/reference/pivtools_cli/lib"
+REF_BULK = os.path.join(HERE, "_ref", "libbulkxcorr2d_ref.so")
+REF_KSPACE = os.path.join(HERE, "_ref", "libkspacefit_ref.so")
 
 _f32 = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _f64 = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -28,11 +31,18 @@ _vp = ctypes.c_void_p
 _ci = ctypes.c_int
 
 
+def ref_root() -> str | None:
+    """The reference checkout named by $PIVTOOLS_REF, if it holds the C sources."""
+    r = os.environ.get("PIVTOOLS_REF", "")
+    return r if r and os.path.isfile(os.path.join(r, "pivtools_cli", "lib", "PIV_2d_cross_correlate.c")) else None
+
+
 def build(with_ref: bool = True) -> None:
-    """Compile the restatement (always) and the reference sources (when present)."""
+    """Compile the restatement (always) and, when $PIVTOOLS_REF names a reference
+    checkout, the reference's own libraries from its sources."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if with_ref and os.path.isdir(REF_SRC):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    if with_ref and ref_root():
+        subprocess.run(["make", "-s", "-j4", "-C", HERE, "ref", f"PIVTOOLS_REF={ref_root()}"], check=True)
 
 
 _lib = None
@@ -104,6 +114,124 @@ def ref_warp() -> ctypes.CDLL | None:
                                              _ci, _ci, _ci, _f32, _f32, _ci, _ci, _ci]
     L.fused_symmetric_warp_batch.restype = ctypes.c_int
     return L
+
+
+def ref_bulk() -> ctypes.CDLL | None:
+    """The reference's own libbulkxcorr2d (correlator + fitters), or None if not built."""
+    if not os.path.isfile(REF_BULK):
+        return None
+    L = ctypes.CDLL(REF_BULK)
+    L.bulkxcorr2d.argtypes = [_f32, _f32, _f32, _i32, _ci, _f32, _f32, _i32, _f32, ctypes.c_bool,
+                              _f32, _i32, _ci, _ci, _f32, _f32, _f32, _f32, _f32, _f32, _f32, _vp]
+    L.bulkxcorr2d.restype = ctypes.c_ubyte
+    L.bulkxcorr2d_accumulate_triple.argtypes = [_f32, _f32, _f32, _i32, _ci, _f32, _f32, _i32,
+                                                _f32, _f32, _f32, _f32, _i32, _vp, _ci, _ci,
+                                                _f32, _f32, _f32]
+    L.bulkxcorr2d_accumulate_triple.restype = ctypes.c_ubyte
+    L.bulkxcorr2d_set_peakfit_impl.argtypes = [_ci]
+    L.bulkxcorr2d_set_peakfit_impl.restype = ctypes.c_int
+    return L
+
+
+def ref_kspace() -> ctypes.CDLL | None:
+    """The reference's own libkspacefit, or None if not built."""
+    if not os.path.isfile(REF_KSPACE):
+        return None
+    L = ctypes.CDLL(REF_KSPACE)
+    L.kspace_lm_fit_batch.argtypes = [_f64, _f64, _f64, _u8, _vp, _ci, _ci, _ci, _ci, _ci, _ci,
+                                      _f64, _i32, _f64, _f64, _f64, _f64, _f64, _f64, _i32,
+                                      _i32, _u8]
+    L.kspace_lm_fit_batch.restype = ctypes.c_int
+    return L
+
+
+def ref_bulkxcorr2d(A, B, mask, ctr_x, ctr_y, win_size, weight_a, weight_b, n_peaks=1,
+                    peak_finder=3, ensemble=False, want_planes=False, peakfit_impl=0):
+    """The reference's compiled bulkxcorr2d (PIV_2d_cross_correlate.c:203-397) with
+    the output dict of bulkxcorr2d() below; outputs are zero-filled first, as the
+    reference's caller does."""
+    L = ref_bulk()
+    if L is None:
+        raise RuntimeError("reference correlator not built (make -C oracle ref)")
+    A = np.ascontiguousarray(A, np.float32)
+    B = np.ascontiguousarray(B, np.float32)
+    if A.ndim == 2:
+        A, B = A[None], B[None]
+    n, H, W = A.shape
+    ny, nx = len(ctr_y), len(ctr_x)
+    h, w = win_size
+    shp = (n, n_peaks, ny, nx)
+    out = {k: np.zeros(shp, np.float32) for k in ("pk_x", "pk_y", "pk_h", "sx", "sy", "sxy")}
+    out["pk_ratio"] = np.zeros((n, ny, nx), np.float32)
+    planes = np.zeros(n * ny * nx * h * w, np.float32) if want_planes else None
+    if L.bulkxcorr2d_set_peakfit_impl(int(peakfit_impl)) != 0:
+        raise RuntimeError("reference batch fitter unavailable")
+    try:
+        e = L.bulkxcorr2d(
+            A, B, np.ascontiguousarray(mask, np.float32).ravel(), np.array([H, W], np.int32), n,
+            np.ascontiguousarray(ctr_x, np.float32), np.ascontiguousarray(ctr_y, np.float32),
+            np.array([ny, nx], np.int32), np.ascontiguousarray(weight_a, np.float32).ravel().copy(),
+            bool(ensemble), np.ascontiguousarray(weight_b, np.float32).ravel(),
+            np.array([h, w], np.int32), n_peaks, peak_finder, out["pk_x"], out["pk_y"],
+            out["pk_h"], out["sx"], out["sy"], out["sxy"], out["pk_ratio"], _ptr(planes))
+    finally:
+        L.bulkxcorr2d_set_peakfit_impl(0)
+    out["error"] = int(e)
+    if planes is not None:
+        out["planes"] = planes.reshape(n, ny, nx, h, w)
+    return out
+
+
+def ref_accumulate_triple(A, B, mask, ctr_x, ctr_y, win_size, w_ab_a, w_ab_b, w_auto_a,
+                          w_auto_b, fit_size=None, mean_subtract=0, per_pair_norm=0):
+    """The reference's compiled bulkxcorr2d_accumulate_triple
+    (PIV_2d_cross_correlate.c:627-833) into zeroed sums; returns [AB, AA, BB]."""
+    L = ref_bulk()
+    if L is None:
+        raise RuntimeError("reference correlator not built (make -C oracle ref)")
+    A = np.ascontiguousarray(A, np.float32)
+    B = np.ascontiguousarray(B, np.float32)
+    n, H, W = A.shape
+    ny, nx = len(ctr_y), len(ctr_x)
+    oh, ow = fit_size if fit_size is not None else win_size
+    sums = [np.zeros(ny * nx * oh * ow, np.float32) for _ in range(3)]
+    fs = None if fit_size is None else np.array(fit_size, np.int32)
+    e = L.bulkxcorr2d_accumulate_triple(
+        A, B, np.ascontiguousarray(mask, np.float32).ravel(), np.array([H, W], np.int32), n,
+        np.ascontiguousarray(ctr_x, np.float32), np.ascontiguousarray(ctr_y, np.float32),
+        np.array([ny, nx], np.int32), *[np.ascontiguousarray(x, np.float32).ravel() for x in
+                                        (w_ab_a, w_ab_b, w_auto_a, w_auto_b)],
+        np.array(win_size, np.int32), _ptr(fs), mean_subtract, per_pair_norm, *sums)
+    if e:
+        raise ValueError(f"reference accumulate_triple error {e}")
+    return [s.reshape(ny, nx, oh, ow) for s in sums]
+
+
+def ref_kspace_fit(R_AA, R_BB, R_AB, mask, corr_size, use_kx4=0, use_ky4=0, P_win=None,
+                   n_threads=0):
+    """The reference's compiled kspace_lm_fit_batch (kspace_lm_fit.c:669-884) with the
+    output dict of kspace_fit() below."""
+    L = ref_kspace()
+    if L is None:
+        raise RuntimeError("reference k-space fitter not built (make -C oracle ref)")
+    h, w = corr_size
+    R_AA = np.ascontiguousarray(R_AA, np.float64).ravel()
+    R_BB = np.ascontiguousarray(R_BB, np.float64).ravel()
+    R_AB = np.ascontiguousarray(R_AB, np.float64).ravel()
+    n = R_AA.size // (h * w)
+    m = np.ascontiguousarray(mask, np.uint8).ravel()
+    P = None if P_win is None else np.ascontiguousarray(P_win, np.float64).ravel()
+    o = dict(gauss_flat=np.zeros((n, 16)), status=np.zeros(n, np.int32),
+             initial_guess=np.zeros((n, 16)), gain=np.zeros(n), N0=np.zeros(n),
+             b4x=np.zeros(n), b4y=np.zeros(n), cost_per_pt=np.zeros(n),
+             n_valid=np.zeros(n, np.int32), iters=np.zeros(n, np.int32),
+             conv=np.zeros(n, np.uint8))
+    r = L.kspace_lm_fit_batch(R_AA, R_BB, R_AB, m, _ptr(P), n, h, w, use_kx4, use_ky4, n_threads,
+                              o["gauss_flat"], o["status"], o["initial_guess"], o["gain"],
+                              o["N0"], o["b4x"], o["b4y"], o["cost_per_pt"], o["n_valid"],
+                              o["iters"], o["conv"])
+    o["ret"] = int(r)
+    return o
 
 
 # --------------------------------------------------------------------------- #

@@ -326,6 +326,22 @@ class MultipassPIV:
                 out[i].add_pass(pr)
         return out
 
+    def pass_inputs(self, k, A, B):
+        """The frames pass k of the last run correlated, rebuilt on the device: the
+        raw frames for pass 0, else both frames warped again by pass k-1's padded
+        predictor (still held in its buffers).  Returns device tensors (views of
+        internal buffers for k > 0, overwritten by the next run or call)."""
+        if k == 0:
+            return A, B
+        n = self._last_n
+        prev = self.passes[k - 1]
+        fa, fb = self.warped
+        self._ok(self.Lw.pivb_warp_dev(A.data_ptr(), B.data_ptr(), fa.data_ptr(), fb.data_ptr(),
+                                       prev["pdy"].data_ptr(), prev["pdx"].data_ptr(), n, self.H, self.W,
+                                       prev["nyp"], prev["nxp"], self.H * self.W, self.tables[k].data_ptr(),
+                                       self.cfg.interp_mode, 0, 0, self.cfg.warp_impl, self._stream()), "warp")
+        return fa[:n], fb[:n]
+
     def vectors_per_step(self) -> int:
         p = self.passes[-1]
         return self.N * p["ny"] * p["nx"]

@@ -7,12 +7,17 @@ Python package).  The fixtures are committed; tests never need the reference.
 
     python tests/golden/make_golden.py            # peakfit_ref.npz, warp_ref.npz
     python tests/golden/make_golden.py kspace     # kspace_ref.npz
+    python tests/golden/make_golden.py kspace_c   # kspace_c_ref.npz (compiled k-space fitter)
     python tests/golden/make_golden.py ensemble   # ensemble_ref.npz
     python tests/golden/make_golden.py ingest     # ingest_ref.npz
     python tests/golden/make_golden.py validate   # validate_ref.npz
     python tests/golden/make_golden.py results    # results_in.npz, results_ref/
     python tests/golden/make_golden.py floor      # floor_ref.npz
     python tests/golden/make_golden.py vmask      # vmask_ref.npz
+    python tests/golden/make_golden.py xcorr      # xcorr_ref.npz, triple_ref.npz
+
+The reference checkout is named by $PIVTOOLS_REF (its libraries are built from it
+by `make -C oracle ref PIVTOOLS_REF=...`).
 """
 
 from __future__ import annotations
@@ -28,7 +33,11 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle as O  # noqa: E402
 
-REF_ROOT = "/root/reference"
+REF_ROOT = os.environ.get("PIVTOOLS_REF", "")
+if not os.path.isdir(os.path.join(REF_ROOT, "pivtools_cli")):
+    raise SystemExit("set PIVTOOLS_REF to the reference checkout")
+sys.path.insert(0, os.path.join(ROOT, "python-pivtools_b200"))
+sys.path.insert(0, HERE)
 
 
 def gauss(shape, amp, i0, j0, s1, s2, cov, kind):
@@ -236,6 +245,27 @@ def make_kspace():
             out[f"{key}_init"] = np.asarray(ig)
     np.savez_compressed(os.path.join(HERE, "kspace_ref.npz"), **out)
     print("kspace_ref.npz written")
+
+
+def make_kspace_c():
+    """Outputs of the reference's compiled kspace_lm_fit_batch (kspace_lm_fit.c,
+    built by make -C oracle ref) on kspace_ref.npz's inputs."""
+    g = np.load(os.path.join(HERE, "kspace_ref.npz"))
+    if O.ref_kspace() is None:
+        raise SystemExit("build the reference k-space fitter first: make -C oracle ref")
+    corr = tuple(int(v) for v in g["corr"])
+    out = {}
+    for shape in ("gaussian", "kx4", "ky4", "kx4+ky4"):
+        for floor in ("flat", "coloured"):
+            o = O.ref_kspace_fit(g["R_AA"], g["R_BB"], g["R_AB"], g["mask"], corr,
+                                 use_kx4=int("kx4" in shape), use_ky4=int("ky4" in shape),
+                                 P_win=g["P_win"] if floor == "coloured" else None, n_threads=1)
+            assert o["ret"] == 0
+            key = f"{shape}_{floor}"
+            for k in ("gauss_flat", "status", "initial_guess", "gain", "N0", "iters"):
+                out[f"{key}_{k}"] = o[k]
+    np.savez_compressed(os.path.join(HERE, "kspace_c_ref.npz"), **out)
+    print("kspace_c_ref.npz written")
 
 
 def _reference_functions(path, names):
@@ -561,14 +591,57 @@ def make_vmask():
     print("vmask_ref.npz written")
 
 
+def make_xcorr():
+    """Outputs of the reference's compiled bulkxcorr2d and
+    bulkxcorr2d_accumulate_triple on the seeded cases of xcorr_cases.py."""
+    import xcorr_cases as XC
+
+    if O.ref_bulk() is None:
+        raise SystemExit("build the reference correlator first: make -C oracle ref")
+    out = {}
+    names = []
+    for c in XC.all_cases():
+        r = O.ref_bulkxcorr2d(c["A"], c["B"], c["mask"], c["cx"], c["cy"], c["win"], c["wa"], c["wb"],
+                              n_peaks=c["n_peaks"], peak_finder=c["finder"], ensemble=c["ensemble"],
+                              want_planes=len(c["plane_idx"]) > 0, peakfit_impl=c["impl"])
+        nm = c["name"]
+        names.append(nm)
+        out[f"{nm}__error"] = np.int32(r["error"])
+        out[f"{nm}__checksum"] = np.float64(XC.checksum(c))
+        for k in XC.OUT_KEYS:
+            out[f"{nm}__{k}"] = r[k]
+        if len(c["plane_idx"]):
+            h, w = c["win"]
+            out[f"{nm}__planes"] = r["planes"].reshape(-1, h, w)[c["plane_idx"]]
+    out["names"] = np.array(names)
+    np.savez_compressed(os.path.join(HERE, "xcorr_ref.npz"), **out)
+    print("xcorr_ref.npz written:", len(names), "cases")
+    tout = {}
+    tnames = []
+    for c in XC.triple_cases():
+        s = O.ref_accumulate_triple(c["A"], c["B"], np.zeros((len(c["cy"]), len(c["cx"])), np.float32),
+                                    c["cx"], c["cy"], c["win"], *c["w"], fit_size=c["fit"],
+                                    mean_subtract=c["ms"], per_pair_norm=c["pn"])
+        tnames.append(c["name"])
+        for k, v in zip(("ab", "aa", "bb"), s):
+            tout[f"{c['name']}__{k}"] = v.reshape(-1, *v.shape[2:])[c["keep"]]
+    tout["names"] = np.array(tnames)
+    np.savez_compressed(os.path.join(HERE, "triple_ref.npz"), **tout)
+    print("triple_ref.npz written:", len(tnames), "cases")
+
+
 if __name__ == "__main__":
     what = sys.argv[1:] or ["peakfit", "warp"]
+    if "xcorr" in what:
+        make_xcorr()
     if "peakfit" in what:
         make_peakfit()
     if "warp" in what:
         make_warp()
     if "kspace" in what:
         make_kspace()
+    if "kspace_c" in what:
+        make_kspace_c()
     if "ensemble" in what:
         make_ensemble()
     if "ingest" in what:

@@ -208,3 +208,24 @@ def test_vector_masks_match_reference_fixture():
             for k in range(3):
                 ref = g[f"c{ci}_t{ti}_p{k}"]
                 assert ref.any() and np.array_equal(got[k], ref), (ci, thr, k)
+
+
+@pytest.mark.parametrize("shape", ["gaussian", "kx4", "ky4", "kx4+ky4"])
+@pytest.mark.parametrize("floor", ["flat", "coloured"])
+def test_kspace_matches_reference_c_library(oracle, shape, floor):
+    """The restated fitter against the reference's compiled kspace_lm_fit.c
+    (fixture golden/kspace_c_ref.npz): equal statuses, Sigma and mu within 1e-8."""
+    g = np.load(os.path.join(GOLD, "kspace_ref.npz"))
+    c = np.load(os.path.join(GOLD, "kspace_c_ref.npz"))
+    corr = tuple(int(v) for v in g["corr"])
+    o = oracle.kspace_fit(g["R_AA"], g["R_BB"], g["R_AB"], g["mask"], corr,
+                          use_kx4=int("kx4" in shape), use_ky4=int("ky4" in shape),
+                          P_win=g["P_win"] if floor == "coloured" else None)
+    key = f"{shape}_{floor}"
+    assert np.array_equal(o["status"], c[f"{key}_status"])
+    ok = o["status"] == 0
+    assert ok.any()
+    gp = c[f"{key}_gauss_flat"]
+    assert np.abs(o["gauss_flat"][ok, 9:12] - gp[ok, 9:12]).max() < 1e-8
+    assert np.abs(o["gauss_flat"][ok, 14:16] - gp[ok, 14:16]).max() < 1e-8
+    np.testing.assert_allclose(o["initial_guess"], c[f"{key}_initial_guess"], rtol=0, atol=1e-12)

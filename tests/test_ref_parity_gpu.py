@@ -1,0 +1,199 @@
+"""GPU parity against the reference's own compiled libraries.
+
+The GPU C-ABI (host-pointer `bulkxcorr2d`, `bulkxcorr2d_accumulate_triple`,
+`kspace_lm_fit_batch`) is compared with outputs of the reference's
+libbulkxcorr2d / libkspacefit built from its sources (fixtures
+`golden/xcorr_ref.npz`, `golden/triple_ref.npz`, `golden/kspace_c_ref.npz`, made by
+`golden/make_golden.py`), and -- where `oracle/_ref/libbulkxcorr2d_ref.so` is
+present -- live on the multipass workload's pass geometries at full size.
+
+Bars (the path's parity contract):
+  * correlation planes within 1e-5 of each plane's peak;
+  * 3-point fits: NaN sentinels identical and displacements within 0.005 px,
+    except windows whose two tallest candidate maxima lie within 1e-5 relative
+    (the integer argmax then follows rounding), which are listed;
+  * LM fits (gauss4-6): at most 6% NaN-sentinel flips and at most 3% of jointly
+    fitted windows beyond 0.005 px -- the reference's trust rule is a hard
+    threshold that 1e-7 plane differences cross (its own restatement flips up to
+    4% against it on the same inputs); the rates are printed;
+  * skipped windows (outside the frame, masked) untouched; error codes equal;
+  * accumulated ensemble sums within 1e-5 of each plane's peak;
+  * k-space fits: identical status, Sigma and mu within 1e-8.
+"""
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from pivtools_b200 import _lib, correlator, geometry
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+sys.path.insert(0, GOLD)
+import xcorr_cases as XC  # noqa: E402
+
+
+def _gpu_rect_supported():
+    return bool(getattr(_lib.bulkxcorr2d_lib(), "pivb_rect_windows_supported", lambda: 0)())
+
+
+@pytest.fixture(scope="module")
+def fixture():
+    return np.load(os.path.join(GOLD, "xcorr_ref.npz"))
+
+
+def _ref(g, name):
+    r = {k: g[f"{name}__{k}"] for k in XC.OUT_KEYS}
+    if f"{name}__planes" in g:
+        r["planes"] = g[f"{name}__planes"]
+    return r
+
+
+def _gpu(case, dump=True):
+    correlator.set_peakfit_impl(case["impl"])
+    try:
+        o = correlator.bulkxcorr2d(case["A"], case["B"], case["cx"], case["cy"], case["win"], case["wa"],
+                                   case["wb"], mask=case["mask"], n_peaks=case["n_peaks"],
+                                   peak_finder=case["finder"], ensemble=case["ensemble"], dump_planes=dump)
+    finally:
+        correlator.set_peakfit_impl(0)
+    return {"pk_x": o["pk_loc_x"], "pk_y": o["pk_loc_y"], "pk_h": o["pk_height"], "sx": o["sx"],
+            "sy": o["sy"], "sxy": o["sxy"], "pk_ratio": o["pk_ratio"], "planes": o.get("planes")}
+
+
+def _check_three_point(st, planes, case):
+    """Every output beyond the bar must come from a documented near-tie plane."""
+    ties = []
+    nwin = len(case["cy"]) * len(case["cx"])
+    for k in st["far_idx"]:
+        w = (k // (case["n_peaks"] * nwin)) * nwin + k % nwin
+        if not XC.near_tie(planes[w]):
+            raise AssertionError(f"output {k} differs from the reference and is not a near-tie: {st}")
+        ties.append(int(k))
+    return ties
+
+
+@pytest.mark.parametrize("case", XC.all_cases(), ids=lambda c: c["name"])
+def test_correlator_matches_reference_library(cuda, fixture, case):
+    nm = case["name"]
+    h, w = case["win"]
+    if h != w and not _gpu_rect_supported():
+        pytest.skip("rectangular windows are not built on the GPU path")
+    assert XC.checksum(case) == float(fixture[f"{nm}__checksum"]), "case inputs changed"
+    o = _gpu(case)
+    planes = o["planes"].reshape(-1, h, w)
+    st = XC.compare(case, o, _ref(fixture, nm), planes)
+    print(f"\n{nm}: windows {st['n']}, NaN flips {st['nan_flip']}, beyond 0.005 px {st['n_far']}, "
+          f"max |d| {st['max_d']:.2e} px, median |d| {st['median_d']:.1e} px, "
+          f"plane err {st.get('plane_rel', float('nan')):.1e}, height err {st['height_rel']:.1e}")
+    assert st["zeros_equal"], nm
+    if "plane_rel" in st:
+        assert st["plane_rel"] <= 1e-5, st["plane_rel"]
+    assert st["height_rel"] <= 1e-4, st["height_rel"]
+    if case["finder"] == 3:
+        ties = _check_three_point(st, planes, case)
+        assert len(ties) <= max(1, 0.005 * st["n"]), ties
+        if ties:
+            print(f"{nm}: near-tie windows {ties}")
+    else:
+        assert st["nan_flip"] <= 0.06 * st["n"], st
+        assert st["n_far"] <= max(1, 0.03 * st["n"]), st
+        assert st["median_d"] < 1e-4, st
+
+
+@pytest.mark.parametrize("case", XC.triple_cases(), ids=lambda c: c["name"])
+def test_triple_matches_reference_library(cuda, case):
+    g = np.load(os.path.join(GOLD, "triple_ref.npz"))
+    L = _lib.bulkxcorr2d_lib()
+    A, B = case["A"], case["B"]
+    n, H, W = A.shape
+    ny, nx = len(case["cy"]), len(case["cx"])
+    oh, ow = case["fit"] if case["fit"] is not None else case["win"]
+    outs = [np.zeros(ny * nx * oh * ow, np.float32) for _ in range(3)]
+    fs = None if case["fit"] is None else np.array(case["fit"], np.int32)
+    code = L.bulkxcorr2d_accumulate_triple(
+        A, B, np.zeros(ny * nx, np.float32), np.array([H, W], np.int32), n, case["cx"], case["cy"],
+        np.array([ny, nx], np.int32), *[np.ascontiguousarray(x, np.float32).ravel() for x in case["w"]],
+        np.array(case["win"], np.int32), None if fs is None else fs.ctypes.data, case["ms"], case["pn"], *outs)
+    assert code == 0
+    for k, v in zip(("ab", "aa", "bb"), outs):
+        R = g[f"{case['name']}__{k}"]
+        V = v.reshape(ny * nx, oh, ow)[case["keep"]]
+        sc = np.abs(R).reshape(len(R), -1).max(axis=1)
+        sc[sc == 0] = 1.0
+        err = (np.abs(V - R).reshape(len(R), -1).max(axis=1) / sc).max()
+        assert err <= 1e-5, (k, err)
+
+
+@pytest.mark.parametrize("shape", ["gaussian", "kx4", "ky4", "kx4+ky4"])
+@pytest.mark.parametrize("floor", ["flat", "coloured"])
+def test_kspace_matches_reference_library(cuda, shape, floor):
+    g = np.load(os.path.join(GOLD, "kspace_ref.npz"))
+    c = np.load(os.path.join(GOLD, "kspace_c_ref.npz"))
+    L = _lib.kspacefit_lib()
+    h, w = (int(v) for v in g["corr"])
+    n = g["R_AA"].size // (h * w)
+    o = dict(gauss=np.zeros((n, 16)), status=np.zeros(n, np.int32), init=np.zeros((n, 16)))
+    d = [np.zeros(n) for _ in range(5)] + [np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.uint8)]
+    P = np.ascontiguousarray(g["P_win"], np.float64) if floor == "coloured" else None
+    r = L.kspace_lm_fit_batch(np.ascontiguousarray(g["R_AA"]), np.ascontiguousarray(g["R_BB"]),
+                              np.ascontiguousarray(g["R_AB"]), np.ascontiguousarray(g["mask"], np.uint8),
+                              None if P is None else P.ctypes.data, n, h, w, int("kx4" in shape),
+                              int("ky4" in shape), 0, o["gauss"], o["status"], o["init"], *d)
+    assert r == 0
+    key = f"{shape}_{floor}"
+    assert np.array_equal(o["status"], c[f"{key}_status"])
+    ok = o["status"] == 0
+    gp = c[f"{key}_gauss_flat"]
+    assert np.abs(o["gauss"][ok, 9:12] - gp[ok, 9:12]).max() < 1e-8
+    assert np.abs(o["gauss"][ok, 14:16] - gp[ok, 14:16]).max() < 1e-8
+    np.testing.assert_allclose(o["init"], c[f"{key}_initial_guess"], rtol=0, atol=1e-12)
+
+
+def test_multipass_passes_match_reference_and_fp64(cuda, oracle):
+    """The multipass workload's geometry at full size: one 2048^2 channel-flow
+    pair through the four passes (128/64/32/32 px at 50/50/50/75%, bicubic warps,
+    3-point fits).  Each pass's GPU vectors, from inside the resident pipeline,
+    are compared with (a) the reference's compiled bulkxcorr2d on the same warped
+    frames (when it is built here) and (b) the FP64 oracle on the same frames: RMS
+    displacement difference <= 0.01 px per pass against FP64 (the accuracy half
+    of the metric), and the 3-point bar against the reference."""
+    import torch
+
+    from pivtools_b200 import multipass, synthetic
+
+    HW = (2048, 2048)
+    A, B = synthetic.channel_batch_torch(1, HW, seed=2026, device=cuda)
+    mp = multipass.MultipassPIV(HW, 1, device=cuda)
+    mp.run(A, B)
+    torch.cuda.synchronize()
+    ref_lib = oracle.ref_bulk() is not None
+    for k, (p, g) in enumerate(zip(mp.passes, mp.geo)):
+        fa, fb = mp.pass_inputs(k, A, B)
+        fa, fb = fa[0].cpu().numpy(), fb[0].cpu().numpy()
+        gx = p["out"]["pk_loc_x"][0, 0].cpu().numpy()
+        gy = p["out"]["pk_loc_y"][0, 0].cpu().numpy()
+        w = geometry.window_weight(g.window_size, "gaussian")
+        m = np.zeros((p["ny"], p["nx"]), np.float32)
+        o64 = oracle.bulkxcorr2d(fa, fb, m, g.grid.win_ctrs_x, g.grid.win_ctrs_y, g.window_size, w, w)
+        both = np.isfinite(gx) & np.isfinite(o64["pk_x"][0, 0])
+        rms = float(np.sqrt(np.mean((gx - o64["pk_x"][0, 0])[both] ** 2 + (gy - o64["pk_y"][0, 0])[both] ** 2)))
+        print(f"\npass {k} ({g.window_size[0]} px, {p['ny']}x{p['nx']}): RMS vs FP64 {rms:.2e} px, "
+              f"NaN flips vs FP64 {int((np.isnan(gx) != np.isnan(o64['pk_x'][0, 0])).sum())}")
+        assert rms <= 0.01, (k, rms)
+        if ref_lib:
+            r = oracle.ref_bulkxcorr2d(fa, fb, m, g.grid.win_ctrs_x, g.grid.win_ctrs_y, g.window_size, w, w)
+            rx, ry = r["pk_x"][0, 0], r["pk_y"][0, 0]
+            d = np.maximum(np.abs(gx - rx), np.abs(gy - ry))
+            flips = np.isnan(gx) != np.isnan(rx)
+            far = np.nonzero(flips | (np.isfinite(d) & (d > 0.005)))
+            print(f"pass {k}: vs reference library: max |d| {np.nanmax(d):.2e} px, NaN flips {int(flips.sum())}, "
+                  f"beyond 0.005 px {len(far[0])}")
+            if len(far[0]):
+                rp = oracle.ref_bulkxcorr2d(fa, fb, m, g.grid.win_ctrs_x, g.grid.win_ctrs_y, g.window_size, w, w,
+                                            want_planes=True)["planes"][0]
+                for i, j in zip(*far):
+                    assert XC.near_tie(rp[i, j]), (k, i, j, gx[i, j], rx[i, j])
+            assert len(far[0]) <= max(1, 0.001 * d.size)
