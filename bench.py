@@ -45,7 +45,9 @@ def _args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--pairs", type=int, default=64)
     ap.add_argument("--no-graph", action="store_true")
-    ap.add_argument("--cpu-pairs", type=int, default=1)
+    ap.add_argument("--cpu-pairs", type=int, default=2, help="CPU baseline leg: pairs in its batch")
+    ap.add_argument("--ref-pairs", type=int, default=4, help="reference arm: pairs per (sampled) step")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the per-pass RMS against FP64")
     ap.add_argument("--workload", default="multipass", choices=["multipass", "ensemble", "serve"],
                     help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
                          "serve: Poisson request stream with continuous batching")
@@ -124,72 +126,129 @@ def _dist():
     return ws, rank, local
 
 
+def _workload_config(n_pairs, ws, vec_step, win_step):
+    """The workload as both arms state it (identical keys and values)."""
+    return {"workload": WORKLOAD, "pairs_per_step_per_gpu": n_pairs, "image": "2048x2048 uint16 counts",
+            "passes": "128/64/32/32 px, 50/50/50/75%", "window_weight": "gaussian", "peak_finder": "gauss3",
+            "warp": "bicubic symmetric, smoothed predictor",
+            "validation": "gate win/2 then win/4; peak_mag 0.25; normalised median 5x5 (eps 0.1, thr 2)",
+            "infill": "least squares between passes and after the last",
+            "vectors_per_step_per_gpu": vec_step, "windows_per_step_per_gpu": win_step,
+            "l2": "inputs 4.3 GB > L2, no flush", "parallelism": f"dp{ws} (pairs)"}
+
+
+def _ref_frames(n_pairs, seed):
+    """Host frames of the workload for the CPU arms (the same generator as the GPU
+    arm's, run on the host)."""
+    from pivtools_b200 import synthetic
+
+    A, B = synthetic.channel_batch_torch(n_pairs, HW, seed=seed, device="cpu")
+    return A.numpy(), B.numpy()
+
+
+def _ref_pipeline():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_multipass as RM
+    from pivtools_b200 import geometry, multipass
+
+    cfg = multipass.MultipassConfig()
+    geo = geometry.multipass_geometry(HW, cfg.window_sizes, cfg.overlaps, cfg.window_type)
+    return RM, RM.RefMultipass(geo, window_type=cfg.window_type, peak_finder=cfg.peak_finder,
+                               infill="biharmonic", final_infill=cfg.final_infill)
+
+
 def _cpu_baseline(n_pairs: int):
-    """CPU leg: the oracle port's correlation of all four passes plus the
-    reference's own warp (compiled from source, when present; else the oracle
-    warp), all host threads, on n_pairs pairs.  Returns (vectors/s, sample)."""
+    """CPU leg: the reference's multipass (its compiled libbulkxcorr2d and
+    libfusedwarp, built from its sources, under OpenMP on every host core; the
+    driver's glue restated in NumPy/SciPy/cv2) on n_pairs pairs in one batch, then
+    one pair on one thread.  Returns the cpu_baseline object."""
+    RM, rm = _ref_pipeline()
+    A, B = _ref_frames(n_pairs, seed=900)
+    cores = os.cpu_count() or 1
+    RM.set_threads(cores)
+    rm.run(A[:1], B[:1])                        # load libraries, warm caches
+    t0 = time.perf_counter()
+    rm.run(A, B)
+    dt = time.perf_counter() - t0
+    RM.set_threads(1)
+    t1 = time.perf_counter()
+    rm.run(A[:1], B[:1])
+    dt1 = time.perf_counter() - t1
+    RM.set_threads(cores)
+    vec = 64009
+    return {"value": n_pairs * vec / dt, "unit": "vectors/s", "cores": cores, "kind": "reference",
+            "value_1_thread": vec / dt1,
+            "sample": f"{n_pairs} pairs of the workload in one batch through the reference's compiled "
+                      f"libbulkxcorr2d + libfusedwarp (OpenMP, {cores} threads; glue in NumPy/SciPy/cv2, "
+                      f"biharmonic infill): {dt:.2f} s; 1 pair on 1 thread: {dt1:.2f} s"}
+
+
+def run_reference(args):
+    """The reference's own CPU path on this workload: every step is one batch of
+    --ref-pairs pairs (a bounded sample of the 64-pair step) through the
+    reference's pass loop over its compiled libraries, all host threads."""
+    ws, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    RM, rm = _ref_pipeline()
+    P = args.ref_pairs
+    A, B = _ref_frames(P, seed=2026)
+    cores = os.cpu_count() or 1
+    RM.set_threads(cores)
+    for _ in range(args.warmup):
+        rm.run(A, B)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        rm.run(A, B)
+        times.append(time.perf_counter() - t0)
+    ms = statistics.median(times) * 1e3
+    vec = 64009
+    value = P * vec / (ms * 1e-3)
+    geo_win = 31 * 31 + 63 * 63 + 127 * 127 + 253 * 253
+    sample = (f"{P} pairs per step (of the 64-pair workload step) through the reference's compiled "
+              f"libbulkxcorr2d + libfusedwarp, OpenMP {cores} threads, glue in NumPy/SciPy/cv2, biharmonic "
+              f"infill; median of {args.steps} steps")
+    line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": _workload_config(64, ws, 64 * vec, 64 * geo_win),
+            "impl": "reference", "sample_pairs_per_step": P,
+            "cpu_baseline": {"value": value, "unit": "vectors/s", "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "vectors/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _rms_vs_fp64(mp, A, B):
+    """Per pass, pair 0: the resident pipeline's 3-point displacements against
+    the FP64 oracle (and, when built, the reference's compiled correlator) on the
+    same frames the pass correlated.  RMS over windows both fit."""
     import numpy as np
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    from pivtools_b200 import geometry, synthetic
+    from pivtools_b200 import geometry
 
-    geo = geometry.multipass_geometry(HW, [(128, 128), (64, 64), (32, 32), (32, 32)], [50, 50, 50, 75])
-    pairs = [synthetic.particle_pair(HW, seed=900 + k, flow="channel")[:2] for k in range(n_pairs)]
-    ref_warp = O.ref_warp()
-    cores = os.cpu_count() or 1
-    t0 = time.perf_counter()
-    for A, B in pairs:
-        for k, g in enumerate(geo):
-            fa, fb = A, B
-            if k > 0:
-                prev = geo[k - 1]
-                pdy = np.zeros((len(prev.ctrs_y_all), len(prev.ctrs_x_all)), np.float32)
-                if ref_warp is not None:
-                    ref_warp.fused_warp_set_impl(1)
-                    fa = np.zeros_like(A)
-                    fb = np.zeros_like(B)
-                    ref_warp.fused_symmetric_warp_batch(A[None], B[None], fa, fb, pdy[None], pdy[None], 1, HW[0],
-                                                        HW[1], pdy.shape[0], pdy.shape[1], prev.ctrs_y_all,
-                                                        prev.ctrs_x_all, 0, 0, 0)
-                else:
-                    fa, fb = O.fused_warp_batch(A[None], B[None], pdy[None], pdy[None], prev.ctrs_y_all,
-                                                prev.ctrs_x_all)
-                    fa, fb = fa[0], fb[0]
-            w = geometry.window_weight(g.window_size, "gaussian")
-            O.bulkxcorr2d(fa, fb, np.zeros((g.grid.n_win_y, g.grid.n_win_x), np.float32), g.grid.win_ctrs_x,
-                          g.grid.win_ctrs_y, g.window_size, w, w, peak_finder=3)
-    dt = time.perf_counter() - t0
-    vec = n_pairs * geo[-1].grid.n_win_y * geo[-1].grid.n_win_x
-    sample = (f"{n_pairs} pair(s) of 2048^2: oracle-port FP64-FFT correlation of the 4 passes + "
-              f"{'reference fused_warp.c (SIMD route)' if ref_warp is not None else 'oracle warp'} x3, "
-              f"validation/infill omitted; {dt:.2f} s")
-    return vec / dt, sample, cores
-
-
-def run_reference(args):
-    ws, rank, _ = (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
-    if rank != 0:
-        return
-    vals = []
-    sample = ""
-    cores = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        _cpu_baseline(args.cpu_pairs)
-    t_all = []
-    for _ in range(args.steps):
-        v, sample, cores = _cpu_baseline(args.cpu_pairs)
-        vals.append(v)
-    value = statistics.median(vals)
-    vec_step = 64009 * args.pairs
-    line = {"metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": vec_step / value * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "pairs_per_step": args.pairs, "timed_sample_pairs": args.cpu_pairs},
-            "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": "vectors/s", "cores": cores, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": "vectors/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    out = []
+    for k, (p, g) in enumerate(zip(mp.passes, mp.geo)):
+        fa, fb = mp.pass_inputs(k, A[:1], B[:1])
+        fa, fb = fa[0].cpu().numpy(), fb[0].cpu().numpy()
+        gx = p["out"]["pk_loc_x"][0, 0].cpu().numpy()
+        gy = p["out"]["pk_loc_y"][0, 0].cpu().numpy()
+        w = geometry.window_weight(g.window_size, mp.cfg.window_type)
+        m = np.zeros((p["ny"], p["nx"]), np.float32)
+        row = {"pass": k, "window": g.window_size[0], "windows": int(gx.size)}
+        for name, fn in (("fp64", O.bulkxcorr2d), ("reference", O.ref_bulkxcorr2d if O.ref_bulk() else None)):
+            if fn is None:
+                continue
+            r = fn(fa, fb, m, g.grid.win_ctrs_x, g.grid.win_ctrs_y, g.window_size, w, w)
+            rx, ry = r["pk_x"][0, 0], r["pk_y"][0, 0]
+            both = np.isfinite(gx) & np.isfinite(rx)
+            row[f"rms_px_vs_{name}"] = float(np.sqrt(np.mean((gx - rx)[both] ** 2 + (gy - ry)[both] ** 2)))
+            row[f"nan_flips_vs_{name}"] = int((np.isnan(gx) != np.isnan(rx)).sum())
+        out.append(row)
+    return out
 
 
 def run_b200(args):
@@ -333,38 +392,46 @@ def run_b200(args):
     e2e_same = bool(torch.allclose(ux_h, fin["ux"].cpu(), rtol=0, atol=0, equal_nan=True)
                     and torch.allclose(uy_h, fin["uy"].cpu(), rtol=0, atol=0, equal_nan=True))
 
+    accuracy = None
+    if rank == 0 and ws == 1 and not args.no_accuracy:
+        with torch.cuda.stream(stream):
+            mp.run(A, B)                        # the resident buffers hold this run's passes
+        stream.synchronize()
+        accuracy = _rms_vs_fp64(mp, A, B)
     cpu = None
     if rank == 0 and ws == 1 and os.environ.get("PIVB_SKIP_CPU") != "1":
-        v, sample, cores = _cpu_baseline(args.cpu_pairs)
-        cpu = {"value": v, "unit": "vectors/s", "cores": cores, "kind": "port", "sample": sample}
+        cpu = _cpu_baseline(args.cpu_pairs)
 
     if rank == 0:
+        fp32_tflops = fp32_flops / (kern_ms * 1e-3) / 1e12
+        if mp.Ld is not None:
+            roof = {"bound": "tensor", "achieved": windows * 1.769e6 / (kern_ms * 1e-3) / 1e12,
+                    "peak": bf16_peak, "unit": "TFLOP/s",
+                    "frac": windows * 1.769e6 / (kern_ms * 1e-3) / 1e12 / bf16_peak, "traffic": None,
+                    "peak_kind": peak_kind, "tensor_flops_per_window": 1.769e6,
+                    "kernel": "dft32 tcgen05 kernel + lm_records_kernel (final pass, 4.1M windows)",
+                    "kernel_ms": kern_ms, "hbm_view": {"achieved_gbs": achieved, "frac": achieved / hbm_peak}}
+        else:
+            roof = {"bound": "fp32", "achieved": fp32_tflops, "peak": FP32_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+                    "frac": fp32_tflops / FP32_NOMINAL_TFLOPS, "traffic": traffic,
+                    "traffic_unit": "bytes per launch (DRAM read + write)",
+                    "peak_kind": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz; no measured FP32 figure)",
+                    "flops_per_window": 80.1e3, "flops_per_launch": fp32_flops,
+                    "kernel": "xcorr_kernel<32> + lm_records_kernel (final pass, 4.1M windows)",
+                    "kernel_ms": kern_ms,
+                    "hbm_view": {"algorithmic_bytes": alg_bytes, "achieved_gbs": achieved, "peak_gbs": hbm_peak,
+                                 "frac": achieved / hbm_peak, "peak_kind": peak_kind}}
         line = {
             "metric": METRIC, "value": value, "unit": "vectors/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "pairs_per_step_per_gpu": N, "image": "2048x2048",
-                       "passes": "128/64/32/32 px, 50/50/50/75%", "peak_finder": "gauss3", "warp": "bicubic",
-                       "vectors_per_step_per_gpu": vec_step, "windows_per_step_per_gpu": mp.windows_per_step(),
-                       "cuda_graph": graph is not None, "l2": "inputs 4.3 GB > L2, no flush",
-                       "engine_32px": "tensor-core DFT-as-GEMM (split BF16 x3)" if args.engine32 == "dft" else "FP32 FFT",
-                       "parallelism": f"dp{ws} (pairs)"},
-            "pair_latency_ms": {"p50": step_ms[len(step_ms) // 2] / N, "p99": step_ms[-1] / N,
-                                "note": "per-pair share of a batched step; served latency comes from the serving loop"},
-            "roofline": ({"bound": "tensor", "achieved": windows * 1.769e6 / (kern_ms * 1e-3) / 1e12,
-                          "peak": bf16_peak, "unit": "TFLOP/s",
-                          "frac": windows * 1.769e6 / (kern_ms * 1e-3) / 1e12 / bf16_peak, "traffic": None,
-                          "peak_kind": peak_kind, "tensor_flops_per_window": 1.769e6,
-                          "kernel": "dft32 tcgen05 kernel + lm_records_kernel (final pass, 4.1M windows)",
-                          "kernel_ms": kern_ms, "hbm_view": {"achieved_gbs": achieved, "frac": achieved / hbm_peak}}
-                         if mp.Ld is not None else
-                         {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                          "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
-                          "kernel": "xcorr_kernel<32> + lm_records_kernel (final pass, 4.1M windows)", "kernel_ms": kern_ms,
-                          "algorithmic_bytes": alg_bytes,
-                          "fp32_view": {"flops_per_launch": fp32_flops, "peak_tflops_nominal": FP32_NOMINAL_TFLOPS,
-                                        "frac_of_nominal": fp32_flops / (kern_ms * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS,
-                                        "achieved_tflops": fp32_flops / (kern_ms * 1e-3) / 1e12}}),
+            "config": _workload_config(N, ws, vec_step, mp.windows_per_step()),
+            "impl_detail": {"cuda_graph": graph is not None,
+                            "engine_32px": ("tensor-core DFT-as-GEMM (split BF16 x3)" if args.engine32 == "dft"
+                                            else "FP32 FFT"),
+                            "infill": mp.cfg.infill if hasattr(mp.cfg, "infill") else "harmonic (Jacobi)"},
+            "step_ms": {"p50": step_ms[len(step_ms) // 2], "max": step_ms[-1]},
+            "roofline": roof,
             "e2e": {"value": e2e_val, "unit": "vectors/s", "h2d_bytes_per_step": 2 * N * HW[0] * HW[1] * 2,
                     "d2h_bytes_per_step": 2 * N * p["ny"] * p["nx"] * 4, "frames": "uint16",
                     "chunk_pairs": chunk, "gpu_launches_per_step": e2e_launches, "host_frames_pinned": True,
@@ -372,6 +439,11 @@ def run_b200(args):
             "gpu_launches": mp.launches_per_step * args.steps,
             "clocks": clk.summary(),
         }
+        if accuracy is not None:
+            line["accuracy"] = {"per_pass": accuracy,
+                                "rms_px_vs_fp64": max(r["rms_px_vs_fp64"] for r in accuracy),
+                                "note": "pair 0, each pass against the FP64 oracle (and the reference's compiled "
+                                        "correlator) on the frames that pass correlated; the headline is the worst pass"}
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)

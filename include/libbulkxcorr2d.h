@@ -143,9 +143,11 @@ int pivb_accumulate_dev(const float *d_A, const float *d_B, long long img_stride
  * pipeline that cannot take the device synchronisation cudaFree implies.  The
  * deferred-LM scratch is a fixed 16 MiB file-scope device array: at most 131072
  * windows per call when LM records are needed (nPeaks 1, finder 4-6); larger calls
- * return 1 (NOMEM) with a message on stderr.  The first call on a device resolves
- * the array's address (cudaGetSymbolAddress) and must precede any stream capture.
- * All calls share the array; calls overlapping on the GPU race. */
+ * return 1 (NOMEM) with a message on stderr.  The first call on a device, of any
+ * window size, resolves the array's address (cudaGetSymbolAddress) and sets up
+ * the correlation kernels of every built window size on that device; make it
+ * before any stream capture.  All calls share the array; calls overlapping on
+ * the GPU race. */
 int pivb_xcorr_dev_noalloc(const float *d_A, const float *d_B, long long img_stride,
                            const float *d_mask, int H, int W, int n_images, const float *d_ctr_x,
                            const float *d_ctr_y, int n_win_y, int n_win_x, const float *d_wA,

@@ -14,6 +14,7 @@
 
 #include <mutex>
 
+#include "device_state.h"
 #include "xcorr_kernels.cuh"
 
 using namespace piv;
@@ -28,25 +29,20 @@ volatile int g_timing = 0;
 double g_t_fft = 0.0, g_t_fit = 0.0;
 volatile int g_peakfit_impl = 0;
 
+// Staging workspace of the host-pointer entry points on one device: a device
+// block, a stream and timing events, all created on that device.
 struct Workspace {
     void *dev = nullptr;
     size_t cap = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    int device = -1;
 
     int ensure(size_t bytes)
     {
-        int d;
-        if (cudaGetDevice(&d) != cudaSuccess) return PIV_ERROR_CUDA;
-        if (device != d) {
-            // first use on this device
-            if (stream == nullptr) {
-                if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return PIV_ERROR_CUDA;
-                for (auto &e : ev)
-                    if (cudaEventCreate(&e) != cudaSuccess) return PIV_ERROR_CUDA;
-            }
-            device = d;
+        if (stream == nullptr) {
+            if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) return PIV_ERROR_CUDA;
+            for (auto &e : ev)
+                if (cudaEventCreate(&e) != cudaSuccess) return PIV_ERROR_CUDA;
         }
         if (bytes > cap) {
             if (dev) cudaFree(dev);
@@ -62,7 +58,15 @@ struct Workspace {
         return PIV_ERROR_NONE;
     }
 };
-Workspace g_ws;
+Workspace g_ws_dev[kMaxDevices];
+// The current device's workspace (nullptr without a usable device).  Host-pointer
+// calls use it under g_mu; the timing events are also recorded by the device
+// entry points (after ensure(0) has created them).
+Workspace *cur_ws()
+{
+    const int d = current_device();
+    return d < 0 ? nullptr : &g_ws_dev[d];
+}
 
 // Bump allocator over one device block.
 struct Carve {
@@ -90,34 +94,38 @@ bool size_ok(int n)
     }
 }
 
-int g_num_sms = 0;
-int num_sms()
+// Resident CTAs per SM of xcorr_kernel<N, MULTI> on `dev`, set up once per device
+// (raises the kernel's dynamic shared-memory limit there first); -1 on failure.
+template <int N, bool MULTI>
+int xcorr_blocks_per_sm(int dev)
 {
-    if (g_num_sms == 0) {
-        int d = 0;
-        cudaGetDevice(&d);
-        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, d);
-        if (g_num_sms <= 0) g_num_sms = 148;
-    }
-    return g_num_sms;
+    using G = WinGeo<N>;
+    static PerDeviceOnce per_sm;
+    return per_sm.get(dev, [] {
+        auto kern = xcorr_kernel<N, MULTI>;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES) != cudaSuccess)
+            return -1;
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, G::CTA_THREADS, G::SMEM_BYTES) != cudaSuccess)
+            return -1;
+        return nb > 0 ? nb : 1;
+    });
 }
 
 template <int N, bool MULTI>
 int launch_xcorr_n(const XcorrParams &p, cudaStream_t s)
 {
     using G = WinGeo<N>;
-    static int per_sm = -1;
     auto kern = xcorr_kernel<N, MULTI>;
+    const int dev = current_device();
+    if (dev < 0) return PIV_ERROR_CUDA;
+    const int per_sm = xcorr_blocks_per_sm<N, MULTI>(dev);
     if (per_sm < 0) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES) != cudaSuccess)
-            return PIV_ERROR_CUDA;
-        int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, G::CTA_THREADS, G::SMEM_BYTES) != cudaSuccess)
-            return PIV_ERROR_CUDA;
-        per_sm = nb > 0 ? nb : 1;
+        cudaGetLastError();
+        return PIV_ERROR_CUDA;
     }
     long long want = (p.total + G::GROUPS_PER_CTA - 1) / G::GROUPS_PER_CTA;
-    long long cap = (long long)per_sm * num_sms();
+    long long cap = (long long)per_sm * device_sms(dev);
     int grid = (int)(want < cap ? want : cap);
     if (grid < 1) grid = 1;
     kern<<<grid, G::CTA_THREADS, G::SMEM_BYTES, s>>>(p);
@@ -210,11 +218,16 @@ PIV_EXPORT int pivb_xcorr_dev(const float *d_A, const float *d_B, long long img_
     p.lm = defer ? static_cast<LmRecord *>(d_scratch) : nullptr;
     p.total = total;
     p.neg_zero = -0.0f;
-    const bool timing = g_timing != 0;
-    if (timing) cudaEventRecord(g_ws.ev[0], s);
+    Workspace *tw = nullptr;
+    if (g_timing != 0) {
+        tw = cur_ws();
+        if (tw == nullptr || tw->ensure(0)) return PIV_ERROR_CUDA;
+    }
+    const bool timing = tw != nullptr;
+    if (timing) cudaEventRecord(tw->ev[0], s);
     int e = (n_peaks > 1 && !ensemble) ? launch_xcorr<true>(win_h, p, s) : launch_xcorr<false>(win_h, p, s);
     if (e) return e;
-    if (timing) cudaEventRecord(g_ws.ev[1], s);
+    if (timing) cudaEventRecord(tw->ev[1], s);
     if (defer) {
         const unsigned blocks = (unsigned)((total + 127) / 128);
         if (peakfit_impl) lm_records_kernel<1><<<blocks, 128, 0, s>>>(p, win_h);
@@ -222,11 +235,11 @@ PIV_EXPORT int pivb_xcorr_dev(const float *d_A, const float *d_B, long long img_
         if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
     }
     if (timing) {
-        cudaEventRecord(g_ws.ev[2], s);
-        if (cudaEventSynchronize(g_ws.ev[2]) != cudaSuccess) return PIV_ERROR_CUDA;
+        cudaEventRecord(tw->ev[2], s);
+        if (cudaEventSynchronize(tw->ev[2]) != cudaSuccess) return PIV_ERROR_CUDA;
         float t0 = 0.f, t1 = 0.f;
-        cudaEventElapsedTime(&t0, g_ws.ev[0], g_ws.ev[1]);
-        cudaEventElapsedTime(&t1, g_ws.ev[1], g_ws.ev[2]);
+        cudaEventElapsedTime(&t0, tw->ev[0], tw->ev[1]);
+        cudaEventElapsedTime(&t1, tw->ev[1], tw->ev[2]);
         g_t_fft += t0 * 1e-3;
         g_t_fit += t1 * 1e-3;
     }
@@ -253,17 +266,23 @@ int accum_grid(long long nwt)
 {
     using G = WinGeo<N>;
     constexpr bool SM = accum_in_smem<N>();
-    static int per_sm = -1;
-    auto kern = accum_kernel<N, SM>;
+    static PerDeviceOnce per_sm_dev;
     const size_t smem = SM ? accum_smem_bytes<N>() : (size_t)(G::SMEM_BYTES - G::WT_BYTES);
-    if (per_sm < 0) {
+    const int dev = current_device();
+    if (dev < 0) return -1;
+    const int per_sm = per_sm_dev.get(dev, [smem] {
+        auto kern = accum_kernel<N, SM>;
         if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
         int nb = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, G::CTA_THREADS, smem) != cudaSuccess) return -1;
-        per_sm = nb > 0 ? nb : 1;
+        return nb > 0 ? nb : 1;
+    });
+    if (per_sm < 0) {
+        cudaGetLastError();
+        return -1;
     }
     long long want = (nwt + G::GROUPS_PER_CTA - 1) / G::GROUPS_PER_CTA;
-    long long cap = (long long)per_sm * num_sms();
+    long long cap = (long long)per_sm * device_sms(dev);
     return (int)(want < cap ? (want < 1 ? 1 : want) : cap);
 }
 
@@ -420,10 +439,12 @@ PIV_EXPORT unsigned char bulkxcorr2d(const float *fImageA, const float *fImageB,
     size_t bytes = 2 * pad256(img * 4) + pad256(nwt * 4) + pad256(nwx * 4) + pad256(nwy * 4) +
                    3 * pad256(npl * 4) + 6 * pad256(nout * 4) + pad256(nrat * 4) +
                    (fCorrelPlane_Out ? pad256((size_t)total * npl * 4) : 0) + scratch + 4096;
-    int e = g_ws.ensure(bytes);
+    Workspace *wsp = cur_ws();
+    if (wsp == nullptr) return PIV_ERROR_CUDA;
+    int e = wsp->ensure(bytes);
     if (e) return (unsigned char)e;
-    cudaStream_t s = g_ws.stream;
-    Carve c(g_ws.dev);
+    cudaStream_t s = wsp->stream;
+    Carve c(wsp->dev);
     float *dA = c.take<float>(img), *dB = c.take<float>(img);
     float *dmask = c.take<float>(nwt), *dcx = c.take<float>(nwx), *dcy = c.take<float>(nwy);
     float *dwa = c.take<float>(npl), *dwb = c.take<float>(npl), *dcw = c.take<float>(npl);
@@ -481,15 +502,17 @@ int accumulate_host(const float *A, const float *B, const float *mask, const int
     const int oh = fs ? fs[0] : h, ow = fs ? fs[1] : w;
     const size_t img = (size_t)n_images * H * W, npl = (size_t)h * w, nout = (size_t)nwt * oh * ow;
     const int nacc = triple ? 3 : 1;
-    int e = g_ws.ensure(16);   // device + stream setup before the occupancy query
+    Workspace *wsp = cur_ws();
+    if (wsp == nullptr) return PIV_ERROR_CUDA;
+    int e = wsp->ensure(16);   // device + stream setup before the occupancy query
     if (e) return e;
     const size_t scr = accum_scratch(h, nwt);
     if (scr == (size_t)-1) return PIV_ERROR_CUDA;
     size_t bytes = 2 * pad256(img * 4) + pad256(nwt * 4) + pad256(nwx * 4) + pad256(nwy * 4) + 4 * pad256(npl * 4) +
                    nacc * pad256(nout * 4) + pad256(scr) + 4096;
-    if ((e = g_ws.ensure(bytes))) return e;
-    cudaStream_t s = g_ws.stream;
-    Carve c(g_ws.dev);
+    if ((e = wsp->ensure(bytes))) return e;
+    cudaStream_t s = wsp->stream;
+    Carve c(wsp->dev);
     float *dA = c.take<float>(img), *dB = c.take<float>(img);
     float *dm = c.take<float>(nwt), *dcx = c.take<float>(nwx), *dcy = c.take<float>(nwy);
     float *dw[4];
@@ -586,10 +609,12 @@ static int fit_planes_host(const float *planes, int n_planes, const int *N, int 
     const size_t nloc = layout == 0 ? (size_t)n_planes * 3 * nPeaks : (size_t)3 * lanes;
     size_t bytes = pad256(n_planes * npl * 4) * (nPeaks > 1 ? 2 : 1) + pad256(npl * 4) + 2 * pad256(nloc * 4) +
                    pad256((size_t)n_planes * 4) + 4096;
-    int e = g_ws.ensure(bytes);
+    Workspace *wsp = cur_ws();
+    if (wsp == nullptr) return PIV_ERROR_CUDA;
+    int e = wsp->ensure(bytes);
     if (e) return e;
-    cudaStream_t s = g_ws.stream;
-    Carve c(g_ws.dev);
+    cudaStream_t s = wsp->stream;
+    Carve c(wsp->dev);
     float *dp = c.take<float>(n_planes * npl);
     float *dw = wt ? c.take<float>(npl) : nullptr;
     float *dl = loc ? c.take<float>(nloc) : nullptr;
@@ -673,10 +698,12 @@ PIV_EXPORT unsigned convolve(const float *w1, const float *w2, float *conv, cons
     const int h = N[0], w = N[1];
     if (h <= 0 || w <= 0) return PIV_ERROR_NOPLAN_BWD;
     const size_t n = (size_t)h * w;
-    int e = g_ws.ensure(3 * pad256(n * 4) + 1024);
+    Workspace *wsp = cur_ws();
+    if (wsp == nullptr) return PIV_ERROR_CUDA;
+    int e = wsp->ensure(3 * pad256(n * 4) + 1024);
     if (e) return e;
-    cudaStream_t s = g_ws.stream;
-    Carve c(g_ws.dev);
+    cudaStream_t s = wsp->stream;
+    Carve c(wsp->dev);
     float *a = c.take<float>(n), *b = c.take<float>(n), *o = c.take<float>(n);
     if (cudaMemcpyAsync(a, w1, n * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return PIV_ERROR_CUDA;
     if (cudaMemcpyAsync(b, w2, n * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return PIV_ERROR_CUDA;
@@ -693,10 +720,12 @@ PIV_EXPORT unsigned xcorr(const float *w1, const float *w2, float *corr, const i
     const int h = N[0], w = N[1];
     if (h <= 0 || w <= 0 || !size_ok(h) || !size_ok(w)) return PIV_ERROR_NOPLAN_BWD;
     const size_t n = (size_t)h * w;
-    int e = g_ws.ensure(3 * pad256(n * 4) + 1024);
+    Workspace *wsp = cur_ws();
+    if (wsp == nullptr) return PIV_ERROR_CUDA;
+    int e = wsp->ensure(3 * pad256(n * 4) + 1024);
     if (e) return e;
-    cudaStream_t s = g_ws.stream;
-    Carve c(g_ws.dev);
+    cudaStream_t s = wsp->stream;
+    Carve c(wsp->dev);
     float *a = c.take<float>(n), *b = c.take<float>(n), *o = c.take<float>(n);
     if (cudaMemcpyAsync(a, w1, n * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return PIV_ERROR_CUDA;
     if (cudaMemcpyAsync(b, w2, n * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) return PIV_ERROR_CUDA;
@@ -710,9 +739,10 @@ static float minmax_host(const float *v, int n, int want_max)
 {
     if (n <= 0) return NAN;
     std::lock_guard<std::mutex> lock(g_mu);
-    if (g_ws.ensure(pad256((size_t)n * 4) + 1024)) return NAN;
-    cudaStream_t s = g_ws.stream;
-    Carve c(g_ws.dev);
+    Workspace *wsp = cur_ws();
+    if (wsp == nullptr || wsp->ensure(pad256((size_t)n * 4) + 1024)) return NAN;
+    cudaStream_t s = wsp->stream;
+    Carve c(wsp->dev);
     float *d = c.take<float>(n), *out = c.take<float>(1);
     int *last = c.take<int>(1);
     const int minus1 = -1;
@@ -767,17 +797,50 @@ PIV_EXPORT int pivb_device_info(char *name, int len)
 // race on the array.
 //
 // Set-up: the first call on a device (with that device current) resolves the
-// array's device address with cudaGetSymbolAddress and fixes each kernel's
-// launch configuration; make that first call before any stream capture.
+// array's device address with cudaGetSymbolAddress and sets up the launch
+// configuration of the correlation kernels of every built window size, single-
+// and multi-peak (their shared-memory limit and occupancy on that device); make
+// that first call, of any size, before any stream capture.
 // Neither this set-up nor a call allocates memory: no cudaMalloc, cudaFree or
 // allocating library routine is used.
 #define PIVB_NOALLOC_SCRATCH_BYTES (16u << 20)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[PIVB_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-constexpr int kNoallocMaxDevices = 64;
-void *g_noalloc_addr[kNoallocMaxDevices] = {};
+void *g_noalloc_addr[kMaxDevices] = {};
 std::mutex g_noalloc_mu;
+
+template <bool MULTI>
+bool setup_all_sizes(int dev)
+{
+    return xcorr_blocks_per_sm<8, MULTI>(dev) >= 0 && xcorr_blocks_per_sm<12, MULTI>(dev) >= 0 &&
+           xcorr_blocks_per_sm<16, MULTI>(dev) >= 0 && xcorr_blocks_per_sm<24, MULTI>(dev) >= 0 &&
+           xcorr_blocks_per_sm<32, MULTI>(dev) >= 0 && xcorr_blocks_per_sm<48, MULTI>(dev) >= 0 &&
+           xcorr_blocks_per_sm<64, MULTI>(dev) >= 0 && xcorr_blocks_per_sm<96, MULTI>(dev) >= 0 &&
+           xcorr_blocks_per_sm<128, MULTI>(dev) >= 0;
+}
+
+// Device address of the scratch array on the current device, set up on the
+// first call there (see above); nullptr on failure.
+void *noalloc_setup()
+{
+    const int dev = current_device();
+    if (dev < 0) return nullptr;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (g_noalloc_addr[dev] == nullptr) {
+        void *addr = nullptr;
+        if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || addr == nullptr) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        if (!setup_all_sizes<false>(dev) || !setup_all_sizes<true>(dev)) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        g_noalloc_addr[dev] = addr;
+    }
+    return g_noalloc_addr[dev];
+}
 }  // namespace
 
 // pivb_xcorr_dev without the scratch arguments (see the block comment above).
@@ -792,10 +855,11 @@ PIV_EXPORT int pivb_xcorr_dev_noalloc(const float *d_A, const float *d_B, long l
     if (!size_ok(win_h) || !size_ok(win_w)) return PIV_ERROR_NOPLAN_BWD;
     if (win_h != win_w) return PIV_ERROR_NOPLAN;
     if (n_peaks < 1 || n_images < 0) return PIV_ERROR_OUT_OF_BOUNDS;
+    void *scratch = noalloc_setup();
+    if (scratch == nullptr) return PIV_ERROR_CUDA;
     const long long total = (long long)n_images * n_win_y * n_win_x;
     if (total == 0) return PIV_ERROR_NONE;
     const bool lm = !ensemble && n_peaks == 1 && peak_finder >= 4 && peak_finder <= 6;
-    LmRecord *records = nullptr;
     if (lm) {
         const size_t need = (size_t)total * sizeof(LmRecord);
         if (need > PIVB_NOALLOC_SCRATCH_BYTES) {
@@ -805,19 +869,8 @@ PIV_EXPORT int pivb_xcorr_dev_noalloc(const float *d_A, const float *d_B, long l
                     total, need, PIVB_NOALLOC_SCRATCH_BYTES, (unsigned)(PIVB_NOALLOC_SCRATCH_BYTES / sizeof(LmRecord)));
             return PIV_ERROR_NOMEM;
         }
-        int dev = -1;
-        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices) return PIV_ERROR_CUDA;
-        {
-            std::lock_guard<std::mutex> lock(g_noalloc_mu);
-            if (g_noalloc_addr[dev] == nullptr) {
-                void *addr = nullptr;
-                if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || addr == nullptr)
-                    return PIV_ERROR_CUDA;
-                g_noalloc_addr[dev] = addr;
-            }
-            records = static_cast<LmRecord *>(g_noalloc_addr[dev]);
-        }
     }
+    LmRecord *records = lm ? static_cast<LmRecord *>(scratch) : nullptr;
     cudaStream_t s = (cudaStream_t)stream;
     XcorrParams p{};
     p.A = d_A; p.B = d_B; p.img_stride = img_stride; p.mask = d_mask;

@@ -19,6 +19,7 @@
 
 #include <mutex>
 
+#include "device_state.h"
 #include "f32x2.cuh"
 #include "piv_common.cuh"
 
@@ -427,7 +428,13 @@ struct Ws {
         }
         return 0;
     }
-} g_ws;
+} g_ws_dev[piv::kMaxDevices];
+// the current device's staging workspace (nullptr without a usable device)
+inline Ws *cur_ws()
+{
+    const int d = piv::current_device();
+    return d < 0 ? nullptr : &g_ws_dev[d];
+}
 
 inline size_t pad256(size_t b) { return (b + 255) & ~size_t(255); }
 
@@ -527,9 +534,10 @@ PIV_EXPORT int fused_symmetric_warp_batch(const float *imgs_a, const float *imgs
     const size_t npred = (size_t)(shared_predictor ? 1 : N) * nPY * nPX;
     const size_t tb = pivb_warp_table_bytes(H, W);
     const size_t bytes = 4 * pad256(img * 4) + 2 * pad256(npred * 4) + pad256(nPY * 4) + pad256(nPX * 4) + tb + 4096;
-    if (g_ws.ensure(bytes)) return 1;
-    cudaStream_t s = g_ws.s;
-    char *base = static_cast<char *>(g_ws.dev);
+    Ws *wsp = cur_ws();
+    if (wsp == nullptr || wsp->ensure(bytes)) return 1;
+    cudaStream_t s = wsp->s;
+    char *base = static_cast<char *>(wsp->dev);
     size_t off = 0;
     auto take = [&](size_t b) { char *p = base + off; off += pad256(b); return p; };
     float *ia = (float *)take(img * 4), *ib = (float *)take(img * 4);

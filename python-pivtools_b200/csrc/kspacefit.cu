@@ -17,6 +17,7 @@
 
 #include <mutex>
 
+#include "device_state.h"
 #include "piv_common.cuh"
 
 namespace {
@@ -573,9 +574,14 @@ struct Ws {
         }
         return 0;
     }
-} g_ws;
+} g_ws_dev[piv::kMaxDevices];
+// the current device's staging workspace (nullptr without a usable device)
+inline Ws *cur_ws()
+{
+    const int d = piv::current_device();
+    return d < 0 ? nullptr : &g_ws_dev[d];
+}
 inline size_t pad256(size_t b) { return (b + 255) & ~size_t(255); }
-int g_sms = 0;
 
 }  // namespace
 
@@ -587,7 +593,8 @@ PIV_EXPORT size_t pivb_kspace_scratch_bytes(int n_windows, int h, int w)
     const size_t P = (size_t)h * w;
     const size_t per_warp = PER_BIN * P * 8;
     if (per_warp <= 48 * 1024) return 256;
-    int sms = g_sms > 0 ? g_sms : 148;
+    const int dev = piv::current_device();
+    const int sms = dev < 0 ? 148 : piv::device_sms(dev);
     return 256 + pad256((size_t)sms * 8 * per_warp);
 }
 
@@ -601,12 +608,9 @@ PIV_EXPORT int pivb_kspace_fit_dev(const double *d_RAA, const double *d_RBB, con
     if (!size_ok(h) || !size_ok(w)) return -1;
     if (n_windows <= 0) return 0;
     cudaStream_t s = (cudaStream_t)stream;
-    if (g_sms == 0) {
-        int d = 0;
-        cudaGetDevice(&d);
-        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, d);
-        if (g_sms <= 0) g_sms = 148;
-    }
+    const int dev = piv::current_device();
+    if (dev < 0) return -2;
+    const int n_sms = piv::device_sms(dev);
     if (scratch_bytes < pivb_kspace_scratch_bytes(n_windows, h, w) || !d_scratch) return -2;
     const size_t P = (size_t)h * w;
     const size_t per_warp = PER_BIN * P * 8;
@@ -639,8 +643,8 @@ PIV_EXPORT int pivb_kspace_fit_dev(const double *d_RAA, const double *d_RBB, con
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fit_kernel, warps * 32, smem) != cudaSuccess) return -2;
     if (per_sm < 1) per_sm = 1;
     long long want = ((long long)n_windows + warps - 1) / warps;
-    long long cap = (long long)per_sm * g_sms;
-    if (!p.use_smem) cap = (long long)g_sms * 8 / warps;   // scratch slots
+    long long cap = (long long)per_sm * n_sms;
+    if (!p.use_smem) cap = (long long)n_sms * 8 / warps;   // scratch slots
     int grid = (int)(want < cap ? want : cap);
     fit_kernel<<<grid, warps * 32, smem, s>>>(p, warps);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
@@ -660,18 +664,14 @@ PIV_EXPORT int kspace_lm_fit_batch(const double *R_AA, const double *R_BB, const
     if (n_windows <= 0) return 0;
     std::lock_guard<std::mutex> lock(g_mu);
     const size_t P = (size_t)corr_h * corr_w, nw = (size_t)n_windows;
-    if (g_ws.ensure(16)) return -2;
-    if (g_sms == 0) {
-        int d = 0;
-        cudaGetDevice(&d);
-        cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, d);
-    }
+    Ws *wsp = cur_ws();
+    if (wsp == nullptr || wsp->ensure(16)) return -2;
     const size_t scr = pivb_kspace_scratch_bytes(n_windows, corr_h, corr_w);
     const size_t bytes = 3 * pad256(nw * P * 8) + pad256(nw) + (P_win ? pad256(nw * P * 8) : 0) + 2 * pad256(nw * 128) +
                          5 * pad256(nw * 8) + 3 * pad256(nw * 4) + pad256(nw) + pad256(scr) + 4096;
-    if (g_ws.ensure(bytes)) return -2;
-    cudaStream_t s = g_ws.s;
-    char *base = static_cast<char *>(g_ws.dev);
+    if (wsp->ensure(bytes)) return -2;
+    cudaStream_t s = wsp->s;
+    char *base = static_cast<char *>(wsp->dev);
     size_t off = 0;
     auto take = [&](size_t b) { char *q = base + off; off += pad256(b); return q; };
     double *aa = (double *)take(nw * P * 8), *bb = (double *)take(nw * P * 8), *ab = (double *)take(nw * P * 8);
@@ -725,9 +725,10 @@ PIV_EXPORT int kspace_fft2_centered(const double *plane, int H, int W, double *o
     if (!size_ok(H) || !size_ok(W)) return -1;
     std::lock_guard<std::mutex> lock(g_mu);
     const size_t P = (size_t)H * W;
-    if (g_ws.ensure(5 * pad256(P * 8) + 1024)) return -2;
-    cudaStream_t s = g_ws.s;
-    double *d = static_cast<double *>(g_ws.dev);
+    Ws *wsp = cur_ws();
+    if (wsp == nullptr || wsp->ensure(5 * pad256(P * 8) + 1024)) return -2;
+    cudaStream_t s = wsp->s;
+    double *d = static_cast<double *>(wsp->dev);
     double *re = d + P, *im = d + 2 * P, *tmp = d + 3 * P;
     if (cudaMemcpyAsync(d, plane, P * 8, cudaMemcpyHostToDevice, s) != cudaSuccess) return -2;
     fft_probe_kernel<<<1, 32, (size_t)(2 * W + 2 * H) * 8, s>>>(d, H, W, re, im, tmp);
@@ -792,9 +793,10 @@ PIV_EXPORT int kspace_debug_prep(const double *R_AA, const double *R_BB, const d
     if (!size_ok(H) || !size_ok(W)) return -1;
     std::lock_guard<std::mutex> lock(g_mu);
     const size_t P = (size_t)H * W;
-    if (g_ws.ensure(12 * pad256(P * 8) + 1024)) return -2;
-    cudaStream_t s = g_ws.s;
-    double *d = static_cast<double *>(g_ws.dev);
+    Ws *wsp = cur_ws();
+    if (wsp == nullptr || wsp->ensure(12 * pad256(P * 8) + 1024)) return -2;
+    cudaStream_t s = wsp->s;
+    double *d = static_cast<double *>(wsp->dev);
     double *aa = d, *bb = d + P, *ab = d + 2 * P, *pc = d + 3 * P, *dv = d + 4 * P, *seed = d + 5 * P,
            *work = d + 6 * P;
     if (cudaMemcpyAsync(aa, R_AA, P * 8, cudaMemcpyHostToDevice, s) != cudaSuccess) return -2;

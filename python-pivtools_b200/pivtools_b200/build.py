@@ -48,10 +48,13 @@ def _stale(out: str, srcs: list[str]) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, only: list[str] | None = None) -> list[str]:
-    """Compile every target whose sources changed; return the paths built."""
+    """Compile every target whose sources changed (the targets in parallel);
+    return the paths built."""
+    from concurrent.futures import ThreadPoolExecutor
+
     os.makedirs(LIBDIR, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    built = []
+    jobs = []
     for lib, tu in TARGETS.items():
         if only and lib not in only:
             continue
@@ -61,13 +64,19 @@ def build(force: bool = False, verbose: bool = False, only: list[str] | None = N
         out = os.path.join(LIBDIR, lib)
         if not force and not _stale(out, [src] + headers):
             continue
+        jobs.append((src, out))
+
+    def one(job):
+        src, out = job
         cmd = [_nvcc(), *NVCC_FLAGS, "-o", out + ".tmp", src]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
         os.replace(out + ".tmp", out)
-        built.append(out)
-    return built
+        return out
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        return list(ex.map(one, jobs))
 
 
 if __name__ == "__main__":

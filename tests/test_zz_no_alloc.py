@@ -82,3 +82,62 @@ def test_no_alloc_refuses_oversized_call(cuda):
     # (refused on the host before any launch; the frames are never read)
     args[6] = 200000 // (case["g"].n_win_y * case["g"].n_win_x) + 1
     assert L.pivb_xcorr_dev_noalloc(*args, s) == 1
+
+
+def _skipped_grid_args(torch, dev, n_win_y, n_win_x, out):
+    """A call whose every window lies outside a 64 x 64 frame: the correlation
+    kernel writes only each window's record flag, so a full-size call stays cheap."""
+    A = torch.zeros((1, 64, 64), device=dev)
+    w = torch.ones((32, 32), device=dev)
+    cx = torch.full((n_win_x,), -1000.0, device=dev)
+    cy = torch.full((n_win_y,), -1000.0, device=dev)
+    keep = (A, w, cx, cy)
+    args = [A.data_ptr(), A.data_ptr(), A.stride(0), None, 64, 64, 1, cx.data_ptr(), cy.data_ptr(), n_win_y,
+            n_win_x, w.data_ptr(), w.data_ptr(), w.data_ptr(), 32, 32, 0, 1, 4, 0] + \
+        [out[k].data_ptr() for k in KEYS] + [None]
+    return args, keep
+
+
+def test_no_alloc_limit_is_exactly_131072_windows(cuda):
+    """131072 LM windows (256 x 512, one pair) fill the array exactly and are
+    accepted; one more window row-pair (131073 windows as 1 x 131073) is refused."""
+    import torch
+
+    L = _lib.bulkxcorr2d_lib()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {k: torch.full((256 * 512,), -7.0, device=cuda) for k in KEYS}
+    args, keep = _skipped_grid_args(torch, cuda, 256, 512, out)
+    assert L.pivb_xcorr_dev_noalloc(*args, s) == 0
+    torch.cuda.synchronize()
+    for k in KEYS:
+        assert bool((out[k] == -7.0).all()), k          # every window skipped, outputs untouched
+    big = {k: torch.full((131073,), -7.0, device=cuda) for k in KEYS}
+    args, keep = _skipped_grid_args(torch, cuda, 1, 131073, big)
+    assert L.pivb_xcorr_dev_noalloc(*args, s) == 1      # refused on the host, nothing launched
+    torch.cuda.synchronize()
+    assert bool((big["pk_x"] == -7.0).all())
+
+
+@pytest.mark.parametrize("finder,n_peaks", [(3, 1), (3, 3), (6, 2)])
+def test_no_alloc_without_lm_records_matches(cuda, finder, n_peaks):
+    """Calls that need no LM records (3-point fits, several peaks) equal the
+    scratch-taking entry point too."""
+    import torch
+
+    L = _lib.bulkxcorr2d_lib()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    case = _setup(torch, cuda, 21 + finder + n_peaks, 32, finder)
+    g = case["g"]
+    shape = (1, n_peaks, g.n_win_y, g.n_win_x)
+    ref = {k: torch.full(shape if k != "ratio" else (1, g.n_win_y, g.n_win_x), -7.0, device=cuda) for k in KEYS}
+    got = {k: torch.full_like(v, -7.0) for k, v in ref.items()}
+    ra, ga = _args(case, ref), _args(case, got)
+    ra[17] = ga[17] = n_peaks
+    total = g.n_win_y * g.n_win_x
+    nbytes = max(int(L.pivb_xcorr_scratch_bytes(total, n_peaks, finder)), int(L.pivb_xcorr_record_bytes(total)))
+    scratch = torch.empty(nbytes, dtype=torch.uint8, device=cuda)
+    assert L.pivb_xcorr_dev(*ra, scratch.data_ptr(), nbytes, s) == 0
+    assert L.pivb_xcorr_dev_noalloc(*ga, s) == 0
+    torch.cuda.synchronize()
+    for k in KEYS:
+        assert np.array_equal(got[k].cpu().numpy(), ref[k].cpu().numpy(), equal_nan=True), k
