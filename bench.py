@@ -55,7 +55,9 @@ def _args():
     ap.add_argument("--engine32", default="fft", choices=["fft", "dft"],
                     help="32 px passes on the FP32 FFT path or the tensor-core DFT-as-GEMM path")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: offered pairs/s")
-    ap.add_argument("--duration", type=float, default=20.0, help="serve: seconds of arrivals")
+    ap.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="multipass: skip the served-latency leg (Poisson arrivals, --rate for --duration s)")
     return ap.parse_args()
 
 
@@ -154,7 +156,7 @@ def _ref_pipeline():
     cfg = multipass.MultipassConfig()
     geo = geometry.multipass_geometry(HW, cfg.window_sizes, cfg.overlaps, cfg.window_type)
     return RM, RM.RefMultipass(geo, window_type=cfg.window_type, peak_finder=cfg.peak_finder,
-                               infill="biharmonic", final_infill=cfg.final_infill)
+                               infill=cfg.infill, final_infill=cfg.final_infill)
 
 
 def _cpu_baseline(n_pairs: int):
@@ -401,6 +403,11 @@ def run_b200(args):
     cpu = None
     if rank == 0 and ws == 1 and os.environ.get("PIVB_SKIP_CPU") != "1":
         cpu = _cpu_baseline(args.cpu_pairs)
+    served = None
+    if rank == 0 and ws == 1 and not args.no_serve:
+        del pipe, Ah, Bh
+        torch.cuda.empty_cache()
+        served = _serve_leg(dev, args.rate, args.duration)
 
     if rank == 0:
         fp32_tflops = fp32_flops / (kern_ms * 1e-3) / 1e12
@@ -429,7 +436,7 @@ def run_b200(args):
             "impl_detail": {"cuda_graph": graph is not None,
                             "engine_32px": ("tensor-core DFT-as-GEMM (split BF16 x3)" if args.engine32 == "dft"
                                             else "FP32 FFT"),
-                            "infill": mp.cfg.infill if hasattr(mp.cfg, "infill") else "harmonic (Jacobi)"},
+                            "infill": f"{mp.cfg.infill} least squares (FP64 CG on the GPU)"},
             "step_ms": {"p50": step_ms[len(step_ms) // 2], "max": step_ms[-1]},
             "roofline": roof,
             "e2e": {"value": e2e_val, "unit": "vectors/s", "h2d_bytes_per_step": 2 * N * HW[0] * HW[1] * 2,
@@ -439,6 +446,10 @@ def run_b200(args):
             "gpu_launches": mp.launches_per_step * args.steps,
             "clocks": clk.summary(),
         }
+        if served is not None:
+            line["latency_ms"] = {"p50": served["latency_ms"]["p50"], "p99": served["latency_ms"]["p99"],
+                                  "source": "served leg: request arrival to result in host memory"}
+            line["served"] = served
         if accuracy is not None:
             line["accuracy"] = {"per_pass": accuracy,
                                 "rms_px_vs_fp64": max(r["rms_px_vs_fp64"] for r in accuracy),
@@ -581,30 +592,27 @@ def run_ensemble(args):
         torch.distributed.destroy_process_group()
 
 
-def run_serve(args):
-    """Serving mix: Poisson arrivals at --rate pairs/s for --duration s; each
+def _serve_leg(dev, rate, duration, seed_base=0):
+    """Serving mix: Poisson arrivals at `rate` pairs/s for `duration` s; each
     request is one uint16 pair of a size drawn from {512^2, 1024^2, 2048^2,
     2048x4096} with a schedule drawn from {32; 64-32; 128-64-32-16 px} at 50%
     overlap, particle images of the single-pair workload's particle and flow model
     (uniform (3.3, -1.7) px plus a Gaussian random field of 0.5 px std and 40 px
-    correlation length; a small pool per size, cycled), frames
-    in pinned host memory, a 120 GB device budget.  Reports vectors/s over the run
-    and p50/p99 request latency (arrival to result in host memory)."""
+    correlation length; a small pool per size, cycled), frames in pinned host
+    memory, a 120 GB device budget.  Returns the served statistics: vectors/s
+    over the run and request latency (arrival to result in host memory)."""
     import numpy as np
     import torch
 
     from pivtools_b200 import serving, synthetic
 
-    ws, rank, local = _dist()
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     sizes = [(512, 512), (1024, 1024), (2048, 2048), (2048, 4096)]
     scheds = [(32,), (64, 32), (128, 64, 32, 16)]
     pool = {}
     for si, shp in enumerate(sizes):
         pool[shp] = []
         for k in range(2):
-            A, B, _ = synthetic.particle_pair(shp, seed=7000 + 10 * si + k + 1000 * rank, flow="uniform_grf",
+            A, B, _ = synthetic.particle_pair(shp, seed=7000 + 10 * si + k + 1000 * seed_base, flow="uniform_grf",
                                               device=dev)
             pool[shp].append((A.to(torch.int32).to(torch.uint16).cpu().pin_memory(),
                               B.to(torch.int32).to(torch.uint16).cpu().pin_memory()))
@@ -617,18 +625,16 @@ def run_serve(args):
             for r in srv.drain():
                 srv.release(r)
     torch.cuda.synchronize()
-    arr = serving.poisson_arrivals(args.rate, args.duration, seed=11 + rank)
-    rng = np.random.default_rng(12 + rank)
+    arr = serving.poisson_arrivals(rate, duration, seed=11 + seed_base)
+    rng = np.random.default_rng(12 + seed_base)
     picks = [(sizes[rng.integers(4)], scheds[rng.integers(3)], int(rng.integers(2))) for _ in arr]
     reqs = []
     vec = 0
     d2h = []
-    if ws > 1:
-        torch.distributed.barrier()
     import gc
 
     gc.disable()                                # no collector pauses inside the served window
-    with ClockSampler(local) as clk:
+    try:
         t0 = time.perf_counter()
         i = 0
         while i < len(arr) or not srv.idle():
@@ -643,35 +649,61 @@ def run_serve(args):
                 srv.release(r)
             time.sleep(5e-5)
         t1 = time.perf_counter()
-    gc.enable()
+    finally:
+        gc.enable()
     lat = np.array([r.done - r.arrival for r in reqs]) * 1e3
     wall = t1 - t0
     by_sched = {}
     for (shp, sch, _), l in zip(picks, lat):
         by_sched.setdefault("-".join(map(str, sch)), []).append(l)
+    out = {"vectors_per_s": vec / wall, "wall_s": wall, "requests": len(reqs), "offered_pairs_per_s": rate,
+           "served_pairs_per_s": len(reqs) / wall, "duration_s": duration,
+           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max()),
+                          "by_schedule": {k: {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),
+                                              "n": len(v)} for k, v in sorted(by_sched.items())}},
+           "h2d_bytes_per_request": float(np.mean([2 * p[0][0] * p[0][1] * 2 for p in picks])),
+           "d2h_bytes_per_request": float(np.mean(d2h)),
+           "max_batch": srv.max_batch, "hbm_budget_gb": 120, "engines": len(srv.engines),
+           "engine_bytes_gb": srv.used_bytes / 1e9,
+           "workload": f"Poisson {rate:g} pairs/s for {duration:g} s; sizes 512^2, 1024^2, 2048^2, 2048x4096 "
+                       "uint16; schedules 32 / 64-32 / 128-64-32-16 px at 50%; flow (3.3, -1.7) px + GRF 0.5 px"}
+    del srv, pool
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_serve(args):
+    """The serving mix alone (see _serve_leg) as its own JSON line."""
+    import torch
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     if ws > 1:
-        t = torch.tensor([wall], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        wall = float(t.item())
+        torch.distributed.barrier()
+    with ClockSampler(local) as clk:
+        st = _serve_leg(dev, args.rate, args.duration, seed_base=rank)
+    wall = st["wall_s"]
+    vec_total = st["vectors_per_s"] * wall
+    if ws > 1:
+        t = torch.tensor([wall, vec_total], device=dev, dtype=torch.float64)
+        w = t.clone()
+        torch.distributed.all_reduce(w, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
+        wall, vec_total = float(w[0].item()), float(t[1].item())
     if rank == 0:
         line = {
-            "metric": "served vectors/s with p50/p99 pair latency on 1 B200", "value": vec * ws / wall,
-            "unit": "vectors/s", "n_gpus": ws, "steps": len(reqs), "warmup": 2 * len(sizes) * len(scheds),
-            "ms_per_step": wall * 1e3 / max(len(reqs), 1), "higher_is_better": True, "scaling": "weak",
+            "metric": "served vectors/s with p50/p99 pair latency on 1 B200", "value": vec_total / wall,
+            "unit": "vectors/s", "n_gpus": ws, "steps": st["requests"], "warmup": 24,
+            "ms_per_step": wall * 1e3 / max(st["requests"], 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"Poisson {args.rate:g} pairs/s for {args.duration:g} s; sizes 512^2, 1024^2, "
-                                   "2048^2, 2048x4096 uint16; schedules 32 / 64-32 / 128-64-32-16 px at 50%; "
-                                   "flow (3.3, -1.7) px + GRF 0.5 px",
-                       "max_batch": srv.max_batch, "hbm_budget_gb": 120, "engines": len(srv.engines),
-                       "engine_bytes_gb": srv.used_bytes / 1e9},
-            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                           "max": float(lat.max()),
-                           "by_schedule": {k: {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),
-                                               "n": len(v)} for k, v in sorted(by_sched.items())}},
-            "offered_pairs_per_s": args.rate, "served_pairs_per_s": len(reqs) / wall,
-            "e2e": {"value": vec * ws / wall, "unit": "vectors/s",
-                    "h2d_bytes_per_step": float(np.mean([2 * p[0][0] * p[0][1] * 2 for p in picks])),
-                    "d2h_bytes_per_step": float(np.mean(d2h))},
+            "config": {"workload": st["workload"], "max_batch": st["max_batch"], "hbm_budget_gb": 120,
+                       "engines": st["engines"], "engine_bytes_gb": st["engine_bytes_gb"]},
+            "latency_ms": st["latency_ms"], "offered_pairs_per_s": st["offered_pairs_per_s"],
+            "served_pairs_per_s": st["served_pairs_per_s"],
+            "e2e": {"value": vec_total / wall, "unit": "vectors/s", "h2d_bytes_per_step": st["h2d_bytes_per_request"],
+                    "d2h_bytes_per_step": st["d2h_bytes_per_request"]},
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -27,11 +27,18 @@ int pivb_validate_dev(const float *pk_x, const float *pk_y, const float *pk_h, c
                       float *ux, float *uy, unsigned char *invalid, signed char *nan_reason,
                       float *work, void *stream);
 
-/* Harmonic inpainting of the invalid vectors in place (infilling.py:336-376).
- * work: 2*N*ny*nx floats. */
+/* Least-squares inpainting of the invalid vectors in place: the reference's
+ * infill_harmonic (order 1) / infill_biharmonic (order 2) (infilling.py:150-283,
+ * 336-421): squared first / second differences along y and x in physical units
+ * (pitch spacing_y, spacing_x) minimised over the invalid cells, valid cells
+ * fixed, rows touching a masked window (mask, (ny, nx), nullable) dropped; the
+ * normal equations solved in FP64 by conjugate gradients to relative residual
+ * tol (at most max_iter iterations).  One CTA per pair; deterministic.
+ * work: pivb_infill_work_bytes(N, ny, nx) bytes. */
+size_t pivb_infill_work_bytes(int N, int ny, int nx);
 int pivb_infill_dev(float *ux, float *uy, const unsigned char *invalid, const float *mask, int N,
-                    int ny, int nx, float spacing_y, float spacing_x, int max_iter, float tol,
-                    float *work, void *stream);
+                    int ny, int nx, float spacing_y, float spacing_x, int order, int max_iter,
+                    double tol, void *work, size_t work_bytes, void *stream);
 
 /* Edge padding onto the predictor grid + Gaussian smoothing (taps: 2*radius+1
  * normalised weights on the device; radius 0 = none).  work: N*nyp*nxp floats. */

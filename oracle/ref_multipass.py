@@ -226,6 +226,7 @@ class RefMultipass:
         B = np.ascontiguousarray(B, np.float32)
         N, H, W = A.shape
         old = None
+        self.history = []          # per pass: (ux, uy, invalid) after validation and infilling
         for k, (g, w) in enumerate(zip(self.geo, self.weights)):
             ny, nx = g.grid.n_win_y, g.grid.n_win_x
             pdy = pdx = None
@@ -265,6 +266,7 @@ class RefMultipass:
                     if bad[i].any():
                         f = fill_least_squares(np.stack([ux[i], uy[i]]), bad[i], pitch, self.order)
                         ux[i], uy[i] = f[0], f[1]
+            self.history.append((ux.copy(), uy.copy(), bad.copy()))
             if not last:
                 (py0, px0), (py1, px1) = g.n_pre, g.n_post
                 old = np.pad(np.stack([uy, ux], axis=-1), ((0, 0), (py0, py1), (px0, px1), (0, 0)), mode="edge")

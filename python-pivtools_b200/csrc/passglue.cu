@@ -5,16 +5,18 @@
 //   validate  -- large-displacement gate, add the window-grid predictor, peak
 //                magnitude and normalised-median outlier tests
 //                (outlier_detection.py:56-84, :87-243);
-//   infill    -- harmonic inpainting of invalid vectors: minimise the squared
-//                gradients (physical units) over the invalid cells with the valid
-//                cells held fixed and zero flux at the grid edge
-//                (infilling.py:336-376), solved by Jacobi iteration;
+//   infill    -- least-squares inpainting of invalid vectors: minimise the
+//                squared first (harmonic) or second (biharmonic) differences in
+//                physical units over the invalid cells with the valid cells held
+//                fixed (infilling.py:150-283, 336-421), solved exactly (FP64
+//                conjugate gradients on the normal equations);
 //   pad       -- edge-replicate padding onto the padded predictor grid
 //                (cpu_instantaneous.py:836-853) and the separable Gaussian
 //                smoothing of scipy.ndimage.gaussian_filter(mode='nearest')
 //                (cpu_instantaneous.py:1040-1048, :1140-1152);
-//   remap     -- Keys-cubic (a = -0.75) interpolation of the padded predictor at
-//                the next pass's window centres, replicate border
+//   remap     -- the padded predictor at the next pass's window centres exactly
+//                as cv2.remap(INTER_CUBIC, BORDER_REPLICATE) computes it: 1/32-px
+//                fixed-point coordinates, Keys a = -0.75 coefficient table
 //                (cpu_instantaneous.py:1050-1071).
 // The device has no libraries here: each step is a plain CUDA kernel over the
 // small vector grids, one launch per step for the whole batch of pairs.
@@ -183,127 +185,233 @@ __global__ void median_kernel(ValParams p, const float *gx, const float *gy)
     }
 }
 
-// Harmonic inpainting: one CTA per pair, Jacobi sweeps over the invalid cells.
-// Weights 1/dx^2 (x neighbours) and 1/dy^2 (y neighbours); neighbours outside
-// the grid or masked drop out (zero flux).  Cells start from the mean of the
-// pair's valid vectors; iteration stops at max_iter or when the largest update
-// is below tol (px).  The invalid cells are listed once in shared memory (any
-// order: a Jacobi sweep's updates are independent) so that a sweep touches only
-// them; grids with more invalid cells than the list holds sweep the whole grid.
-constexpr int kInfillList = 6144;
+// Least-squares infilling (infilling.py:150-283, _fill_least_squares): minimise
+// the sum of squared finite differences of order 1 (harmonic; stencil -1, 1) or
+// 2 (biharmonic; 1, -2, 1) along y and x, each difference divided by pitch^order,
+// over the fill cells with every known cell held at its value.  Only difference
+// rows that touch a fill cell enter; rows touching an excluded cell (a masked
+// window, or a non-finite value outside the fill set) are dropped, which gives
+// the frame edge's natural boundary condition there.  The normal equations
+// A x = b (A = Lf^T Lf, b = -Lf^T Lk u_k) are solved matrix-free in FP64 by
+// conjugate gradients to a relative residual `tol`, both components at once.
+//
+// One CTA per pair.  The fill cells are listed in grid order (each warp scans a
+// contiguous segment, ballot-compacts, and a block prefix over the warps places
+// the segments), threads own fixed list entries, and every dot product is a
+// fixed-order block reduction: results are bit-reproducible run to run.  A
+// group of fill cells that no row links to a known cell has b = 0 there and
+// stays at 0 (the reference raises for such a field; a pass on the GPU cannot
+// stop, so a pair without any valid vector comes out as zeros).
+constexpr int kLsqThreads = 512;
+constexpr int kLsqWarps = kLsqThreads / 32;
 
-__device__ __forceinline__ void infill_cell(int w, int ny, int nx, float wy, float wx, const float *mask,
-                                            const float *sx, const float *sy, float *dx, float *dy, float &local)
+struct LsqParams {
+    float *ux, *uy;                  // (N, ny, nx), in place
+    const unsigned char *invalid;    // (N, ny, nx) 1 = fill
+    const float *mask;               // (ny, nx) 1 = excluded, or null
+    int ny, nx, order, max_iter;
+    double w2y, w2x;                 // 1 / pitch^(2 order)
+    double tol2;                     // squared relative residual
+    char *work;                      // per pair: work_stride bytes
+    size_t work_stride;
+};
+
+__device__ __forceinline__ double2 lsq_block_sum2(double a, double b, double2 *red)
 {
-    const int r = w / nx, c = w % nx;
-    float su = 0.0f, sv = 0.0f, sw = 0.0f;
-    const int nr[4] = {r - 1, r + 1, r, r};
-    const int nc[4] = {c, c, c - 1, c + 1};
-    const float ww[4] = {wy, wy, wx, wx};
-    for (int k = 0; k < 4; ++k) {
-        if (nr[k] < 0 || nr[k] >= ny || nc[k] < 0 || nc[k] >= nx) continue;
-        const int q = nr[k] * nx + nc[k];
-        if (mask && mask[q] != 0.0f) continue;
-        su += ww[k] * sx[q];
-        sv += ww[k] * sy[q];
-        sw += ww[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
     }
-    const float nu = sw > 0.0f ? su / sw : sx[w], nv = sw > 0.0f ? sv / sw : sy[w];
-    local = fmaxf(local, fmaxf(fabsf(nu - sx[w]), fabsf(nv - sy[w])));
-    dx[w] = nu;
-    dy[w] = nv;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[warp] = make_double2(a, b);
+    __syncthreads();
+    double2 t = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < kLsqWarps; ++k) {
+        t.x += red[k].x;
+        t.y += red[k].y;
+    }
+    __syncthreads();
+    return t;
 }
 
-__global__ void __launch_bounds__(512) infill_kernel(float *ux, float *uy, const unsigned char *invalid,
-                                                     const float *mask, int ny, int nx, float wy, float wx,
-                                                     int max_iter, float tol, float *work)
+// Sum over the kept rows through fill cell (r, c) of coef(cell) * row value,
+// scaled by w^2: with `known` false the row value is sum coef * V (V zero off
+// the fill set: this is (A V)_cell), with `known` true it is the known cells'
+// part sum coef * u (giving -b_cell).
+template <int ORDER>
+__device__ __forceinline__ void lsq_rows(const unsigned char *cls, int r, int c, int ny, int nx, double w2y,
+                                         double w2x, const double *V0, const double *V1, const float *U0,
+                                         const float *U1, bool known, double &o0, double &o1)
 {
-    const int n = blockIdx.x;
-    const int plane = ny * nx;
-    float *X = ux + (long long)n * plane, *Y = uy + (long long)n * plane;
-    const unsigned char *bad = invalid + (long long)n * plane;
-    float *X2 = work + (long long)n * 2 * plane, *Y2 = X2 + plane;
-    __shared__ float s_max;
-    __shared__ int s_cnt;
-    __shared__ int s_list[kInfillList];
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
-    for (int w = threadIdx.x; w < plane; w += blockDim.x)
-        if (bad[w]) {
-            const int k = atomicAdd(&s_cnt, 1);
-            if (k < kInfillList) s_list[k] = w;
-        }
-    __syncthreads();
-    const int n_bad = s_cnt;
-    if (n_bad == 0) return;
-    const bool listed = n_bad <= kInfillList;
-    // initial guess: mean of the valid vectors (the iteration converges to the
-    // unique harmonic solution from any start; a good start shortens it)
-    // deterministic block reduction (fixed order), so repeated runs agree bit for bit
-    __shared__ float s_part[3][16];
-    __shared__ float s_su, s_sv, s_n;
-    {
-        float su = 0.0f, sv = 0.0f, cnt = 0.0f;
-        for (int w = threadIdx.x; w < plane; w += blockDim.x)
-            if (!bad[w] && !(mask && mask[w] != 0.0f)) { su += X[w]; sv += Y[w]; cnt += 1.0f; }
+    constexpr double coef[3] = {ORDER == 1 ? -1.0 : 1.0, ORDER == 1 ? 1.0 : -2.0, 1.0};
+    double a0 = 0.0, a1 = 0.0;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            su += __shfl_xor_sync(0xffffffffu, su, o);
-            sv += __shfl_xor_sync(0xffffffffu, sv, o);
-            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-        }
-        if ((threadIdx.x & 31) == 0) {
-            s_part[0][threadIdx.x >> 5] = su;
-            s_part[1][threadIdx.x >> 5] = sv;
-            s_part[2][threadIdx.x >> 5] = cnt;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            float a = 0.0f, b = 0.0f, c = 0.0f;
-            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { a += s_part[0][k]; b += s_part[1][k]; c += s_part[2][k]; }
-            s_su = a; s_sv = b; s_n = c;
-        }
-    }
-    __syncthreads();
-    const float mu = s_n > 0.0f ? s_su / s_n : 0.0f, mv = s_n > 0.0f ? s_sv / s_n : 0.0f;
-    for (int w = threadIdx.x; w < plane; w += blockDim.x) {
-        if (bad[w]) { X[w] = mu; Y[w] = mv; }
-        X2[w] = X[w];
-        Y2[w] = Y[w];
-    }
-    __syncthreads();
-    for (int it = 0; it < max_iter; ++it) {
-        if (threadIdx.x == 0) s_max = 0.0f;
-        __syncthreads();
-        float local = 0.0f;
-        // valid cells are equal in both buffers and never change
-        const float *sx = (it & 1) ? X2 : X, *sy = (it & 1) ? Y2 : Y;
-        float *dx = (it & 1) ? X : X2, *dy = (it & 1) ? Y : Y2;
-        if (listed) {
-            for (int i = threadIdx.x; i < n_bad; i += blockDim.x)
-                infill_cell(s_list[i], ny, nx, wy, wx, mask, sx, sy, dx, dy, local);
-        } else {
-            for (int w = threadIdx.x; w < plane; w += blockDim.x)
-                if (bad[w]) infill_cell(w, ny, nx, wy, wx, mask, sx, sy, dx, dy, local);
-        }
-        atomicMax(reinterpret_cast<int *>(&s_max), __float_as_int(local));   // local >= 0
-        __syncthreads();
-        const bool done = s_max < tol;
-        __syncthreads();
-        if (done || it == max_iter - 1) {
-            if (!(it & 1)) {   // result is in X2/Y2
-                if (listed) {
-                    for (int i = threadIdx.x; i < n_bad; i += blockDim.x) {
-                        const int w = s_list[i];
-                        X[w] = X2[w];
-                        Y[w] = Y2[w];
+    for (int axis = 0; axis < 2; ++axis) {
+        const int pos = axis == 0 ? r : c, len = axis == 0 ? ny : nx;
+        const int step = axis == 0 ? nx : 1;
+        const int cell = r * nx + c;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int j = 0; j <= ORDER; ++j) {
+            const int st = pos - j;                       // first node of the row
+            if (st < 0 || st + ORDER >= len) continue;
+            const int q0 = cell - j * step;
+            bool kept = true;
+            double v0 = 0.0, v1 = 0.0;
+#pragma unroll
+            for (int t = 0; t <= ORDER; ++t) {
+                const int q = q0 + t * step;
+                const unsigned char k = cls[q];
+                kept = kept && k != 2;
+                if (known) {
+                    if (k == 0) {
+                        v0 += coef[t] * (double)U0[q];
+                        v1 += coef[t] * (double)U1[q];
                     }
                 } else {
-                    for (int w = threadIdx.x; w < plane; w += blockDim.x) { X[w] = X2[w]; Y[w] = Y2[w]; }
+                    v0 += coef[t] * V0[q];
+                    v1 += coef[t] * V1[q];
                 }
             }
-            break;
+            if (kept) {
+                s0 += coef[j] * v0;
+                s1 += coef[j] * v1;
+            }
         }
+        const double w2 = axis == 0 ? w2y : w2x;
+        a0 += w2 * s0;
+        a1 += w2 * s1;
+    }
+    o0 = a0;
+    o1 = a1;
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(kLsqThreads) lsq_infill_kernel(LsqParams p)
+{
+    const int n = blockIdx.x;
+    const int plane = p.ny * p.nx;
+    float *U0 = p.ux + (long long)n * plane, *U1 = p.uy + (long long)n * plane;
+    const unsigned char *bad = p.invalid + (long long)n * plane;
+    char *wk = p.work + (size_t)n * p.work_stride;
+    auto carve = [&](size_t bytes) { char *q = wk; wk += (bytes + 255) & ~size_t(255); return q; };
+    unsigned char *cls = reinterpret_cast<unsigned char *>(carve((size_t)plane));
+    int *list = reinterpret_cast<int *>(carve((size_t)plane * 4));
+    double *P0 = reinterpret_cast<double *>(carve((size_t)plane * 8));
+    double *P1 = reinterpret_cast<double *>(carve((size_t)plane * 8));
+    double *X0 = reinterpret_cast<double *>(carve((size_t)plane * 8));
+    double *X1 = reinterpret_cast<double *>(carve((size_t)plane * 8));
+    double *R0 = reinterpret_cast<double *>(carve((size_t)plane * 8));
+    double *R1 = reinterpret_cast<double *>(carve((size_t)plane * 8));
+    double *Q0 = reinterpret_cast<double *>(carve((size_t)plane * 8));
+    double *Q1 = reinterpret_cast<double *>(carve((size_t)plane * 8));
+    __shared__ double2 red[kLsqWarps];
+    __shared__ int s_cnt[kLsqWarps];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    // classes: 1 fill, 2 excluded, 0 known; the search direction is zero off the fill set
+    for (int w = tid; w < plane; w += kLsqThreads) {
+        const bool m = p.mask && p.mask[w] != 0.0f;
+        unsigned char k = 0;
+        if (bad[w] && !m) k = 1;
+        else if (m || !isfinite(U0[w]) || !isfinite(U1[w])) k = 2;
+        cls[w] = k;
+        P0[w] = 0.0;
+        P1[w] = 0.0;
+    }
+    __syncthreads();
+    // fill cells listed in grid order
+    const int seg = (plane + kLsqWarps - 1) / kLsqWarps;
+    const int a = min(plane, warp * seg), b = min(plane, a + seg);
+    int cnt = 0;
+    for (int w0 = a; w0 < b; w0 += 32) {
+        const int w = w0 + lane;
+        cnt += __popc(__ballot_sync(0xffffffffu, w < b && cls[w] == 1));
+    }
+    if (lane == 0) s_cnt[warp] = cnt;
+    __syncthreads();
+    int base = 0, nf = 0;
+    for (int k = 0; k < kLsqWarps; ++k) {
+        base += k < warp ? s_cnt[k] : 0;
+        nf += s_cnt[k];
+    }
+    for (int w0 = a; w0 < b; w0 += 32) {
+        const int w = w0 + lane;
+        const bool f = w < b && cls[w] == 1;
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        if (f) list[base + __popc(m & ((1u << lane) - 1u))] = w;
+        base += __popc(m);
+    }
+    __syncthreads();
+    if (nf == 0) return;
+
+    // r0 = b (x0 = 0), p0 = r0
+    double rr0 = 0.0, rr1 = 0.0;
+    for (int i = tid; i < nf; i += kLsqThreads) {
+        const int w = list[i];
+        double k0, k1;
+        lsq_rows<ORDER>(cls, w / p.nx, w % p.nx, p.ny, p.nx, p.w2y, p.w2x, nullptr, nullptr, U0, U1, true, k0, k1);
+        X0[i] = 0.0;
+        X1[i] = 0.0;
+        R0[i] = -k0;
+        R1[i] = -k1;
+        P0[w] = -k0;
+        P1[w] = -k1;
+        rr0 += k0 * k0;
+        rr1 += k1 * k1;
+    }
+    double2 rr = lsq_block_sum2(rr0, rr1, red);      // includes the barrier the P writes need
+    const double stop0 = p.tol2 * rr.x, stop1 = p.tol2 * rr.y;
+    bool act0 = rr.x > 0.0, act1 = rr.y > 0.0;
+    for (int it = 0; it < p.max_iter && (act0 || act1); ++it) {
+        double pq0 = 0.0, pq1 = 0.0;
+        for (int i = tid; i < nf; i += kLsqThreads) {
+            const int w = list[i];
+            double q0, q1;
+            lsq_rows<ORDER>(cls, w / p.nx, w % p.nx, p.ny, p.nx, p.w2y, p.w2x, P0, P1, nullptr, nullptr, false, q0,
+                            q1);
+            Q0[i] = q0;
+            Q1[i] = q1;
+            pq0 += P0[w] * q0;
+            pq1 += P1[w] * q1;
+        }
+        const double2 pq = lsq_block_sum2(pq0, pq1, red);
+        act0 = act0 && pq.x > 0.0;
+        act1 = act1 && pq.y > 0.0;
+        const double al0 = act0 ? rr.x / pq.x : 0.0, al1 = act1 ? rr.y / pq.y : 0.0;
+        double rn0 = 0.0, rn1 = 0.0;
+        for (int i = tid; i < nf; i += kLsqThreads) {
+            const int w = list[i];
+            if (act0) {
+                X0[i] += al0 * P0[w];
+                R0[i] -= al0 * Q0[i];
+                rn0 += R0[i] * R0[i];
+            }
+            if (act1) {
+                X1[i] += al1 * P1[w];
+                R1[i] -= al1 * Q1[i];
+                rn1 += R1[i] * R1[i];
+            }
+        }
+        const double2 rn = lsq_block_sum2(rn0, rn1, red);
+        const double be0 = act0 ? rn.x / rr.x : 0.0, be1 = act1 ? rn.y / rr.y : 0.0;
+        for (int i = tid; i < nf; i += kLsqThreads) {
+            const int w = list[i];
+            if (act0) P0[w] = R0[i] + be0 * P0[w];
+            if (act1) P1[w] = R1[i] + be1 * P1[w];
+        }
+        if (act0) rr.x = rn.x;
+        if (act1) rr.y = rn.y;
+        act0 = act0 && rr.x > stop0;
+        act1 = act1 && rr.y > stop1;
+        __syncthreads();
+    }
+    for (int i = tid; i < nf; i += kLsqThreads) {
+        const int w = list[i];
+        U0[w] = (float)X0[i];
+        U1[w] = (float)X1[i];
     }
 }
 
@@ -338,37 +446,66 @@ __global__ void gauss_kernel(const float *in, float *out, int N, int ny, int nx,
     out[i] = (float)acc;
 }
 
-__device__ __forceinline__ void keys4(float d, float *w)
+
+// OpenCV's INTER_CUBIC coefficients (Keys, A = -0.75) at fraction x, in float
+// arithmetic with its operation order (no contraction).
+__device__ __forceinline__ void cv_cubic(float x, float (&c)[4])
 {
-    const float s0 = 1.0f + d, q2 = 1.0f - d, s3 = 2.0f - d;
-    w[1] = (1.25f * d - 2.25f) * d * d + 1.0f;
-    w[2] = (1.25f * q2 - 2.25f) * q2 * q2 + 1.0f;
-    w[0] = ((-0.75f * s0 + 3.75f) * s0 - 6.0f) * s0 + 3.0f;
-    w[3] = ((-0.75f * s3 + 3.75f) * s3 - 6.0f) * s3 + 3.0f;
+    const float A = -0.75f;
+    const float x1 = __fadd_rn(x, 1.0f), y = __fsub_rn(1.0f, x);
+    c[0] = __fsub_rn(__fmul_rn(__fadd_rn(__fmul_rn(__fsub_rn(__fmul_rn(A, x1), 5.0f * A), x1), 8.0f * A), x1),
+                     4.0f * A);
+    c[1] = __fadd_rn(__fmul_rn(__fmul_rn(__fsub_rn(__fmul_rn(A + 2.0f, x), A + 3.0f), x), x), 1.0f);
+    c[2] = __fadd_rn(__fmul_rn(__fmul_rn(__fsub_rn(__fmul_rn(A + 2.0f, y), A + 3.0f), y), y), 1.0f);
+    c[3] = __fsub_rn(__fsub_rn(__fsub_rn(1.0f, c[0]), c[1]), c[2]);
 }
 
-// Cubic remap of both padded planes at fractional grid coordinates.
+// Predictor remap as cv2.remap(INTER_CUBIC, BORDER_REPLICATE) computes it for
+// float32 planes and float maps (cpu_instantaneous.py:1050-1071): coordinates
+// rounded to 1/32 px (round half to even), 4 x 4 taps weighted by products of
+// the 32-entry coefficient table; inside the plane the four row sums are formed
+// left to right and added in row order, at the border every tap (clamped
+// indices) is added to a running sum in row-major order.
 __global__ void remap_kernel(const float *pdy, const float *pdx, int N, int nyp, int nxp, const float *map_y,
                              const float *map_x, int ny, int nx, float *oy, float *ox)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (long long)N * ny * nx) return;
     const int n = (int)(i / ((long long)ny * nx)), w = (int)(i % ((long long)ny * nx));
-    const float fy = map_y[w], fx = map_x[w];
-    const float fyf = floorf(fy), fxf = floorf(fx);
-    float wy[4], wx[4];
-    keys4(fy - fyf, wy);
-    keys4(fx - fxf, wx);
-    const int by = (int)fyf - 1, bx = (int)fxf - 1;
+    const int sx = __float2int_rn(__fmul_rn(map_x[w], 32.0f));
+    const int sy = __float2int_rn(__fmul_rn(map_y[w], 32.0f));
+    const int bx = (sx >> 5) - 1, by = (sy >> 5) - 1;
+    float cy[4], cx[4], wt[16];
+    cv_cubic(__fmul_rn((float)(sy & 31), 1.0f / 32.0f), cy);
+    cv_cubic(__fmul_rn((float)(sx & 31), 1.0f / 32.0f), cx);
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) wt[m * 4 + q] = __fmul_rn(cy[m], cx[q]);
     const float *Py = pdy + (long long)n * nyp * nxp, *Px = pdx + (long long)n * nyp * nxp;
-    float vy = 0.0f, vx = 0.0f;
-    for (int m = 0; m < 4; ++m) {
-        const int r = min(max(by + m, 0), nyp - 1);
-        for (int q = 0; q < 4; ++q) {
-            const int c = min(max(bx + q, 0), nxp - 1);
-            const float wt = wy[m] * wx[q];
-            vy += wt * Py[r * nxp + c];
-            vx += wt * Px[r * nxp + c];
+    float vy, vx;
+    if (bx >= 0 && bx < nxp - 3 && by >= 0 && by < nyp - 3) {
+        float ry[4], rx[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const float *a = Py + (long long)(by + m) * nxp + bx, *b = Px + (long long)(by + m) * nxp + bx;
+            ry[m] = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(a[0], wt[4 * m]), __fmul_rn(a[1], wt[4 * m + 1])),
+                                        __fmul_rn(a[2], wt[4 * m + 2])), __fmul_rn(a[3], wt[4 * m + 3]));
+            rx[m] = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(b[0], wt[4 * m]), __fmul_rn(b[1], wt[4 * m + 1])),
+                                        __fmul_rn(b[2], wt[4 * m + 2])), __fmul_rn(b[3], wt[4 * m + 3]));
+        }
+        vy = __fadd_rn(__fadd_rn(__fadd_rn(ry[0], ry[1]), ry[2]), ry[3]);
+        vx = __fadd_rn(__fadd_rn(__fadd_rn(rx[0], rx[1]), rx[2]), rx[3]);
+    } else {
+        vy = 0.0f;
+        vx = 0.0f;
+        for (int m = 0; m < 4; ++m) {
+            const int r = min(max(by + m, 0), nyp - 1);
+            for (int q = 0; q < 4; ++q) {
+                const int c = min(max(bx + q, 0), nxp - 1);
+                vy = __fadd_rn(vy, __fmul_rn(Py[(long long)r * nxp + c], wt[m * 4 + q]));
+                vx = __fadd_rn(vx, __fmul_rn(Px[(long long)r * nxp + c], wt[m * 4 + q]));
+            }
         }
     }
     oy[i] = vy;
@@ -404,14 +541,40 @@ PIV_EXPORT int pivb_validate_dev(const float *pk_x, const float *pk_y, const flo
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
-// Harmonic infilling of the invalid vectors, in place.  work: 2*N*ny*nx floats.
-PIV_EXPORT int pivb_infill_dev(float *ux, float *uy, const unsigned char *invalid, const float *mask, int N, int ny,
-                               int nx, float spacing_y, float spacing_x, int max_iter, float tol, float *work,
-                               void *stream)
+// Work bytes of pivb_infill_dev per call (per pair: a class byte, a list index
+// and eight FP64 values per grid cell).
+static size_t lsq_pair_bytes(int ny, int nx)
 {
-    if (N <= 0 || ny <= 0 || nx <= 0 || spacing_y <= 0.0f || spacing_x <= 0.0f) return 1;
-    const float wy = 1.0f / (spacing_y * spacing_y), wx = 1.0f / (spacing_x * spacing_x);
-    infill_kernel<<<N, 512, 0, (cudaStream_t)stream>>>(ux, uy, invalid, mask, ny, nx, wy, wx, max_iter, tol, work);
+    const size_t plane = (size_t)ny * nx;
+    auto pad = [](size_t b) { return (b + 255) & ~size_t(255); };
+    return pad(plane) + pad(plane * 4) + 8 * pad(plane * 8);
+}
+
+PIV_EXPORT size_t pivb_infill_work_bytes(int N, int ny, int nx)
+{
+    if (N <= 0 || ny <= 0 || nx <= 0) return 0;
+    return (size_t)N * lsq_pair_bytes(ny, nx);
+}
+
+// Least-squares infilling of the invalid vectors in place (order 1 harmonic,
+// 2 biharmonic).  work: pivb_infill_work_bytes(N, ny, nx) bytes.
+PIV_EXPORT int pivb_infill_dev(float *ux, float *uy, const unsigned char *invalid, const float *mask, int N, int ny,
+                               int nx, float spacing_y, float spacing_x, int order, int max_iter, double tol,
+                               void *work, size_t work_bytes, void *stream)
+{
+    if (N <= 0 || ny <= 0 || nx <= 0 || !(spacing_y > 0.0f) || !(spacing_x > 0.0f)) return 1;
+    if (order != 1 && order != 2) return 1;
+    if (work == nullptr || work_bytes < pivb_infill_work_bytes(N, ny, nx)) return 1;
+    LsqParams p{};
+    p.ux = ux; p.uy = uy; p.invalid = invalid; p.mask = mask;
+    p.ny = ny; p.nx = nx; p.order = order; p.max_iter = max_iter;
+    p.w2y = 1.0 / pow((double)spacing_y, 2.0 * order);
+    p.w2x = 1.0 / pow((double)spacing_x, 2.0 * order);
+    p.tol2 = tol * tol;
+    p.work = static_cast<char *>(work);
+    p.work_stride = lsq_pair_bytes(ny, nx);
+    if (order == 1) lsq_infill_kernel<1><<<N, kLsqThreads, 0, (cudaStream_t)stream>>>(p);
+    else lsq_infill_kernel<2><<<N, kLsqThreads, 0, (cudaStream_t)stream>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

@@ -167,8 +167,10 @@ def pass_lib() -> ctypes.CDLL:
     L.pivb_validate_dev.restype = ci
     L.pivb_floor_interp_dev.argtypes = [vp, ci, vp, ci, vp, vp, ci, vp, vp]
     L.pivb_floor_interp_dev.restype = ci
-    L.pivb_infill_dev.argtypes = [vp, vp, vp, vp, ci, ci, ci, fl, fl, ci, fl, vp, vp]
+    L.pivb_infill_dev.argtypes = [vp, vp, vp, vp, ci, ci, ci, fl, fl, ci, ci, ctypes.c_double, vp, csz, vp]
     L.pivb_infill_dev.restype = ci
+    L.pivb_infill_work_bytes.argtypes = [ci, ci, ci]
+    L.pivb_infill_work_bytes.restype = csz
     L.pivb_pad_smooth_dev.argtypes = [vp, vp, ci, ci, ci, ci, ci, ci, ci, vp, ci, vp, vp, vp, vp]
     L.pivb_pad_smooth_dev.restype = ci
     L.pivb_remap_dev.argtypes = [vp, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, vp]

@@ -40,11 +40,12 @@ class MultipassConfig:
     median_epsilon: float = 0.1
     median_threshold: float = 2.0
     median_size: int = 5
-    infill_iters: int = 400
-    infill_tol: float = 1e-3
+    infill: str = "biharmonic"      # least-squares infill between passes and after the last:
+                                    # "biharmonic" (the reference's default) or "harmonic"
+    infill_max_iter: int = 2000     # conjugate-gradient iteration cap (exact solves need far fewer)
+    infill_tol: float = 1e-12       # relative residual of the FP64 normal equations
     final_infill: bool = True
     predictor_fill: str = "harmonic"  # masked windows in the predictor: "harmonic" or "none" (kept at 0)
-    predictor_fill_iters: int = 2000
     engine_32: str = "fft"          # 32 px passes: "fft" (FP32 FFT) or "dft" (tensor-core DFT-as-GEMM)
 
 
@@ -83,6 +84,9 @@ class MultipassPIV:
         self.Lp = _lib.pass_lib()
         if self.cfg.engine_32 not in ("fft", "dft"):
             raise ValueError(f"engine_32 {self.cfg.engine_32!r}")
+        if self.cfg.infill not in ("biharmonic", "harmonic"):
+            raise ValueError(f"infill {self.cfg.infill!r} (valid: 'biharmonic', 'harmonic')")
+        self.infill_order = 2 if self.cfg.infill == "biharmonic" else 1
         if self.cfg.predictor_fill not in ("harmonic", "none"):
             raise ValueError(f"predictor_fill {self.cfg.predictor_fill!r} (valid: 'harmonic', 'none')")
         if vector_masks is not None and len(vector_masks) != len(self.geo):
@@ -97,6 +101,7 @@ class MultipassPIV:
         max_scratch = 0
         max_vec = 0
         max_pad = 0
+        max_infill = 0
         for k, g in enumerate(self.geo):
             ny, nx = g.grid.n_win_y, g.grid.n_win_x
             nyp, nxp = len(g.ctrs_y_all), len(g.ctrs_x_all)
@@ -147,9 +152,11 @@ class MultipassPIV:
                               int(self.Lx.pivb_xcorr_record_bytes(N * ny * nx)))
             max_vec = max(max_vec, N * ny * nx)
             max_pad = max(max_pad, N * nyp * nxp)
+            max_infill = max(max_infill, int(self.Lp.pivb_infill_work_bytes(N, ny, nx)))
             self.passes.append(p)
         self.scratch = torch.empty(max(max_scratch, 256), dtype=torch.uint8, device=dev)
         self.work = torch.empty(max(2 * max_vec, max_pad), dtype=f32, device=dev)
+        self.infill_work = torch.empty(max(max_infill, 256), dtype=torch.uint8, device=dev)
         # predictor copies with the masked windows filled (the stored field keeps 0 there)
         self.fill = (torch.empty((2, max_vec), dtype=f32, device=dev)
                      if any(self._fills(k) for k in range(len(self.passes))) else None)
@@ -261,7 +268,8 @@ class MultipassPIV:
             if not last or cfg.final_infill:
                 self._ok(self.Lp.pivb_infill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), mptr,
                                                  N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
-                                                 cfg.infill_iters, cfg.infill_tol, self.work.data_ptr(), s), "infill")
+                                                 self.infill_order, cfg.infill_max_iter, cfg.infill_tol,
+                                                 self.infill_work.data_ptr(), self.infill_work.numel(), s), "infill")
             if not last:
                 src_x, src_y = p["ux"], p["uy"]
                 if self._fills(k):
@@ -273,8 +281,9 @@ class MultipassPIV:
                     src_y.copy_(p["uy"].reshape(-1)[:nv])
                     self._ok(self.Lp.pivb_infill_dev(src_x.data_ptr(), src_y.data_ptr(), p["mask_u8"].data_ptr(),
                                                      None, N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
-                                                     cfg.predictor_fill_iters, cfg.infill_tol, self.work.data_ptr(),
-                                                     s), "predictor fill")
+                                                     1, cfg.infill_max_iter, cfg.infill_tol,
+                                                     self.infill_work.data_ptr(), self.infill_work.numel(), s),
+                                     "predictor fill")
                 self._ok(self.Lp.pivb_pad_smooth_dev(src_x.data_ptr(), src_y.data_ptr(), N, p["ny"], p["nx"],
                                                      p["nyp"], p["nxp"], p["pre"][0], p["pre"][1],
                                                      p["taps"].data_ptr(), p["radius"], p["pdy"].data_ptr(),

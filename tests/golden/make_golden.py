@@ -14,6 +14,7 @@ Python package).  The fixtures are committed; tests never need the reference.
     python tests/golden/make_golden.py results    # results_in.npz, results_ref/
     python tests/golden/make_golden.py floor      # floor_ref.npz
     python tests/golden/make_golden.py vmask      # vmask_ref.npz
+    python tests/golden/make_golden.py infill     # infill_ref.npz
     python tests/golden/make_golden.py xcorr      # xcorr_ref.npz, triple_ref.npz
 
 The reference checkout is named by $PIVTOOLS_REF (its libraries are built from it
@@ -444,6 +445,38 @@ def make_validate():
     print("validate_ref.npz written")
 
 
+def make_infill():
+    """Outputs of the reference's infill_harmonic and infill_biharmonic
+    (pivtools_cli/piv/piv_backend/infilling.py:336-421) on infill_cases().  The
+    module's config import is given the one constant it reads."""
+    import importlib.util
+    import types
+
+    cfg = types.ModuleType("pivtools_core.config")
+    cfg.PREDICTOR_FILL_METHODS = ("harmonic", "nearest", "none")
+    pc = types.ModuleType("pivtools_core")
+    pc.config = cfg
+    sys.modules.setdefault("pivtools_core", pc)
+    sys.modules.setdefault("pivtools_core.config", cfg)
+    path = os.path.join(REF_ROOT, "pivtools_cli/piv/piv_backend/infilling.py")
+    spec = importlib.util.spec_from_file_location("ref_infilling", path)
+    inf = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(inf)
+    from infill_cases import infill_cases
+
+    out = {}
+    for k, c in enumerate(infill_cases()):
+        U, V = c["ux"].copy(), c["uy"].copy()
+        U[c["fill"]] = np.nan
+        V[c["fill"]] = np.nan
+        for name, fn in (("harmonic", inf.infill_harmonic), ("biharmonic", inf.infill_biharmonic)):
+            fu, fv = fn(U, V, c["fill"], spacing=c["pitch"], exclude=c["exclude"])
+            out[f"c{k}_{name}_ux"] = np.asarray(fu, np.float64)
+            out[f"c{k}_{name}_uy"] = np.asarray(fv, np.float64)
+    np.savez_compressed(os.path.join(HERE, "infill_ref.npz"), **out)
+    print("infill_ref.npz written")
+
+
 def results_inputs():
     """Seeded per-pass fields of one pair over three passes (NaNs, masked windows,
     values beyond the float16 range, every reason code)."""
@@ -654,3 +687,5 @@ if __name__ == "__main__":
         make_floor()
     if "vmask" in what:
         make_vmask()
+    if "infill" in what:
+        make_infill()

@@ -130,48 +130,6 @@ def test_validation_reason_codes(oracle, cuda, med_thr, masked, peak_thr):
     assert (10 in codes) == (peak_thr >= 0 or med_thr > 0) and (13 in codes) == (peak_thr < 0)
 
 
-def test_infill_harmonic_matches_sparse_solve(cuda):
-    import torch
-    from scipy.sparse import lil_matrix
-    from scipy.sparse.linalg import spsolve
-
-    L = _lib.pass_lib()
-    rng = np.random.default_rng(5)
-    ny, nx, sy, sx = 17, 21, 8.0, 16.0
-    yy, xx = np.mgrid[0:ny, 0:nx]
-    u = (np.sin(xx / 5.0) + yy / 7.0).astype(np.float32)
-    v = (np.cos(yy / 4.0) - xx / 9.0).astype(np.float32)
-    bad = rng.random((ny, nx)) < 0.15
-    bad[0:3, 0:4] = True
-    U, V = u.copy(), v.copy()
-    U[bad] = np.nan
-    V[bad] = np.nan
-    tu, tv = _t(U[None], cuda), _t(V[None], cuda)
-    tb = _t(bad[None].astype(np.uint8), cuda)
-    work = torch.empty(2 * ny * nx, device=cuda)
-    assert L.pivb_infill_dev(tu.data_ptr(), tv.data_ptr(), tb.data_ptr(), None, 1, ny, nx, sy, sx, 20000, 1e-7,
-                             work.data_ptr(), _stream()) == 0
-    torch.cuda.synchronize()
-    # direct solve of the same Laplace system
-    idx = -np.ones((ny, nx), int)
-    idx[bad] = np.arange(bad.sum())
-    for F, got in ((u, tu), (v, tv)):
-        A = lil_matrix((bad.sum(), bad.sum()))
-        b = np.zeros(bad.sum())
-        for r, c in zip(*np.nonzero(bad)):
-            i = idx[r, c]
-            for dr, dc, w in ((-1, 0, 1 / sy ** 2), (1, 0, 1 / sy ** 2), (0, -1, 1 / sx ** 2), (0, 1, 1 / sx ** 2)):
-                rr, cc = r + dr, c + dc
-                if 0 <= rr < ny and 0 <= cc < nx:
-                    A[i, i] += w
-                    if bad[rr, cc]:
-                        A[i, idx[rr, cc]] -= w
-                    else:
-                        b[i] += w * F[rr, cc]
-        sol = spsolve(A.tocsr(), b)
-        np.testing.assert_allclose(got[0].cpu().numpy()[bad], sol, atol=2e-3)
-
-
 def test_pad_smooth_and_remap(cuda):
     import torch
     from scipy.ndimage import gaussian_filter
@@ -195,31 +153,23 @@ def test_pad_smooth_and_remap(cuda):
         ref = np.pad(uy[n], ((pre[0], post[0]), (pre[1], post[1])), mode="edge")
         ref = gaussian_filter(ref.astype(np.float64), sigma=0.65, truncate=2 / (2 * 0.65), mode="nearest")
         np.testing.assert_allclose(pdy[n].cpu().numpy(), ref, atol=1e-5)
-    # remap at fractional coordinates vs a Keys-cubic restatement
-    my = rng.uniform(0, nyp - 1, (5, 7)).astype(np.float32)
-    mx = rng.uniform(0, nxp - 1, (5, 7)).astype(np.float32)
-    oy = torch.empty((N, 5, 7), device=cuda)
+    # remap at fractional coordinates, inside and across the border, exactly as
+    # the reference driver's cv2.remap(INTER_CUBIC, BORDER_REPLICATE)
+    import cv2
+
+    my = rng.uniform(-2.0, nyp + 1.0, (23, 29)).astype(np.float32)
+    mx = rng.uniform(-2.0, nxp + 1.0, (23, 29)).astype(np.float32)
+    my[0, :8] = (np.arange(8, dtype=np.float32) + np.float32(0.5)) / np.float32(64.0) + np.float32(3.0)  # half steps
+    oy = torch.empty((N, 23, 29), device=cuda)
     ox = torch.empty_like(oy)
     tmy, tmx = _t(my, cuda), _t(mx, cuda)
-    assert L.pivb_remap_dev(pdy.data_ptr(), pdx.data_ptr(), N, nyp, nxp, tmy.data_ptr(), tmx.data_ptr(), 5, 7,
+    assert L.pivb_remap_dev(pdy.data_ptr(), pdx.data_ptr(), N, nyp, nxp, tmy.data_ptr(), tmx.data_ptr(), 23, 29,
                             oy.data_ptr(), ox.data_ptr(), _stream()) == 0
     torch.cuda.synchronize()
-
-    def keys(t):
-        t = abs(t)
-        return np.where(t < 1, (1.25 * t - 2.25) * t * t + 1, np.where(t < 2, ((-0.75 * t + 3.75) * t - 6) * t + 3, 0))
-
-    P = pdy[0].cpu().numpy().astype(np.float64)
-    for a in range(5):
-        for b in range(7):
-            y0, x0 = np.floor(my[a, b]), np.floor(mx[a, b])
-            val = 0.0
-            for m in range(-1, 3):
-                for q in range(-1, 3):
-                    r = int(min(max(y0 + m, 0), nyp - 1))
-                    c = int(min(max(x0 + q, 0), nxp - 1))
-                    val += keys(my[a, b] - (y0 + m)) * keys(mx[a, b] - (x0 + q)) * P[r, c]
-            assert abs(oy[0, a, b].item() - val) < 1e-4
+    for n in range(N):
+        for plane, got in ((pdy, oy), (pdx, ox)):
+            ref = cv2.remap(plane[n].cpu().numpy(), mx, my, cv2.INTER_CUBIC, borderMode=cv2.BORDER_REPLICATE)
+            assert np.array_equal(got[n].cpu().numpy(), ref)
 
 
 @pytest.mark.parametrize("flow", ["uniform", "channel"])

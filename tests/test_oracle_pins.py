@@ -229,3 +229,23 @@ def test_kspace_matches_reference_c_library(oracle, shape, floor):
     assert np.abs(o["gauss_flat"][ok, 9:12] - gp[ok, 9:12]).max() < 1e-8
     assert np.abs(o["gauss_flat"][ok, 14:16] - gp[ok, 14:16]).max() < 1e-8
     np.testing.assert_allclose(o["initial_guess"], c[f"{key}_initial_guess"], rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("method,order", [("harmonic", 1), ("biharmonic", 2)])
+def test_least_squares_fill_matches_reference(method, order):
+    """The restated least-squares infill (oracle/ref_multipass.py) against the
+    reference's own infill_harmonic / infill_biharmonic (golden/infill_ref.npz)."""
+    import sys
+
+    sys.path.insert(0, GOLD)
+    import ref_multipass as RM
+    from infill_cases import infill_cases
+
+    g = np.load(os.path.join(GOLD, "infill_ref.npz"))
+    for k, c in enumerate(infill_cases()):
+        U, V = c["ux"].copy(), c["uy"].copy()
+        U[c["fill"]] = np.nan
+        V[c["fill"]] = np.nan
+        out = RM.fill_least_squares(np.stack([U, V]), c["fill"], c["pitch"], order, c["exclude"])
+        np.testing.assert_allclose(out[0], g[f"c{k}_{method}_ux"], rtol=0, atol=1e-9)
+        np.testing.assert_allclose(out[1], g[f"c{k}_{method}_uy"], rtol=0, atol=1e-9)

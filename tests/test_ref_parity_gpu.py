@@ -197,3 +197,38 @@ def test_multipass_passes_match_reference_and_fp64(cuda, oracle):
                 for i, j in zip(*far):
                     assert XC.near_tie(rp[i, j]), (k, i, j, gx[i, j], rx[i, j])
             assert len(far[0]) <= max(1, 0.001 * d.size)
+
+
+def test_multipass_matches_reference_pipeline(cuda, oracle):
+    """The whole resident multipass against the reference's pass loop over its
+    compiled libraries (oracle/ref_multipass.py: bulkxcorr2d, fused warp, the
+    driver's validation, biharmonic infill, scipy smoothing and cv2 remap) on
+    one 768^2 channel-flow pair, passes 64/32/32 px at 50/50/75%.  Small plane
+    differences travel through the predictors, so the bar is statistical: per
+    pass at least 99% of the vectors within 1e-3 px and invalid flags equal on
+    at least 99.5% of the windows."""
+    import torch
+
+    if oracle.ref_bulk() is None or oracle.ref_warp() is None:
+        pytest.skip("reference libraries not built here (make -C oracle ref PIVTOOLS_REF=...)")
+    import ref_multipass as RM
+
+    from pivtools_b200 import multipass, synthetic
+
+    HW = (768, 768)
+    cfg = multipass.MultipassConfig(window_sizes=[(64, 64), (32, 32), (32, 32)], overlaps=[50, 50, 75])
+    A, B = synthetic.channel_batch_torch(1, HW, seed=77, device=cuda, peak=8.0)
+    mp = multipass.MultipassPIV(HW, 1, cfg, device=cuda)
+    mp.run(A, B)
+    torch.cuda.synchronize()
+    rm = RM.RefMultipass(mp.geo, window_type=cfg.window_type, peak_finder=cfg.peak_finder, infill=cfg.infill)
+    rm.run(A.cpu().numpy(), B.cpu().numpy())
+    for k, (p, (rx, ry, rbad)) in enumerate(zip(mp.passes, rm.history)):
+        gx, gy = p["ux"][0].cpu().numpy(), p["uy"][0].cpu().numpy()
+        gbad = p["invalid"][0].cpu().numpy().astype(bool)
+        d = np.maximum(np.abs(gx - rx[0]), np.abs(gy - ry[0]))
+        same_flag = (gbad == rbad[0]).mean()
+        print(f"\npass {k}: invalid {int(gbad.sum())} (reference {int(rbad[0].sum())}), flags equal {same_flag:.4f}, "
+              f"within 1e-3 px {(d <= 1e-3).mean():.4f}, median |d| {np.median(d):.1e} px, max |d| {d.max():.2e} px")
+        assert same_flag >= 0.995, k
+        assert (d <= 1e-3).mean() >= 0.99, k
