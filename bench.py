@@ -48,6 +48,7 @@ def _args():
     ap.add_argument("--cpu-pairs", type=int, default=2, help="CPU baseline leg: pairs in its batch")
     ap.add_argument("--ref-pairs", type=int, default=4, help="reference arm: pairs per (sampled) step")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the per-pass RMS against FP64")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the compiled launch defaults")
     ap.add_argument("--workload", default="multipass", choices=["multipass", "ensemble", "serve"],
                     help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
                          "serve: Poisson request stream with continuous batching")
@@ -270,6 +271,13 @@ def run_b200(args):
         for _ in range(max(args.warmup, 1)):
             mp.run(A, B)
     stream.synchronize()
+    tuned = None
+    if not args.no_autotune:
+        # launch shapes measured on this workload before the graph is captured
+        # (a fresh measurement every run: no cache)
+        from pivtools_b200 import autotune
+
+        tuned = autotune.tune(mp, A, B, reps=3, cache=None)
     graph = None
     if not args.no_graph:
         graph = torch.cuda.CUDAGraph()
@@ -446,6 +454,9 @@ def run_b200(args):
             "gpu_launches": mp.launches_per_step * args.steps,
             "clocks": clk.summary(),
         }
+        if tuned is not None:
+            line["autotune"] = {"settings": tuned["settings"], "step_ms_default": tuned["step_ms_default"],
+                                "step_ms_tuned": tuned["step_ms_tuned"], "trials": tuned["trials"]}
         if served is not None:
             line["latency_ms"] = {"p50": served["latency_ms"]["p50"], "p99": served["latency_ms"]["p99"],
                                   "source": "served leg: request arrival to result in host memory"}

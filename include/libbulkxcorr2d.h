@@ -102,10 +102,19 @@ size_t pivb_xcorr_scratch_bytes(long long n_windows_total, int n_peaks, int peak
  * correlation kernel, with identical results); no counterpart in the reference. */
 size_t pivb_xcorr_record_bytes(long long n_windows_total);
 
+/* Scratch bytes pivb_xcorr_dev needs for h x w windows: pivb_xcorr_scratch_bytes
+ * for square windows; for rectangular windows (h != w, both in 8..128) the
+ * planes of the staged rectangular path, processed in chunks of at most 256 MiB
+ * of windows.  No counterpart in the reference. */
+size_t pivb_xcorr_scratch_bytes_hw(long long n_windows_total, int win_h, int win_w, int n_peaks,
+                                   int peak_finder);
+
 /* numel / (wB (*) wB) into d_out [h*w] (the fit patch's loss-of-correlation weight). */
 int pivb_correl_weight_dev(const float *d_wB, int h, int w, float *d_out, void *stream);
 
-/* bulkxcorr2d on device pointers; img_stride = elements between frames. */
+/* bulkxcorr2d on device pointers; img_stride = elements between frames.
+ * Rectangular windows (win_h != win_w) take the staged path and need
+ * pivb_xcorr_scratch_bytes_hw bytes of scratch (else 1, NOMEM). */
 int pivb_xcorr_dev(const float *d_A, const float *d_B, long long img_stride, const float *d_mask,
                    int H, int W, int n_images, const float *d_ctr_x, const float *d_ctr_y,
                    int n_win_y, int n_win_x, const float *d_wA, const float *d_wB,

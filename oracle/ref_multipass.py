@@ -163,13 +163,13 @@ def median_flags(zx, zy, eps=0.1, thr=2.0, size=5):
     return flag | (n_present < 6)
 
 
-def validate(pk_x, pk_y, pk_h, pred_dy, pred_dx, thresh, peak_thr=0.25, eps=0.1, med_thr=2.0, size=5):
+def validate(pk_x, pk_y, pk_h, pred_dy, pred_dx, thresh_x, thresh_y, peak_thr=0.25, eps=0.1, med_thr=2.0, size=5):
     """(N, ny, nx) primary-peak outputs -> (ux, uy, invalid) with NaN at invalid."""
     x = pk_x.astype(np.float32).copy()
     y = pk_y.astype(np.float32).copy()
     h = pk_h.astype(np.float32).copy()
     with np.errstate(invalid="ignore"):
-        gone = (np.abs(x) > thresh) | (np.abs(y) > thresh)
+        gone = (np.abs(x) > thresh_x) | (np.abs(y) > thresh_y)
     x[gone] = np.nan
     y[gone] = np.nan
     h[gone] = np.nan
@@ -257,8 +257,9 @@ class RefMultipass:
                                   peak_finder=self.finder)
             if r["error"]:
                 raise RuntimeError(f"reference bulkxcorr2d error {r['error']}")
-            thr = g.window_size[0] / 2.0 if k == 0 else g.window_size[0] / 4.0
-            ux, uy, bad = validate(r["pk_x"][:, 0], r["pk_y"][:, 0], r["pk_h"][:, 0], pdy, pdx, thr)
+            div = 2.0 if k == 0 else 4.0
+            ux, uy, bad = validate(r["pk_x"][:, 0], r["pk_y"][:, 0], r["pk_h"][:, 0], pdy, pdx,
+                                   g.window_size[1] / div, g.window_size[0] / div)
             last = k + 1 == len(self.geo)
             if not last or self.final_infill:
                 pitch = (float(g.grid.win_spacing_y), float(g.grid.win_spacing_x))

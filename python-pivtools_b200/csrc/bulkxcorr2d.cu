@@ -12,10 +12,12 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "device_state.h"
 #include "xcorr_kernels.cuh"
+#include "xcorr_rect.cuh"
 
 using namespace piv;
 
@@ -112,6 +114,20 @@ int xcorr_blocks_per_sm(int dev)
     });
 }
 
+// Launch settings the autotuner may change (process-wide): a cap on resident
+// correlation CTAs per SM for each window size (0 = the occupancy maximum), and
+// the block size of the per-window record (fit) kernel.
+int size_index(int n)
+{
+    switch (n) {
+    case 8: return 0; case 12: return 1; case 16: return 2; case 24: return 3; case 32: return 4;
+    case 48: return 5; case 64: return 6; case 96: return 7; case 128: return 8;
+    default: return -1;
+    }
+}
+std::atomic<int> g_ctas_cap[9];
+std::atomic<int> g_record_block{128};
+
 template <int N, bool MULTI>
 int launch_xcorr_n(const XcorrParams &p, cudaStream_t s)
 {
@@ -124,8 +140,9 @@ int launch_xcorr_n(const XcorrParams &p, cudaStream_t s)
         cudaGetLastError();
         return PIV_ERROR_CUDA;
     }
+    const int tuned = g_ctas_cap[size_index(N)].load(std::memory_order_relaxed);
     long long want = (p.total + G::GROUPS_PER_CTA - 1) / G::GROUPS_PER_CTA;
-    long long cap = (long long)per_sm * device_sms(dev);
+    long long cap = (long long)(tuned > 0 && tuned < per_sm ? tuned : per_sm) * device_sms(dev);
     int grid = (int)(want < cap ? want : cap);
     if (grid < 1) grid = 1;
     kern<<<grid, G::CTA_THREADS, G::SMEM_BYTES, s>>>(p);
@@ -156,6 +173,145 @@ int launch_xcorr(int N, const XcorrParams &p, cudaStream_t s)
 // ---------------------------------------------------------------------------
 
 // Bytes of scratch the device correlation entry point needs for a call.
+namespace {
+
+// Rectangular windows: the staged path of xcorr_rect.cuh over chunks of windows
+// whose planes fit a fixed scratch budget.
+constexpr size_t kRectChunkBudget = 256u << 20;
+
+size_t rect_window_bytes(int h, int w, int n_peaks)
+{
+    const size_t hw = (size_t)h * w;
+    return hw * 8 + hw * 4 + (n_peaks > 1 ? hw * 4 : 0) + (size_t)6 * n_peaks * 4 + 12;
+}
+
+long long rect_chunk(long long total, int h, int w, int n_peaks)
+{
+    long long c = (long long)(kRectChunkBudget / rect_window_bytes(h, w, n_peaks));
+    if (c < 1) c = 1;
+    return c < total ? c : total;
+}
+
+size_t rect_scratch_bytes(long long total, int h, int w, int n_peaks)
+{
+    if (total <= 0) return 0;
+    const size_t c = (size_t)rect_chunk(total, h, w, n_peaks), hw = (size_t)h * w;
+    return pad256(c * hw * 8) + pad256(c * hw * 4) + (n_peaks > 1 ? pad256(c * hw * 4) : 0) +
+           2 * pad256(c * 3 * n_peaks * 4) + 3 * pad256(c * 4);
+}
+
+template <int L, int AXIS>
+void rect_fft_n(const RectParams &p, cudaStream_t s)
+{
+    const long long threads = (long long)p.count * (AXIS == 0 ? p.w : p.h) * RectLine<L>::P;
+    rect_line_fft<L, AXIS><<<(unsigned)((threads + 127) / 128), 128, 0, s>>>(p);
+}
+
+template <int AXIS>
+void rect_fft(int L, const RectParams &p, cudaStream_t s)
+{
+    switch (L) {
+    case 8: rect_fft_n<8, AXIS>(p, s); break;
+    case 12: rect_fft_n<12, AXIS>(p, s); break;
+    case 16: rect_fft_n<16, AXIS>(p, s); break;
+    case 24: rect_fft_n<24, AXIS>(p, s); break;
+    case 32: rect_fft_n<32, AXIS>(p, s); break;
+    case 48: rect_fft_n<48, AXIS>(p, s); break;
+    case 64: rect_fft_n<64, AXIS>(p, s); break;
+    case 96: rect_fft_n<96, AXIS>(p, s); break;
+    default: rect_fft_n<128, AXIS>(p, s); break;
+    }
+}
+
+// The whole rectangular correlation + fit of `total` windows on stream s.
+int xcorr_rect(RectParams p, long long total, int n_peaks, int peak_finder, int peakfit_impl, const float *cw,
+               float *pk_x, float *pk_y, float *pk_h, float *sx, float *sy, float *sxy, float *pk_ratio,
+               void *scratch, cudaStream_t s)
+{
+    const long long chunk = rect_chunk(total, p.h, p.w, n_peaks);
+    const size_t c = (size_t)chunk, hw = (size_t)p.h * p.w;
+    Carve cv(scratch);
+    p.Z = cv.take<float2>(c * hw);
+    p.pl = cv.take<float>(c * hw);
+    float *work = n_peaks > 1 ? cv.take<float>(c * hw) : nullptr;
+    float *loc = cv.take<float>(c * 3 * n_peaks);
+    float *sd = cv.take<float>(c * 3 * n_peaks);
+    p.enorm = cv.take<float>(c);
+    p.valid = cv.take<int>(c);
+    float *ratio = cv.take<float>(c);
+    const bool batch = peakfit_impl && n_peaks == 1 && peak_finder >= 4 && peak_finder <= 6;
+    RectOut o{pk_x, pk_y, pk_h, sx, sy, sxy, pk_ratio, loc, sd, ratio, n_peaks};
+    for (long long w0 = 0; w0 < total; w0 += chunk) {
+        p.w0 = w0;
+        p.count = (int)(total - w0 < chunk ? total - w0 : chunk);
+        const unsigned elems = (unsigned)(((long long)p.count * hw + 255) / 256);
+        rect_gather_kernel<<<p.count, kRectThreads, 0, s>>>(p);
+        rect_fft<0>(p.h, p, s);
+        rect_fft<1>(p.w, p, s);
+        rect_product_kernel<<<elems, 256, 0, s>>>(p);
+        rect_fft<1>(p.w, p, s);
+        rect_fft<0>(p.h, p, s);
+        rect_shift_kernel<<<elems, 256, 0, s>>>(p);
+        if (!p.ensemble) {
+            if (batch)
+                fit_planes_kernel<1><<<p.count, 128, 0, s>>>(p.pl, p.h, p.w, n_peaks, peak_finder, cw, loc, sd, 0, 0,
+                                                             ratio, work);
+            else
+                fit_planes_kernel<0><<<p.count, 128, 0, s>>>(p.pl, p.h, p.w, n_peaks, peak_finder, cw, loc, sd, 0, 0,
+                                                             ratio, work);
+            rect_finish_kernel<<<(p.count + 127) / 128, 128, 0, s>>>(p, o);
+        }
+        if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
+    }
+    return PIV_ERROR_NONE;
+}
+
+}  // namespace
+
+// Autotuner hooks (no counterpart in the reference): cap the resident
+// correlation CTAs per SM of window size `win` (0 restores the occupancy
+// maximum); read the cap and the occupancy maximum on the current device; set
+// the record kernel's block size (32, 64 or 128).  Process-wide settings;
+// 0 on success, 1 for arguments out of range.
+PIV_EXPORT int pivb_xcorr_set_ctas_per_sm(int win, int ctas)
+{
+    const int k = size_index(win);
+    if (k < 0 || ctas < 0 || ctas > 64) return 1;
+    g_ctas_cap[k].store(ctas);
+    return 0;
+}
+
+PIV_EXPORT int pivb_xcorr_get_ctas_per_sm(int win)
+{
+    const int k = size_index(win);
+    return k < 0 ? -1 : g_ctas_cap[k].load();
+}
+
+PIV_EXPORT int pivb_xcorr_max_ctas_per_sm(int win)
+{
+    const int dev = current_device();
+    if (dev < 0) return -1;
+    switch (win) {
+    case 8: return xcorr_blocks_per_sm<8, false>(dev);
+    case 12: return xcorr_blocks_per_sm<12, false>(dev);
+    case 16: return xcorr_blocks_per_sm<16, false>(dev);
+    case 24: return xcorr_blocks_per_sm<24, false>(dev);
+    case 32: return xcorr_blocks_per_sm<32, false>(dev);
+    case 48: return xcorr_blocks_per_sm<48, false>(dev);
+    case 64: return xcorr_blocks_per_sm<64, false>(dev);
+    case 96: return xcorr_blocks_per_sm<96, false>(dev);
+    case 128: return xcorr_blocks_per_sm<128, false>(dev);
+    default: return -1;
+    }
+}
+
+PIV_EXPORT int pivb_xcorr_set_record_block(int threads)
+{
+    if (threads != 32 && threads != 64 && threads != 128) return 1;
+    g_record_block.store(threads);
+    return 0;
+}
+
 PIV_EXPORT size_t pivb_xcorr_scratch_bytes(long long n_windows_total, int n_peaks, int peak_finder)
 {
     if (n_peaks == 1 && peak_finder >= 4 && peak_finder <= 6)
@@ -165,6 +321,16 @@ PIV_EXPORT size_t pivb_xcorr_scratch_bytes(long long n_windows_total, int n_peak
 
 // Bytes of the per-window records with which pivb_xcorr_dev defers every
 // single-peak fit (3-point included) to a thread-per-window kernel.
+// Scratch bytes pivb_xcorr_dev needs for windows of h x w: for square windows
+// pivb_xcorr_scratch_bytes (LM records only); for rectangular windows the planes
+// of the staged path, for chunks of at most 256 MiB of windows.
+PIV_EXPORT size_t pivb_xcorr_scratch_bytes_hw(long long n_windows_total, int win_h, int win_w, int n_peaks,
+                                              int peak_finder)
+{
+    if (win_h == win_w) return pivb_xcorr_scratch_bytes(n_windows_total, n_peaks, peak_finder);
+    return rect_scratch_bytes(n_windows_total, win_h, win_w, n_peaks < 1 ? 1 : n_peaks);
+}
+
 PIV_EXPORT size_t pivb_xcorr_record_bytes(long long n_windows_total)
 {
     return pad256((size_t)n_windows_total * sizeof(LmRecord));
@@ -194,10 +360,21 @@ PIV_EXPORT int pivb_xcorr_dev(const float *d_A, const float *d_B, long long img_
                               float *d_planes, void *d_scratch, size_t scratch_bytes, void *stream)
 {
     if (!size_ok(win_h) || !size_ok(win_w)) return PIV_ERROR_NOPLAN_BWD;
-    if (win_h != win_w) return PIV_ERROR_NOPLAN;   // square windows only
     if (n_peaks < 1 || n_images < 0) return PIV_ERROR_OUT_OF_BOUNDS;
     const long long total = (long long)n_images * n_win_y * n_win_x;
     if (total == 0) return PIV_ERROR_NONE;
+    if (win_h != win_w) {
+        // rectangular windows: the staged path (planes in the caller's scratch)
+        if (d_scratch == nullptr || scratch_bytes < rect_scratch_bytes(total, win_h, win_w, n_peaks))
+            return PIV_ERROR_NOMEM;
+        RectParams rp{};
+        rp.A = d_A; rp.B = d_B; rp.img_stride = img_stride; rp.mask = d_mask;
+        rp.H = H; rp.W = W; rp.nwy = n_win_y; rp.nwx = n_win_x; rp.nwt = (long long)n_win_y * n_win_x;
+        rp.ctr_x = d_ctr_x; rp.ctr_y = d_ctr_y; rp.wA = d_wA; rp.wB = d_wB;
+        rp.h = win_h; rp.w = win_w; rp.ensemble = ensemble; rp.planes_out = d_planes;
+        return xcorr_rect(rp, total, n_peaks, peak_finder, peakfit_impl, d_cw, d_pk_x, d_pk_y, d_pk_h, d_sx, d_sy,
+                          d_sxy, d_pk_ratio, d_scratch, (cudaStream_t)stream);
+    }
     const bool lm = !ensemble && n_peaks == 1 && peak_finder >= 4 && peak_finder <= 6;
     if (lm && (d_scratch == nullptr || scratch_bytes < pivb_xcorr_scratch_bytes(total, n_peaks, peak_finder)))
         return PIV_ERROR_NOMEM;
@@ -229,9 +406,10 @@ PIV_EXPORT int pivb_xcorr_dev(const float *d_A, const float *d_B, long long img_
     if (e) return e;
     if (timing) cudaEventRecord(tw->ev[1], s);
     if (defer) {
-        const unsigned blocks = (unsigned)((total + 127) / 128);
-        if (peakfit_impl) lm_records_kernel<1><<<blocks, 128, 0, s>>>(p, win_h);
-        else lm_records_kernel<0><<<blocks, 128, 0, s>>>(p, win_h);
+        const int tb = g_record_block.load(std::memory_order_relaxed);
+        const unsigned blocks = (unsigned)((total + tb - 1) / tb);
+        if (peakfit_impl) lm_records_kernel<1><<<blocks, tb, 0, s>>>(p, win_h);
+        else lm_records_kernel<0><<<blocks, tb, 0, s>>>(p, win_h);
         if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
     }
     if (timing) {
@@ -424,7 +602,6 @@ PIV_EXPORT unsigned char bulkxcorr2d(const float *fImageA, const float *fImageB,
 {
     const int h = nWindowSize[0], w = nWindowSize[1];
     if (!size_ok(h) || !size_ok(w)) return PIV_ERROR_NOPLAN_BWD;
-    if (h != w) return PIV_ERROR_NOPLAN;
     std::lock_guard<std::mutex> lock(g_mu);
     const int H = nImageSize[0], W = nImageSize[1];
     const int nwy = nWindows[0], nwx = nWindows[1];
@@ -435,7 +612,7 @@ PIV_EXPORT unsigned char bulkxcorr2d(const float *fImageA, const float *fImageB,
     const size_t nrat = (size_t)N_images * nwt;
     const size_t npl = (size_t)h * w;
     const int impl = g_peakfit_impl;
-    const size_t scratch = pivb_xcorr_scratch_bytes(total, nPeaks, iPeakFinder);
+    const size_t scratch = pivb_xcorr_scratch_bytes_hw(total, h, w, nPeaks, iPeakFinder);
     size_t bytes = 2 * pad256(img * 4) + pad256(nwt * 4) + pad256(nwx * 4) + pad256(nwy * 4) +
                    3 * pad256(npl * 4) + 6 * pad256(nout * 4) + pad256(nrat * 4) +
                    (fCorrelPlane_Out ? pad256((size_t)total * npl * 4) : 0) + scratch + 4096;

@@ -17,6 +17,7 @@
 #include <math.h>
 #include <stdio.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "device_state.h"
@@ -233,6 +234,7 @@ struct WarpParams {
     const float4 *wyb;         // per row: predictor row weights as pairs {w0,w0,w1,w1}, {w2,w2,w3,w3}
     const int *byr;            // per row: first predictor row of the 4x4 stencil
     int round_shifts;
+    int rows;                  // output rows per thread
     float neg_zero;            // -0.0f, passed at run time (see mulz2)
 };
 
@@ -251,17 +253,19 @@ __global__ void row_weights_kernel(const float *ly, int H, float4 *wyb, int *byr
     byr[i] = (int)ff - 1;
 }
 
-// Output rows per thread.  The rows of one thread share the column-side work
-// (predictor column weights and indices) and, while they fall in the same
-// predictor cell row, the 4x4 predictor patch, which stays in registers
-// (measured with the paired kernel: 16 rows 3% faster than 8, 4 rows 7% slower).
+// Output rows per thread (default).  The rows of one thread share the
+// column-side work (predictor column weights and indices) and, while they fall
+// in the same predictor cell row, the 4x4 predictor patch, which stays in
+// registers (measured with the paired kernel: 16 rows 3% faster than 8, 4 rows
+// 7% slower).  Rows per thread and the block height are launch settings
+// (pivb_warp_set_launch) that the autotuner may change.
 constexpr int kWarpRows = 16;
 
 template <int MODE, int IMPL>
 __global__ void __launch_bounds__(128) warp_kernel(WarpParams p)
 {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * kWarpRows;
+    const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * p.rows;
     const int n = blockIdx.z;
     if (j >= p.W || i0 >= p.H) return;
     const float *dy = p.pdy + n * p.pred_stride, *dx = p.pdx + n * p.pred_stride;
@@ -276,7 +280,7 @@ __global__ void __launch_bounds__(128) warp_kernel(WarpParams p)
     float py[4][4], px[4][4];
     int cur_by = -0x7fffffff;
     const float *a = p.ia + n * p.img_stride, *b = p.ib + n * p.img_stride;
-    const int i_end = min(i0 + kWarpRows, p.H);
+    const int i_end = min(i0 + p.rows, p.H);
 #pragma unroll 1
     for (int i = i0; i < i_end; ++i) {
         // Phase A: bicubic predictor, products and sums in the scalar route's order
@@ -332,7 +336,7 @@ __global__ void __launch_bounds__(128) warp_bicubic_x2_kernel(WarpParams p)
 {
     using namespace piv;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * kWarpRows;
+    const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * p.rows;
     const int n = blockIdx.z;
     if (j >= p.W || i0 >= p.H) return;
     const float2 nz = dup2(p.neg_zero);
@@ -353,7 +357,7 @@ __global__ void __launch_bounds__(128) warp_bicubic_x2_kernel(WarpParams p)
     const float *a = p.ia + n * p.img_stride, *b = p.ib + n * p.img_stride;
     const int H = p.H, W = p.W;
     const float fj = (float)j;
-    const int i_end = min(i0 + kWarpRows, H);
+    const int i_end = min(i0 + p.rows, H);
 #pragma unroll 1
     for (int i = i0; i < i_end; ++i) {
         const int by = p.byr[i];
@@ -412,6 +416,8 @@ __global__ void __launch_bounds__(128) warp_bicubic_x2_kernel(WarpParams p)
 
 std::mutex g_mu;
 volatile int g_impl = 1;
+// launch settings of the warp kernels (process-wide): rows per thread, block height
+std::atomic<int> g_rows{kWarpRows}, g_block_y{4};
 struct Ws {
     void *dev = nullptr;
     size_t cap = 0;
@@ -507,8 +513,10 @@ PIV_EXPORT int pivb_warp_dev(const float *d_ia, const float *d_ib, float *d_oa, 
     p.N = N; p.H = H; p.W = W; p.nPY = nPY; p.nPX = nPX;
     p.ly = t.ly; p.lx = t.lx; p.lut = t.lut; p.wyb = t.wyb; p.byr = t.byr;
     p.round_shifts = round_shifts;
+    p.rows = g_rows.load(std::memory_order_relaxed);
     p.neg_zero = -0.0f;
-    dim3 blk(32, 4), grd((W + 31) / 32, (H + 4 * kWarpRows - 1) / (4 * kWarpRows), N);   // 32 x 4 measured best
+    const int by = g_block_y.load(std::memory_order_relaxed);
+    dim3 blk(32, by), grd((W + 31) / 32, (H + by * p.rows - 1) / (by * p.rows), N);   // 32 x 4 x 16 measured best
     cudaStream_t s = (cudaStream_t)stream;
     if (interp_mode == 0) {
         if (impl) warp_bicubic_x2_kernel<<<grd, blk, 0, s>>>(p);
@@ -518,6 +526,23 @@ PIV_EXPORT int pivb_warp_dev(const float *d_ia, const float *d_ib, float *d_oa, 
         else warp_kernel<1, 0><<<grd, blk, 0, s>>>(p);
     }
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Launch settings of the warp kernels, for the autotuner (no counterpart in the
+// reference): output rows per thread (1..64) and threads per block column
+// (1, 2 or 4 rows of 32 threads).  Process-wide; returns 0, or 1 when out of range.
+PIV_EXPORT int pivb_warp_set_launch(int rows, int block_y)
+{
+    if (rows < 1 || rows > 64 || (block_y != 1 && block_y != 2 && block_y != 4)) return 1;
+    g_rows.store(rows);
+    g_block_y.store(block_y);
+    return 0;
+}
+
+PIV_EXPORT void pivb_warp_get_launch(int *rows, int *block_y)
+{
+    if (rows) *rows = g_rows.load();
+    if (block_y) *block_y = g_block_y.load();
 }
 
 // fused_warp.h:78-93

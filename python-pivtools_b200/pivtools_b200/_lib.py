@@ -80,6 +80,8 @@ def bulkxcorr2d_lib() -> ctypes.CDLL:
     L.pivb_xcorr_scratch_bytes.restype = csz
     L.pivb_correl_weight_dev.argtypes = [vp, ci, ci, vp, vp]
     L.pivb_correl_weight_dev.restype = ci
+    L.pivb_xcorr_scratch_bytes_hw.argtypes = [cll, ci, ci, ci, ci]
+    L.pivb_xcorr_scratch_bytes_hw.restype = csz
     L.pivb_xcorr_record_bytes.argtypes = [cll]
     L.pivb_xcorr_record_bytes.restype = csz
     L.pivb_xcorr_dev.argtypes = [vp, vp, cll, vp, ci, ci, ci, vp, vp, ci, ci, vp, vp, vp, ci, ci, ci, ci,
@@ -109,6 +111,14 @@ def bulkxcorr2d_lib() -> ctypes.CDLL:
     L.pivb_accumulate_dev.restype = ci
     L.pivb_accumulate_scratch_bytes.argtypes = [ci, cll]
     L.pivb_accumulate_scratch_bytes.restype = csz
+    L.pivb_xcorr_set_ctas_per_sm.argtypes = [ci, ci]
+    L.pivb_xcorr_set_ctas_per_sm.restype = ci
+    L.pivb_xcorr_get_ctas_per_sm.argtypes = [ci]
+    L.pivb_xcorr_get_ctas_per_sm.restype = ci
+    L.pivb_xcorr_max_ctas_per_sm.argtypes = [ci]
+    L.pivb_xcorr_max_ctas_per_sm.restype = ci
+    L.pivb_xcorr_set_record_block.argtypes = [ci]
+    L.pivb_xcorr_set_record_block.restype = ci
     L._pivb_bound = True
     return L
 
@@ -132,6 +142,10 @@ def fusedwarp_lib() -> ctypes.CDLL:
     L.pivb_warp_setup_dev.restype = ci
     L.pivb_warp_table_bytes.argtypes = [ci, ci]
     L.pivb_warp_table_bytes.restype = csz
+    L.pivb_warp_set_launch.argtypes = [ci, ci]
+    L.pivb_warp_set_launch.restype = ci
+    L.pivb_warp_get_launch.argtypes = [vp, vp]
+    L.pivb_warp_get_launch.restype = None
     L._pivb_bound = True
     return L
 

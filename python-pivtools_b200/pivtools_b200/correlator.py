@@ -122,7 +122,7 @@ class DeviceCorrelator:
         h, w = weight_a.shape
         cw = self.correl_weight(weight_b)
         total = N * ny * nx
-        nbytes = int(self.L.pivb_xcorr_scratch_bytes(total, n_peaks, peak_finder))
+        nbytes = int(self.L.pivb_xcorr_scratch_bytes_hw(total, h, w, n_peaks, peak_finder))
         scr = self.scratch(nbytes)
         stride = A.stride(0) if img_stride is None else img_stride
         code = self.L.pivb_xcorr_dev(

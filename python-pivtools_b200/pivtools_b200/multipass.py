@@ -108,7 +108,8 @@ class MultipassPIV:
             w = torch.tensor(geometry.window_weight(g.window_size, self.cfg.window_type), device=dev)
             cw = torch.empty_like(w)
             p = dict(
-                ny=ny, nx=nx, nyp=nyp, nxp=nxp, win=g.window_size[0], weight=w, cw=cw,
+                ny=ny, nx=nx, nyp=nyp, nxp=nxp, win=g.window_size[0], win_h=g.window_size[0],
+                win_w=g.window_size[1], weight=w, cw=cw,
                 cx=torch.tensor(g.grid.win_ctrs_x, device=dev), cy=torch.tensor(g.grid.win_ctrs_y, device=dev),
                 cx_all=torch.tensor(g.ctrs_x_all, device=dev), cy_all=torch.tensor(g.ctrs_y_all, device=dev),
                 # zero-filled once: skipped (masked) windows are never written
@@ -148,8 +149,10 @@ class MultipassPIV:
                 p["radius"] = rad
             # room for the per-window records, so every single-peak fit (3-point
             # included) runs in the thread-per-window record kernel
-            max_scratch = max(max_scratch, int(self.Lx.pivb_xcorr_scratch_bytes(N * ny * nx, 1, self.cfg.peak_finder)),
-                              int(self.Lx.pivb_xcorr_record_bytes(N * ny * nx)))
+            wh, ww = g.window_size
+            max_scratch = max(max_scratch,
+                              int(self.Lx.pivb_xcorr_scratch_bytes_hw(N * ny * nx, wh, ww, 1, self.cfg.peak_finder)),
+                              int(self.Lx.pivb_xcorr_record_bytes(N * ny * nx)) if wh == ww else 0)
             max_vec = max(max_vec, N * ny * nx)
             max_pad = max(max_pad, N * nyp * nxp)
             max_infill = max(max_infill, int(self.Lp.pivb_infill_work_bytes(N, ny, nx)))
@@ -169,7 +172,7 @@ class MultipassPIV:
             self._ok(self.Lw.pivb_warp_setup_dev(prev["cy_all"].data_ptr(), prev["nyp"], prev["cx_all"].data_ptr(),
                                                  prev["nxp"], H, W, self.tables[k].data_ptr(), s), "warp setup")
         for p in self.passes:
-            self._ok(self.Lx.pivb_correl_weight_dev(p["weight"].data_ptr(), p["win"], p["win"], p["cw"].data_ptr(), s),
+            self._ok(self.Lx.pivb_correl_weight_dev(p["weight"].data_ptr(), p["win_h"], p["win_w"], p["cw"].data_ptr(), s),
                      "correlation weight")
         self.launches_per_step = self._count_launches()
         self.planes = None
@@ -186,7 +189,7 @@ class MultipassPIV:
         torch = self.torch
         self.planes = None
         if on:
-            self.planes = [torch.zeros((self.N, p["ny"], p["nx"], p["win"], p["win"]), dtype=torch.float32,
+            self.planes = [torch.zeros((self.N, p["ny"], p["nx"], p["win_h"], p["win_w"]), dtype=torch.float32,
                                        device=self.device) for p in self.passes]
             torch.cuda.current_stream(self.device).synchronize()
 
@@ -248,20 +251,23 @@ class MultipassPIV:
             nbytes = scr.numel()
             mptr = None if p["mask"] is None else p["mask"].data_ptr()
             args = (fa.data_ptr(), fb.data_ptr(), H * W, mptr, H, W, N, p["cx"].data_ptr(), p["cy"].data_ptr(),
-                    p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win"],
-                    p["win"], 0, 1, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(),
+                    p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win_h"],
+                    p["win_w"], 0, 1, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(),
                     o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(),
                     o["sxy"].data_ptr(), p["ratio"].data_ptr(),
                     None if self.planes is None else self.planes[k].data_ptr(), scr.data_ptr(), nbytes)
-            if self.Ld is not None and p["win"] == 32:
+            if self.Ld is not None and p["win_h"] == 32 and p["win_w"] == 32:
                 self._ok(self.Ld.pivb_dft_xcorr_dev(*args, self.dft_status.data_ptr(), s), "correlation (tensor core)")
             else:
                 self._ok(self.Lx.pivb_xcorr_dev(*args, s), "correlation")
-            thr = p["win"] / 2.0 if k == 0 else p["win"] / 4.0
+            # large-displacement gate: half the window on the first pass, a quarter after
+            # (cpu_instantaneous.py:575-585), per axis
+            thr_x = p["win_w"] / 2.0 if k == 0 else p["win_w"] / 4.0
+            thr_y = p["win_h"] / 2.0 if k == 0 else p["win_h"] / 4.0
             self._ok(self.Lp.pivb_validate_dev(
                 o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(),
                 None if pred_dy is None else pred_dy.data_ptr(), None if pred_dx is None else pred_dx.data_ptr(),
-                mptr, N, p["ny"], p["nx"], thr, thr, cfg.peak_mag_threshold, cfg.median_epsilon,
+                mptr, N, p["ny"], p["nx"], thr_x, thr_y, cfg.peak_mag_threshold, cfg.median_epsilon,
                 cfg.median_threshold, cfg.median_size, p["ux"].data_ptr(), p["uy"].data_ptr(),
                 p["invalid"].data_ptr(), p["reason"].data_ptr(), self.work.data_ptr(), s), "validate")
             last = k + 1 == len(self.passes)

@@ -36,7 +36,7 @@ import xcorr_cases as XC  # noqa: E402
 
 
 def _gpu_rect_supported():
-    return bool(getattr(_lib.bulkxcorr2d_lib(), "pivb_rect_windows_supported", lambda: 0)())
+    return hasattr(_lib.bulkxcorr2d_lib(), "pivb_xcorr_scratch_bytes_hw")
 
 
 @pytest.fixture(scope="module")
@@ -199,11 +199,15 @@ def test_multipass_passes_match_reference_and_fp64(cuda, oracle):
             assert len(far[0]) <= max(1, 0.001 * d.size)
 
 
-def test_multipass_matches_reference_pipeline(cuda, oracle):
+@pytest.mark.parametrize("sizes,overlaps", [([(64, 64), (32, 32), (32, 32)], [50, 50, 75]),
+                                            ([(32, 64), (16, 32), (16, 32)], [50, 50, 50])],
+                         ids=["square", "rectangular"])
+def test_multipass_matches_reference_pipeline(cuda, oracle, sizes, overlaps):
     """The whole resident multipass against the reference's pass loop over its
     compiled libraries (oracle/ref_multipass.py: bulkxcorr2d, fused warp, the
     driver's validation, biharmonic infill, scipy smoothing and cv2 remap) on
-    one 768^2 channel-flow pair, passes 64/32/32 px at 50/50/75%.  Small plane
+    one 768^2 channel-flow pair, square (64/32/32 px at 50/50/75%) and
+    rectangular (32x64 / 16x32 / 16x32 at 50%) windows.  Small plane
     differences travel through the predictors, so the bar is statistical: per
     pass at least 99% of the vectors within 1e-3 px and invalid flags equal on
     at least 99.5% of the windows."""
@@ -216,7 +220,7 @@ def test_multipass_matches_reference_pipeline(cuda, oracle):
     from pivtools_b200 import multipass, synthetic
 
     HW = (768, 768)
-    cfg = multipass.MultipassConfig(window_sizes=[(64, 64), (32, 32), (32, 32)], overlaps=[50, 50, 75])
+    cfg = multipass.MultipassConfig(window_sizes=sizes, overlaps=overlaps)
     A, B = synthetic.channel_batch_torch(1, HW, seed=77, device=cuda, peak=8.0)
     mp = multipass.MultipassPIV(HW, 1, cfg, device=cuda)
     mp.run(A, B)
