@@ -647,6 +647,21 @@ def make_xcorr():
             h, w = c["win"]
             out[f"{nm}__planes"] = r["planes"].reshape(-1, h, w)[c["plane_idx"]]
     out["names"] = np.array(names)
+    # loss-of-correlation weight numel / (wB (*) wB) as bulkxcorr2d forms it
+    # (PIV_2d_cross_correlate.c:216-222 over xcorr.c's convolve)
+    L = O.ref_bulk()
+    L.convolve.argtypes = [O._f32, O._f32, O._f32, O._i32]
+    L.convolve.restype = ctypes.c_uint
+    from pivtools_b200 import geometry
+
+    cw_sizes = sorted({c["win"] for c in XC.all_cases()})
+    for (h, w) in cw_sizes:
+        for wt in ("gaussian", "blackman", "square"):
+            wb = geometry.window_weight((h, w), wt).ravel()
+            conv = np.zeros(h * w, np.float32)
+            assert L.convolve(wb, wb, conv, np.array([h, w], np.int32)) == 0
+            out[f"cw_{wt}_{h}x{w}"] = (np.float32(h * w) / conv).reshape(h, w)
+    out["cw_sizes"] = np.array(cw_sizes, np.int32)
     np.savez_compressed(os.path.join(HERE, "xcorr_ref.npz"), **out)
     print("xcorr_ref.npz written:", len(names), "cases")
     tout = {}

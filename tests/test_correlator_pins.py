@@ -100,3 +100,17 @@ def test_restated_correlator_live_against_reference_library(oracle):
     assert np.array_equal(np.isnan(r["pk_x"]), np.isnan(o["pk_x"]))
     d = np.maximum(np.abs(r["pk_x"] - o["pk_x"]), np.abs(r["pk_y"] - o["pk_y"]))
     assert np.nanmax(d) <= 1e-3
+
+
+def test_correlation_weight_matches_reference(oracle, fixture):
+    """numel / (wB (*) wB), the fit patch's loss-of-correlation weight
+    (PIV_2d_cross_correlate.c:216-222, xcorr.c:204-271): the oracle's FP64 direct
+    sum against the reference's FP32 zero-padded-FFT convolve, square and
+    rectangular windows, three weight types, within 2e-6 relative."""
+    from pivtools_b200 import geometry
+
+    for h, w in fixture["cw_sizes"]:
+        for wt in ("gaussian", "blackman", "square"):
+            ref = fixture[f"cw_{wt}_{h}x{w}"]
+            got = oracle.correl_weight(geometry.window_weight((int(h), int(w)), wt))
+            assert (np.abs(got - ref) / np.abs(ref)).max() <= 2e-6, (h, w, wt)

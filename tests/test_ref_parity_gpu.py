@@ -236,3 +236,23 @@ def test_multipass_matches_reference_pipeline(cuda, oracle, sizes, overlaps):
               f"within 1e-3 px {(d <= 1e-3).mean():.4f}, median |d| {np.median(d):.1e} px, max |d| {d.max():.2e} px")
         assert same_flag >= 0.995, k
         assert (d <= 1e-3).mean() >= 0.99, k
+
+
+def test_correlation_weight_matches_reference_library(cuda, fixture):
+    """pivb_correl_weight_dev against the reference's numel / convolve(wB, wB)
+    for every window size of the fixtures (square and rectangular) and three
+    weight types: within 2e-6 relative (FP64 direct sum against FP32 FFT)."""
+    import ctypes
+
+    import torch
+
+    L = _lib.bulkxcorr2d_lib()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for h, w in fixture["cw_sizes"]:
+        for wt in ("gaussian", "blackman", "square"):
+            wb = torch.tensor(geometry.window_weight((int(h), int(w)), wt), device=cuda)
+            out = torch.empty_like(wb)
+            assert L.pivb_correl_weight_dev(wb.data_ptr(), int(h), int(w), out.data_ptr(), s) == 0
+            torch.cuda.synchronize()
+            ref = fixture[f"cw_{wt}_{h}x{w}"]
+            assert (np.abs(out.cpu().numpy() - ref) / np.abs(ref)).max() <= 2e-6, (h, w, wt)
