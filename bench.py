@@ -49,7 +49,7 @@ def _args():
     ap.add_argument("--ref-pairs", type=int, default=4, help="reference arm: pairs per (sampled) step")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the per-pass RMS against FP64")
     ap.add_argument("--no-autotune", action="store_true", help="keep the compiled launch defaults")
-    ap.add_argument("--workload", default="multipass", choices=["multipass", "ensemble", "serve"],
+    ap.add_argument("--workload", default="multipass", choices=["multipass", "ensemble", "serve", "dft"],
                     help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
                          "serve: Poisson request stream with continuous batching")
     ap.add_argument("--chunk", type=int, default=32, help="e2e: pairs per host-to-device chunk")
@@ -57,6 +57,8 @@ def _args():
                     help="32 px passes on the FP32 FFT path or the tensor-core DFT-as-GEMM path")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: offered pairs/s")
     ap.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals")
+    ap.add_argument("--packed", action="store_true",
+                    help="serve: packed rounds (one correlation launch per window size and pass)")
     ap.add_argument("--no-serve", action="store_true",
                     help="multipass: skip the served-latency leg (Poisson arrivals, --rate for --duration s)")
     return ap.parse_args()
@@ -603,7 +605,179 @@ def run_ensemble(args):
         torch.distributed.destroy_process_group()
 
 
-def _serve_leg(dev, rate, duration, seed_base=0):
+def _mosaic(n_frames, win, side, seed, dev):
+    """Frames of 0%-overlap windows of `win` px, each window of frame B shifted
+    by its own uniform random (dy, dx) in [-4, 4]^2 px: particle images at
+    0.05 ppp (sigma 0.6 px, intensities U[1000, 4000], Poisson noise on a 100
+    count background).  Returns A, B (n, side, side) float32 on `dev` and the
+    shifts (n, side/win, side/win, 2)."""
+    import numpy as np
+    import torch
+
+    from pivtools_b200 import synthetic
+
+    nw = side // win
+    rng = np.random.default_rng(seed)
+    A = torch.empty((n_frames, side, side), dtype=torch.float32, device=dev)
+    B = torch.empty_like(A)
+    shifts = rng.uniform(-4.0, 4.0, (n_frames, nw, nw, 2))
+    n = int(round(0.05 * side * side))
+    for k in range(n_frames):
+        xs = rng.uniform(-8.0, side + 8.0, n)
+        ys = rng.uniform(-8.0, side + 8.0, n)
+        amp = rng.uniform(1000.0, 4000.0, n)
+        wi = np.clip((ys // win).astype(np.int64), 0, nw - 1)
+        wj = np.clip((xs // win).astype(np.int64), 0, nw - 1)
+        dy, dx = shifts[k, wi, wj, 0], shifts[k, wi, wj, 1]
+        g = torch.Generator(device=dev).manual_seed(int(seed) * 131 + k)
+        ia = synthetic._render_torch((side, side), xs, ys, amp, 0.6, dev)
+        ib = synthetic._render_torch((side, side), xs + dx, ys + dy, amp, 0.6, dev)
+        A[k] = torch.clamp(torch.poisson(ia + 100.0, generator=g), 0, 65535).float()
+        B[k] = torch.clamp(torch.poisson(ib + 100.0, generator=g), 0, 65535).float()
+    return A, B, shifts
+
+
+def run_dft(args):
+    """Tensor-core workload: 200k independent 64x64 and 200k 32x32 windows cut
+    from particle images with uniform random shifts in [-4, 4]^2 px, packed as
+    mosaics of 0%-overlap windows in 4096 x 4096 frames (49 frames of 4,096
+    windows of 64 px, 13 frames of 16,384 windows of 32 px), gauss3 fits.  The
+    32 px windows run on the split-BF16 tensor-core DFT-as-GEMM path and, for
+    the comparison, on the FP32 FFT path; the 64 px windows run on the FFT path
+    (the dense 64-point DFT chain costs 54 n^3 = 14.2 MFLOP of tensor work per
+    window against the FFT's 381 k FP32 flops, a 37x ratio beyond the 22x of the
+    peaks, so no tensor-core 64 px form is built).  Value: windows/s of the whole
+    400k-window step; each path's plane error and displacement RMS against the
+    FP64 oracle on a sample frame are in the line."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from pivtools_b200 import _lib, geometry
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    side = 4096
+    sets = {64: 49, 32: 13}
+    Lx, Ld = _lib.bulkxcorr2d_lib(), _lib.dft_lib()
+    data = {}
+    for n, nf in sets.items():
+        A, B, sh = _mosaic(nf, n, side, seed=4000 + n + 97 * rank, dev=dev)
+        g = geometry.compute_window_centers((side, side), (n, n), 0)
+        w = torch.tensor(geometry.window_weight((n, n), "gaussian"), device=dev)
+        cw = torch.empty_like(w)
+        st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        assert Lx.pivb_correl_weight_dev(w.data_ptr(), n, n, cw.data_ptr(), st) == 0
+        total = nf * g.n_win_y * g.n_win_x
+        out = {k: torch.zeros((nf, 1, g.n_win_y, g.n_win_x), device=dev) for k in ("x", "y", "h", "sx", "sy", "sxy")}
+        rat = torch.zeros((nf, g.n_win_y, g.n_win_x), device=dev)
+        nb = int(Lx.pivb_xcorr_record_bytes(total))
+        data[n] = dict(A=A, B=B, shifts=sh, g=g, w=w, cw=cw, out=out, rat=rat, total=total, nf=nf,
+                       cx=torch.tensor(g.win_ctrs_x, device=dev), cy=torch.tensor(g.win_ctrs_y, device=dev),
+                       scr=torch.empty(nb, dtype=torch.uint8, device=dev), nb=nb)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    def launch(n, engine, planes=None, nf=None):
+        d = data[n]
+        o = d["out"]
+        st = ctypes.c_void_p(stream.cuda_stream)
+        a = (d["A"].data_ptr(), d["B"].data_ptr(), side * side, None, side, side, d["nf"] if nf is None else nf,
+             d["cx"].data_ptr(), d["cy"].data_ptr(), d["g"].n_win_y, d["g"].n_win_x, d["w"].data_ptr(),
+             d["w"].data_ptr(), d["cw"].data_ptr(), n, n, 0, 1, 3, 0, o["x"].data_ptr(), o["y"].data_ptr(),
+             o["h"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(), o["sxy"].data_ptr(), d["rat"].data_ptr(),
+             None if planes is None else planes.data_ptr(), d["scr"].data_ptr(), d["nb"])
+        if engine == "dft":
+            code = Ld.pivb_dft_xcorr_dev(*a, status.data_ptr(), st)
+        else:
+            code = Lx.pivb_xcorr_dev(*a, st)
+        if code != 0:
+            raise RuntimeError(f"{engine} correlation failed ({code})")
+
+    def timed(fn, reps):
+        with torch.cuda.stream(stream):
+            for _ in range(max(args.warmup, 1)):
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    with ClockSampler(local) as clk:
+        ms_step = timed(lambda: (launch(64, "fft"), launch(32, "dft")), args.steps)
+        ms_dft32 = timed(lambda: launch(32, "dft"), args.steps)
+        ms_fft32 = timed(lambda: launch(32, "fft"), args.steps)
+        ms_fft64 = timed(lambda: launch(64, "fft"), args.steps)
+    if int(status.item()) != 0:
+        raise RuntimeError("tensor-core MMA completion not observed")
+    windows = data[64]["total"] + data[32]["total"]
+    value = windows / (ms_step * 1e-3)
+    if ws > 1:
+        t = torch.tensor([ms_step], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_step = float(t.item())
+        value = windows * ws / (ms_step * 1e-3)
+
+    acc = {}
+    if rank == 0 and not args.no_accuracy:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        for n, engine in ((32, "dft"), (32, "fft"), (64, "fft")):
+            d = data[n]
+            g = d["g"]
+            planes = torch.zeros((g.n_win_y * g.n_win_x, n, n), device=dev)
+            launch(n, engine, planes=planes, nf=1)
+            stream.synchronize()
+            gx, gy = d["out"]["x"][0, 0].cpu().numpy(), d["out"]["y"][0, 0].cpu().numpy()
+            fa, fb = d["A"][0].cpu().numpy(), d["B"][0].cpu().numpy()
+            wn = d["w"].cpu().numpy()
+            o = O.bulkxcorr2d(fa, fb, np.zeros((g.n_win_y, g.n_win_x), np.float32), g.win_ctrs_x, g.win_ctrs_y,
+                              (n, n), wn, wn, peak_finder=3, want_f64=True)
+            R = o["planes_f64"].reshape(-1, n, n)
+            P = planes.cpu().numpy()
+            rel = np.abs(P - R).reshape(len(R), -1).max(axis=1) / np.abs(R).reshape(len(R), -1).max(axis=1)
+            ox, oy = o["pk_x"][0, 0], o["pk_y"][0, 0]
+            both = np.isfinite(gx) & np.isfinite(ox)
+            true = d["shifts"][0]
+            acc[f"{engine}{n}"] = {
+                "windows": int(gx.size), "plane_rel_err_max": float(rel.max()),
+                "rms_px_vs_fp64": float(np.sqrt(np.mean((gx - ox)[both] ** 2 + (gy - oy)[both] ** 2))),
+                "nan_flips_vs_fp64": int((np.isnan(gx) != np.isnan(ox)).sum()),
+                "rms_px_vs_true_shift": float(np.sqrt(np.nanmean((gx - true[..., 1]) ** 2 + (gy - true[..., 0]) ** 2)))}
+    if rank == 0:
+        _, bf16_peak, peak_kind = _peaks()
+        n32 = data[32]["total"]
+        tflops = n32 * 1.769e6 / (ms_dft32 * 1e-3) / 1e12
+        line = {
+            "metric": "windows/s, split-BF16 tensor-core DFT-as-GEMM path (32 px) + FP32 FFT path (64 px) on 1 B200",
+            "value": value, "unit": "windows/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3 (32 px) / f32 (64 px)", "data": "synthetic",
+            "config": {"workload": "200k 64x64 + 200k 32x32 independent windows, uniform shifts in [-4, 4] px, "
+                                   "mosaics of 0%-overlap windows in 4096^2 frames (49 + 13 frames), gauss3",
+                       "windows_64": data[64]["total"], "windows_32": n32,
+                       "l2": f"inputs {(49 + 13) * 2 * side * side * 4 / 1e9:.1f} GB > L2"},
+            "paths_ms": {"dft32": ms_dft32, "fft32": ms_fft32, "fft64": ms_fft64},
+            "dft32_vs_fft32": ms_fft32 / ms_dft32,
+            "roofline": {"bound": "tensor", "achieved": tflops, "peak": bf16_peak, "unit": "TFLOP/s",
+                         "frac": tflops / bf16_peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "dft32 tcgen05 kernel + lm_records_kernel", "tensor_flops_per_window": 1.769e6},
+            "accuracy": acc, "clocks": clk.summary(),
+            "e2e": None, "gpu_launches": 2 * args.steps * 2,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def _serve_leg(dev, rate, duration, seed_base=0, packed=False):
     """Serving mix: Poisson arrivals at `rate` pairs/s for `duration` s; each
     request is one uint16 pair of a size drawn from {512^2, 1024^2, 2048^2,
     2048x4096} with a schedule drawn from {32; 64-32; 128-64-32-16 px} at 50%
@@ -627,7 +801,7 @@ def _serve_leg(dev, rate, duration, seed_base=0):
                                               device=dev)
             pool[shp].append((A.to(torch.int32).to(torch.uint16).cpu().pin_memory(),
                               B.to(torch.int32).to(torch.uint16).cpu().pin_memory()))
-    srv = serving.PivServer(device=dev, max_batch=4, hbm_budget_bytes=120e9)
+    srv = serving.PivServer(device=dev, max_batch=4, hbm_budget_bytes=120e9, packed=packed)
     for shp in sizes:                           # build every engine, warm it, pin output buffers
         for sch in scheds:
             srv.reserve_outputs(shp, sch, 64)
@@ -676,7 +850,8 @@ def _serve_leg(dev, rate, duration, seed_base=0):
            "h2d_bytes_per_request": float(np.mean([2 * p[0][0] * p[0][1] * 2 for p in picks])),
            "d2h_bytes_per_request": float(np.mean(d2h)),
            "max_batch": srv.max_batch, "hbm_budget_gb": 120, "engines": len(srv.engines),
-           "engine_bytes_gb": srv.used_bytes / 1e9,
+           "engine_bytes_gb": srv.used_bytes / 1e9, "packed": packed,
+           "pack_stats": dict(srv.pack_stats) if packed else None,
            "workload": f"Poisson {rate:g} pairs/s for {duration:g} s; sizes 512^2, 1024^2, 2048^2, 2048x4096 "
                        "uint16; schedules 32 / 64-32 / 128-64-32-16 px at 50%; flow (3.3, -1.7) px + GRF 0.5 px"}
     del srv, pool
@@ -694,7 +869,7 @@ def run_serve(args):
     if ws > 1:
         torch.distributed.barrier()
     with ClockSampler(local) as clk:
-        st = _serve_leg(dev, args.rate, args.duration, seed_base=rank)
+        st = _serve_leg(dev, args.rate, args.duration, seed_base=rank, packed=args.packed)
     wall = st["wall_s"]
     vec_total = st["vectors_per_s"] * wall
     if ws > 1:
@@ -710,6 +885,7 @@ def run_serve(args):
             "ms_per_step": wall * 1e3 / max(st["requests"], 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": st["workload"], "max_batch": st["max_batch"], "hbm_budget_gb": 120,
+                       "packed": st["packed"], "pack_stats": st["pack_stats"],
                        "engines": st["engines"], "engine_bytes_gb": st["engine_bytes_gb"]},
             "latency_ms": st["latency_ms"], "offered_pairs_per_s": st["offered_pairs_per_s"],
             "served_pairs_per_s": st["served_pairs_per_s"],
@@ -731,6 +907,8 @@ def main():
         run_ensemble(args)
     elif args.workload == "serve":
         run_serve(args)
+    elif args.workload == "dft":
+        run_dft(args)
     else:
         run_b200(args)
 

@@ -146,6 +146,31 @@ int pivb_accumulate_dev(const float *d_A, const float *d_B, long long img_stride
                         float *d_sum, float *d_comp, void *d_scratch, size_t scratch_bytes,
                         void *stream);
 
+/* Packed correlation launches (no counterpart in the reference; the serving
+ * loop's work queue).  One job = the arguments of one single-peak pivb_xcorr_dev
+ * call on device pointers.  pivb_xcorr_jobs_dev correlates and fits up to
+ * pivb_xcorr_jobs_max() jobs of one square window size in one launch of the
+ * correlation kernel and one of the fit kernel; jobs may differ in frames,
+ * frame size, window grid, mask, weights and outputs, and each job's results
+ * equal its own pivb_xcorr_dev call's.  d_records holds
+ * pivb_xcorr_jobs_record_bytes bytes.  The job table is passed as the kernels'
+ * parameter: no copy is issued.  Returns the codes of pivb_xcorr_dev. */
+typedef struct {
+    const float *A, *B;
+    long long img_stride;
+    const float *mask;
+    int H, W, n_images;
+    const float *ctr_x, *ctr_y;
+    int n_win_y, n_win_x;
+    const float *wA, *wB, *cw;
+    float *pk_x, *pk_y, *pk_h, *sx, *sy, *sxy, *pk_ratio;
+} PivbXcorrJob;
+
+int pivb_xcorr_jobs_max(void);
+size_t pivb_xcorr_jobs_record_bytes(const PivbXcorrJob *jobs, int n_jobs, int win);
+int pivb_xcorr_jobs_dev(const PivbXcorrJob *jobs, int n_jobs, int win, int peak_finder,
+                        int peakfit_impl, void *d_records, size_t record_bytes, void *stream);
+
 /* Allocation-free variant of pivb_xcorr_dev (no counterpart in the reference),
  * for callers that cannot allocate device memory: a host whose GPU memory is
  * owned by another allocator, a stream being captured into a CUDA graph, or a

@@ -268,6 +268,156 @@ int xcorr_rect(RectParams p, long long total, int n_peaks, int peak_finder, int 
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Packed correlation launches (no counterpart in the reference)
+// ---------------------------------------------------------------------------
+// One job of a packed launch: the arguments of one single-peak pivb_xcorr_dev
+// call (device pointers).  Declared the same in include/libbulkxcorr2d.h.
+struct PivbXcorrJob {
+    const float *A, *B;
+    long long img_stride;
+    const float *mask;
+    int H, W, n_images;
+    const float *ctr_x, *ctr_y;
+    int n_win_y, n_win_x;
+    const float *wA, *wB, *cw;
+    float *pk_x, *pk_y, *pk_h, *sx, *sy, *sxy, *pk_ratio;
+};
+
+namespace {
+
+int groups_per_cta(int n)
+{
+    switch (n) {
+    case 8: return WinGeo<8>::GROUPS_PER_CTA;
+    case 12: return WinGeo<12>::GROUPS_PER_CTA;
+    case 16: return WinGeo<16>::GROUPS_PER_CTA;
+    case 24: return WinGeo<24>::GROUPS_PER_CTA;
+    case 32: return WinGeo<32>::GROUPS_PER_CTA;
+    case 48: return WinGeo<48>::GROUPS_PER_CTA;
+    case 64: return WinGeo<64>::GROUPS_PER_CTA;
+    case 96: return WinGeo<96>::GROUPS_PER_CTA;
+    case 128: return WinGeo<128>::GROUPS_PER_CTA;
+    default: return -1;
+    }
+}
+
+// Padded window offsets of the jobs (each range a multiple of the CTA's window
+// count); returns the padded total, or -1 for bad arguments.
+long long job_offsets(const PivbXcorrJob *jobs, int n_jobs, int win, long long *off)
+{
+    const int g = groups_per_cta(win);
+    if (g < 1 || n_jobs < 1 || n_jobs > kMaxJobs) return -1;
+    off[0] = 0;
+    for (int j = 0; j < n_jobs; ++j) {
+        if (jobs[j].n_images < 0 || jobs[j].n_win_y < 0 || jobs[j].n_win_x < 0) return -1;
+        const long long t = (long long)jobs[j].n_images * jobs[j].n_win_y * jobs[j].n_win_x;
+        off[j + 1] = off[j] + (t + g - 1) / g * g;
+    }
+    return off[n_jobs];
+}
+
+template <int N>
+int launch_xcorr_jobs_n(const XcorrJobs &pj, cudaStream_t s)
+{
+    using G = WinGeo<N>;
+    static PerDeviceOnce per_sm_dev;
+    const int dev = current_device();
+    if (dev < 0) return PIV_ERROR_CUDA;
+    const int per_sm = per_sm_dev.get(dev, [] {
+        auto kern = xcorr_kernel<N, false, true>;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES) != cudaSuccess)
+            return -1;
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, G::CTA_THREADS, G::SMEM_BYTES) != cudaSuccess)
+            return -1;
+        return nb > 0 ? nb : 1;
+    });
+    if (per_sm < 0) {
+        cudaGetLastError();
+        return PIV_ERROR_CUDA;
+    }
+    const long long want = pj.total / G::GROUPS_PER_CTA;
+    const long long cap = (long long)per_sm * device_sms(dev);
+    const int grid = (int)(want < cap ? (want < 1 ? 1 : want) : cap);
+    xcorr_kernel<N, false, true><<<grid, G::CTA_THREADS, G::SMEM_BYTES, s>>>(pj);
+    return cudaGetLastError() == cudaSuccess ? PIV_ERROR_NONE : PIV_ERROR_CUDA;
+}
+
+int launch_xcorr_jobs(int N, const XcorrJobs &pj, cudaStream_t s)
+{
+    switch (N) {
+    case 8: return launch_xcorr_jobs_n<8>(pj, s);
+    case 12: return launch_xcorr_jobs_n<12>(pj, s);
+    case 16: return launch_xcorr_jobs_n<16>(pj, s);
+    case 24: return launch_xcorr_jobs_n<24>(pj, s);
+    case 32: return launch_xcorr_jobs_n<32>(pj, s);
+    case 48: return launch_xcorr_jobs_n<48>(pj, s);
+    case 64: return launch_xcorr_jobs_n<64>(pj, s);
+    case 96: return launch_xcorr_jobs_n<96>(pj, s);
+    case 128: return launch_xcorr_jobs_n<128>(pj, s);
+    default: return PIV_ERROR_NOPLAN_BWD;
+    }
+}
+
+}  // namespace
+
+// Record bytes a packed launch of these jobs needs (128 per padded window).
+PIV_EXPORT size_t pivb_xcorr_jobs_record_bytes(const PivbXcorrJob *jobs, int n_jobs, int win)
+{
+    long long off[kMaxJobs + 1];
+    const long long total = job_offsets(jobs, n_jobs, win, off);
+    return total < 0 ? 0 : pad256((size_t)total * sizeof(LmRecord));
+}
+
+PIV_EXPORT int pivb_xcorr_jobs_max(void) { return kMaxJobs; }
+
+// Single-peak correlation + fit of up to pivb_xcorr_jobs_max() jobs of one
+// square window size in one launch (and one launch of the fit kernel for all of
+// them): jobs may differ in frames, frame size, window grid, mask, weights and
+// outputs.  Every job's results equal those of its own pivb_xcorr_dev call.
+// d_records: pivb_xcorr_jobs_record_bytes bytes.  The job table travels as the
+// kernels' parameter, so the call issues no copy and needs no synchronisation.
+PIV_EXPORT int pivb_xcorr_jobs_dev(const PivbXcorrJob *jobs, int n_jobs, int win, int peak_finder,
+                                   int peakfit_impl, void *d_records, size_t record_bytes, void *stream)
+{
+    if (!size_ok(win)) return PIV_ERROR_NOPLAN_BWD;
+    if (peak_finder < 3 || peak_finder > 6) return PIV_ERROR_NOPLAN;
+    static XcorrJobs pj;                      // 10 KB: kept off the host stack; filled under the lock
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    const long long total = job_offsets(jobs, n_jobs, win, pj.off);
+    if (total < 0) return PIV_ERROR_OUT_OF_BOUNDS;
+    if (total == 0) return PIV_ERROR_NONE;
+    if (d_records == nullptr || record_bytes < (size_t)total * sizeof(LmRecord)) return PIV_ERROR_NOMEM;
+    pj.total = total;
+    pj.n_jobs = n_jobs;
+    LmRecord *rec = static_cast<LmRecord *>(d_records);
+    for (int j = 0; j < n_jobs; ++j) {
+        const PivbXcorrJob &J = jobs[j];
+        XcorrParams &p = pj.job[j];
+        p = XcorrParams{};
+        p.A = J.A; p.B = J.B; p.img_stride = J.img_stride; p.mask = J.mask;
+        p.H = J.H; p.W = J.W; p.n_img = J.n_images;
+        p.ctr_x = J.ctr_x; p.ctr_y = J.ctr_y; p.nwy = J.n_win_y; p.nwx = J.n_win_x;
+        p.wA = J.wA; p.wB = J.wB; p.cw = J.cw;
+        p.ensemble = 0; p.n_peaks = 1; p.finder = peak_finder;
+        p.pk_x = J.pk_x; p.pk_y = J.pk_y; p.pk_h = J.pk_h; p.sx = J.sx; p.sy = J.sy; p.sxy = J.sxy;
+        p.pk_ratio = J.pk_ratio; p.planes = nullptr;
+        p.lm = rec + pj.off[j];
+        p.total = (long long)J.n_images * J.n_win_y * J.n_win_x;
+        p.neg_zero = -0.0f;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int e = launch_xcorr_jobs(win, pj, s);
+    if (e) return e;
+    const int tb = g_record_block.load(std::memory_order_relaxed);
+    const unsigned blocks = (unsigned)((total + tb - 1) / tb);
+    if (peakfit_impl) lm_records_kernel<1, true><<<blocks, tb, 0, s>>>(pj, win);
+    else lm_records_kernel<0, true><<<blocks, tb, 0, s>>>(pj, win);
+    return cudaGetLastError() == cudaSuccess ? PIV_ERROR_NONE : PIV_ERROR_CUDA;
+}
+
 // Autotuner hooks (no counterpart in the reference): cap the resident
 // correlation CTAs per SM of window size `win` (0 restores the occupancy
 // maximum); read the cap and the occupancy maximum on the current device; set

@@ -1,6 +1,8 @@
 // xcorr_kernels.cuh -- kernels of libbulkxcorr2d.
 #pragma once
 
+#include <type_traits>
+
 #include "xcorr_engine.cuh"
 
 namespace piv {
@@ -34,6 +36,43 @@ struct XcorrParams {
     long long total;           // n_img * nwy * nwx
     float neg_zero;            // -0.0f, passed at run time (see mulz2)
 };
+
+// A packed launch: several jobs (pivb_xcorr_dev calls) of one window size in one
+// grid.  Job j owns the padded window range [off[j], off[j+1]); each offset is a
+// multiple of the CTA's window count, so every CTA iteration lies in one job.
+// Passed whole as a grid-constant kernel parameter (no device copy of the
+// table, nothing to order on the stream).
+constexpr int kMaxJobs = 40;
+struct XcorrJobs {
+    XcorrParams job[kMaxJobs];
+    long long off[kMaxJobs + 1];
+    long long total;           // off[n_jobs]
+    int n_jobs;
+};
+
+// Job of padded window index g (binary search of the offsets); sets the
+// job-local index.
+__device__ __forceinline__ int job_of(const XcorrJobs &pk, long long g, long long &local)
+{
+    int lo = 0, hi = pk.n_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pk.off[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    local = g - pk.off[lo];
+    return lo;
+}
+
+template <bool JOBS>
+using XcorrArg = std::conditional_t<JOBS, XcorrJobs, XcorrParams>;
+
+template <bool JOBS>
+__device__ __forceinline__ const XcorrParams &params_of(const XcorrArg<JOBS> &in, int job)
+{
+    if constexpr (JOBS) return in.job[job];
+    else return in;
+}
 
 __device__ __forceinline__ void write_sentinel(const XcorrParams &p, long long o, float enorm)
 {
@@ -198,10 +237,11 @@ __device__ __forceinline__ void finish_window_rec(int t, int gw, const XcorrPara
 // mean/energy, packed forward FFT, conjugate product, inverse FFT, shift, peak
 // search, 3-point fit.  LM fits of single-peak calls are deferred to
 // lm_records_kernel; MULTI handles nPeaks > 1 entirely in the group leader.
-template <int N, bool MULTI>
+template <int N, bool MULTI, bool JOBS = false>
 __global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS, MULTI ? 1 : WinGeo<N>::MIN_CTAS)
-xcorr_kernel(XcorrParams prm)
+xcorr_kernel(const __grid_constant__ XcorrArg<JOBS> prm_in)
 {
+    static_assert(!(MULTI && JOBS), "packed launches are single-peak");
     using G = WinGeo<N>;
     constexpr int M = G::M, P = G::P;
     extern __shared__ float4 smem_raw[];
@@ -223,23 +263,43 @@ xcorr_kernel(XcorrParams prm)
     // 32 px: both window weights staged once per CTA as pairs {wA, wB} (one
     // 64-bit shared load per sample in the gather)
     float2 *swt = reinterpret_cast<float2 *>(smem + G::GROUPS_PER_CTA * G::PLANE_BYTES + G::RED_BYTES + G::TW_BYTES);
-    if constexpr (N == 32) {
-        for (int i = threadIdx.x; i < N * N; i += G::CTA_THREADS) swt[i] = make_float2(prm.wA[i], prm.wB[i]);
+    const float *staged_wa = nullptr, *staged_wb = nullptr;
+    if constexpr (N == 32 && !JOBS) {
+        for (int i = threadIdx.x; i < N * N; i += G::CTA_THREADS) swt[i] = make_float2(prm_in.wA[i], prm_in.wB[i]);
         __syncthreads();
     }
-    const float2 nz = dup2(prm.neg_zero);
+    const float2 nz = dup2(params_of<JOBS>(prm_in, 0).neg_zero);
     auto wmul = [&](float2 x, float2 w) { return mulz2(x, w, nz); };
     const Group<N> g{t, red};
     const bool active = t < G::T;
     int line, p;
     lane_slot<N>(active ? t : 0, line, p);
-    const long long nwt = (long long)prm.nwy * prm.nwx;
     const long long per_iter = (long long)gridDim.x * G::GROUPS_PER_CTA;
-    const long long n_iter = (prm.total + per_iter - 1) / per_iter;
+    const long long n_iter = (prm_in.total + per_iter - 1) / per_iter;
     const float inv_numel = 1.0f / (float)(N * N);
 
     for (long long it = 0; it < n_iter; ++it) {
-        const long long idx = it * per_iter + (long long)blockIdx.x * G::GROUPS_PER_CTA + gi;
+        long long idx = it * per_iter + (long long)blockIdx.x * G::GROUPS_PER_CTA + gi;
+        int job = 0;
+        if constexpr (JOBS) {
+            // every window of this CTA's chunk belongs to one job (job offsets
+            // are multiples of the chunk), so the whole CTA sees the same job
+            long long local;
+            job = job_of(prm_in, it * per_iter + (long long)blockIdx.x * G::GROUPS_PER_CTA, local);
+            idx = local + gi;
+        }
+        const XcorrParams &prm = params_of<JOBS>(prm_in, job);
+        if constexpr (JOBS && N == 32) {
+            // the staged weight pairs follow the job's weights (uniform over the CTA)
+            if (prm.wA != staged_wa || prm.wB != staged_wb) {
+                __syncthreads();
+                for (int i = threadIdx.x; i < N * N; i += G::CTA_THREADS) swt[i] = make_float2(prm.wA[i], prm.wB[i]);
+                staged_wa = prm.wA;
+                staged_wb = prm.wB;
+                __syncthreads();
+            }
+        }
+        const long long nwt = (long long)prm.nwy * prm.nwx;
         const bool inrange = idx < prm.total;
         int n = 0, iw = 0, r0 = 0, c0 = 0;
         bool valid = inrange;
@@ -395,11 +455,19 @@ xcorr_kernel(XcorrParams prm)
 }
 
 // Deferred single-peak fits (3-point or LM): one thread per window record.
-template <int MODE>
-__global__ void __launch_bounds__(128) lm_records_kernel(XcorrParams prm, int N)
+template <int MODE, bool JOBS = false>
+__global__ void __launch_bounds__(128) lm_records_kernel(const __grid_constant__ XcorrArg<JOBS> prm_in, int N)
 {
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= prm.total) return;
+    long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= prm_in.total) return;
+    int job = 0;
+    if constexpr (JOBS) {
+        long long local;
+        job = job_of(prm_in, idx, local);
+        idx = local;
+    }
+    const XcorrParams &prm = params_of<JOBS>(prm_in, job);
+    if (JOBS && idx >= prm.total) return;        // padding of the job's window range
     const LmRecord &rec = prm.lm[idx];
     if (rec.flag != 1) return;
     float sub[PKN];

@@ -42,6 +42,17 @@ def _load(name: str) -> ctypes.CDLL:
     return L
 
 
+class XcorrJob(ctypes.Structure):
+    """One job of a packed correlation launch (PivbXcorrJob in libbulkxcorr2d.h)."""
+    _fields_ = [("A", ctypes.c_void_p), ("B", ctypes.c_void_p), ("img_stride", ctypes.c_longlong),
+                ("mask", ctypes.c_void_p), ("H", ctypes.c_int), ("W", ctypes.c_int), ("n_images", ctypes.c_int),
+                ("ctr_x", ctypes.c_void_p), ("ctr_y", ctypes.c_void_p), ("n_win_y", ctypes.c_int),
+                ("n_win_x", ctypes.c_int), ("wA", ctypes.c_void_p), ("wB", ctypes.c_void_p), ("cw", ctypes.c_void_p),
+                ("pk_x", ctypes.c_void_p), ("pk_y", ctypes.c_void_p), ("pk_h", ctypes.c_void_p),
+                ("sx", ctypes.c_void_p), ("sy", ctypes.c_void_p), ("sxy", ctypes.c_void_p),
+                ("pk_ratio", ctypes.c_void_p)]
+
+
 def bulkxcorr2d_lib() -> ctypes.CDLL:
     L = _load("libbulkxcorr2d.so")
     if getattr(L, "_pivb_bound", False):
@@ -111,6 +122,11 @@ def bulkxcorr2d_lib() -> ctypes.CDLL:
     L.pivb_accumulate_dev.restype = ci
     L.pivb_accumulate_scratch_bytes.argtypes = [ci, cll]
     L.pivb_accumulate_scratch_bytes.restype = csz
+    L.pivb_xcorr_jobs_max.restype = ci
+    L.pivb_xcorr_jobs_record_bytes.argtypes = [ctypes.POINTER(XcorrJob), ci, ci]
+    L.pivb_xcorr_jobs_record_bytes.restype = csz
+    L.pivb_xcorr_jobs_dev.argtypes = [ctypes.POINTER(XcorrJob), ci, ci, ci, ci, vp, csz, vp]
+    L.pivb_xcorr_jobs_dev.restype = ci
     L.pivb_xcorr_set_ctas_per_sm.argtypes = [ci, ci]
     L.pivb_xcorr_set_ctas_per_sm.restype = ci
     L.pivb_xcorr_get_ctas_per_sm.argtypes = [ci]

@@ -226,77 +226,123 @@ class MultipassPIV:
         (device tensors, views into internal buffers).  n (<= N) processes only the
         first n pairs (a partly filled batch); every pair's result is independent of
         the others in the batch."""
-        cfg = self.cfg
-        s = self._stream()
-        N, H, W = (self.N if n is None else int(n)), self.H, self.W
-        if not 1 <= N <= self.N:
-            raise ValueError(f"n = {N} outside 1..{self.N}")
-        scr = self.scratch
-        for k, p in enumerate(self.passes):
-            if k == 0:
-                fa, fb = A, B
-                pred_dy = pred_dx = None
-            else:
-                prev = self.passes[k - 1]
-                self._ok(self.Lp.pivb_remap_dev(prev["pdy"].data_ptr(), prev["pdx"].data_ptr(), N, prev["nyp"],
-                                                prev["nxp"], p["map_y"].data_ptr(), p["map_x"].data_ptr(), p["ny"],
-                                                p["nx"], p["pred_dy"].data_ptr(), p["pred_dx"].data_ptr(), s), "remap")
-                fa, fb = self.warped
-                self._ok(self.Lw.pivb_warp_dev(A.data_ptr(), B.data_ptr(), fa.data_ptr(), fb.data_ptr(),
-                                               prev["pdy"].data_ptr(), prev["pdx"].data_ptr(), N, H, W, prev["nyp"],
-                                               prev["nxp"], H * W, self.tables[k].data_ptr(), cfg.interp_mode, 0, 0,
-                                               cfg.warp_impl, s), "warp")
-                pred_dy, pred_dx = p["pred_dy"], p["pred_dx"]
-            o = p["out"]
-            nbytes = scr.numel()
-            mptr = None if p["mask"] is None else p["mask"].data_ptr()
-            args = (fa.data_ptr(), fb.data_ptr(), H * W, mptr, H, W, N, p["cx"].data_ptr(), p["cy"].data_ptr(),
-                    p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win_h"],
-                    p["win_w"], 0, 1, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(),
-                    o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(),
-                    o["sxy"].data_ptr(), p["ratio"].data_ptr(),
-                    None if self.planes is None else self.planes[k].data_ptr(), scr.data_ptr(), nbytes)
-            if self.Ld is not None and p["win_h"] == 32 and p["win_w"] == 32:
-                self._ok(self.Ld.pivb_dft_xcorr_dev(*args, self.dft_status.data_ptr(), s), "correlation (tensor core)")
-            else:
-                self._ok(self.Lx.pivb_xcorr_dev(*args, s), "correlation")
-            # large-displacement gate: half the window on the first pass, a quarter after
-            # (cpu_instantaneous.py:575-585), per axis
-            thr_x = p["win_w"] / 2.0 if k == 0 else p["win_w"] / 4.0
-            thr_y = p["win_h"] / 2.0 if k == 0 else p["win_h"] / 4.0
-            self._ok(self.Lp.pivb_validate_dev(
-                o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(),
-                None if pred_dy is None else pred_dy.data_ptr(), None if pred_dx is None else pred_dx.data_ptr(),
-                mptr, N, p["ny"], p["nx"], thr_x, thr_y, cfg.peak_mag_threshold, cfg.median_epsilon,
-                cfg.median_threshold, cfg.median_size, p["ux"].data_ptr(), p["uy"].data_ptr(),
-                p["invalid"].data_ptr(), p["reason"].data_ptr(), self.work.data_ptr(), s), "validate")
-            last = k + 1 == len(self.passes)
-            if not last or cfg.final_infill:
-                self._ok(self.Lp.pivb_infill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), mptr,
-                                                 N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
-                                                 self.infill_order, cfg.infill_max_iter, cfg.infill_tol,
-                                                 self.infill_work.data_ptr(), self.infill_work.numel(), s), "infill")
-            if not last:
-                src_x, src_y = p["ux"], p["uy"]
-                if self._fills(k):
-                    # harmonic fill of the masked windows, every other window fixed
-                    # (infilling.py:808-874 with the harmonic least-squares fill)
-                    nv = N * p["ny"] * p["nx"]
-                    src_x, src_y = self.fill[0, :nv], self.fill[1, :nv]
-                    src_x.copy_(p["ux"].reshape(-1)[:nv])
-                    src_y.copy_(p["uy"].reshape(-1)[:nv])
-                    self._ok(self.Lp.pivb_infill_dev(src_x.data_ptr(), src_y.data_ptr(), p["mask_u8"].data_ptr(),
-                                                     None, N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
-                                                     1, cfg.infill_max_iter, cfg.infill_tol,
-                                                     self.infill_work.data_ptr(), self.infill_work.numel(), s),
-                                     "predictor fill")
-                self._ok(self.Lp.pivb_pad_smooth_dev(src_x.data_ptr(), src_y.data_ptr(), N, p["ny"], p["nx"],
-                                                     p["nyp"], p["nxp"], p["pre"][0], p["pre"][1],
-                                                     p["taps"].data_ptr(), p["radius"], p["pdy"].data_ptr(),
-                                                     p["pdx"].data_ptr(), self.work.data_ptr(), s), "pad/smooth")
+        N = self._batch(n)
+        for k in range(len(self.passes)):
+            fa, fb = self.stage_pre(k, A, B, N)
+            self._correlate(k, fa, fb, N)
+            self.stage_post(k, N)
         self._last_n = N
         last = self.passes[-1]
         return last["ux"], last["uy"]
+
+    def _batch(self, n):
+        N = self.N if n is None else int(n)
+        if not 1 <= N <= self.N:
+            raise ValueError(f"n = {N} outside 1..{self.N}")
+        return N
+
+    # The pass split into stages, so that a scheduler can interleave several
+    # engines' passes and pack their correlations into shared launches
+    # (serving.PivServer(packed=True)).  run() is stage_pre, the correlation and
+    # stage_post for each pass in turn.
+    def stage_pre(self, k, A, B, N):
+        """Pass k's frames: the raw frames on pass 0, else the predictor of pass
+        k-1 remapped to this pass's windows and both frames warped by it."""
+        if k == 0:
+            return A, B
+        cfg, p, prev = self.cfg, self.passes[k], self.passes[k - 1]
+        s = self._stream()
+        H, W = self.H, self.W
+        self._ok(self.Lp.pivb_remap_dev(prev["pdy"].data_ptr(), prev["pdx"].data_ptr(), N, prev["nyp"],
+                                        prev["nxp"], p["map_y"].data_ptr(), p["map_x"].data_ptr(), p["ny"],
+                                        p["nx"], p["pred_dy"].data_ptr(), p["pred_dx"].data_ptr(), s), "remap")
+        fa, fb = self.warped
+        self._ok(self.Lw.pivb_warp_dev(A.data_ptr(), B.data_ptr(), fa.data_ptr(), fb.data_ptr(),
+                                       prev["pdy"].data_ptr(), prev["pdx"].data_ptr(), N, H, W, prev["nyp"],
+                                       prev["nxp"], H * W, self.tables[k].data_ptr(), cfg.interp_mode, 0, 0,
+                                       cfg.warp_impl, s), "warp")
+        return fa, fb
+
+    def _correlate(self, k, fa, fb, N):
+        cfg, p = self.cfg, self.passes[k]
+        s = self._stream()
+        H, W = self.H, self.W
+        o = p["out"]
+        scr = self.scratch
+        mptr = None if p["mask"] is None else p["mask"].data_ptr()
+        args = (fa.data_ptr(), fb.data_ptr(), H * W, mptr, H, W, N, p["cx"].data_ptr(), p["cy"].data_ptr(),
+                p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win_h"],
+                p["win_w"], 0, 1, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(),
+                o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(),
+                o["sxy"].data_ptr(), p["ratio"].data_ptr(),
+                None if self.planes is None else self.planes[k].data_ptr(), scr.data_ptr(), scr.numel())
+        if self.Ld is not None and p["win_h"] == 32 and p["win_w"] == 32:
+            self._ok(self.Ld.pivb_dft_xcorr_dev(*args, self.dft_status.data_ptr(), s), "correlation (tensor core)")
+        else:
+            self._ok(self.Lx.pivb_xcorr_dev(*args, s), "correlation")
+
+    def packable(self, k):
+        """Whether pass k's correlation can join a packed launch (square windows,
+        one peak, the FFT engine, no plane dump)."""
+        p = self.passes[k]
+        return (p["win_h"] == p["win_w"] and self.planes is None and 3 <= self.cfg.peak_finder <= 6
+                and not (self.Ld is not None and p["win_h"] == 32))
+
+    def job(self, k, fa, fb, N):
+        """Pass k's correlation as one job of a packed launch (_lib.XcorrJob)."""
+        p = self.passes[k]
+        o = p["out"]
+        return _lib.XcorrJob(fa.data_ptr(), fb.data_ptr(), self.H * self.W,
+                             None if p["mask"] is None else p["mask"].data_ptr(), self.H, self.W, N,
+                             p["cx"].data_ptr(), p["cy"].data_ptr(), p["ny"], p["nx"], p["weight"].data_ptr(),
+                             p["weight"].data_ptr(), p["cw"].data_ptr(), o["pk_loc_x"].data_ptr(),
+                             o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(),
+                             o["sy"].data_ptr(), o["sxy"].data_ptr(), p["ratio"].data_ptr())
+
+    def stage_post(self, k, N):
+        """Validation, infilling and (before the last pass) the next predictor."""
+        cfg, p = self.cfg, self.passes[k]
+        s = self._stream()
+        o = p["out"]
+        mptr = None if p["mask"] is None else p["mask"].data_ptr()
+        pred_dy = p["pred_dy"] if k > 0 else None
+        pred_dx = p["pred_dx"] if k > 0 else None
+        # large-displacement gate: half the window on the first pass, a quarter after
+        # (cpu_instantaneous.py:575-585), per axis
+        thr_x = p["win_w"] / 2.0 if k == 0 else p["win_w"] / 4.0
+        thr_y = p["win_h"] / 2.0 if k == 0 else p["win_h"] / 4.0
+        self._ok(self.Lp.pivb_validate_dev(
+            o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(),
+            None if pred_dy is None else pred_dy.data_ptr(), None if pred_dx is None else pred_dx.data_ptr(),
+            mptr, N, p["ny"], p["nx"], thr_x, thr_y, cfg.peak_mag_threshold, cfg.median_epsilon,
+            cfg.median_threshold, cfg.median_size, p["ux"].data_ptr(), p["uy"].data_ptr(),
+            p["invalid"].data_ptr(), p["reason"].data_ptr(), self.work.data_ptr(), s), "validate")
+        last = k + 1 == len(self.passes)
+        if not last or cfg.final_infill:
+            self._ok(self.Lp.pivb_infill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), mptr,
+                                             N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
+                                             self.infill_order, cfg.infill_max_iter, cfg.infill_tol,
+                                             self.infill_work.data_ptr(), self.infill_work.numel(), s), "infill")
+        if not last:
+            src_x, src_y = p["ux"], p["uy"]
+            if self._fills(k):
+                # harmonic fill of the masked windows, every other window fixed
+                # (infilling.py:808-874 with the harmonic least-squares fill)
+                nv = N * p["ny"] * p["nx"]
+                src_x, src_y = self.fill[0, :nv], self.fill[1, :nv]
+                src_x.copy_(p["ux"].reshape(-1)[:nv])
+                src_y.copy_(p["uy"].reshape(-1)[:nv])
+                self._ok(self.Lp.pivb_infill_dev(src_x.data_ptr(), src_y.data_ptr(), p["mask_u8"].data_ptr(),
+                                                 None, N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
+                                                 1, cfg.infill_max_iter, cfg.infill_tol,
+                                                 self.infill_work.data_ptr(), self.infill_work.numel(), s),
+                                 "predictor fill")
+            self._ok(self.Lp.pivb_pad_smooth_dev(src_x.data_ptr(), src_y.data_ptr(), N, p["ny"], p["nx"],
+                                                 p["nyp"], p["nxp"], p["pre"][0], p["pre"][1],
+                                                 p["taps"].data_ptr(), p["radius"], p["pdy"].data_ptr(),
+                                                 p["pdx"].data_ptr(), self.work.data_ptr(), s), "pad/smooth")
+        if last:
+            self._last_n = N
 
     def collect(self, n=None):
         """Per-pair results of the last run, every pass, as host PIVResult objects

@@ -18,6 +18,15 @@ Engines are created on first use while the estimated device memory stays within
 the budget; a request whose engine does not fit waits until one can be made.
 Every pair's result is independent of what it is batched with (the kernels work
 per pair and per window), so a request's field is the same alone and in a mix.
+
+Packed mode (`packed=True`) runs the waiting requests of every idle class
+together as one round on one stream (up to two rounds in flight on two
+streams): a round advances all its engines pass by pass, and each pass's
+correlations of one window size -- requests of different frame sizes and
+schedules -- go into one packed launch (pivb_xcorr_jobs_dev: a work list of
+per-request jobs in one grid, plus one launch of the fit kernel), so a round
+issues one correlation launch per window size and pass instead of one per
+engine.  Requests arriving during a round join a later one.
 """
 
 from __future__ import annotations
@@ -63,10 +72,11 @@ def schedule_config(schedule, overlap=50):
 
 
 class PivServer:
-    def __init__(self, device=None, max_batch=4, hbm_budget_bytes=120e9, overlap=50):
+    def __init__(self, device=None, max_batch=4, hbm_budget_bytes=120e9, overlap=50, packed=False):
         import torch
 
         self.torch = torch
+        self.packed = packed
         self.device = torch.device("cuda" if device is None else device)
         self.max_batch = max_batch
         self.budget = float(hbm_budget_bytes)
@@ -76,7 +86,15 @@ class PivServer:
         self.waiting: dict = {}
         self.n_submitted = 0
         self.Lp = _lib.pass_lib()
+        self.Lx = _lib.bulkxcorr2d_lib()
         self._free: dict = {}          # (ny, nx) -> reusable pinned output pairs
+        # packed mode: up to `packed_rounds` rounds in flight, each on its own
+        # stream with its own fit records; an engine belongs to one round at a time
+        self.packed_rounds = 2
+        self._pack_streams = [torch.cuda.Stream(device=self.device) for _ in range(self.packed_rounds)] if packed else []
+        self._rounds = []              # in flight: (requests, event, engines, stream index)
+        self._records = [None] * self.packed_rounds
+        self.pack_stats = {"rounds": 0, "packed_launches": 0, "jobs": 0, "single_launches": 0}
 
     # ------------------------------------------------------------------ #
     @staticmethod
@@ -172,8 +190,98 @@ class PivServer:
         e.busy = batch
         e.event = ev
 
+    def _records_buffer(self, si, nbytes):
+        torch = self.torch
+        if self._records[si] is None or self._records[si].numel() < nbytes:
+            self._records[si] = torch.empty(max(int(nbytes), 1 << 20), dtype=torch.uint8, device=self.device)
+        return self._records[si]
+
+    def _launch_packed(self, work, si):
+        """One packed round on stream `si`: `work` is a list of (engine, batch)."""
+        torch = self.torch
+        stream = self._pack_streams[si]
+        st = ctypes.c_void_p(stream.cuda_stream)
+        jmax = int(self.Lx.pivb_xcorr_jobs_max())
+        with torch.cuda.stream(stream):
+            for e, batch in work:
+                for i, r in enumerate(batch):
+                    e.u16[0][i].copy_(r.A, non_blocking=True)
+                    e.u16[1][i].copy_(r.B, non_blocking=True)
+                n = len(batch) * e.u16[0].shape[1] * e.u16[0].shape[2]
+                for j in range(2):
+                    if self.Lp.pivb_u16_to_f32_dev(e.u16[j].data_ptr(), e.f32[j].data_ptr(), n, st) != 0:
+                        raise RuntimeError("u16 -> f32 conversion failed")
+            n_pass = max(len(e.mp.passes) for e, _ in work)
+            for k in range(n_pass):
+                act = [(e, b) for e, b in work if k < len(e.mp.passes)]
+                frames = [e.mp.stage_pre(k, e.f32[0], e.f32[1], len(b)) for e, b in act]
+                groups: dict = {}
+                for (e, b), fr in zip(act, frames):
+                    if e.mp.packable(k):
+                        key = (e.mp.passes[k]["win_h"], e.mp.cfg.peak_finder, e.mp.cfg.peakfit_impl)
+                        groups.setdefault(key, []).append(e.mp.job(k, fr[0], fr[1], len(b)))
+                    else:
+                        e.mp._correlate(k, fr[0], fr[1], len(b))
+                        self.pack_stats["single_launches"] += 1
+                for (win, finder, impl), jobs in groups.items():
+                    for c0 in range(0, len(jobs), jmax):
+                        chunk = jobs[c0:c0 + jmax]
+                        arr = (_lib.XcorrJob * len(chunk))(*chunk)
+                        nb = int(self.Lx.pivb_xcorr_jobs_record_bytes(arr, len(chunk), win))
+                        rec = self._records_buffer(si, nb)
+                        code = self.Lx.pivb_xcorr_jobs_dev(arr, len(chunk), win, finder, impl, rec.data_ptr(),
+                                                           rec.numel(), st)
+                        if code != 0:
+                            raise RuntimeError(f"packed correlation failed with code {code}")
+                        self.pack_stats["packed_launches"] += 1
+                        self.pack_stats["jobs"] += len(chunk)
+                for e, b in act:
+                    e.mp.stage_post(k, len(b))
+            for e, batch in work:
+                last = e.mp.passes[-1]
+                for i, r in enumerate(batch):
+                    r.ux.copy_(last["ux"][i], non_blocking=True)
+                    r.uy.copy_(last["uy"][i], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        self.pack_stats["rounds"] += 1
+        for e, b in work:
+            e.busy = b
+        self._rounds.append(([r for _, b in work for r in b], ev, [e for e, _ in work], si))
+
+    def _poll_packed(self):
+        finished = []
+        now = None
+        for rd in list(self._rounds):
+            reqs, ev, engines, _ = rd
+            if ev.query():
+                now = time.perf_counter() if now is None else now
+                for r in reqs:
+                    r.done = now
+                    r.finished = True
+                finished.extend(reqs)
+                for e in engines:
+                    e.busy = []
+                self._rounds = [x for x in self._rounds if x is not rd]
+        if len(self._rounds) < self.packed_rounds:
+            work = []
+            for key, q in self.waiting.items():
+                if not q:
+                    continue
+                e = self._engine(*key)
+                if e is None or e.busy:
+                    continue
+                work.append((e, [q.popleft() for _ in range(min(self.max_batch, len(q)))]))
+            if work:
+                used = {rd[3] for rd in self._rounds}
+                si = next(i for i in range(self.packed_rounds) if i not in used)
+                self._launch_packed(work, si)
+        return finished
+
     def poll(self):
         """One scheduling round; returns the requests finished in it."""
+        if self.packed:
+            return self._poll_packed()
         finished = []
         now = None
         for e in self.engines.values():
@@ -196,7 +304,8 @@ class PivServer:
         return finished
 
     def idle(self):
-        return all(not e.busy for e in self.engines.values()) and all(not q for q in self.waiting.values())
+        return (not self._rounds and all(not e.busy for e in self.engines.values())
+                and all(not q for q in self.waiting.values()))
 
     def drain(self, timeout_s=120.0):
         t0 = time.perf_counter()
