@@ -53,6 +53,8 @@ def _args():
                     help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
                          "serve: Poisson request stream with continuous batching")
     ap.add_argument("--chunk", type=int, default=32, help="e2e: pairs per host-to-device chunk")
+    ap.add_argument("--dft-frames", type=int, nargs=2, default=[49, 13], metavar=("F64", "F32"),
+                    help="dft: 4096^2 mosaic frames of 64 px and of 32 px windows (smaller for profiling)")
     ap.add_argument("--engine32", default="fft", choices=["fft", "dft"],
                     help="32 px passes on the FP32 FFT path or the tensor-core DFT-as-GEMM path")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: offered pairs/s")
@@ -684,14 +686,11 @@ def run_dft(args):
     """Tensor-core workload: 200k independent 64x64 and 200k 32x32 windows cut
     from particle images with uniform random shifts in [-4, 4]^2 px, packed as
     mosaics of 0%-overlap windows in 4096 x 4096 frames (49 frames of 4,096
-    windows of 64 px, 13 frames of 16,384 windows of 32 px), gauss3 fits.  The
-    32 px windows run on the split-BF16 tensor-core DFT-as-GEMM path and, for
-    the comparison, on the FP32 FFT path; the 64 px windows run on the FFT path
-    (the dense 64-point DFT chain costs 54 n^3 = 14.2 MFLOP of tensor work per
-    window against the FFT's 381 k FP32 flops, a 37x ratio beyond the 22x of the
-    peaks, so no tensor-core 64 px form is built).  Value: windows/s of the whole
-    400k-window step; each path's plane error and displacement RMS against the
-    FP64 oracle on a sample frame are in the line."""
+    windows of 64 px, 13 frames of 16,384 windows of 32 px), gauss3 fits.  Both
+    window sizes run on the split-BF16 tensor-core DFT-as-GEMM path (the step);
+    each size also runs on the FP32 FFT path for the comparison.  Value:
+    windows/s of the whole 400k-window step; each path's plane error and
+    displacement RMS against the FP64 oracle on a sample frame are in the line."""
     import ctypes
 
     import numpy as np
@@ -703,7 +702,7 @@ def run_dft(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     side = 4096
-    sets = {64: 49, 32: 13}
+    sets = {64: args.dft_frames[0], 32: args.dft_frames[1]}
     Lx, Ld = _lib.bulkxcorr2d_lib(), _lib.dft_lib()
     data = {}
     for n, nf in sets.items():
@@ -752,8 +751,9 @@ def run_dft(args):
         return e0.elapsed_time(e1) / reps
 
     with ClockSampler(local) as clk:
-        ms_step = timed(lambda: (launch(64, "fft"), launch(32, "dft")), args.steps)
+        ms_step = timed(lambda: (launch(64, "dft"), launch(32, "dft")), args.steps)
         ms_dft32 = timed(lambda: launch(32, "dft"), args.steps)
+        ms_dft64 = timed(lambda: launch(64, "dft"), args.steps)
         ms_fft32 = timed(lambda: launch(32, "fft"), args.steps)
         ms_fft64 = timed(lambda: launch(64, "fft"), args.steps)
     if int(status.item()) != 0:
@@ -771,7 +771,7 @@ def run_dft(args):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
 
-        for n, engine in ((32, "dft"), (32, "fft"), (64, "fft")):
+        for n, engine in ((32, "dft"), (32, "fft"), (64, "dft"), (64, "fft")):
             d = data[n]
             g = d["g"]
             planes = torch.zeros((g.n_win_y * g.n_win_x, n, n), device=dev)
@@ -795,22 +795,30 @@ def run_dft(args):
                 "rms_px_vs_true_shift": float(np.sqrt(np.nanmean((gx - true[..., 1]) ** 2 + (gy - true[..., 0]) ** 2)))}
     if rank == 0:
         _, bf16_peak, peak_kind = _peaks()
-        n32 = data[32]["total"]
-        tflops = n32 * 1.769e6 / (ms_dft32 * 1e-3) / 1e12
+        n32, n64 = data[32]["total"], data[64]["total"]
+        # tensor flops per window (split BF16, three products): 54 n^3
+        tf32, tf64 = 54.0 * 32 ** 3, 54.0 * 64 ** 3
+        tflops = (n32 * tf32 + n64 * tf64) / (ms_step * 1e-3) / 1e12
         line = {
-            "metric": "windows/s, split-BF16 tensor-core DFT-as-GEMM path (32 px) + FP32 FFT path (64 px) on 1 B200",
+            "metric": "windows/s, split-BF16 tensor-core DFT-as-GEMM path (64 px + 32 px windows) on 1 B200",
             "value": value, "unit": "windows/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "bf16x3 (32 px) / f32 (64 px)", "data": "synthetic",
+            "dtype": "bf16x3", "data": "synthetic",
             "config": {"workload": "200k 64x64 + 200k 32x32 independent windows, uniform shifts in [-4, 4] px, "
-                                   "mosaics of 0%-overlap windows in 4096^2 frames (49 + 13 frames), gauss3",
-                       "windows_64": data[64]["total"], "windows_32": n32,
-                       "l2": f"inputs {(49 + 13) * 2 * side * side * 4 / 1e9:.1f} GB > L2"},
-            "paths_ms": {"dft32": ms_dft32, "fft32": ms_fft32, "fft64": ms_fft64},
-            "dft32_vs_fft32": ms_fft32 / ms_dft32,
+                                   "mosaics of 0%-overlap windows in 4096^2 frames (49 + 13 frames), gauss3"
+                                   if tuple(args.dft_frames) == (49, 13) else
+                                   f"{n64} 64x64 + {n32} 32x32 independent windows (reduced case)",
+                       "windows_64": n64, "windows_32": n32,
+                       "l2": f"inputs {sum(sets.values()) * 2 * side * side * 4 / 1e9:.1f} GB > L2"},
+            "paths_ms": {"dft32": ms_dft32, "dft64": ms_dft64, "fft32": ms_fft32, "fft64": ms_fft64},
+            "dft_vs_fft": {"32": ms_fft32 / ms_dft32, "64": ms_fft64 / ms_dft64,
+                           "step": (ms_fft32 + ms_fft64) / ms_step, "target": 5.0},
             "roofline": {"bound": "tensor", "achieved": tflops, "peak": bf16_peak, "unit": "TFLOP/s",
                          "frac": tflops / bf16_peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "dft32 tcgen05 kernel + lm_records_kernel", "tensor_flops_per_window": 1.769e6},
+                         "kernel": "dft64 + dft32 tcgen05 kernels + lm_records_kernel",
+                         "tensor_flops_per_window": {"32": tf32, "64": tf64},
+                         "per_path_tflops": {"dft32": n32 * tf32 / (ms_dft32 * 1e-3) / 1e12,
+                                             "dft64": n64 * tf64 / (ms_dft64 * 1e-3) / 1e12}},
             "accuracy": acc, "clocks": clk.summary(),
             "e2e": None, "gpu_launches": 2 * args.steps * 2,
         }

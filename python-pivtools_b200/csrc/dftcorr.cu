@@ -554,6 +554,467 @@ const uint4 *consts_for_current_device()
 
 }  // namespace dft32
 
+// ---------------------------------------------------------------------------
+// DFT-as-GEMM correlation, 64 x 64 windows
+// ---------------------------------------------------------------------------
+// One CTA per SM (512 threads, 16 warps; 225 KB of shared memory) takes groups
+// of four windows through the same four GEMMs as the 32 px chain, sized for
+// n = 64:
+//
+//   stage 1  Y = X W1          per image, rows (window, y) in two 128-row tiles,
+//                              K = x (64), N = 64: Re Y(kx) for kx < 32, the
+//                              Nyquist column Y(32) in the slot of Im Y(0),
+//                              Im Y(kx) for kx > 32;
+//   stage 2  F^T = Y^T W2      per image, rows (window, kx) (4 x 32), K = (Re, Im)
+//                              x y (128), N = (Re, Im) x ky (128);
+//            C = F_B conj(F_A) per element, row kx = 0 (DC and Nyquist packed)
+//                              unpacked by Hermitian symmetry and repacked;
+//   stage 3  conj(G)^T = conj(C)^T W2   the inverse column DFT as the forward DFT
+//                              of the conjugate (so W2 serves both directions);
+//   stage 4  c = G W4          rows (window, y) in two tiles, K = (Re, Im) x kx
+//                              (64), N = x (64): the Hermitian inverse row DFT.
+//
+// Tensor memory: 256 columns, reused by every stage.  Shared memory: the three
+// constant operands (96 KB, hi + lo) and two 64 KB work buffers, which hold in
+// turn the stage-1 operands of images A and B, the stage-2 operands of A and B,
+// the conjugate spectrum product (buffer 0) with the kx = 0 exchange (buffer 1),
+// the stage-4 operand (buffer 1) and finally the four fftshifted float planes
+// (row stride 65, across both buffers).
+namespace dft64 {
+
+using namespace piv;
+
+constexpr int N = 64;
+constexpr int G = 4;                      // windows per group
+constexpr int THREADS = 512;
+constexpr uint32_t C1 = 0, C1_BYTES = 64 * 64 * 2;
+constexpr uint32_t C2 = C1 + 2 * C1_BYTES, C2_BYTES = 128 * 128 * 2;
+constexpr uint32_t C4 = C2 + 2 * C2_BYTES, C4_BYTES = 64 * 64 * 2;
+constexpr uint32_t CONST_BYTES = C4 + 2 * C4_BYTES;         // 96 KB
+constexpr uint32_t BUF = 64 * 1024;
+constexpr uint32_t WORK_BYTES = 2 * BUF;
+constexpr int PLANE_LD = WinGeo<N>::STF;                    // 65
+constexpr uint32_t MISC_BYTES = 1024;
+constexpr uint32_t SMEM_BYTES = CONST_BYTES + WORK_BYTES + MISC_BYTES;
+constexpr uint32_t TMEM_COLS = 256;
+static_assert(G * N * PLANE_LD * 4 <= WORK_BYTES, "planes alias the work buffers");
+static_assert(G * N * 4 * 4 <= BUF, "kx = 0 exchange fits buffer 1");
+static_assert(SMEM_BYTES <= 232448, "one CTA per SM");
+
+struct WinInfo {
+    long long idx;
+    int n, iw;
+    float enorm;
+    int flags;     // 1 valid, 2 in range
+};
+
+// One candidate strip per thread of the window's 128 (rows and columns [16, 48)
+// of the shifted plane, strips of 8 rows; the rolled 3x3 test of search_plane),
+// then the warp's reduction; the caller merges the window's four warps.
+__device__ __forceinline__ void search_strip(const float *pl, int t, PeakAcc &acc, bool &nan)
+{
+    constexpr int H2 = N / 2, Q = N / 4, S = 8;
+    acc.init();
+    nan = false;
+    const int j = Q + t % H2, r0 = Q + (t / H2) * S;
+    const float *c0 = pl + (r0 - 1) * PLANE_LD + j;
+    float m0 = 0.0f, m1 = 0.0f, c1 = 0.0f;
+#pragma unroll
+    for (int k = 0; k < S + 2; ++k) {
+        const float l = c0[k * PLANE_LD - 1], c = c0[k * PLANE_LD], r = c0[k * PLANE_LD + 1];
+        nan |= (l != l) | (c != c) | (r != r);
+        const float m2 = fmaxf(l, fmaxf(c, r));
+        if (k >= 2) {
+            const float v = c1;
+            const bool mx = v >= fmaxf(m0, fmaxf(m1, m2));
+            acc.add((mx && v > 0.0f) ? v : -1.0f, (r0 + k - 2) * N + j);
+        }
+        m0 = m1;
+        m1 = m2;
+        c1 = c;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float ob = __shfl_xor_sync(0xffffffffu, acc.best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, acc.idx, o);
+        const float o1 = __shfl_xor_sync(0xffffffffu, acc.p1, o);
+        const float o2 = __shfl_xor_sync(0xffffffffu, acc.p2, o);
+        acc.merge(ob, oi, o1, o2);
+    }
+    nan = __any_sync(0xffffffffu, nan);
+}
+
+__global__ void __launch_bounds__(THREADS, 1) kernel(XcorrParams prm, const uint4 *__restrict__ consts, int *status)
+{
+    extern __shared__ __align__(1024) unsigned char sm[];
+    __shared__ WinInfo info[G];
+    unsigned char *cst = sm;
+    unsigned char *buf0 = sm + CONST_BYTES, *buf1 = buf0 + BUF;
+    float *misc = reinterpret_cast<float *>(sm + CONST_BYTES + WORK_BYTES);
+    float *red = misc;                                     // [G][4 warps][4]
+    int *nanred = reinterpret_cast<int *>(misc + 64);      // [G][4]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(misc + 96);
+    uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 1);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    const int wg = warp >> 2, wq = warp & 3;
+    for (int i = t; i < (int)(CONST_BYTES / 16); i += THREADS) reinterpret_cast<uint4 *>(cst)[i] = consts[i];
+    if (t == 0) umma::mbar_init(bar, 1);
+    if (warp == 0) umma::tmem_alloc(slot, TMEM_COLS);
+    dft32::cta_sync_for_mma();
+    const uint32_t tm = *slot;
+    const uint32_t lane_base = tm + ((uint32_t)(32 * wq) << 16);
+    const uint32_t cst_a = umma::smem_u32(cst), b0_a = umma::smem_u32(buf0), b1_a = umma::smem_u32(buf1);
+    const uint32_t bar_a = umma::smem_u32(bar);
+    uint32_t phase = 0;
+    bool ok = true;
+    const long long nwt = (long long)prm.nwy * prm.nwx;
+    const long long ngroups = (prm.total + G - 1) / G;
+    const float inv_numel = 1.0f / (float)(N * N);
+
+    // Wait for the stage's MMAs; every thread learns whether any wait ran out.
+    auto wait_stage = [&]() -> bool {
+        const bool mine = umma::mbar_wait(bar_a, phase);
+        phase ^= 1u;
+        umma::fence_after();
+        return __syncthreads_and(mine ? 1 : 0) != 0;
+    };
+
+    for (long long grp = blockIdx.x; grp < ngroups && ok; grp += gridDim.x) {
+        // ---- stage 0: gather, weight, mean, energy (PIV_2d_cross_correlate.c:299-353).
+        //      Warp (wq, wg) takes rows 16 wq .. 16 wq + 15 of window wg; lane = columns
+        //      lane and lane + 32.
+        {
+            const int wl = wg, rb = wq;
+            const long long idx = grp * G + wl;
+            const bool inrange = idx < prm.total;
+            bool valid = inrange;
+            int n = 0, iw = 0, r0 = 0, c0 = 0;
+            if (inrange) {
+                n = (int)(idx / nwt);
+                iw = (int)(idx - (long long)n * nwt);
+                const int ii = iw % prm.nwx, jj = iw / prm.nwx;
+                if (prm.mask && prm.mask[iw] == 1.0f) valid = false;
+                r0 = (int)floor((double)prm.ctr_y[jj] - ((double)N - 1.0) / 2.0 + 0.5);
+                c0 = (int)floor((double)prm.ctr_x[ii] - ((double)N - 1.0) / 2.0 + 0.5);
+                if (r0 < 0 || c0 < 0 || r0 + N > prm.H || c0 + N > prm.W) valid = false;
+            }
+            float a0[16], a1[16], b0[16], b1[16];
+            float sa = 0.0f, sb = 0.0f;
+            if (valid) {
+                const long long base = (long long)n * prm.img_stride + (long long)(r0 + 16 * rb) * prm.W + c0 + lane;
+                const float *fa = prm.A + base, *fb = prm.B + base;
+                const float *wa = prm.wA + 16 * rb * N + lane, *wb = prm.wB + 16 * rb * N + lane;
+#pragma unroll
+                for (int y = 0; y < 16; ++y) {
+                    a0[y] = __ldg(fa + y * prm.W) * __ldg(wa + y * N);
+                    a1[y] = __ldg(fa + y * prm.W + 32) * __ldg(wa + y * N + 32);
+                    b0[y] = __ldg(fb + y * prm.W) * __ldg(wb + y * N);
+                    b1[y] = __ldg(fb + y * prm.W + 32) * __ldg(wb + y * N + 32);
+                    sa += a0[y] + a1[y];
+                    sb += b0[y] + b1[y];
+                }
+            } else {
+#pragma unroll
+                for (int y = 0; y < 16; ++y) { a0[y] = 0.0f; a1[y] = 0.0f; b0[y] = 0.0f; b1[y] = 0.0f; }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                sa += __shfl_xor_sync(0xffffffffu, sa, o);
+                sb += __shfl_xor_sync(0xffffffffu, sb, o);
+            }
+            if (lane == 0) { red[(wl * 4 + rb) * 4 + 0] = sa; red[(wl * 4 + rb) * 4 + 1] = sb; }
+            __syncthreads();
+            const float *rw = red + wl * 16;
+            const float ma = (((rw[0] + rw[4]) + rw[8]) + rw[12]) / (float)(N * N);
+            const float mb = (((rw[1] + rw[5]) + rw[9]) + rw[13]) / (float)(N * N);
+            float ea = 0.0f, eb = 0.0f;
+#pragma unroll
+            for (int y = 0; y < 16; ++y) {
+                if (valid && !prm.ensemble) { a0[y] -= ma; a1[y] -= ma; b0[y] -= mb; b1[y] -= mb; }
+                ea += a0[y] * a0[y] + a1[y] * a1[y];
+                eb += b0[y] * b0[y] + b1[y] * b1[y];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                ea += __shfl_xor_sync(0xffffffffu, ea, o);
+                eb += __shfl_xor_sync(0xffffffffu, eb, o);
+            }
+            if (lane == 0) { red[(wl * 4 + rb) * 4 + 2] = ea; red[(wl * 4 + rb) * 4 + 3] = eb; }
+            __syncthreads();
+            if (t == wl * 128) {          // lane 0 of warp (0, wl)
+                const float eA = ((rw[2] + rw[6]) + rw[10]) + rw[14];
+                const float eB = ((rw[3] + rw[7]) + rw[11]) + rw[15];
+                info[wl].idx = idx;
+                info[wl].n = n;
+                info[wl].iw = iw;
+                info[wl].enorm = 1.0f / sqrtf(eA * eB);
+                info[wl].flags = (valid ? 1 : 0) | (inrange ? 2 : 0);
+            }
+            // A1 tiles (MN-major, 16 KB hi + 16 KB lo): image A in buffer 0, B in buffer 1;
+            // tile m = window / 2 at 32 KB * m; row (window % 2) * 64 + y, K = x
+            const int m = wl >> 1;
+            unsigned char *ta = buf0 + m * 32768, *tb = buf1 + m * 32768;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const uint32_t row = (uint32_t)((wl & 1) * 64 + 16 * rb + 8 * q);
+                const uint32_t o0 = umma::mnmajor_offset(128, row, lane);
+                const uint32_t o1 = umma::mnmajor_offset(128, row, 32 + lane);
+                dft32::store8(ta + o0, ta + 16384 + o0, a0 + 8 * q);
+                dft32::store8(ta + o1, ta + 16384 + o1, a1 + 8 * q);
+                dft32::store8(tb + o0, tb + 16384 + o0, b0 + 8 * q);
+                dft32::store8(tb + o1, tb + 16384 + o1, b1 + 8 * q);
+            }
+        }
+        dft32::cta_sync_for_mma();
+        // ---- stage 1: tiles (image, m) -> tensor-memory columns 64 (2 image + m)
+        if (t == 0) {
+            for (int img = 0; img < 2; ++img)
+                for (int m = 0; m < 2; ++m) {
+                    const uint32_t a = (img ? b1_a : b0_a) + m * 32768;
+                    dft32::gemm3(tm + 64 * (2 * img + m), a, a + 16384, cst_a + C1, cst_a + C1 + C1_BYTES, 64, 4,
+                                 true);
+                }
+            umma::commit(bar_a);
+        }
+        if (!(ok = wait_stage())) break;
+        // ---- Y -> A2 (MN-major, 32 KB hi + 32 KB lo per image, in that image's buffer).
+        //      Row (window, kx) = window * 32 + kx; K: Re at y, Im at 64 + y.  Warp
+        //      (wq, wg) reads tile wg: lane 32 wq + lane = (window % 2) * 64 + y.
+        {
+            const int tt = wg, img = tt >> 1, m = tt & 1;
+            const int wl = 2 * m + (wq >> 1), y = (wq & 1) * 32 + lane;
+            float v[32];
+            unsigned char *dst = img ? buf1 : buf0;
+#pragma unroll 1
+            for (int h = 0; h < 2; ++h) {       // h = 0: Re Y(kx), h = 1: Im Y(kx) (Y(32) at kx = 0)
+                umma::tmem_ld32(lane_base + 64 * tt + 32 * h, v);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t o = umma::mnmajor_offset(128, (uint32_t)(wl * 32 + 8 * q), (uint32_t)(64 * h + y));
+                    dft32::store8(dst + o, dst + 32768 + o, v + 8 * q);
+                }
+            }
+        }
+        dft32::cta_sync_for_mma();
+        // ---- stage 2: images A, B; N = 128, K = 128; D at columns 0 (A) and 128 (B)
+        if (t == 0) {
+            dft32::gemm3(tm, b0_a, b0_a + 32768, cst_a + C2, cst_a + C2 + C2_BYTES, 128, 8, true);
+            dft32::gemm3(tm + 128, b1_a, b1_a + 32768, cst_a + C2, cst_a + C2 + C2_BYTES, 128, 8, true);
+            umma::commit(bar_a);
+        }
+        if (!(ok = wait_stage())) break;
+        // ---- spectrum product -> conj(C) as A3 (K-major, 32 KB hi + 32 KB lo, buffer 0);
+        //      lane 32 wq + lane = (window wq, kx = lane); warp group wg takes ky in
+        //      [16 wg, 16 wg + 16).  Rows kx = 0 (lane 0) need F(-ky): exchanged
+        //      through buffer 1.
+        {
+            const int k0 = 16 * wg;
+            float ar[16], ai[16], br[16], bi[16];
+            umma::tmem_ld16(lane_base + k0, ar);
+            umma::tmem_ld16(lane_base + 64 + k0, ai);
+            umma::tmem_ld16(lane_base + 128 + k0, br);
+            umma::tmem_ld16(lane_base + 192 + k0, bi);
+            float *xchg = reinterpret_cast<float *>(buf1) + wq * (N * 4);    // [ky][ar, ai, br, bi]
+            if (lane == 0) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    float *e = xchg + (k0 + j) * 4;
+                    e[0] = ar[j]; e[1] = ai[j]; e[2] = br[j]; e[3] = bi[j];
+                }
+            }
+            __syncthreads();
+            float cr[16], ci[16];
+            if (lane != 0) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    cr[j] = br[j] * ar[j] + bi[j] * ai[j];
+                    ci[j] = bi[j] * ar[j] - br[j] * ai[j];
+                }
+            } else {
+                // P = F(., 0) + i F(., 32); F0 = (P + conj P(-ky)) / 2, F32 = (P - conj P(-ky)) / 2i
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int ky = k0 + j, mk = (N - ky) & (N - 1);
+                    const float *e = xchg + mk * 4;
+                    const float amr = e[0], ami = e[1], bmr = e[2], bmi = e[3];
+                    const float a0r = 0.5f * (ar[j] + amr), a0i = 0.5f * (ai[j] - ami);
+                    const float a1r = 0.5f * (ai[j] + ami), a1i = -0.5f * (ar[j] - amr);
+                    const float b0r = 0.5f * (br[j] + bmr), b0i = 0.5f * (bi[j] - bmi);
+                    const float b1r = 0.5f * (bi[j] + bmi), b1i = -0.5f * (br[j] - bmr);
+                    const float c0r = b0r * a0r + b0i * a0i, c0i = b0i * a0r - b0r * a0i;
+                    const float c1r = b1r * a1r + b1i * a1i, c1i = b1i * a1r - b1r * a1i;
+                    cr[j] = c0r - c1i;        // Q = C0 + i C32
+                    ci[j] = c0i + c1r;
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 16; ++j) ci[j] = -ci[j];          // conj(C)
+            const uint32_t r = (uint32_t)(wq * 32 + lane);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const uint32_t o_re = umma::kmajor_offset(128, r, (uint32_t)(k0 + 8 * c));
+                const uint32_t o_im = umma::kmajor_offset(128, r, (uint32_t)(64 + k0 + 8 * c));
+                dft32::store8(buf0 + o_re, buf0 + 32768 + o_re, cr + 8 * c);
+                dft32::store8(buf0 + o_im, buf0 + 32768 + o_im, ci + 8 * c);
+            }
+        }
+        dft32::cta_sync_for_mma();
+        // ---- stage 3: N = 128, K = 128, D = conj(G) at column 0
+        if (t == 0) {
+            dft32::gemm3(tm, b0_a, b0_a + 32768, cst_a + C2, cst_a + C2 + C2_BYTES, 128, 8, false);
+            umma::commit(bar_a);
+        }
+        if (!(ok = wait_stage())) break;
+        // ---- G -> A4 (MN-major, buffer 1; tile m = window / 2: 16 KB hi + 16 KB lo at
+        //      32 KB * m).  Row (window % 2) * 64 + y; K: Re at kx, Im at 32 + kx.
+        //      Lane 32 wq + lane = (window wq, kx = lane); warp group wg takes y in
+        //      [16 wg, 16 wg + 16).
+        {
+            const int y0 = 16 * wg, wl = wq, kx = lane;
+            float gre[16], gim[16];
+            umma::tmem_ld16(lane_base + y0, gre);
+            umma::tmem_ld16(lane_base + 64 + y0, gim);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) gim[j] = -gim[j];        // G = conj(D)
+            unsigned char *tile = buf1 + (wl >> 1) * 32768;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const uint32_t row = (uint32_t)((wl & 1) * 64 + y0 + 8 * q);
+                const uint32_t o_re = umma::mnmajor_offset(128, row, (uint32_t)kx);
+                const uint32_t o_im = umma::mnmajor_offset(128, row, (uint32_t)(32 + kx));
+                dft32::store8(tile + o_re, tile + 16384 + o_re, gre + 8 * q);
+                dft32::store8(tile + o_im, tile + 16384 + o_im, gim + 8 * q);
+            }
+        }
+        dft32::cta_sync_for_mma();
+        // ---- stage 4: two tiles, N = 64, K = 64, D at columns 0 and 64
+        if (t == 0) {
+            for (int m = 0; m < 2; ++m)
+                dft32::gemm3(tm + 64 * m, b1_a + m * 32768, b1_a + m * 32768 + 16384, cst_a + C4,
+                             cst_a + C4 + C4_BYTES, 64, 4, true);
+            umma::commit(bar_a);
+        }
+        if (!(ok = wait_stage())) break;
+        // ---- planes: scale, fftshift into shared memory (across both buffers, whose
+        //      operands the finished MMAs no longer read).  Warp (wq, wg): tile wg & 1,
+        //      columns 32 (wg >> 1) .. +31; lane 32 wq + lane = (window % 2) * 64 + y.
+        float *planes = reinterpret_cast<float *>(buf0);
+        {
+            const int m = wg & 1, h = wg >> 1;
+            const int wl = 2 * m + (wq >> 1), y = (wq & 1) * 32 + lane;
+            float c[32];
+            umma::tmem_ld32(lane_base + 64 * m + 32 * h, c);
+            float *pl = planes + wl * (N * PLANE_LD) + ((y + N / 2) & (N - 1)) * PLANE_LD;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) pl[(32 * h + j + N / 2) & (N - 1)] = c[j] * inv_numel;
+        }
+        __syncthreads();
+        // ---- search (window wg, warps wq = 0..3 one candidate strip per thread), merge,
+        //      then the FFT path's finish: with record scratch warp (0, wg) writes the
+        //      window's record line, otherwise its lane 0 fits in place
+        {
+            const int wl = wg;
+            const float *pl = planes + wl * (N * PLANE_LD);
+            const WinInfo wi = info[wl];
+            if (prm.planes && (wi.flags & 1)) {
+                float *dst = prm.planes + wi.idx * (long long)(N * N);
+                for (int k = wq * 32 + lane; k < N * N; k += 128) dst[k] = pl[(k / N) * PLANE_LD + (k % N)];
+            }
+            PeakAcc acc;
+            bool nan;
+            search_strip(pl, wq * 32 + lane, acc, nan);
+            if (lane == 0) {
+                float *e = red + (wl * 4 + wq) * 4;
+                e[0] = acc.best; e[1] = __int_as_float(acc.idx); e[2] = acc.p1; e[3] = acc.p2;
+                nanred[wl * 4 + wq] = nan ? 1 : 0;
+            }
+            __syncthreads();
+            if (wq == 0) {
+                acc.init();
+                bool has_nan = false;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float *e = red + (wl * 4 + k) * 4;
+                    acc.merge(e[0], __float_as_int(e[1]), e[2], e[3]);
+                    has_nan |= nanred[wl * 4 + k] != 0;
+                }
+                if (wi.flags & 2) {
+                    if (prm.lm)
+                        finish_window_rec<N>(lane, 32, prm, const_cast<float *>(pl), PLANE_LD, acc, has_nan, wi.idx,
+                                             wi.n, wi.iw, nwt, (wi.flags & 1) != 0, wi.enorm);
+                    else if (lane == 0)
+                        finish_window<N, false>(prm, const_cast<float *>(pl), PLANE_LD, acc, has_nan, wi.idx, wi.n,
+                                                wi.iw, nwt, (wi.flags & 1) != 0, wi.enorm);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (!ok) {
+        // a completion was not observed: record it, give the MMAs in flight a
+        // bounded time to finish before the tensor memory is released
+        if (t == 0) atomicExch(status, 1);
+        umma::mbar_wait(bar_a, phase ^ 1u);
+    }
+    umma::fence_before();
+    __syncthreads();
+    if (warp == 0) umma::tmem_free(tm, TMEM_COLS);
+}
+
+// ---- constant operands, built on the host in double precision and split to BF16
+void build_consts(unsigned char *c)
+{
+    const double tp = 2.0 * M_PI / N;
+    // W1: row j -> Re Y(j) (j < 32), Y(32) (j = 32), Im Y(j - 32) (j > 32); K = x
+    dft32::put(c, C1, C1_BYTES, 64, 64, [&](int j, int x) {
+        if (j < 32) return cos(tp * j * x);
+        if (j == 32) return (x & 1) ? -1.0 : 1.0;
+        return -sin(tp * (j - 32) * x);
+    });
+    // W2: row j -> Re F(ky = j) (j < 64), Im F(ky = j - 64); K: Re Y(y = k) (k < 64), Im Y(y = k - 64)
+    dft32::put(c, C2, C2_BYTES, 128, 128, [&](int j, int k) {
+        const int ky = j & 63, y = k & 63;
+        const double cs = cos(tp * ky * y), sn = sin(tp * ky * y);
+        if (j < 64) return k < 64 ? cs : sn;
+        return k < 64 ? -sn : cs;
+    });
+    // W4: row x -> c(x); K: Re G(kx = k) (k < 32), Im G(kx = k - 32); kx = 0 carries G(0) and G(32)
+    dft32::put(c, C4, C4_BYTES, 64, 64, [&](int x, int k) {
+        const int kx = k & 31;
+        if (k < 32) return kx == 0 ? 1.0 : 2.0 * cos(tp * kx * x);
+        return kx == 0 ? ((x & 1) ? -1.0 : 1.0) : -2.0 * sin(tp * kx * x);
+    });
+}
+
+std::mutex g_mu;
+void *g_consts[64] = {};
+
+const uint4 *consts_for_current_device()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_consts[dev]) {
+        static unsigned char host[CONST_BYTES];
+        memset(host, 0, sizeof(host));
+        build_consts(host);
+        void *d = nullptr;
+        if (cudaMalloc(&d, CONST_BYTES) != cudaSuccess) return nullptr;
+        if (cudaMemcpy(d, host, CONST_BYTES, cudaMemcpyHostToDevice) != cudaSuccess) {
+            cudaFree(d);
+            return nullptr;
+        }
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) != cudaSuccess) {
+            cudaFree(d);
+            return nullptr;
+        }
+        g_consts[dev] = d;
+    }
+    return static_cast<const uint4 *>(g_consts[dev]);
+}
+
+}  // namespace dft64
+
 }  // namespace
 
 // Self-test of the tensor-core path: D (128 x N) = A (128 x K) B (N x K)^T with
@@ -605,7 +1066,8 @@ PIV_EXPORT int pivb_dft_xcorr_dev(const float *d_A, const float *d_B, long long 
                                   size_t scratch_bytes, int *d_status, void *stream)
 {
     using namespace piv;
-    if (win_h != 32 || win_w != 32) return PIV_ERROR_NOPLAN;
+    const int nw = win_h;
+    if (win_h != win_w || (nw != 32 && nw != 64)) return PIV_ERROR_NOPLAN;
     if (ensemble || n_peaks != 1 || peak_finder < 3 || peak_finder > 6 || n_images < 0 || !d_status)
         return PIV_ERROR_OUT_OF_BOUNDS;
     const long long total = (long long)n_images * n_win_y * n_win_x;
@@ -614,7 +1076,7 @@ PIV_EXPORT int pivb_dft_xcorr_dev(const float *d_A, const float *d_B, long long 
     if (lm && (d_scratch == nullptr || scratch_bytes < (size_t)total * sizeof(LmRecord))) return PIV_ERROR_NOMEM;
     // with record scratch the 3-point fits also run in the thread-per-window record kernel
     const bool defer = lm || (d_scratch != nullptr && scratch_bytes >= (size_t)total * sizeof(LmRecord));
-    const uint4 *consts = dft32::consts_for_current_device();
+    const uint4 *consts = nw == 32 ? dft32::consts_for_current_device() : dft64::consts_for_current_device();
     if (!consts) return PIV_ERROR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
     XcorrParams p{};
@@ -631,14 +1093,20 @@ PIV_EXPORT int pivb_dft_xcorr_dev(const float *d_A, const float *d_B, long long 
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const long long groups = (total + dft32::G - 1) / dft32::G;
-    const int grid = (int)(groups < 2LL * sms ? groups : 2LL * sms);
-    dft32::kernel<<<grid, dft32::THREADS, dft32::SMEM_BYTES, s>>>(p, consts, d_status);
+    if (nw == 32) {
+        const long long groups = (total + dft32::G - 1) / dft32::G;
+        const int grid = (int)(groups < 2LL * sms ? groups : 2LL * sms);
+        dft32::kernel<<<grid, dft32::THREADS, dft32::SMEM_BYTES, s>>>(p, consts, d_status);
+    } else {
+        const long long groups = (total + dft64::G - 1) / dft64::G;
+        const int grid = (int)(groups < (long long)sms ? groups : (long long)sms);
+        dft64::kernel<<<grid, dft64::THREADS, dft64::SMEM_BYTES, s>>>(p, consts, d_status);
+    }
     if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
     if (defer) {
         const unsigned blocks = (unsigned)((total + 127) / 128);
-        if (peakfit_impl) lm_records_kernel<1><<<blocks, 128, 0, s>>>(p, 32);
-        else lm_records_kernel<0><<<blocks, 128, 0, s>>>(p, 32);
+        if (peakfit_impl) lm_records_kernel<1><<<blocks, 128, 0, s>>>(p, nw);
+        else lm_records_kernel<0><<<blocks, 128, 0, s>>>(p, nw);
         if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
     }
     return PIV_ERROR_NONE;

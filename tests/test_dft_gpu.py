@@ -1,5 +1,5 @@
-"""DFT-as-GEMM correlation on the tensor core (libpivb_dft, 32 x 32 windows)
-against the FP64 oracle and the FP32 FFT path, through the C-ABI.
+"""DFT-as-GEMM correlation on the tensor core (libpivb_dft, 32 x 32 and 64 x 64
+windows) against the FP64 oracle and the FP32 FFT path, through the C-ABI.
 
 Split-precision BF16 hi + lo operands with three products keep ~16 significant
 bits per GEMM operand, so the bars are those of the tensor-core variant:
@@ -16,11 +16,11 @@ import pytest
 from pivtools_b200 import _lib, geometry, synthetic
 
 pytestmark = pytest.mark.gpu
-N = 32
+SIZES = (32, 64)
 KEYS = ("pk_x", "pk_y", "pk_h", "sx", "sy", "sxy", "ratio")
 
 
-def _case(torch, dev, seed, shape=(256, 288), overlap=50, flow="uniform_grf"):
+def _case(torch, dev, seed, N, shape=(256, 288), overlap=50, flow="uniform_grf"):
     A, B, _ = synthetic.particle_pair(shape, seed=seed, flow=flow)
     g = geometry.compute_window_centers(A.shape, (N, N), overlap)
     w = geometry.window_weight((N, N), "gaussian")
@@ -28,6 +28,7 @@ def _case(torch, dev, seed, shape=(256, 288), overlap=50, flow="uniform_grf"):
 
 
 def _run(L, torch, dev, A, B, g, w, finder, dft, planes=True, impl=0):
+    N = w.shape[0]
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     tA, tB = torch.tensor(A[None], device=dev), torch.tensor(B[None], device=dev)
     tw = torch.tensor(w, device=dev)
@@ -59,11 +60,12 @@ def _run(L, torch, dev, A, B, g, w, finder, dft, planes=True, impl=0):
     return res
 
 
-def test_dft_planes_and_gauss3_against_oracle(oracle, cuda):
+@pytest.mark.parametrize("N", SIZES)
+def test_dft_planes_and_gauss3_against_oracle(oracle, cuda, N):
     import torch
 
     L = _lib.dft_lib()
-    A, B, g, w = _case(torch, cuda, 301)
+    A, B, g, w = _case(torch, cuda, 301, N, shape=(256, 288) if N == 32 else (384, 416))
     got = _run(L, torch, cuda, A, B, g, w, 3, dft=True)
     orc = oracle.bulkxcorr2d(A, B, np.zeros((g.n_win_y, g.n_win_x), np.float32), g.win_ctrs_x, g.win_ctrs_y, (N, N),
                              w, w, peak_finder=3, want_planes=True, want_f64=True)
@@ -82,12 +84,13 @@ def test_dft_planes_and_gauss3_against_oracle(oracle, cuda):
     np.testing.assert_allclose(got["pk_h"][both], orc["pk_h"].ravel()[both], rtol=2e-3)
 
 
+@pytest.mark.parametrize("N", SIZES)
 @pytest.mark.parametrize("finder", [4, 6])
-def test_dft_lm_fits_track_fft_path(cuda, finder):
+def test_dft_lm_fits_track_fft_path(cuda, finder, N):
     import torch
 
     L = _lib.dft_lib()
-    A, B, g, w = _case(torch, cuda, 310 + finder, shape=(320, 320), overlap=75)
+    A, B, g, w = _case(torch, cuda, 310 + finder, N, shape=(320, 320) if N == 32 else (448, 448), overlap=75)
     got = _run(L, torch, cuda, A, B, g, w, finder, dft=True, planes=False)
     ref = _run(L, torch, cuda, A, B, g, w, finder, dft=False, planes=False)
     both = np.isfinite(got["pk_x"]) & np.isfinite(ref["pk_x"])
@@ -96,18 +99,21 @@ def test_dft_lm_fits_track_fft_path(cuda, finder):
     assert np.sqrt(np.mean(d ** 2)) <= 0.02 and np.percentile(d, 99) <= 0.05
 
 
-def test_dft_batch_of_frames_and_ragged_groups(cuda):
+@pytest.mark.parametrize("N", SIZES)
+def test_dft_batch_of_frames_and_ragged_groups(cuda, N):
     """Several frames per call, a window count that is not a multiple of the
-    eight-window group, a masked window and an out-of-bounds centre."""
+    window group (eight windows at 32 px, four at 64 px), a masked window and an
+    out-of-bounds centre."""
     import torch
 
     L = _lib.dft_lib()
     Lx = _lib.bulkxcorr2d_lib()
-    frames = [synthetic.particle_pair((160, 176), seed=330 + k)[:2] for k in range(3)]
+    shape = (160, 176) if N == 32 else (320, 352)
+    frames = [synthetic.particle_pair(shape, seed=330 + k)[:2] for k in range(3)]
     A = np.stack([f[0] for f in frames]); B = np.stack([f[1] for f in frames])
     g = geometry.compute_window_centers(A.shape[1:], (N, N), 50)
     cxs = np.array(g.win_ctrs_x, np.float32)
-    cxs[-1] = 175.0            # pushes the last column of windows out of the frame
+    cxs[-1] = shape[1] - 1.0   # pushes the last column of windows out of the frame
     w = geometry.window_weight((N, N), "gaussian")
     mask = np.zeros((g.n_win_y, g.n_win_x), np.float32)
     mask[1, 2] = 1.0
@@ -119,7 +125,7 @@ def test_dft_batch_of_frames_and_ragged_groups(cuda):
     assert Lx.pivb_correl_weight_dev(tw.data_ptr(), N, N, cw.data_ptr(), s) == 0
     cx, cy, tm = torch.tensor(cxs, device=dev), torch.tensor(g.win_ctrs_y, device=dev), torch.tensor(mask, device=dev)
     total = 3 * g.n_win_y * g.n_win_x
-    assert total % 8 != 0
+    assert total % (8 if N == 32 else 4) != 0
     res = []
     for fn in ("dft", "fft"):
         out = {k: torch.full((3, 1, g.n_win_y, g.n_win_x), -7.0, device=dev) for k in KEYS}
@@ -144,8 +150,10 @@ def test_dft_batch_of_frames_and_ragged_groups(cuda):
 
 def test_dft_rejects_unsupported(cuda):
     L = _lib.dft_lib()
-    args = [1, 1, 0, None, 64, 64, 1, 1, 1, 1, 1, 1, 1, 1, 64, 64, 0, 1, 3, 0] + [1] * 7 + [None, None, 0, 1, None]
-    assert L.pivb_dft_xcorr_dev(*args) == 8          # 64 x 64 not on this path
+    args = [1, 1, 0, None, 64, 64, 1, 1, 1, 1, 1, 1, 1, 1, 48, 48, 0, 1, 3, 0] + [1] * 7 + [None, None, 0, 1, None]
+    assert L.pivb_dft_xcorr_dev(*args) == 8          # 48 x 48 not on this path
+    args[14], args[15] = 32, 64
+    assert L.pivb_dft_xcorr_dev(*args) == 8          # nor rectangular windows
     args[14] = args[15] = 32
     args[17] = 2
     assert L.pivb_dft_xcorr_dev(*args) == 9          # n_peaks > 1
