@@ -608,6 +608,29 @@ struct WinInfo {
     int flags;     // 1 valid, 2 in range
 };
 
+// Pull the rows of the next group's windows into L2 while this group is on the
+// tensor core: thread t takes row t % 64 of image (t / 64) % 2 of window t / 128
+// (its 256 bytes span two or three 128-byte lines).  Windows the gather skips
+// (out of range, masked, outside the frame) are not touched.
+__device__ __forceinline__ void prefetch_group(const XcorrParams &prm, long long grp, long long nwt, int t)
+{
+    const long long idx = grp * G + (t >> 7);
+    if (idx >= prm.total) return;
+    const int n = (int)(idx / nwt);
+    const int iw = (int)(idx - (long long)n * nwt);
+    const int ii = iw % prm.nwx, jj = iw / prm.nwx;
+    if (prm.mask && prm.mask[iw] == 1.0f) return;
+    const int r0 = (int)floor((double)prm.ctr_y[jj] - ((double)N - 1.0) / 2.0 + 0.5);
+    const int c0 = (int)floor((double)prm.ctr_x[ii] - ((double)N - 1.0) / 2.0 + 0.5);
+    if (r0 < 0 || c0 < 0 || r0 + N > prm.H || c0 + N > prm.W) return;
+    const float *img = ((t >> 6) & 1) ? prm.B : prm.A;
+    const char *row = reinterpret_cast<const char *>(img + (long long)n * prm.img_stride +
+                                                     (long long)(r0 + (t & 63)) * prm.W + c0);
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(row));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 128));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 4 * N - 4));
+}
+
 // One candidate strip per thread of the window's 128 (rows and columns [16, 48)
 // of the shifted plane, strips of 8 rows; the rolled 3x3 test of search_plane),
 // then the warp's reduction; the caller merges the window's four warps.
@@ -657,6 +680,9 @@ __global__ void __launch_bounds__(THREADS, 1) kernel(XcorrParams prm, const uint
     uint32_t *slot = reinterpret_cast<uint32_t *>(bar + 1);
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int wg = warp >> 2, wq = warp & 3;
+    const long long nwt = (long long)prm.nwy * prm.nwx;
+    const long long ngroups = (prm.total + G - 1) / G;
+    if (blockIdx.x < ngroups) prefetch_group(prm, blockIdx.x, nwt, t);
     for (int i = t; i < (int)(CONST_BYTES / 16); i += THREADS) reinterpret_cast<uint4 *>(cst)[i] = consts[i];
     if (t == 0) umma::mbar_init(bar, 1);
     if (warp == 0) umma::tmem_alloc(slot, TMEM_COLS);
@@ -667,8 +693,6 @@ __global__ void __launch_bounds__(THREADS, 1) kernel(XcorrParams prm, const uint
     const uint32_t bar_a = umma::smem_u32(bar);
     uint32_t phase = 0;
     bool ok = true;
-    const long long nwt = (long long)prm.nwy * prm.nwx;
-    const long long ngroups = (prm.total + G - 1) / G;
     const float inv_numel = 1.0f / (float)(N * N);
 
     // Wait for the stage's MMAs; every thread learns whether any wait ran out.
@@ -776,6 +800,7 @@ __global__ void __launch_bounds__(THREADS, 1) kernel(XcorrParams prm, const uint
                 }
             umma::commit(bar_a);
         }
+        if (grp + gridDim.x < ngroups) prefetch_group(prm, grp + gridDim.x, nwt, t);
         if (!(ok = wait_stage())) break;
         // ---- Y -> A2 (MN-major, 32 KB hi + 32 KB lo per image, in that image's buffer).
         //      Row (window, kx) = window * 32 + kx; K: Re at y, Im at 64 + y.  Warp
