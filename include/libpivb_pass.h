@@ -90,6 +90,24 @@ int pivb_decode_frames_dev(const unsigned char *raw, long long stride, int n_fra
                            int height, int format, const unsigned char *dark, long long dark_stride, int dark_frames,
                            int rot, float *out, long long out_stride, void *stream);
 
+/* Bytes of one LaVision pixel payload of npix pixels in `encoding` (below), or -1
+ * for an unknown encoding or a pixel count the packing cannot hold. */
+long long pivb_payload_bytes(long long npix, int encoding);
+
+/* Unpack n_frames LaVision pixel payloads (device memory, payload_stride bytes
+ * apart) into float32 frames of npix pixels (out_stride floats apart), applying
+ * the intensity scale in float32 as the reference's readers do (v * slope if
+ * use_slope, then + offset if use_offset; im7_reader.py:1148-1152,
+ * set_reader.py:2003-2008).  encoding: 0 raw-16-bit and the .im7 WORD buffer
+ * (little-endian uint16), 1 raw-8-bit (widened, not rescaled), 2 mono-12p,
+ * 3 mono-12pmsb, 4 mono-12packed, 5 mono-10p, 6 mono-10pmsb (the .set decoders of
+ * set_reader.py:1196-1447), 7 the .im7 FLOAT buffer (little-endian float32).
+ * Replaces the host decode of set_reader.py:1516-1549 and the float conversion of
+ * im7_reader.py:1044-1053.  Returns 0, or 1 for bad arguments. */
+int pivb_unpack_pixels_dev(const unsigned char *payload, long long payload_stride, int n_frames, long long npix,
+                           int encoding, int use_slope, float slope, int use_offset, float offset, float *out,
+                           long long out_stride, void *stream);
+
 /* Coloured-floor regressor for the k-space fit (kspace_floor_psd.py:241-275 and
  * single_pass_accumulator.py:836-880): P_win (n_win, hw) FP64 from the fraction
  * grid P_grid (n_fracs, n_fracs, hw) FP64 indexed [fy][fx], fs (n_fracs) the

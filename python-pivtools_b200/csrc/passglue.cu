@@ -637,6 +637,109 @@ PIV_EXPORT int pivb_u16_to_f32_dev(const unsigned short *in, float *out, long lo
 }
 
 // ---------------------------------------------------------------------------
+// LaVision pixel payloads -> float32 frames
+// ---------------------------------------------------------------------------
+namespace {
+
+// Pixel p of one payload in encoding enc (the .set decoders of
+// pivtools_core/image_handling/readers/set_reader.py:1196-1447 and the .im7
+// WORD/FLOAT buffers of im7_reader.py:216-226), as raw sensor counts.
+__device__ __forceinline__ float payload_pixel(const unsigned char *__restrict__ f, long long p, int enc)
+{
+    switch (enc) {
+    case 0: {                                            // raw-16-bit / .im7 WORD: little-endian uint16
+        const unsigned char *b = f + 2 * p;
+        return (float)((unsigned)b[0] | ((unsigned)b[1] << 8));
+    }
+    case 1: return (float)f[p];                          // raw-8-bit: widened, not rescaled
+    case 2: case 3: case 4: {                            // 2 pixels in 3 bytes
+        const unsigned char *b = f + 3 * (p >> 1);
+        const unsigned b0 = b[0], b1 = b[1], b2 = b[2];
+        unsigned v;
+        if (enc == 2) v = (p & 1) ? ((b1 >> 4) | (b2 << 4)) : (b0 | ((b1 & 0x0Fu) << 8));          // mono-12p
+        else if (enc == 3) v = (p & 1) ? (((b1 & 0x0Fu) << 8) | b2) : ((b0 << 4) | (b1 >> 4));    // mono-12pmsb
+        else v = (p & 1) ? ((b2 << 4) | (b1 >> 4)) : ((b0 << 4) | (b1 & 0x0Fu));                  // mono-12packed
+        return (float)v;
+    }
+    case 5: case 6: {                                    // 4 pixels in 5 bytes
+        const unsigned char *b = f + 5 * (p >> 2);
+        const int j = (int)(p & 3);
+        const unsigned c0 = b[j], c1 = b[j + 1];
+        unsigned v;
+        if (enc == 5) {                                  // mono-10p: little-endian bit stream
+            const unsigned w = c0 | (c1 << 8);
+            v = (w >> (2 * j)) & 0x3FFu;
+        } else {                                         // mono-10pmsb: big-endian bit stream
+            const unsigned w = (c0 << 8) | c1;
+            v = (w >> (6 - 2 * j)) & 0x3FFu;
+        }
+        return (float)v;
+    }
+    default: {                                           // .im7 FLOAT: little-endian float32
+        float v;
+        memcpy(&v, f + 4 * p, 4);
+        return v;
+    }
+    }
+}
+
+__global__ void unpack_pixels_kernel(const unsigned char *__restrict__ payload, long long payload_stride, int n_frames,
+                                     long long npix, int enc, int use_slope, float slope, int use_offset, float offset,
+                                     float *__restrict__ out, long long out_stride)
+{
+    const long long total = npix * n_frames;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(i / npix);
+        const long long p = i - (long long)k * npix;
+        float v = payload_pixel(payload + (long long)k * payload_stride, p, enc);
+        if (use_slope) v = __fmul_rn(v, slope);
+        if (use_offset) v = __fadd_rn(v, offset);
+        out[(long long)k * out_stride + p] = v;
+    }
+}
+
+}  // namespace
+
+// Bytes of one payload of npix pixels in encoding enc, or -1 for an unknown
+// encoding or a pixel count the packing cannot hold.
+PIV_EXPORT long long pivb_payload_bytes(long long npix, int enc)
+{
+    if (npix <= 0) return -1;
+    switch (enc) {
+    case 0: return 2 * npix;
+    case 1: return npix;
+    case 2: case 3: case 4: return (npix & 1) ? -1 : npix / 2 * 3;
+    case 5: case 6: return (npix & 3) ? -1 : npix / 4 * 5;
+    case 7: return 4 * npix;
+    default: return -1;
+    }
+}
+
+// Unpack n_frames LaVision pixel payloads (encoding: 0 raw-16-bit or .im7 WORD,
+// 1 raw-8-bit, 2 mono-12p, 3 mono-12pmsb, 4 mono-12packed, 5 mono-10p,
+// 6 mono-10pmsb, 7 .im7 FLOAT) into float32 frames of npix pixels, applying the
+// intensity scale as the readers do in float32 (v * slope if use_slope, then
+// + offset if use_offset; im7_reader.py:1148-1152).  payload_stride: bytes between
+// payloads; out_stride: elements between output frames.  Returns 0, or 1 for bad
+// arguments.
+PIV_EXPORT int pivb_unpack_pixels_dev(const unsigned char *payload, long long payload_stride, int n_frames,
+                                      long long npix, int encoding, int use_slope, float slope, int use_offset,
+                                      float offset, float *out, long long out_stride, void *stream)
+{
+    if (!payload || !out || n_frames <= 0) return 1;
+    const long long bytes = pivb_payload_bytes(npix, encoding);
+    if (bytes < 0 || payload_stride < bytes || out_stride < npix) return 1;
+    const long long total = npix * n_frames;
+    const long long want = (total + 255) / 256;
+    const unsigned grid = (unsigned)(want < 148 * 32 ? want : 148 * 32);
+    unpack_pixels_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(payload, payload_stride, n_frames, npix, encoding,
+                                                                  use_slope, slope, use_offset, offset, out,
+                                                                  out_stride);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// ---------------------------------------------------------------------------
 // Ensemble pass: frame sums and the finalise of the accumulated planes
 // (pivtools_cli/piv/piv_backend/single_pass_accumulator.py:292-320, 508-800)
 // ---------------------------------------------------------------------------

@@ -215,6 +215,28 @@ def pass_lib() -> ctypes.CDLL:
     L.pivb_ensemble_finalize_dev.restype = ci
     L.pivb_decode_frames_dev.argtypes = [vp, cll, ci, ci, ci, ci, ci, vp, cll, ci, ci, vp, cll, vp]
     L.pivb_decode_frames_dev.restype = ci
+    L.pivb_payload_bytes.argtypes = [cll, ci]
+    L.pivb_payload_bytes.restype = cll
+    L.pivb_unpack_pixels_dev.argtypes = [vp, cll, ci, cll, ci, ci, fl, ci, fl, vp, cll, vp]
+    L.pivb_unpack_pixels_dev.restype = ci
+    L._pivb_bound = True
+    return L
+
+
+def lavision_lib() -> ctypes.CDLL:
+    """Host codecs of the LaVision containers (libpivb_lavision.so)."""
+    L = _load("libpivb_lavision.so")
+    if getattr(L, "_pivb_bound", False):
+        return L
+    llp = ctypes.POINTER(ctypes.c_longlong)
+    L.pivb_davis_tokens_decode.argtypes = [vp, cll, llp, llp, vp, cll, llp]
+    L.pivb_davis_tokens_decode.restype = ci
+    L.pivb_lz4_block_decode.argtypes = [vp, cll, vp, cll]
+    L.pivb_lz4_block_decode.restype = ci
+    L.pivb_zlib_inflate_exact.argtypes = [vp, cll, vp, cll]
+    L.pivb_zlib_inflate_exact.restype = ci
+    L.pivb_zlib_inflate_prefix.argtypes = [vp, cll, vp, cll]
+    L.pivb_zlib_inflate_prefix.restype = cll
     L._pivb_bound = True
     return L
 

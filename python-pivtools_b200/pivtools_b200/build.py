@@ -2,7 +2,8 @@
 
 Each reference library name gets its own shared object with the same exported
 C symbols: libbulkxcorr2d.so, libfusedwarp.so, libkspacefit.so.  nvcc
-cross-compiles on a machine without a GPU.
+cross-compiles on a machine without a GPU; the host-only LaVision codec library
+(libpivb_lavision.so) is built with the system C++ compiler.
 """
 
 from __future__ import annotations
@@ -30,7 +31,12 @@ TARGETS = {
     "libkspacefit.so": "kspacefit.cu",
     "libpivb_pass.so": "passglue.cu",
     "libpivb_dft.so": "dftcorr.cu",
+    "libpivb_lavision.so": "lavision_codecs.cpp",
 }
+
+# host-only translation units: the system C++ compiler, zlib
+HOST_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-shared"]
+HOST_LIBS = ["-lz"]
 
 
 def _nvcc() -> str:
@@ -68,7 +74,10 @@ def build(force: bool = False, verbose: bool = False, only: list[str] | None = N
 
     def one(job):
         src, out = job
-        cmd = [_nvcc(), *NVCC_FLAGS, "-o", out + ".tmp", src]
+        if src.endswith(".cpp"):
+            cmd = [os.environ.get("CXX_HOST", "g++"), *HOST_FLAGS, "-o", out + ".tmp", src, *HOST_LIBS]
+        else:
+            cmd = [_nvcc(), *NVCC_FLAGS, "-o", out + ".tmp", src]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

@@ -16,6 +16,7 @@ Python package).  The fixtures are committed; tests never need the reference.
     python tests/golden/make_golden.py vmask      # vmask_ref.npz
     python tests/golden/make_golden.py infill     # infill_ref.npz
     python tests/golden/make_golden.py xcorr      # xcorr_ref.npz, triple_ref.npz
+    python tests/golden/make_golden.py lavision   # lavision_ref.npz
 
 The reference checkout is named by $PIVTOOLS_REF (its libraries are built from it
 by `make -C oracle ref PIVTOOLS_REF=...`).
@@ -678,6 +679,133 @@ def make_xcorr():
     print("triple_ref.npz written:", len(tnames), "cases")
 
 
+def _load_reference_module(name):
+    """One module of the reference's readers package (the package stubs of
+    _load_reference_readers already in place), the LZ4 binding standing in for
+    python-lz4 where that is absent."""
+    import importlib.util
+
+    import lavision_oracle as LO
+
+    LO.install_lz4_stub()
+    _load_reference_readers()
+    R = os.path.join(REF_ROOT, "pivtools_core/image_handling/readers")
+    full = "pivtools_core.image_handling.readers." + name
+    if full in sys.modules and getattr(sys.modules[full], "__file__", None):
+        return sys.modules[full]
+    spec = importlib.util.spec_from_file_location(full, os.path.join(R, name + ".py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[full] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _frames_u16(rng, F, H, W):
+    """Camera-like uint16 frames: a smooth background, particles and noise, so the
+    token coder meets small deltas (nibble runs, int8) and large jumps alike."""
+    yy, xx = np.mgrid[0:H, 0:W]
+    out = np.empty((F, 1, H, W), np.uint16)
+    for k in range(F):
+        img = 500 + 40 * np.sin(xx / 7.0 + k) + 30 * np.cos(yy / 5.0)
+        img += rng.integers(0, 4, (H, W))
+        for _ in range(max(1, H * W // 40)):
+            y, x = rng.integers(0, H), rng.integers(0, W)
+            img[y, x] += rng.integers(200, 4000)
+        out[k, 0] = np.clip(img, 0, 65535).astype(np.uint16)
+    return out
+
+
+def make_lavision():
+    """Fixtures of the LaVision decode: .im7 files of every pack type (written by
+    oracle/lavision_oracle.py) with the reference reader's read_im7 and
+    read_im7_camera results; the reference's own lvpyio fixtures (pack 1 and
+    version-1 pack 20, decoded by LaVision's lvpyio 1.3.1); .set entry payloads
+    under every codec and decoder with the reference's _decompress_entry and
+    _decode_pixels results."""
+    import json
+    import tempfile
+    import types
+    import zlib
+
+    import lavision_oracle as LO
+
+    im7 = _load_reference_module("im7_reader")
+    st = _load_reference_module("set_reader")
+    rng = np.random.default_rng(2024)
+    out, meta = {}, {"im7": [], "lvpyio": [], "set": []}
+
+    def attrs(slope, offset):
+        return LO.im7_attributes(slope, offset)
+
+    cases = []
+    fr = _frames_u16(rng, 3, 20, 24)
+    cases.append(("p0_word", LO.im7_pack0(fr, attrs(2.5, 100.0)), [(2, 1, None), (1, 2, 1)]))
+    ff = rng.normal(0, 50, (2, 1, 12, 16)).astype(np.float32)
+    cases.append(("p0_float", LO.im7_pack0(ff, attrs(None, None)), [(1, 2, None)]))
+    fr1 = _frames_u16(rng, 3, 18, 22)
+    cases.append(("p1_tokens", LO.im7_pack1(fr1, attrs(0.5, None), rng), [(2, 1, None), (1, 2, None), (3, 1, None)]))
+    fr1b = _frames_u16(rng, 1, 40, 33)
+    cases.append(("p1_single", LO.im7_pack1(fr1b, attrs(None, None), rng), [(1, 2, None)]))
+    fr2 = _frames_u16(rng, 2, 16, 20)
+    cases.append(("p2_rows", LO.im7_pack2(fr2, attrs(1.0, -3.0), per_row=True), [(2, 1, None), (1, 2, None)]))
+    fr2b = _frames_u16(rng, 1, 16, 20)
+    cases.append(("p2_frame", LO.im7_pack2(fr2b, attrs(None, None), per_row=False), [(1, 1, None)]))
+    fr20 = _frames_u16(rng, 2, 32, 48)
+    cases.append(("p20_v0", LO.im7_pack20_v0(fr20, attrs(3.0, 1.5)), [(1, 2, None), (2, 1, None)]))
+    fr20b = _frames_u16(rng, 4, 24, 40)
+    cases.append(("p20_v1", LO.im7_pack20_v1(fr20b, attrs(None, None)), [(1, 2, None), (2, 2, 1)]))
+    with tempfile.TemporaryDirectory() as td:
+        for name, blob, cams in cases:
+            path = os.path.join(td, name + ".im7")
+            with open(path, "wb") as f:
+                f.write(blob)
+            _, px, sc = im7.read_im7(path)
+            out[name + "_file"] = np.frombuffer(blob, np.uint8)
+            out[name + "_pixels"] = px
+            entry = {"name": name, "slope": sc.slope, "offset": sc.offset, "cams": []}
+            for i, (cam, fpc, nfr) in enumerate(cams):
+                r = im7.read_im7_camera(path, camera_no=cam, frames_per_camera=fpc, frames=nfr)
+                out[f"{name}_cam{i}"] = r
+                entry["cams"].append([cam, fpc, nfr])
+            meta["im7"].append(entry)
+    fx = os.path.join(REF_ROOT, "unit-tests", "fixtures")
+    for sub, name in (("im7_pack1", "carry_3frames"), ("im7_pack1", "high_nibble_8"),
+                      ("im7_v1_pack20", "three_frames")):
+        path = os.path.join(fx, sub, name + ".im7")
+        with open(path, "rb") as f:
+            out[f"lv_{name}_file"] = np.frombuffer(f.read(), np.uint8)
+        out[f"lv_{name}_lvpyio"] = np.load(os.path.join(fx, sub, name + ".lvpyio.npy"))
+        _, px, _ = im7.read_im7(path)
+        out[f"lv_{name}_ref"] = px
+        meta["lvpyio"].append(name)
+    W, H = 16, 12
+    for dec in ("raw-16-bit", "raw-8-bit", "mono-12p", "mono-12pmsb", "mono-12packed", "mono-10p", "mono-10pmsb"):
+        nbytes = st._payload_bytes(dec, W, H)
+        payload = rng.integers(0, 256, nbytes).astype(np.uint8).tobytes()
+        out[f"set_{dec}_pixels"] = st._decode_pixels(payload, dec, W, H)
+        out[f"set_{dec}_payload"] = np.frombuffer(payload, np.uint8)
+        for codec in ("", "Zlib", "LZ4", "IMX"):
+            if codec == "Zlib":
+                stored = zlib.compress(payload)
+            elif codec == "LZ4":
+                stored = LO.lz4_encode(payload)
+            elif codec == "IMX":
+                stored, _ = LO.tokens_encode(np.frombuffer(payload, "<u2"), 0, rng)
+            else:
+                stored = payload
+            fi = types.SimpleNamespace(codec=codec, frame_idx=0,
+                                       data_path=type("P", (), {"name": "x-1.ims",
+                                                                "parent": type("Q", (), {"name": "rec"})()})())
+            got = st._decompress_entry(stored, fi, 0, nbytes)
+            got = bytes(got) if not isinstance(got, np.ndarray) else got.tobytes()
+            assert got == payload, (dec, codec)
+            out[f"set_{dec}_{codec or 'none'}_stored"] = np.frombuffer(stored, np.uint8)
+        meta["set"].append({"decoder": dec, "width": W, "height": H})
+    out["meta"] = np.array(json.dumps(meta))
+    np.savez_compressed(os.path.join(HERE, "lavision_ref.npz"), **out)
+    print("lavision_ref.npz written")
+
+
 if __name__ == "__main__":
     what = sys.argv[1:] or ["peakfit", "warp"]
     if "xcorr" in what:
@@ -704,3 +832,5 @@ if __name__ == "__main__":
         make_vmask()
     if "infill" in what:
         make_infill()
+    if "lavision" in what:
+        make_lavision()

@@ -18,6 +18,7 @@ HEADER_LIB = {
     "libkspacefit.h": "libkspacefit.so",
     "libpivb_pass.h": "libpivb_pass.so",
     "libpivb_dft.h": "libpivb_dft.so",
+    "libpivb_lavision.h": "libpivb_lavision.so",
 }
 
 
