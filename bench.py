@@ -410,7 +410,7 @@ def run_b200(args):
     Bh = B.cpu().to(torch.int32).to(torch.uint16).pin_memory()
     if not (Ah.is_pinned() and Bh.is_pinned() and ux_h.is_pinned() and uy_h.is_pinned()):
         raise RuntimeError("host frames are not page-locked")
-    e2e_steps = max(2, min(args.steps, 5))
+    e2e_steps = max(2, args.steps)
     with torch.cuda.stream(stream):
         pipe.run(Ah, Bh, ux_h, uy_h)          # warm-up
     torch.cuda.synchronize()
