@@ -90,6 +90,24 @@ int pivb_decode_frames_dev(const unsigned char *raw, long long stride, int n_fra
                            int height, int format, const unsigned char *dark, long long dark_stride, int dark_frames,
                            int rot, float *out, long long out_stride, void *stream);
 
+/* Validation of one pass whose correlation returned n_peaks >= 1 peaks per
+ * window (pk_* in the correlator's layout (N, n_peaks, ny, nx)), with the
+ * reference's secondary-peak substitution when `secondary` is set
+ * (cpu_instantaneous.py:676-760, config secondary_peak): the primary peak is
+ * gated, predicted and tested as by pivb_validate_dev; then n_peaks - 1 rounds in
+ * which every invalid vector with peaks left takes its next peak, is judged
+ * afresh (NaN: reason 13) and is tested by the peak-magnitude and normalised-
+ * median tests on the field of the current choices (reason 12 if it fails); at
+ * the end a NaN height of the chosen peak invalidates (13).  Outputs as
+ * pivb_validate_dev plus choice (N, ny, nx) uint8: the 1-based peak each valid
+ * vector took, 0 for invalid and masked vectors.  work: 4*N*ny*nx floats.
+ * Returns 0, or 1 for bad arguments. */
+int pivb_validate_peaks_dev(const float *pk_x, const float *pk_y, const float *pk_h, int n_peaks, int secondary,
+                            const float *pred_dy, const float *pred_dx, const float *mask, int N, int ny, int nx,
+                            float thresh_x, float thresh_y, float peak_thr, float med_eps, float med_thr,
+                            int med_size, float *ux, float *uy, unsigned char *invalid, signed char *nan_reason,
+                            unsigned char *choice, float *work, void *stream);
+
 /* Bytes of one LaVision pixel payload of npix pixels in `encoding` (below), or -1
  * for an unknown encoding or a pixel count the packing cannot hold. */
 long long pivb_payload_bytes(long long npix, int encoding);

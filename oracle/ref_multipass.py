@@ -187,6 +187,75 @@ def validate(pk_x, pk_y, pk_h, pred_dy, pred_dx, thresh_x, thresh_y, peak_thr=0.
     return np.where(bad, np.float32(np.nan), zx), np.where(bad, np.float32(np.nan), zy), bad
 
 
+def validate_peaks(pk_x, pk_y, pk_h, pred_dy, pred_dx, thresh_x, thresh_y, secondary=True, peak_thr=0.25,
+                   eps=0.1, med_thr=2.0, size=5):
+    """(N, P, ny, nx) peak outputs -> (ux, uy, invalid, reason, choice): the driver's
+    validation with several peaks and the secondary-peak substitution
+    (cpu_instantaneous.py:589-760; no masked windows), in its order of steps: gate
+    and predictor on every peak, primary outlier tests on the zero-filled field,
+    then per round the next peak for every invalid vector with peaks left, judged
+    afresh and tested on the field of the current choices (NaN cells drop out of
+    the medians), then the NaN-height and unclassified codes."""
+    x = pk_x.astype(np.float32).copy()
+    y = pk_y.astype(np.float32).copy()
+    h = pk_h.astype(np.float32).copy()
+    N, P, ny, nx = x.shape
+    with np.errstate(invalid="ignore"):
+        large = (np.abs(x) > thresh_x) | (np.abs(y) > thresh_y)
+    fit_fail0 = np.isnan(x[:, 0]) | np.isnan(y[:, 0])
+    large0 = large[:, 0]
+    x[large] = np.nan
+    y[large] = np.nan
+    h[large] = np.nan
+    if pred_dx is not None:
+        x += pred_dx[:, None]
+        y += pred_dy[:, None]
+    ux = x[:, 0].copy()
+    uy = y[:, 0].copy()
+    nan_mask = np.isnan(ux) | np.isnan(uy)
+    ux[nan_mask] = 0.0
+    uy[nan_mask] = 0.0
+    choice = np.ones((N, ny, nx), np.intp)
+    reason = np.zeros((N, ny, nx), np.int8)
+    reason[fit_fail0] = 1
+    reason[large0] = 6
+
+    def outliers(fx, fy, pm):
+        with np.errstate(invalid="ignore"):
+            o = (pm < peak_thr) | np.isnan(pm) if peak_thr >= 0 else np.zeros(fx.shape, bool)
+        if med_thr > 0:
+            o = o | median_flags(fx, fy, eps, med_thr, size)
+        return o
+
+    out = outliers(ux, uy, h[:, 0])
+    nan_mask |= out
+    reason[out & (reason == 0)] = 10
+    if secondary:
+        for _ in range(1, P):
+            active = nan_mask & (choice < P)
+            if not active.any():
+                break
+            choice[active] += 1
+            idx = choice[:, None] - 1
+            ux = np.take_along_axis(x, idx, axis=1)[:, 0]
+            uy = np.take_along_axis(y, idx, axis=1)[:, 0]
+            sub_nan = np.isnan(ux) | np.isnan(uy)
+            nan_mask[active] = sub_nan[active]
+            reason[active] = np.where(sub_nan[active], 13, 0)
+            pm = np.take_along_axis(h, idx, axis=1)[:, 0]
+            re = active & outliers(ux, uy, pm) & ~sub_nan
+            nan_mask |= re
+            reason[re] = 12
+    pm = np.take_along_axis(h, choice[:, None] - 1, axis=1)[:, 0]
+    nan_mask |= np.isnan(pm)
+    reason[np.isnan(pm) & (reason == 0)] = 13
+    reason[nan_mask & (reason == 0)] = 9
+    ux = np.where(nan_mask, np.float32(np.nan), ux).astype(np.float32)
+    uy = np.where(nan_mask, np.float32(np.nan), uy).astype(np.float32)
+    choice[nan_mask] = 0
+    return ux, uy, nan_mask, reason, choice
+
+
 # ---------------------------------------------------------------------------
 # The pass loop
 # ---------------------------------------------------------------------------
@@ -200,7 +269,7 @@ class RefMultipass:
     default, config.yaml:60-66) or 'harmonic'."""
 
     def __init__(self, geo, window_type="gaussian", peak_finder=3, infill="biharmonic", final_infill=True,
-                 smoothing=True):
+                 smoothing=True, n_peaks=1, secondary_peak=False):
         self.bulk = O.ref_bulk()
         self.warp = O.ref_warp()
         if self.bulk is None or self.warp is None:
@@ -215,6 +284,8 @@ class RefMultipass:
         self.order = {"harmonic": 1, "biharmonic": 2}[infill]
         self.final_infill = final_infill
         self.smoothing = smoothing
+        self.n_peaks = n_peaks
+        self.secondary = secondary_peak
         self.warp.fused_warp_set_impl(1)        # the SIMD route, the reference's default
 
     def run(self, A, B):
@@ -254,12 +325,16 @@ class RefMultipass:
                     raise RuntimeError("reference fused_symmetric_warp_batch failed")
             mask = np.zeros((ny, nx), np.float32)
             r = O.ref_bulkxcorr2d(fa, fb, mask, g.grid.win_ctrs_x, g.grid.win_ctrs_y, g.window_size, w, w,
-                                  peak_finder=self.finder)
+                                  n_peaks=self.n_peaks, peak_finder=self.finder)
             if r["error"]:
                 raise RuntimeError(f"reference bulkxcorr2d error {r['error']}")
             div = 2.0 if k == 0 else 4.0
-            ux, uy, bad = validate(r["pk_x"][:, 0], r["pk_y"][:, 0], r["pk_h"][:, 0], pdy, pdx,
-                                   g.window_size[1] / div, g.window_size[0] / div)
+            if self.n_peaks > 1:
+                ux, uy, bad, _, _ = validate_peaks(r["pk_x"], r["pk_y"], r["pk_h"], pdy, pdx, g.window_size[1] / div,
+                                                   g.window_size[0] / div, secondary=self.secondary)
+            else:
+                ux, uy, bad = validate(r["pk_x"][:, 0], r["pk_y"][:, 0], r["pk_h"][:, 0], pdy, pdx,
+                                       g.window_size[1] / div, g.window_size[0] / div)
             last = k + 1 == len(self.geo)
             if not last or self.final_infill:
                 pitch = (float(g.grid.win_spacing_y), float(g.grid.win_spacing_x))

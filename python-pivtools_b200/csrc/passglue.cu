@@ -82,12 +82,16 @@ struct ValParams {
     float *ux, *uy;                       // out: displacement, NaN where invalid, 0 at masked
     unsigned char *invalid;               // out: 1 where the vector must be infilled
     signed char *reason;                  // out (nullable): why the vector is invalid (codes below)
+    long long pk_stride;                  // elements between the images' peak arrays (ny*nx for one peak)
+    int hnan_late;                        // 1: a NaN peak height invalidates only at the end of the
+                                          //    secondary-peak stage (not in the primary tests)
 };
 
 // Invalid-vector reason codes (pivtools_cli/piv/piv_backend/nan_reason_codes.py:18-25).
 // The first stage that claims a vector keeps it; masked windows always read -1.
 enum : signed char {
-    kMasked = -1, kValid = 0, kFitFail = 1, kLargeDisp = 6, kUnclassified = 9, kOutlier = 10, kPeakMagNaN = 13
+    kMasked = -1, kValid = 0, kFitFail = 1, kLargeDisp = 6, kUnclassified = 9, kOutlier = 10,
+    kSecondaryOutlier = 12, kPeakMagNaN = 13
 };
 
 // Stage 1: gate + predictor.  ux/uy receive the gated field (NaN where the
@@ -101,15 +105,17 @@ __global__ void gate_kernel(ValParams p, int apply)
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long nv = (long long)p.N * p.ny * p.nx;
     if (i >= nv) return;
-    const int w = (int)(i % ((long long)p.ny * p.nx));
+    const long long plane = (long long)p.ny * p.nx;
+    const int w = (int)(i % plane);
+    const long long src = (i / plane) * p.pk_stride + w;
     const bool masked = p.mask && p.mask[w] != 0.0f;
-    float x = p.pk_x[i], y = p.pk_y[i], h = p.pk_h[i];
+    float x = p.pk_x[src], y = p.pk_y[src], h = p.pk_h[src];
     const bool fit_fail = (x != x) || (y != y);
     const bool large = fabsf(x) > p.thresh_x || fabsf(y) > p.thresh_y;   // false for NaN
     if (masked || large) { x = qnanf(); y = qnanf(); h = qnanf(); }
     if (p.pred_dx) { x += p.pred_dx[i]; y += p.pred_dy[i]; }
     const bool pk_fail = p.peak_thr >= 0.0f && ((h < p.peak_thr) || (h != h));
-    bool bad = (x != x) || (y != y) || pk_fail || (h != h);
+    bool bad = (x != x) || (y != y) || pk_fail || (!p.hnan_late && h != h);
     bad = bad && !masked;
     if (apply && bad) { x = qnanf(); y = qnanf(); }
     p.ux[i] = masked ? 0.0f : x;
@@ -180,7 +186,10 @@ __global__ void median_kernel(ValParams p, const float *gx, const float *gy)
     if (p.reason) {
         signed char rc = p.reason[i];
         if (rc == kValid && outlier) rc = kOutlier;
-        if (rc == kValid && bad) rc = (p.pk_h[i] != p.pk_h[i]) ? kPeakMagNaN : kUnclassified;
+        if (rc == kValid && bad) {
+            const float hr = p.pk_h[(long long)n * p.pk_stride + w];
+            rc = (hr != hr) ? kPeakMagNaN : kUnclassified;
+        }
         p.reason[i] = rc;
     }
 }
@@ -529,7 +538,7 @@ PIV_EXPORT int pivb_validate_dev(const float *pk_x, const float *pk_y, const flo
     if (N <= 0 || ny <= 0 || nx <= 0 || med_size < 3 || med_size > 5 || !(med_size & 1)) return 1;
     cudaStream_t s = (cudaStream_t)stream;
     ValParams p{pk_x, pk_y, pk_h, pred_dy, pred_dx, mask, N, ny, nx, thresh_x, thresh_y, peak_thr, med_eps,
-                med_thr, med_size, ux, uy, invalid, nan_reason};
+                med_thr, med_size, ux, uy, invalid, nan_reason, (long long)ny * nx, 0};
     const long long nv = (long long)N * ny * nx;
     gate_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, med_thr > 0.0f ? 0 : 1);
     if (med_thr > 0.0f) {
@@ -538,6 +547,221 @@ PIV_EXPORT int pivb_validate_dev(const float *pk_x, const float *pk_y, const flo
         cudaMemcpyAsync(gy, uy, nv * 4, cudaMemcpyDeviceToDevice, s);
         median_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, gx, gy);
     }
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// ---------------------------------------------------------------------------
+// Secondary-peak substitution (cpu_instantaneous.py:676-760)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct SecParams {
+    const float *pk_x, *pk_y, *pk_h;      // (N, P, ny, nx): every peak of the correlator
+    int P;
+    const float *pred_dy, *pred_dx;       // (N, ny, nx) or null
+    const float *mask;                    // (ny, nx) or null
+    int N, ny, nx;
+    float thresh_x, thresh_y, peak_thr, med_eps, med_thr;
+    int med_size;
+    float *ux, *uy;                       // out
+    unsigned char *invalid;               // in/out
+    signed char *reason;                  // in/out
+    unsigned char *choice;                // in/out: 1-based peak of each vector (0 = invalid)
+    float *cx, *cy;                       // work: the field of the current choices
+    unsigned char *active;                // work: substituted in this round
+    int substitute;                       // 0: only copy each vector's current choice
+};
+
+// Peak k of vector i after the gate and the predictor (NaN where masked, gated or
+// not found), and its gated height.
+__device__ __forceinline__ void gated_peak(const SecParams &q, long long i, int k, float &x, float &y, float &h)
+{
+    const long long plane = (long long)q.ny * q.nx;
+    const long long n = i / plane, w = i - n * plane;
+    const long long src = (n * q.P + k) * plane + w;
+    x = q.pk_x[src];
+    y = q.pk_y[src];
+    h = q.pk_h[src];
+    const bool masked = q.mask && q.mask[w] != 0.0f;
+    const bool large = fabsf(x) > q.thresh_x || fabsf(y) > q.thresh_y;
+    if (masked || large) { x = qnanf(); y = qnanf(); h = qnanf(); }
+    if (q.pred_dx) { x += q.pred_dx[i]; y += q.pred_dy[i]; }
+}
+
+// One substitution round: every invalid vector with peaks left takes its next
+// peak and is judged afresh (NaN -> still invalid, reason 13; else valid until
+// the outlier tests below); every vector's current choice is written to cx/cy.
+__global__ void subst_kernel(SecParams q)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nv = (long long)q.N * q.ny * q.nx;
+    if (i >= nv) return;
+    const int w = (int)(i % ((long long)q.ny * q.nx));
+    if (q.mask && q.mask[w] != 0.0f) {
+        q.cx[i] = qnanf();
+        q.cy[i] = qnanf();
+        q.active[i] = 0;
+        return;
+    }
+    int c = q.choice[i];
+    const bool act = q.substitute && q.invalid[i] && c < q.P;
+    if (act) q.choice[i] = (unsigned char)(++c);
+    float x, y, h;
+    gated_peak(q, i, c - 1, x, y, h);
+    q.cx[i] = x;
+    q.cy[i] = y;
+    q.active[i] = act ? 1 : 0;
+    if (act) {
+        const bool sub_nan = (x != x) || (y != y);
+        q.invalid[i] = sub_nan ? 1 : 0;
+        q.reason[i] = sub_nan ? kPeakMagNaN : kValid;
+    }
+}
+
+// The outlier tests on the substituted field (outlier_detection.py:382-460 with
+// the masked windows NaN): the peak magnitude of the current choice and the
+// normalised median over cx/cy, whose NaN cells drop out of the medians and are
+// absent from the 3x3 guard (masked cells count as present).  Only vectors
+// substituted in this round and finite are re-flagged (reason 12).
+__global__ void sec_median_kernel(SecParams q)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nv = (long long)q.N * q.ny * q.nx;
+    if (i >= nv || !q.active[i]) return;
+    const int plane = q.ny * q.nx;
+    const int n = (int)(i / plane), w = (int)(i % plane), r = w / q.nx, c = w % q.nx;
+    const float u0 = q.cx[i], v0 = q.cy[i];
+    if (u0 != u0 || v0 != v0) return;
+    float x, y, h;
+    gated_peak(q, i, q.choice[i] - 1, x, y, h);
+    bool outlier = q.peak_thr >= 0.0f && ((h < q.peak_thr) || (h != h));
+    if (q.med_thr > 0.0f) {
+        const float *X = q.cx + (long long)n * plane, *Y = q.cy + (long long)n * plane;
+        const int hs = q.med_size / 2;
+        float nu[24], nvv[24];
+        int present = 0;
+#pragma unroll
+        for (int t = 0; t < 25; ++t) {
+            const int dr = t / 5 - 2, dc = t % 5 - 2;
+            const int rr = r + dr, cc = c + dc;
+            const bool inside = rr >= 0 && rr < q.ny && cc >= 0 && cc < q.nx && abs(dr) <= hs && abs(dc) <= hs;
+            float a = qnanf(), b = qnanf();
+            if (inside) {
+                const bool mk = q.mask && q.mask[rr * q.nx + cc] != 0.0f;
+                if (!mk) {
+                    a = X[rr * q.nx + cc];
+                    b = Y[rr * q.nx + cc];
+                }
+                const bool fin = (a == a) && (b == b);
+                if (abs(dr) <= 1 && abs(dc) <= 1 && (fin || mk)) ++present;
+            }
+            if (t == 12) continue;
+            nu[t < 12 ? t : t - 1] = a;
+            nvv[t < 12 ? t : t - 1] = b;
+        }
+        const float mu = median24(nu), mv = median24(nvv);
+        const float r0 = sqrtf((u0 - mu) * (u0 - mu) + (v0 - mv) * (v0 - mv));
+        float ri[24];
+#pragma unroll
+        for (int j = 0; j < 24; ++j)
+            ri[j] = sqrtf((nu[j] - mu) * (nu[j] - mu) + (nvv[j] - mv) * (nvv[j] - mv));
+        const float rm = median24(ri);
+        const float nr = r0 / (rm + q.med_eps);
+        outlier = outlier || (nr > q.med_thr) || !isfinite(nr) || present < 6;
+    }
+    if (outlier) {
+        q.invalid[i] = 1;
+        q.reason[i] = kSecondaryOutlier;
+    }
+}
+
+// The end of the stage: a NaN peak height of the chosen peak invalidates (13),
+// remaining invalid vectors without a reason are 9, invalid vectors become NaN
+// and lose their choice, masked windows read 0 with reason -1.
+__global__ void sec_final_kernel(SecParams q)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nv = (long long)q.N * q.ny * q.nx;
+    if (i >= nv) return;
+    const int w = (int)(i % ((long long)q.ny * q.nx));
+    if (q.mask && q.mask[w] != 0.0f) {
+        q.ux[i] = 0.0f;
+        q.uy[i] = 0.0f;
+        q.invalid[i] = 0;
+        q.reason[i] = kMasked;
+        q.choice[i] = 0;
+        return;
+    }
+    const int c = q.choice[i];
+    float x, y, h;
+    gated_peak(q, i, (c > 0 ? c : 1) - 1, x, y, h);
+    const bool hnan = h != h;
+    const bool bad = q.invalid[i] || hnan;
+    signed char rc = q.reason[i];
+    if (hnan && rc == kValid) rc = kPeakMagNaN;
+    if (bad && rc == kValid) rc = kUnclassified;
+    q.reason[i] = rc;
+    q.invalid[i] = bad ? 1 : 0;
+    q.ux[i] = bad ? qnanf() : q.cx[i];
+    q.uy[i] = bad ? qnanf() : q.cy[i];
+    q.choice[i] = bad ? 0 : (unsigned char)c;
+}
+
+__global__ void choice_init_kernel(unsigned char *choice, long long nv)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nv) choice[i] = 1;
+}
+
+}  // namespace
+
+// Validation of one pass whose correlation returned P >= 1 peaks per window
+// (pk_* in the correlator's layout (N, P, ny, nx)), with the reference's
+// secondary-peak substitution when `secondary` is set (config secondary_peak):
+// the primary peak is gated, predicted and tested as by pivb_validate_dev; then
+// P - 1 rounds in which every invalid vector with peaks left takes its next peak,
+// is judged afresh (NaN: reason 13), and is tested by the peak-magnitude and
+// normalised-median tests on the field of the current choices (reason 12 when it
+// fails); at the end a NaN height of the chosen peak invalidates (13).  Outputs
+// as pivb_validate_dev, plus choice (N, ny, nx): the 1-based peak each valid
+// vector took, 0 for invalid and masked ones.  work: 4*N*ny*nx floats.
+// Returns 0, or 1 for bad arguments.
+PIV_EXPORT int pivb_validate_peaks_dev(const float *pk_x, const float *pk_y, const float *pk_h, int n_peaks,
+                                       int secondary, const float *pred_dy, const float *pred_dx,
+                                       const float *mask, int N, int ny, int nx, float thresh_x, float thresh_y,
+                                       float peak_thr, float med_eps, float med_thr, int med_size, float *ux,
+                                       float *uy, unsigned char *invalid, signed char *nan_reason,
+                                       unsigned char *choice, float *work, void *stream)
+{
+    if (N <= 0 || ny <= 0 || nx <= 0 || n_peaks < 1 || n_peaks > 255 || med_size < 3 || med_size > 5 ||
+        !(med_size & 1) || !nan_reason || !choice || !work)
+        return 1;
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long plane = (long long)ny * nx, nv = (long long)N * plane;
+    const bool sec = secondary && n_peaks > 1;
+    ValParams p{pk_x, pk_y, pk_h, pred_dy, pred_dx, mask, N, ny, nx, thresh_x, thresh_y, peak_thr, med_eps,
+                med_thr, med_size, ux, uy, invalid, nan_reason, (long long)n_peaks * plane, sec ? 1 : 0};
+    gate_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, (med_thr > 0.0f || sec) ? 0 : 1);
+    if (med_thr > 0.0f) {
+        float *gx = work, *gy = work + nv;
+        cudaMemcpyAsync(gx, ux, nv * 4, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(gy, uy, nv * 4, cudaMemcpyDeviceToDevice, s);
+        median_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, gx, gy);
+    }
+    choice_init_kernel<<<blocks(nv, 256), 256, 0, s>>>(choice, nv);
+    SecParams q{pk_x, pk_y, pk_h, n_peaks, pred_dy, pred_dx, mask, N, ny, nx, thresh_x, thresh_y, peak_thr,
+                med_eps, med_thr, med_size, ux, uy, invalid, nan_reason, choice, work + 2 * nv, work + 3 * nv,
+                reinterpret_cast<unsigned char *>(work), sec ? 1 : 0};
+    if (sec) {
+        for (int round = 1; round < n_peaks; ++round) {
+            subst_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);
+            sec_median_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);
+        }
+    } else {
+        // the primary peak only: the current field is peak 1
+        subst_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);   // substitute = 0: copies peak 1
+    }
+    sec_final_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

@@ -47,6 +47,8 @@ class MultipassConfig:
     final_infill: bool = True
     predictor_fill: str = "harmonic"  # masked windows in the predictor: "harmonic" or "none" (kept at 0)
     engine_32: str = "fft"          # 32 px passes: "fft" (FP32 FFT) or "dft" (tensor-core DFT-as-GEMM)
+    n_peaks: int = 1                # correlation peaks per window (the reference's num_peaks)
+    secondary_peak: bool = False    # substitute the next peak for an invalid vector (needs n_peaks > 1)
 
 
 def _gauss_taps(sigma: float, ksize: int):
@@ -91,6 +93,12 @@ class MultipassPIV:
             raise ValueError(f"predictor_fill {self.cfg.predictor_fill!r} (valid: 'harmonic', 'none')")
         if vector_masks is not None and len(vector_masks) != len(self.geo):
             raise ValueError(f"{len(vector_masks)} vector masks for {len(self.geo)} passes")
+        P = int(self.cfg.n_peaks)
+        if not 1 <= P <= 255:
+            raise ValueError(f"n_peaks {P} outside 1..255")
+        if P > 1 and self.cfg.engine_32 == "dft":
+            raise ValueError("the tensor-core engine returns one peak per window: use engine_32='fft' with n_peaks > 1")
+        self.P = P
         self.Ld = _lib.dft_lib() if self.cfg.engine_32 == "dft" else None
         dev, f32 = self.device, torch.float32
         # device status word of the tensor-core engine (1 = an MMA completion was not observed)
@@ -113,7 +121,7 @@ class MultipassPIV:
                 cx=torch.tensor(g.grid.win_ctrs_x, device=dev), cy=torch.tensor(g.grid.win_ctrs_y, device=dev),
                 cx_all=torch.tensor(g.ctrs_x_all, device=dev), cy_all=torch.tensor(g.ctrs_y_all, device=dev),
                 # zero-filled once: skipped (masked) windows are never written
-                out={k2: torch.zeros((N, 1, ny, nx), dtype=f32, device=dev)
+                out={k2: torch.zeros((N, P, ny, nx), dtype=f32, device=dev)
                      for k2 in ("pk_loc_x", "pk_loc_y", "pk_height", "sx", "sy", "sxy")},
                 ratio=torch.zeros((N, ny, nx), dtype=f32, device=dev),
                 ux=torch.empty((N, ny, nx), dtype=f32, device=dev),
@@ -124,6 +132,10 @@ class MultipassPIV:
                 pdx=torch.empty((N, nyp, nxp), dtype=f32, device=dev),
                 spacing=(float(g.grid.win_spacing_y), float(g.grid.win_spacing_x)),
                 pre=g.n_pre,
+                # large-displacement gate: half the window on the first pass, a quarter
+                # after (cpu_instantaneous.py:575-585), per axis
+                thr=(g.window_size[1] / (2.0 if k == 0 else 4.0), g.window_size[0] / (2.0 if k == 0 else 4.0)),
+                choice=torch.empty((N, ny, nx), dtype=torch.uint8, device=dev) if P > 1 else None,
             )
             bm = None if vector_masks is None else np.asarray(vector_masks[k], bool)
             if bm is not None and bm.shape != (ny, nx):
@@ -151,14 +163,14 @@ class MultipassPIV:
             # included) runs in the thread-per-window record kernel
             wh, ww = g.window_size
             max_scratch = max(max_scratch,
-                              int(self.Lx.pivb_xcorr_scratch_bytes_hw(N * ny * nx, wh, ww, 1, self.cfg.peak_finder)),
+                              int(self.Lx.pivb_xcorr_scratch_bytes_hw(N * ny * nx, wh, ww, P, self.cfg.peak_finder)),
                               int(self.Lx.pivb_xcorr_record_bytes(N * ny * nx)) if wh == ww else 0)
             max_vec = max(max_vec, N * ny * nx)
             max_pad = max(max_pad, N * nyp * nxp)
             max_infill = max(max_infill, int(self.Lp.pivb_infill_work_bytes(N, ny, nx)))
             self.passes.append(p)
         self.scratch = torch.empty(max(max_scratch, 256), dtype=torch.uint8, device=dev)
-        self.work = torch.empty(max(2 * max_vec, max_pad), dtype=f32, device=dev)
+        self.work = torch.empty(max((4 if P > 1 else 2) * max_vec, max_pad), dtype=f32, device=dev)
         self.infill_work = torch.empty(max(max_infill, 256), dtype=torch.uint8, device=dev)
         # predictor copies with the masked windows filled (the stored field keeps 0 there)
         self.fill = (torch.empty((2, max_vec), dtype=f32, device=dev)
@@ -213,6 +225,8 @@ class MultipassPIV:
             n += 1                                        # correlation
             n += 1 if (3 <= self.cfg.peak_finder <= 6) else 0  # deferred fit (record kernel)
             n += 2 if self.cfg.median_threshold > 0 else 1  # validate (+ median)
+            if self.P > 1:                                # choices, substitution rounds, final
+                n += 2 + (2 * (self.P - 1) if self.cfg.secondary_peak else 1)
             if k + 1 < len(self.geo) or self.cfg.final_infill:
                 n += 1                                    # infill
             if k + 1 < len(self.geo):
@@ -272,7 +286,7 @@ class MultipassPIV:
         mptr = None if p["mask"] is None else p["mask"].data_ptr()
         args = (fa.data_ptr(), fb.data_ptr(), H * W, mptr, H, W, N, p["cx"].data_ptr(), p["cy"].data_ptr(),
                 p["ny"], p["nx"], p["weight"].data_ptr(), p["weight"].data_ptr(), p["cw"].data_ptr(), p["win_h"],
-                p["win_w"], 0, 1, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(),
+                p["win_w"], 0, self.P, cfg.peak_finder, cfg.peakfit_impl, o["pk_loc_x"].data_ptr(),
                 o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), o["sx"].data_ptr(), o["sy"].data_ptr(),
                 o["sxy"].data_ptr(), p["ratio"].data_ptr(),
                 None if self.planes is None else self.planes[k].data_ptr(), scr.data_ptr(), scr.numel())
@@ -285,7 +299,7 @@ class MultipassPIV:
         """Whether pass k's correlation can join a packed launch (square windows,
         one peak, the FFT engine, no plane dump)."""
         p = self.passes[k]
-        return (p["win_h"] == p["win_w"] and self.planes is None and 3 <= self.cfg.peak_finder <= 6
+        return (p["win_h"] == p["win_w"] and self.planes is None and 3 <= self.cfg.peak_finder <= 6 and self.P == 1
                 and not (self.Ld is not None and p["win_h"] == 32))
 
     def job(self, k, fa, fb, N):
@@ -307,16 +321,30 @@ class MultipassPIV:
         mptr = None if p["mask"] is None else p["mask"].data_ptr()
         pred_dy = p["pred_dy"] if k > 0 else None
         pred_dx = p["pred_dx"] if k > 0 else None
-        # large-displacement gate: half the window on the first pass, a quarter after
-        # (cpu_instantaneous.py:575-585), per axis
-        thr_x = p["win_w"] / 2.0 if k == 0 else p["win_w"] / 4.0
-        thr_y = p["win_h"] / 2.0 if k == 0 else p["win_h"] / 4.0
+        thr_x, thr_y = p["thr"]
+        if self.P > 1:
+            self._ok(self.Lp.pivb_validate_peaks_dev(
+                o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), self.P,
+                int(bool(cfg.secondary_peak)), None if pred_dy is None else pred_dy.data_ptr(),
+                None if pred_dx is None else pred_dx.data_ptr(), mptr, N, p["ny"], p["nx"], thr_x, thr_y,
+                cfg.peak_mag_threshold, cfg.median_epsilon, cfg.median_threshold, cfg.median_size,
+                p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), p["reason"].data_ptr(),
+                p["choice"].data_ptr(), self.work.data_ptr(), s), "validate (peaks)")
+        else:
+            self._validate_one_peak(p, o, pred_dy, pred_dx, mptr, N, thr_x, thr_y, s)
+        self._post_infill(k, N, mptr, s)
+
+    def _validate_one_peak(self, p, o, pred_dy, pred_dx, mptr, N, thr_x, thr_y, s):
+        cfg = self.cfg
         self._ok(self.Lp.pivb_validate_dev(
             o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(),
             None if pred_dy is None else pred_dy.data_ptr(), None if pred_dx is None else pred_dx.data_ptr(),
             mptr, N, p["ny"], p["nx"], thr_x, thr_y, cfg.peak_mag_threshold, cfg.median_epsilon,
             cfg.median_threshold, cfg.median_size, p["ux"].data_ptr(), p["uy"].data_ptr(),
             p["invalid"].data_ptr(), p["reason"].data_ptr(), self.work.data_ptr(), s), "validate")
+
+    def _post_infill(self, k, N, mptr, s):
+        cfg, p = self.cfg, self.passes[k]
         last = k + 1 == len(self.passes)
         if not last or cfg.final_infill:
             self._ok(self.Lp.pivb_infill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), mptr,
@@ -367,14 +395,23 @@ class MultipassPIV:
                 pred = torch.stack((p["pred_dy"][:n], p["pred_dx"][:n]), dim=-1).cpu().numpy()
             else:
                 pred = np.zeros((n, ny, nx, 2), np.float32)
-            gone = (reason == -1) | (reason == 6)           # masked or gated: the reference NaNs their peaks
-            peak_mag = np.where(gone[:, None], np.float32(np.nan), o["pk_height"])
+            # masked windows and peaks beyond the displacement gate: the reference NaNs
+            # their heights (cpu_instantaneous.py:602-607), peak by peak
+            thr_x, thr_y = p["thr"]
+            with np.errstate(invalid="ignore"):
+                gone = (np.abs(o["pk_loc_x"]) > thr_x) | (np.abs(o["pk_loc_y"]) > thr_y)
+            gone |= p["b_mask"][None, None]
+            peak_mag = np.where(gone, np.float32(np.nan), o["pk_height"])
+            if self.P > 1:
+                choice = p["choice"][:n].cpu().numpy().astype(np.intp)
+            else:
+                choice = np.where(nan_mask, 0, 1).astype(np.intp)
             planes = None if self.planes is None else self.planes[k][:n].cpu().numpy()
             for i in range(n):
                 pr = PIVPassResult(
                     n_windows=np.array([ny, nx], dtype=np.int32), ux_mat=ux[i].copy(), uy_mat=uy[i].copy(),
                     nan_mask=nan_mask[i].copy(), nan_reason=reason[i].copy(), peak_mag=peak_mag[i].copy(),
-                    peak_ratio=ratio[i].copy(), peak_choice=np.where(nan_mask[i], 0, 1).astype(np.intp),
+                    peak_ratio=ratio[i].copy(), peak_choice=choice[i].copy(),
                     predictor_field=pred[i].copy(), b_mask=p["b_mask"].copy(),
                     window_size=tuple(self.cfg.window_sizes[k]), win_ctrs_x=g.grid.win_ctrs_x,
                     win_ctrs_y=g.grid.win_ctrs_y)
