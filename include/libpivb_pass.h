@@ -90,6 +90,15 @@ int pivb_decode_frames_dev(const unsigned char *raw, long long stride, int n_fra
                            int height, int format, const unsigned char *dark, long long dark_stride, int dark_frames,
                            int rot, float *out, long long out_stride, void *stream);
 
+/* The 'nearest' fill of a predictor's masked windows (config
+ * masking.predictor_fill: nearest; infilling.py:808-874, 114-141): out[n][w] =
+ * in[n][idx[w]] for N fields of `plane` windows (ux and uy alike), idx the
+ * donor map of the mask (pivtools_b200.geometry.nearest_donor_map: the nearest
+ * unmasked window in physical distance; each unmasked window its own donor).
+ * Returns 0, or 1 for bad arguments. */
+int pivb_gather_fill_dev(const float *ux, const float *uy, const int *idx, int N, long long plane, float *out_x,
+                         float *out_y, void *stream);
+
 /* Validation of one pass whose correlation returned n_peaks >= 1 peaks per
  * window (pk_* in the correlator's layout (N, n_peaks, ny, nx)), with the
  * reference's secondary-peak substitution when `secondary` is set

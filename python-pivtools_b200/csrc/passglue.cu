@@ -550,6 +550,33 @@ PIV_EXPORT int pivb_validate_dev(const float *pk_x, const float *pk_y, const flo
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
+namespace {
+__global__ void gather_fill_kernel(const float *__restrict__ ux, const float *__restrict__ uy,
+                                   const int *__restrict__ idx, long long plane, long long nv, float *out_x,
+                                   float *out_y)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    const long long n = i / plane, w = i - n * plane;
+    const long long src = n * plane + idx[w];
+    out_x[i] = ux[src];
+    out_y[i] = uy[src];
+}
+}  // namespace
+
+// The 'nearest' fill of the masked windows of a predictor (infilling.py:808-874):
+// out[n][w] = in[n][idx[w]] for N fields of `plane` windows, idx the donor map of
+// the mask (each unmasked window its own donor).  Returns 0, or 1 for bad
+// arguments.
+PIV_EXPORT int pivb_gather_fill_dev(const float *ux, const float *uy, const int *idx, int N, long long plane,
+                                    float *out_x, float *out_y, void *stream)
+{
+    if (!ux || !uy || !idx || !out_x || !out_y || N <= 0 || plane <= 0) return 1;
+    const long long nv = (long long)N * plane;
+    gather_fill_kernel<<<blocks(nv, 256), 256, 0, (cudaStream_t)stream>>>(ux, uy, idx, plane, nv, out_x, out_y);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
 // ---------------------------------------------------------------------------
 // Secondary-peak substitution (cpu_instantaneous.py:676-760)
 // ---------------------------------------------------------------------------

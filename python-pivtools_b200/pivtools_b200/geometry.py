@@ -188,3 +188,24 @@ def multipass_geometry(image_shape, window_sizes, overlaps, window_type="gaussia
             pg.pred_map_y = np.interp(wy.ravel(), py, np.arange(len(py))).reshape(wy.shape).astype(np.float32)
         out.append(pg)
     return out
+
+
+def nearest_donor_map(mask, spacing):
+    """Flat index of each window's donor for the 'nearest' predictor fill of the
+    masked windows (infilling.py:114-141, 808-874): the nearest unmasked window in
+    physical distance (pitch (py, px) in pixels), chosen among equidistant donors
+    as scipy's Euclidean distance transform chooses; every unmasked window maps to
+    itself.  Computed once per pass geometry on the host (the mask is shared by all
+    pairs); the fill itself is a gather on the GPU (pivb_gather_fill_dev)."""
+    from scipy import ndimage as ndi
+
+    m = np.asarray(mask, bool)
+    ny, nx = m.shape
+    donor = ~m
+    if not donor.any():
+        raise ValueError("every window is masked: no donor for the nearest fill")
+    iy, ix = ndi.distance_transform_edt(~donor, sampling=(float(spacing[0]), float(spacing[1])),
+                                       return_distances=False, return_indices=True)
+    idx = (iy * nx + ix).astype(np.int32)
+    idx[donor] = np.flatnonzero(donor).astype(np.int32)
+    return idx.reshape(ny, nx)

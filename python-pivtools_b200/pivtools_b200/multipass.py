@@ -45,7 +45,7 @@ class MultipassConfig:
     infill_max_iter: int = 2000     # conjugate-gradient iteration cap (exact solves need far fewer)
     infill_tol: float = 1e-12       # relative residual of the FP64 normal equations
     final_infill: bool = True
-    predictor_fill: str = "harmonic"  # masked windows in the predictor: "harmonic" or "none" (kept at 0)
+    predictor_fill: str = "harmonic"  # masked windows in the predictor: "harmonic", "nearest" or "none" (kept at 0)
     engine_32: str = "fft"          # 32 px passes: "fft" (FP32 FFT) or "dft" (tensor-core DFT-as-GEMM)
     n_peaks: int = 1                # correlation peaks per window (the reference's num_peaks)
     secondary_peak: bool = False    # substitute the next peak for an invalid vector (needs n_peaks > 1)
@@ -89,8 +89,8 @@ class MultipassPIV:
         if self.cfg.infill not in ("biharmonic", "harmonic"):
             raise ValueError(f"infill {self.cfg.infill!r} (valid: 'biharmonic', 'harmonic')")
         self.infill_order = 2 if self.cfg.infill == "biharmonic" else 1
-        if self.cfg.predictor_fill not in ("harmonic", "none"):
-            raise ValueError(f"predictor_fill {self.cfg.predictor_fill!r} (valid: 'harmonic', 'none')")
+        if self.cfg.predictor_fill not in ("harmonic", "nearest", "none"):
+            raise ValueError(f"predictor_fill {self.cfg.predictor_fill!r} (valid: 'harmonic', 'nearest', 'none')")
         if vector_masks is not None and len(vector_masks) != len(self.geo):
             raise ValueError(f"{len(vector_masks)} vector masks for {len(self.geo)} passes")
         P = int(self.cfg.n_peaks)
@@ -149,6 +149,10 @@ class MultipassPIV:
                 # (a broadcast view's astype keeps its odd strides: materialise C order)
                 p["mask_u8"] = torch.tensor(np.ascontiguousarray(np.broadcast_to(bm, (N, ny, nx)), dtype=np.uint8),
                                             device=dev).contiguous()
+                if self.cfg.predictor_fill == "nearest":
+                    # donor of each masked window, fixed by the mask and the pitch
+                    donor = geometry.nearest_donor_map(bm, (g.grid.win_spacing_y, g.grid.win_spacing_x))
+                    p["donor"] = torch.tensor(donor.ravel(), dtype=torch.int32, device=dev)
             if k > 0:
                 p["map_x"] = torch.tensor(g.pred_map_x, device=dev)
                 p["map_y"] = torch.tensor(g.pred_map_y, device=dev)
@@ -216,7 +220,7 @@ class MultipassPIV:
 
     def _fills(self, k):
         return (k + 1 < len(self.passes) and self.passes[k]["mask"] is not None
-                and self.cfg.predictor_fill == "harmonic")
+                and self.cfg.predictor_fill in ("harmonic", "nearest"))
 
     def _count_launches(self):
         n = 0
@@ -358,13 +362,18 @@ class MultipassPIV:
                 # (infilling.py:808-874 with the harmonic least-squares fill)
                 nv = N * p["ny"] * p["nx"]
                 src_x, src_y = self.fill[0, :nv], self.fill[1, :nv]
-                src_x.copy_(p["ux"].reshape(-1)[:nv])
-                src_y.copy_(p["uy"].reshape(-1)[:nv])
-                self._ok(self.Lp.pivb_infill_dev(src_x.data_ptr(), src_y.data_ptr(), p["mask_u8"].data_ptr(),
-                                                 None, N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
-                                                 1, cfg.infill_max_iter, cfg.infill_tol,
-                                                 self.infill_work.data_ptr(), self.infill_work.numel(), s),
-                                 "predictor fill")
+                if cfg.predictor_fill == "nearest":
+                    self._ok(self.Lp.pivb_gather_fill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(),
+                                                          p["donor"].data_ptr(), N, p["ny"] * p["nx"],
+                                                          src_x.data_ptr(), src_y.data_ptr(), s), "predictor fill")
+                else:
+                    src_x.copy_(p["ux"].reshape(-1)[:nv])
+                    src_y.copy_(p["uy"].reshape(-1)[:nv])
+                    self._ok(self.Lp.pivb_infill_dev(src_x.data_ptr(), src_y.data_ptr(), p["mask_u8"].data_ptr(),
+                                                     None, N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
+                                                     1, cfg.infill_max_iter, cfg.infill_tol,
+                                                     self.infill_work.data_ptr(), self.infill_work.numel(), s),
+                             "predictor fill")
             self._ok(self.Lp.pivb_pad_smooth_dev(src_x.data_ptr(), src_y.data_ptr(), N, p["ny"], p["nx"],
                                                  p["nyp"], p["nxp"], p["pre"][0], p["pre"][1],
                                                  p["taps"].data_ptr(), p["radius"], p["pdy"].data_ptr(),

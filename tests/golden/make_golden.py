@@ -17,6 +17,7 @@ Python package).  The fixtures are committed; tests never need the reference.
     python tests/golden/make_golden.py infill     # infill_ref.npz
     python tests/golden/make_golden.py xcorr      # xcorr_ref.npz, triple_ref.npz
     python tests/golden/make_golden.py lavision   # lavision_ref.npz
+    python tests/golden/make_golden.py pfill      # pfill_ref.npz
 
 The reference checkout is named by $PIVTOOLS_REF (its libraries are built from it
 by `make -C oracle ref PIVTOOLS_REF=...`).
@@ -715,6 +716,49 @@ def _frames_u16(rng, F, H, W):
     return out
 
 
+def make_pfill():
+    """Outputs of the reference's fill_masked_predictor with method 'nearest'
+    (pivtools_cli/piv/piv_backend/infilling.py:808-874, 114-141: the nearest
+    unmasked node in physical distance, scipy's Euclidean distance transform
+    choosing among equidistant donors) on seeded (N, ny, nx, 2) predictor fields
+    with blob, edge and stripe masks and isotropic and anisotropic pitches."""
+    import importlib.util
+    import types
+
+    cfg = types.ModuleType("pivtools_core.config")
+    cfg.PREDICTOR_FILL_METHODS = ("harmonic", "nearest", "none")
+    pc = types.ModuleType("pivtools_core")
+    pc.config = cfg
+    sys.modules.setdefault("pivtools_core", pc)
+    sys.modules.setdefault("pivtools_core.config", cfg)
+    path = os.path.join(REF_ROOT, "pivtools_cli/piv/piv_backend/infilling.py")
+    spec = importlib.util.spec_from_file_location("ref_infilling", path)
+    inf = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(inf)
+    rng = np.random.default_rng(515)
+    out = {}
+    cases = []
+    for k, (ny, nx, pitch) in enumerate([(31, 31, (16.0, 16.0)), (40, 57, (16.0, 8.0)), (25, 64, (12.0, 12.0)),
+                                         (63, 63, (32.0, 16.0))]):
+        yy, xx = np.mgrid[0:ny, 0:nx]
+        m = (yy - ny * 0.45) ** 2 + (xx - nx * 0.6) ** 2 < (min(ny, nx) * 0.22) ** 2
+        if k % 2:
+            m |= xx < 2                                 # a masked edge
+        if k == 2:
+            m |= (yy % 7 == 3) & (xx > nx // 3)        # stripes: many equidistant donors
+        field = rng.normal(0, 2, (2, ny, nx, 2)).astype(np.float32)
+        field[:, m] = 0.0
+        filled = inf.fill_masked_predictor(field, m, pitch, "nearest")
+        out[f"c{k}_field"] = field
+        out[f"c{k}_mask"] = m
+        out[f"c{k}_pitch"] = np.array(pitch)
+        out[f"c{k}_filled"] = np.asarray(filled, np.float32)
+        cases.append(k)
+    out["n_cases"] = np.array(len(cases))
+    np.savez_compressed(os.path.join(HERE, "pfill_ref.npz"), **out)
+    print("pfill_ref.npz written")
+
+
 def make_lavision():
     """Fixtures of the LaVision decode: .im7 files of every pack type (written by
     oracle/lavision_oracle.py) with the reference reader's read_im7 and
@@ -834,3 +878,5 @@ if __name__ == "__main__":
         make_infill()
     if "lavision" in what:
         make_lavision()
+    if "pfill" in what:
+        make_pfill()
