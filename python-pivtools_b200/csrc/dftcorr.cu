@@ -598,7 +598,7 @@ constexpr uint32_t MISC_BYTES = 1024;
 constexpr uint32_t SMEM_BYTES = CONST_BYTES + WORK_BYTES + MISC_BYTES;
 constexpr uint32_t TMEM_COLS = 256;
 static_assert(G * N * PLANE_LD * 4 <= WORK_BYTES, "planes alias the work buffers");
-static_assert(G * N * 4 * 4 <= BUF, "kx = 0 exchange fits buffer 1");
+static_assert(G * N * 4 * 4 + G * N * 2 * 4 <= BUF, "kx = 0 exchange fits buffer 1");
 static_assert(SMEM_BYTES <= 232448, "one CTA per SM");
 
 struct WinInfo {
@@ -848,32 +848,39 @@ __global__ void __launch_bounds__(THREADS, 1) kernel(XcorrParams prm, const uint
                 }
             }
             __syncthreads();
-            float cr[16], ci[16];
-            if (lane != 0) {
+            // row kx = 0: lanes 0..15 of the warp unpack one ky each of its ky range
+            // (P = F(., 0) + i F(., 32); F0 = (P + conj P(-ky)) / 2,
+            // F32 = (P - conj P(-ky)) / 2i), multiply and repack Q = C0 + i C32
+            float *q0 = reinterpret_cast<float *>(buf1) + G * N * 4 + wq * (N * 2);   // [ky][Re, Im]
+            if (lane < 16) {
+                const int ky = k0 + lane, mk = (N - ky) & (N - 1);
+                const float *e = xchg + ky * 4, *m = xchg + mk * 4;
+                const float a0r = 0.5f * (e[0] + m[0]), a0i = 0.5f * (e[1] - m[1]);
+                const float a1r = 0.5f * (e[1] + m[1]), a1i = -0.5f * (e[0] - m[0]);
+                const float b0r = 0.5f * (e[2] + m[2]), b0i = 0.5f * (e[3] - m[3]);
+                const float b1r = 0.5f * (e[3] + m[3]), b1i = -0.5f * (e[2] - m[2]);
+                const float c0r = b0r * a0r + b0i * a0i, c0i = b0i * a0r - b0r * a0i;
+                const float c1r = b1r * a1r + b1i * a1i, c1i = b1i * a1r - b1r * a1i;
+                q0[ky * 2] = c0r - c1i;
+                q0[ky * 2 + 1] = c0i + c1r;
+            }
+            __syncwarp();
+            // conj(C) = conj(F_B conj(F_A)) in place: ar <- Re C, ai <- -Im C
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const float cre = br[j] * ar[j] + bi[j] * ai[j];
+                const float cim = bi[j] * ar[j] - br[j] * ai[j];
+                ar[j] = cre;
+                ai[j] = -cim;
+            }
+            if (lane == 0) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    cr[j] = br[j] * ar[j] + bi[j] * ai[j];
-                    ci[j] = bi[j] * ar[j] - br[j] * ai[j];
-                }
-            } else {
-                // P = F(., 0) + i F(., 32); F0 = (P + conj P(-ky)) / 2, F32 = (P - conj P(-ky)) / 2i
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int ky = k0 + j, mk = (N - ky) & (N - 1);
-                    const float *e = xchg + mk * 4;
-                    const float amr = e[0], ami = e[1], bmr = e[2], bmi = e[3];
-                    const float a0r = 0.5f * (ar[j] + amr), a0i = 0.5f * (ai[j] - ami);
-                    const float a1r = 0.5f * (ai[j] + ami), a1i = -0.5f * (ar[j] - amr);
-                    const float b0r = 0.5f * (br[j] + bmr), b0i = 0.5f * (bi[j] - bmi);
-                    const float b1r = 0.5f * (bi[j] + bmi), b1i = -0.5f * (br[j] - bmr);
-                    const float c0r = b0r * a0r + b0i * a0i, c0i = b0i * a0r - b0r * a0i;
-                    const float c1r = b1r * a1r + b1i * a1i, c1i = b1i * a1r - b1r * a1i;
-                    cr[j] = c0r - c1i;        // Q = C0 + i C32
-                    ci[j] = c0i + c1r;
+                    ar[j] = q0[(k0 + j) * 2];
+                    ai[j] = -q0[(k0 + j) * 2 + 1];
                 }
             }
-#pragma unroll
-            for (int j = 0; j < 16; ++j) ci[j] = -ci[j];          // conj(C)
+            float *cr = ar, *ci = ai;
             const uint32_t r = (uint32_t)(wq * 32 + lane);
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
