@@ -559,12 +559,17 @@ def get_im7_frame_shape(filepath) -> tuple:
 
 class _Staging:
     """One growing page-locked buffer per device; a call waits for the previous
-    call's copy out of it (an event) before decoding into it again."""
+    call's copy out of it (an event) before decoding into it again.  `lock` is held
+    by a call from its decode into the buffer until its copy is enqueued, so host
+    threads decoding for the same device take turns on the buffer."""
 
     def __init__(self, torch, device):
+        import threading
+
         self.torch, self.device = torch, device
         self.buf = None
         self.done = None
+        self.lock = threading.Lock()
 
     def get(self, nbytes: int):
         torch = self.torch
@@ -576,13 +581,15 @@ class _Staging:
 
 
 _STAGING: dict = {}
+_STAGING_LOCK = __import__("threading").Lock()
 
 
 def _staging(torch, device) -> _Staging:
     key = (device.type, device.index)
-    if key not in _STAGING:
-        _STAGING[key] = _Staging(torch, device)
-    return _STAGING[key]
+    with _STAGING_LOCK:
+        if key not in _STAGING:
+            _STAGING[key] = _Staging(torch, device)
+        return _STAGING[key]
 
 
 def _to_device_unpack(torch, device, st: _Staging, host, n_frames: int, payload_bytes: int, npix: int, enc: int,
@@ -659,11 +666,12 @@ def read_im7_camera(filepath: Union[str, Path], camera_no: int = 1, frames_per_c
         holder["host"] = host
         return host.numpy().reshape(nn, fb)
 
-    h, _, sc = _read_frames(path, start, end, alloc)
-    enc = ENC_FLOAT if h.buffer_format == BUFFER_FORMAT_FLOAT else ENC_WORD
-    with torch.cuda.device(dev):
-        return _to_device_unpack(torch, dev, st, holder["host"], n, fb, h.size_x * h.size_y, enc, sc.slope,
-                                 sc.offset, out)
+    with st.lock:
+        h, _, sc = _read_frames(path, start, end, alloc)
+        enc = ENC_FLOAT if h.buffer_format == BUFFER_FORMAT_FLOAT else ENC_WORD
+        with torch.cuda.device(dev):
+            return _to_device_unpack(torch, dev, st, holder["host"], n, fb, h.size_x * h.size_y, enc, sc.slope,
+                                     sc.offset, out)
 
 
 # ---------------------------------------------------------------------------
@@ -732,12 +740,13 @@ def decode_set_entry(stored: bytes, codec: str, decoder: str, width: int, height
     expected = set_payload_bytes(decoder, width, height)
     dev = _device(torch, device)
     st = _staging(torch, dev)
-    host = st.get(expected)
-    set_entry_payload(stored, codec, expected, out=host.numpy())
     if out is None:
         out = torch.empty((height, width), dtype=torch.float32, device=dev)
     elif tuple(out.shape) != (height, width) or out.dtype != torch.float32 or not out.is_contiguous():
         raise ValueError(f"decode_set_entry: out must be a contiguous float32 ({height}, {width}) tensor")
-    with torch.cuda.device(dev):
-        return _to_device_unpack(torch, dev, st, host, 1, expected, width * height, SET_DECODERS[decoder], slope,
-                                 offset, out)
+    with st.lock:
+        host = st.get(expected)
+        set_entry_payload(stored, codec, expected, out=host.numpy())
+        with torch.cuda.device(dev):
+            return _to_device_unpack(torch, dev, st, host, 1, expected, width * height, SET_DECODERS[decoder],
+                                     slope, offset, out)
