@@ -87,3 +87,16 @@ def test_multipass_nearest_predictor_fill(cuda):
     # its padded predictor differs (the masked windows are filled differently)
     assert not np.array_equal(out["nearest"][0][1], out["harmonic"][0][1])
     assert np.isfinite(out["nearest"][1][0]).all()
+
+
+def test_multipass_config_refusals_without_gpu():
+    """Configuration errors are refused before any device work."""
+    from pivtools_b200 import multipass
+
+    HW = (256, 256)
+    with pytest.raises(ValueError, match="predictor_fill"):
+        multipass.MultipassPIV(HW, 1, multipass.MultipassConfig(predictor_fill="linear"), device="cuda:0")
+    with pytest.raises(ValueError, match="one peak"):
+        multipass.MultipassPIV(HW, 1, multipass.MultipassConfig(n_peaks=2, engine_32="dft"), device="cuda:0")
+    with pytest.raises(ValueError, match="n_peaks"):
+        multipass.MultipassPIV(HW, 1, multipass.MultipassConfig(n_peaks=0), device="cuda:0")
