@@ -394,7 +394,7 @@ def run_b200(args):
     # 512,072 windows; profiles/xcorr_kernel32_pass4_8pairs.md,
     # profiles/lm_records_gauss3_8pairs.md), scaled by windows processed (frames,
     # records and outputs all grow with the pair count).
-    traffic = (381.07392e6 + 62.736128e6 + 65.61664e6 + 4.807424e6) / 512072 * windows
+    traffic = (362.904064e6 + 63.008768e6 + 65.61664e6 + 4.807424e6) / 512072 * windows
 
     # ---- end to end through host buffers: every step copies its 64 pairs of
     # uint16 frames from pinned memory (chunked, overlapped with compute), converts
