@@ -390,7 +390,7 @@ def run_b200(args):
     fp32_flops = windows * 80.1e3
     # DRAM traffic of one launch pair (correlation + deferred fits): dram__bytes_read.sum
     # + dram__bytes_write.sum of the same kernels and pass captured by ncu on 8 pairs
-    # (xcorr_kernel<32>: 381.1 + 62.7 MB, lm_records_kernel: 65.6 + 4.8 MB, for
+    # (xcorr_kernel<32>: 362.9 + 63.0 MB, lm_records_kernel: 65.6 + 4.8 MB, for
     # 512,072 windows; profiles/xcorr_kernel32_pass4_8pairs.md,
     # profiles/lm_records_gauss3_8pairs.md), scaled by windows processed (frames,
     # records and outputs all grow with the pair count).
