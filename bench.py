@@ -423,6 +423,7 @@ def run_b200(args):
         q0.record(stream)
         for _ in range(e2e_steps):
             pipe.run(Ah, Bh, ux_h, uy_h)
+        pipe.finish()                           # every field read back before the end event
         q1.record(stream)
     stream.synchronize()
     e2e_ms = q0.elapsed_time(q1) / e2e_steps

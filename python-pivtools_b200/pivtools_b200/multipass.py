@@ -486,12 +486,22 @@ class HostPipeline:
         self.copy_stream = torch.cuda.Stream(device=dev)
         self.ev_h2d = [torch.cuda.Event() for _ in range(2)]
         self.ev_conv = [torch.cuda.Event() for _ in range(2)]
+        # results leave through a staging copy on a second copy stream, so a
+        # chunk's read-back overlaps the next chunk's passes
+        last = self.mp.passes[-1]
+        self.out_stage = [torch.empty((2, chunk, last["ny"], last["nx"]), dtype=torch.float32, device=dev)
+                          for _ in range(2)]
+        self.d2h_stream = torch.cuda.Stream(device=dev)
+        self.ev_done = [torch.cuda.Event() for _ in range(2)]
+        self.ev_d2h = [torch.cuda.Event() for _ in range(2)]
+        self._d2h_used = [False, False]
         self._slot = 0
         self.Lp = _lib.pass_lib()
 
     def run(self, Ah, Bh, ux_out, uy_out):
         """Ah, Bh: pinned uint16 (N, H, W) host tensors, N a multiple of the chunk;
-        ux_out, uy_out: pinned float32 (N, ny, nx) host tensors."""
+        ux_out, uy_out: pinned float32 (N, ny, nx) host tensors, complete once the
+        current stream passes finish() (or after a device synchronisation)."""
         torch = self.torch
         if not all(t.is_pinned() for t in (Ah, Bh, ux_out, uy_out)):
             raise ValueError("HostPipeline.run needs page-locked host tensors (use .pin_memory())")
@@ -523,8 +533,19 @@ class HostPipeline:
                 ux, uy = last["ux"], last["uy"]
             else:
                 ux, uy = self.mp.run(self.f32[0], self.f32[1])
-            ux_out[sl].copy_(ux, non_blocking=True)
-            uy_out[sl].copy_(uy, non_blocking=True)
+            # the staging slot is refilled only after its previous read-back
+            if self._d2h_used[s]:
+                comp.wait_event(self.ev_d2h[s])
+            stage = self.out_stage[s]
+            stage[0].copy_(ux)
+            stage[1].copy_(uy)
+            self.ev_done[s].record(comp)
+            self.d2h_stream.wait_event(self.ev_done[s])
+            with torch.cuda.stream(self.d2h_stream):
+                ux_out[sl].copy_(stage[0], non_blocking=True)
+                uy_out[sl].copy_(stage[1], non_blocking=True)
+                self.ev_d2h[s].record(self.d2h_stream)
+            self._d2h_used[s] = True
         if self.use_graph and self._graph is None:
             # every lazy set-up has run once: capture the chunk's passes (capture
             # records, it does not execute)
@@ -535,3 +556,11 @@ class HostPipeline:
             torch.cuda.current_stream(self.mp.device).synchronize()
             self._graph = g
         return ux_out, uy_out
+
+    def finish(self):
+        """Make the current stream wait for every read-back issued so far (the
+        host result tensors are complete once the stream reaches this point)."""
+        comp = self.torch.cuda.current_stream(self.mp.device)
+        for s in range(2):
+            if self._d2h_used[s]:
+                comp.wait_event(self.ev_d2h[s])
