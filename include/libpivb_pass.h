@@ -90,6 +90,17 @@ int pivb_decode_frames_dev(const unsigned char *raw, long long stride, int n_fra
                            int height, int format, const unsigned char *dark, long long dark_stride, int dark_frames,
                            int rot, float *out, long long out_stride, void *stream);
 
+/* Nearest-donor infill of the invalid vectors in place (the reference's
+ * infilling method 'nearest', infilling.py:114-141, 290-333): each invalid
+ * vector takes both components of the nearest donor -- a vector neither invalid
+ * nor masked (mask nullable, 1 = masked) and finite -- in physical distance
+ * (pitch_y, pitch_x in pixels); among equidistant donors the one of smallest
+ * column, then smallest row (the choice of the reference's scipy Euclidean
+ * feature transform).  A pair without any donor keeps 0 there.  Returns 0, or 1
+ * for bad arguments. */
+int pivb_nearest_infill_dev(float *ux, float *uy, const unsigned char *invalid, const float *mask, int N, int ny,
+                            int nx, double pitch_y, double pitch_x, void *stream);
+
 /* The 'nearest' fill of a predictor's masked windows (config
  * masking.predictor_fill: nearest; infilling.py:808-874, 114-141): out[n][w] =
  * in[n][idx[w]] for N fields of `plane` windows (ux and uy alike), idx the

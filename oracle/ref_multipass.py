@@ -120,6 +120,27 @@ def fill_least_squares(fields, fill, pitch, order, exclude=None):
 # Validation between passes (cpu_instantaneous.py:575-760, one peak)
 # ---------------------------------------------------------------------------
 
+def fill_nearest(fields, fill, pitch, exclude=None):
+    """Nearest-donor fill of a (K, ny, nx) stack sharing one fill pattern
+    (infilling.py:114-141): every fill cell takes the values of the nearest cell,
+    in physical distance, that is neither filled nor excluded and finite in every
+    field, through scipy's Euclidean feature transform as the reference calls it."""
+    from scipy import ndimage as ndi
+
+    fields = np.asarray(fields, np.float64)
+    fill = np.asarray(fill, bool)
+    exclude = np.zeros_like(fill) if exclude is None else np.asarray(exclude, bool)
+    out = fields.copy()
+    if not fill.any():
+        return out
+    donor = ~fill & ~exclude & np.all(np.isfinite(fields), axis=0)
+    if not donor.any():
+        raise ValueError("no donor for the nearest fill")
+    iy, ix = ndi.distance_transform_edt(~donor, sampling=pitch, return_distances=False, return_indices=True)
+    out[:, fill] = fields[:, iy, ix][:, fill]
+    return out
+
+
 def _nanmedian_last(a):
     """Median over the last axis ignoring NaN; rows without NaN go through the
     partition-based np.median (the reference uses bottleneck's nanmedian, which
@@ -281,7 +302,7 @@ class RefMultipass:
         self.geo = geo
         self.weights = [geometry.window_weight(g.window_size, window_type) for g in geo]
         self.finder = peak_finder
-        self.order = {"harmonic": 1, "biharmonic": 2}[infill]
+        self.order = {"nearest": 0, "harmonic": 1, "biharmonic": 2}[infill]
         self.final_infill = final_infill
         self.smoothing = smoothing
         self.n_peaks = n_peaks
@@ -340,7 +361,10 @@ class RefMultipass:
                 pitch = (float(g.grid.win_spacing_y), float(g.grid.win_spacing_x))
                 for i in range(N):
                     if bad[i].any():
-                        f = fill_least_squares(np.stack([ux[i], uy[i]]), bad[i], pitch, self.order)
+                        if self.order == 0:
+                            f = fill_nearest(np.stack([ux[i], uy[i]]), bad[i], pitch).astype(np.float32)
+                        else:
+                            f = fill_least_squares(np.stack([ux[i], uy[i]]), bad[i], pitch, self.order)
                         ux[i], uy[i] = f[0], f[1]
             self.history.append((ux.copy(), uy.copy(), bad.copy()))
             if not last:

@@ -577,6 +577,76 @@ PIV_EXPORT int pivb_gather_fill_dev(const float *ux, const float *uy, const int 
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
+namespace {
+// Nearest-donor infill (infilling.py:114-141, 290-333): each fill cell takes both
+// components of the nearest donor -- a cell neither filled nor excluded (masked)
+// and finite in both components -- in physical distance (pitch py, px).  Among
+// equidistant donors the one of smallest column, then smallest row, is taken:
+// the choice scipy's Euclidean feature transform makes (checked against it on
+// random, striped and holed grids with isotropic and anisotropic pitches).  The
+// search walks square rings of growing index radius R and stops once
+// (R * min(py, px))^2 exceeds the best squared distance.  Donors are never
+// written, so the fill is in place.  A pair without any donor keeps 0 there.
+__global__ void nearest_infill_kernel(float *ux, float *uy, const unsigned char *__restrict__ invalid,
+                                      const float *__restrict__ mask, int N, int ny, int nx, double py, double px)
+{
+    const long long plane = (long long)ny * nx;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= plane * N || !invalid[i]) return;
+    const long long n = i / plane;
+    const int w = (int)(i - n * plane), y = w / nx, x = w % nx;
+    const float *X = ux + n * plane, *Y = uy + n * plane;
+    const unsigned char *inv = invalid + n * plane;
+    const double pmin = py < px ? py : px;
+    double best = INFINITY;
+    int bx = 0x7fffffff, by = 0x7fffffff;
+    const int rmax = ny > nx ? ny : nx;
+    for (int R = 1; R <= rmax; ++R) {
+        const double ring = (double)R * pmin;
+        if (ring * ring > best) break;
+        for (int dy = -R; dy <= R; ++dy) {
+            const int yy = y + dy;
+            if (yy < 0 || yy >= ny) continue;
+            const int step = (dy == -R || dy == R) ? 1 : 2 * R;      // whole edge rows, else the two sides
+            for (int dx = -R; dx <= R; dx += step) {
+                const int xx = x + dx;
+                if (xx < 0 || xx >= nx) continue;
+                const int c = yy * nx + xx;
+                if (inv[c] || (mask && mask[c] != 0.0f)) continue;
+                const float a = X[c], b = Y[c];
+                if (a != a || b != b || isinf(a) || isinf(b)) continue;
+                const double d = (dy * py) * (dy * py) + (dx * px) * (dx * px);
+                if (d < best || (d == best && (xx < bx || (xx == bx && yy < by)))) {
+                    best = d;
+                    bx = xx;
+                    by = yy;
+                }
+            }
+        }
+    }
+    if (bx == 0x7fffffff) {
+        ux[i] = 0.0f;
+        uy[i] = 0.0f;
+    } else {
+        ux[i] = X[by * nx + bx];
+        uy[i] = Y[by * nx + bx];
+    }
+}
+}  // namespace
+
+// Nearest-donor infill of the invalid vectors in place (the reference's
+// infilling method 'nearest', infilling.py:290-333), mask (nullable) the
+// excluded (masked) windows.  Returns 0, or 1 for bad arguments.
+PIV_EXPORT int pivb_nearest_infill_dev(float *ux, float *uy, const unsigned char *invalid, const float *mask, int N,
+                                       int ny, int nx, double pitch_y, double pitch_x, void *stream)
+{
+    if (!ux || !uy || !invalid || N <= 0 || ny <= 0 || nx <= 0 || !(pitch_y > 0.0) || !(pitch_x > 0.0)) return 1;
+    const long long nv = (long long)N * ny * nx;
+    nearest_infill_kernel<<<blocks(nv, 256), 256, 0, (cudaStream_t)stream>>>(ux, uy, invalid, mask, N, ny, nx,
+                                                                             pitch_y, pitch_x);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
 // ---------------------------------------------------------------------------
 // Secondary-peak substitution (cpu_instantaneous.py:676-760)
 // ---------------------------------------------------------------------------

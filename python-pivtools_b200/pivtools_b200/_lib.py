@@ -218,6 +218,8 @@ def pass_lib() -> ctypes.CDLL:
     L.pivb_validate_peaks_dev.argtypes = [vp, vp, vp, ci, ci, vp, vp, vp, ci, ci, ci, fl, fl, fl, fl, fl, ci,
                                           vp, vp, vp, vp, vp, vp, vp]
     L.pivb_validate_peaks_dev.restype = ci
+    L.pivb_nearest_infill_dev.argtypes = [vp, vp, vp, vp, ci, ci, ci, ctypes.c_double, ctypes.c_double, vp]
+    L.pivb_nearest_infill_dev.restype = ci
     L.pivb_gather_fill_dev.argtypes = [vp, vp, vp, ci, cll, vp, vp, vp]
     L.pivb_gather_fill_dev.restype = ci
     L.pivb_payload_bytes.argtypes = [cll, ci]

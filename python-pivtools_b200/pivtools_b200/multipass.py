@@ -40,8 +40,8 @@ class MultipassConfig:
     median_epsilon: float = 0.1
     median_threshold: float = 2.0
     median_size: int = 5
-    infill: str = "biharmonic"      # least-squares infill between passes and after the last:
-                                    # "biharmonic" (the reference's default) or "harmonic"
+    infill: str = "biharmonic"      # infill between passes and after the last: least squares
+                                    # "biharmonic" (the reference's default) or "harmonic", or "nearest"
     infill_max_iter: int = 2000     # conjugate-gradient iteration cap (exact solves need far fewer)
     infill_tol: float = 1e-12       # relative residual of the FP64 normal equations
     final_infill: bool = True
@@ -86,8 +86,8 @@ class MultipassPIV:
         self.Lp = _lib.pass_lib()
         if self.cfg.engine_32 not in ("fft", "dft"):
             raise ValueError(f"engine_32 {self.cfg.engine_32!r}")
-        if self.cfg.infill not in ("biharmonic", "harmonic"):
-            raise ValueError(f"infill {self.cfg.infill!r} (valid: 'biharmonic', 'harmonic')")
+        if self.cfg.infill not in ("biharmonic", "harmonic", "nearest"):
+            raise ValueError(f"infill {self.cfg.infill!r} (valid: 'biharmonic', 'harmonic', 'nearest')")
         self.infill_order = 2 if self.cfg.infill == "biharmonic" else 1
         if self.cfg.predictor_fill not in ("harmonic", "nearest", "none"):
             raise ValueError(f"predictor_fill {self.cfg.predictor_fill!r} (valid: 'harmonic', 'nearest', 'none')")
@@ -350,7 +350,11 @@ class MultipassPIV:
     def _post_infill(self, k, N, mptr, s):
         cfg, p = self.cfg, self.passes[k]
         last = k + 1 == len(self.passes)
-        if not last or cfg.final_infill:
+        if (not last or cfg.final_infill) and cfg.infill == "nearest":
+            self._ok(self.Lp.pivb_nearest_infill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(),
+                                                     mptr, N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1], s),
+                     "infill (nearest)")
+        elif not last or cfg.final_infill:
             self._ok(self.Lp.pivb_infill_dev(p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), mptr,
                                              N, p["ny"], p["nx"], p["spacing"][0], p["spacing"][1],
                                              self.infill_order, cfg.infill_max_iter, cfg.infill_tol,

@@ -448,8 +448,9 @@ def make_validate():
 
 
 def make_infill():
-    """Outputs of the reference's infill_harmonic and infill_biharmonic
-    (pivtools_cli/piv/piv_backend/infilling.py:336-421) on infill_cases().  The
+    """Outputs of the reference's infill_harmonic, infill_biharmonic and
+    infill_nearest (pivtools_cli/piv/piv_backend/infilling.py:290-421) on
+    infill_cases().  The
     module's config import is given the one constant it reads."""
     import importlib.util
     import types
@@ -471,7 +472,8 @@ def make_infill():
         U, V = c["ux"].copy(), c["uy"].copy()
         U[c["fill"]] = np.nan
         V[c["fill"]] = np.nan
-        for name, fn in (("harmonic", inf.infill_harmonic), ("biharmonic", inf.infill_biharmonic)):
+        for name, fn in (("harmonic", inf.infill_harmonic), ("biharmonic", inf.infill_biharmonic),
+                         ("nearest", inf.infill_nearest)):
             fu, fv = fn(U, V, c["fill"], spacing=c["pitch"], exclude=c["exclude"])
             out[f"c{k}_{name}_ux"] = np.asarray(fu, np.float64)
             out[f"c{k}_{name}_uy"] = np.asarray(fv, np.float64)

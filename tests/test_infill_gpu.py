@@ -73,3 +73,61 @@ def test_infill_is_deterministic_and_handles_no_donor(cuda):
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     assert np.isfinite(a[0]).all() and np.isfinite(a[1]).all()
     assert np.all(a[0][1] == 0.0) and np.all(a[1][1] == 0.0)
+
+
+def test_nearest_infill_matches_reference(cuda):
+    """pivb_nearest_infill_dev equals the reference's infill_nearest bit for bit
+    (same donors, ties included) on every fixture case, with several pairs in one
+    launch; a pair without donors keeps 0."""
+    import torch
+
+    g = np.load(os.path.join(GOLD, "infill_ref.npz"))
+    L = _lib.pass_lib()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for k, c in enumerate(infill_cases()):
+        U, V = c["ux"].copy(), c["uy"].copy()
+        U[c["fill"]] = np.nan
+        V[c["fill"]] = np.nan
+        ny, nx = U.shape
+        tu = torch.tensor(np.stack([U, U]), device=cuda)
+        tv = torch.tensor(np.stack([V, V]), device=cuda)
+        fill2 = np.stack([c["fill"], np.ones_like(c["fill"])])       # pair 1: everything to fill
+        tb = torch.tensor(fill2.astype(np.uint8), device=cuda)
+        tm = None if c["exclude"] is None else torch.tensor(c["exclude"].astype(np.float32), device=cuda)
+        assert L.pivb_nearest_infill_dev(tu.data_ptr(), tv.data_ptr(), tb.data_ptr(),
+                                         None if tm is None else tm.data_ptr(), 2, ny, nx, c["pitch"][0],
+                                         c["pitch"][1], s) == 0
+        torch.cuda.synchronize()
+        gu, gv = tu.cpu().numpy(), tv.cpu().numpy()
+        assert np.array_equal(gu[0], g[f"c{k}_nearest_ux"].astype(np.float32)), k
+        assert np.array_equal(gv[0], g[f"c{k}_nearest_uy"].astype(np.float32)), k
+        assert np.all(gu[1] == 0.0) and np.all(gv[1] == 0.0)
+
+
+def test_multipass_nearest_infill_matches_oracle_pipeline(cuda, oracle):
+    """The resident multipass with infill 'nearest' against the reference's pass
+    loop over its compiled libraries with the nearest fill (statistical bar of the
+    pipeline tests)."""
+    import torch
+
+    if oracle.ref_bulk() is None or oracle.ref_warp() is None:
+        pytest.skip("reference libraries not built here")
+    import ref_multipass as RM
+
+    from pivtools_b200 import multipass, synthetic
+
+    HW = (512, 512)
+    cfg = multipass.MultipassConfig(window_sizes=[(64, 64), (32, 32), (32, 32)], overlaps=[50, 50, 75],
+                                    infill="nearest")
+    A, B = synthetic.channel_batch_torch(1, HW, seed=83, device=cuda, peak=8.0, rms_frac=0.2, density=0.02)
+    mp = multipass.MultipassPIV(HW, 1, cfg, device=cuda)
+    mp.run(A, B)
+    torch.cuda.synchronize()
+    rm = RM.RefMultipass(mp.geo, window_type=cfg.window_type, peak_finder=cfg.peak_finder, infill="nearest")
+    rm.run(A.cpu().numpy(), B.cpu().numpy())
+    for k, (p, (rx, ry, rbad)) in enumerate(zip(mp.passes, rm.history)):
+        gx, gy = p["ux"][0].cpu().numpy(), p["uy"][0].cpu().numpy()
+        gbad = p["invalid"][0].cpu().numpy().astype(bool)
+        d = np.maximum(np.abs(gx - rx[0]), np.abs(gy - ry[0]))
+        assert (gbad == rbad[0]).mean() >= 0.995, k
+        assert (d <= 1e-3).mean() >= 0.99, k
