@@ -112,21 +112,28 @@ int pivb_gather_fill_dev(const float *ux, const float *uy, const int *idx, int N
 
 /* Validation of one pass whose correlation returned n_peaks >= 1 peaks per
  * window (pk_* in the correlator's layout (N, n_peaks, ny, nx)), with the
- * reference's secondary-peak substitution when `secondary` is set
- * (cpu_instantaneous.py:676-760, config secondary_peak): the primary peak is
- * gated, predicted and tested as by pivb_validate_dev; then n_peaks - 1 rounds in
- * which every invalid vector with peaks left takes its next peak, is judged
- * afresh (NaN: reason 13) and is tested by the peak-magnitude and normalised-
- * median tests on the field of the current choices (reason 12 if it fails); at
+ * reference's further outlier tests and its secondary-peak substitution
+ * (cpu_instantaneous.py:589-760, outlier_detection.py:246-381): the primary peak
+ * is gated, predicted and tested as by pivb_validate_dev, plus the local sigma
+ * test on the vector norm when sigma_thr > 0 (the reference's `sigma` method)
+ * and the divergence/vorticity test when divvort != 0 (`div_vort`; div_thr /
+ * vort_thr < 0: 6 x 1.4826 x MAD of each pair's field), all reported as
+ * outliers (reason 10); with `secondary` (config secondary_peak) and
+ * n_peaks > 1, n_peaks - 1 rounds in which every invalid vector with peaks left
+ * takes its next peak, is judged afresh (NaN: reason 13) and is tested by every
+ * enabled test on the field of the current choices (reason 12 if it fails); at
  * the end a NaN height of the chosen peak invalidates (13).  Outputs as
  * pivb_validate_dev plus choice (N, ny, nx) uint8: the 1-based peak each valid
- * vector took, 0 for invalid and masked vectors.  work: 4*N*ny*nx floats.
- * Returns 0, or 1 for bad arguments. */
+ * vector took, 0 for invalid and masked vectors.  work:
+ * pivb_validate_peaks_work_floats(N, ny, nx) floats.  Returns 0, or 1 for bad
+ * arguments. */
+long long pivb_validate_peaks_work_floats(int N, int ny, int nx);
 int pivb_validate_peaks_dev(const float *pk_x, const float *pk_y, const float *pk_h, int n_peaks, int secondary,
                             const float *pred_dy, const float *pred_dx, const float *mask, int N, int ny, int nx,
                             float thresh_x, float thresh_y, float peak_thr, float med_eps, float med_thr,
-                            int med_size, float *ux, float *uy, unsigned char *invalid, signed char *nan_reason,
-                            unsigned char *choice, float *work, void *stream);
+                            int med_size, float sigma_thr, int divvort, float div_thr, float vort_thr, float *ux,
+                            float *uy, unsigned char *invalid, signed char *nan_reason, unsigned char *choice,
+                            float *work, void *stream);
 
 /* Bytes of one LaVision pixel payload of npix pixels in `encoding` (below), or -1
  * for an unknown encoding or a pixel count the packing cannot hold. */

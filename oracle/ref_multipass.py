@@ -208,8 +208,54 @@ def validate(pk_x, pk_y, pk_h, pred_dy, pred_dx, thresh_x, thresh_y, peak_thr=0.
     return np.where(bad, np.float32(np.nan), zx), np.where(bad, np.float32(np.nan), zy), bad
 
 
+def sigma_flags(ux, uy, thr):
+    """Local 8-neighbour sigma test on the vector norm, per (ny, nx) field
+    (outlier_detection.py:246-319, combine 'norm')."""
+    from scipy import ndimage as ndi
+
+    v = np.sqrt(ux ** 2 + uy ** 2).astype(np.float32)
+    finite = np.isfinite(v).astype(np.float32)
+    v0 = np.where(np.isfinite(v), v, np.float32(0.0))
+    sum9 = ndi.uniform_filter(v0, size=3, mode="constant", cval=0.0) * 9.0
+    sumsq9 = ndi.uniform_filter(v0 * v0, size=3, mode="constant", cval=0.0) * 9.0
+    cnt9 = ndi.uniform_filter(finite, size=3, mode="constant", cval=0.0) * 9.0
+    sum8 = sum9 - v0
+    sumsq8 = sumsq9 - v0 * v0
+    cnt8 = cnt9 - finite
+    with np.errstate(invalid="ignore", divide="ignore"):
+        mean8 = sum8 / cnt8
+        var8 = (sumsq8 / cnt8) - mean8 * mean8
+    std8 = np.sqrt(np.maximum(var8, 0.0))
+    with np.errstate(invalid="ignore"):
+        return ((np.abs(v - mean8) > thr * std8) | ~np.isfinite(v) | ~np.isfinite(mean8) | (std8 == 0)
+                | (cnt8 < 1))
+
+
+def divvort_flags(ux, uy, div_thresh=None, vort_thresh=None):
+    """Divergence/vorticity test of one (ny, nx) field (outlier_detection.py:322-380):
+    periodic central differences, thresholds 6 x 1.4826 x MAD unless given."""
+    dudx = 0.5 * (np.roll(ux, -1, 1) - np.roll(ux, 1, 1))
+    dudy = 0.5 * (np.roll(ux, -1, 0) - np.roll(ux, 1, 0))
+    dvdx = 0.5 * (np.roll(uy, -1, 1) - np.roll(uy, 1, 1))
+    dvdy = 0.5 * (np.roll(uy, -1, 0) - np.roll(uy, 1, 0))
+    div = dudx + dvdy
+    vort = dvdx - dudy
+
+    def thresh(f, given):
+        if given is not None:
+            return given
+        fin = f[np.isfinite(f)]
+        if fin.size == 0:
+            return np.inf
+        med = np.median(fin)
+        return 6 * (1.4826 * np.median(np.abs(fin - med)))
+
+    with np.errstate(invalid="ignore"):
+        return (np.abs(div) > thresh(div, div_thresh)) | (np.abs(vort) > thresh(vort, vort_thresh))
+
+
 def validate_peaks(pk_x, pk_y, pk_h, pred_dy, pred_dx, thresh_x, thresh_y, secondary=True, peak_thr=0.25,
-                   eps=0.1, med_thr=2.0, size=5):
+                   eps=0.1, med_thr=2.0, size=5, sigma_thr=0.0, divvort=False, div_thr=None, vort_thr=None):
     """(N, P, ny, nx) peak outputs -> (ux, uy, invalid, reason, choice): the driver's
     validation with several peaks and the secondary-peak substitution
     (cpu_instantaneous.py:589-760; no masked windows), in its order of steps: gate
@@ -246,6 +292,11 @@ def validate_peaks(pk_x, pk_y, pk_h, pred_dy, pred_dx, thresh_x, thresh_y, secon
             o = (pm < peak_thr) | np.isnan(pm) if peak_thr >= 0 else np.zeros(fx.shape, bool)
         if med_thr > 0:
             o = o | median_flags(fx, fy, eps, med_thr, size)
+        for n in range(fx.shape[0]):
+            if sigma_thr > 0:
+                o[n] |= sigma_flags(fx[n], fy[n], sigma_thr)
+            if divvort:
+                o[n] |= divvort_flags(fx[n], fy[n], div_thr, vort_thr)
         return o
 
     out = outliers(ux, uy, h[:, 0])

@@ -85,6 +85,8 @@ struct ValParams {
     long long pk_stride;                  // elements between the images' peak arrays (ny*nx for one peak)
     int hnan_late;                        // 1: a NaN peak height invalidates only at the end of the
                                           //    secondary-peak stage (not in the primary tests)
+    int med_on;                           // 1: run the normalised-median test in median_kernel
+    const unsigned char *extra;           // (N, ny, nx) outlier flags of further tests, or null
 };
 
 // Invalid-vector reason codes (pivtools_cli/piv/piv_backend/nan_reason_codes.py:18-25).
@@ -144,41 +146,45 @@ __global__ void median_kernel(ValParams p, const float *gx, const float *gy)
     const bool masked = p.mask && p.mask[w] != 0.0f;
     if (masked) return;
     const float *X = gx + (long long)n * plane, *Y = gy + (long long)n * plane;
-    const int h = p.med_size / 2;
-    float nu[24], nvv[24];
-    int present = 0;
+    bool outlier = false;
+    if (p.med_on) {
+        const int h = p.med_size / 2;
+        float nu[24], nvv[24];
+        int present = 0;
 #pragma unroll
-    for (int t = 0; t < 25; ++t) {
-        const int dr = t / 5 - 2, dc = t % 5 - 2;
-        const int rr = r + dr, cc = c + dc;
-        const bool inside = rr >= 0 && rr < p.ny && cc >= 0 && cc < p.nx && abs(dr) <= h && abs(dc) <= h;
-        float a = qnanf(), b = qnanf();
-        if (inside) {
-            const bool mk = p.mask && p.mask[rr * p.nx + cc] != 0.0f;
-            if (!mk) {
-                a = X[rr * p.nx + cc];
-                b = Y[rr * p.nx + cc];
-                // the reference zeroes failed vectors before its outlier tests
-                // (cpu_instantaneous.py:627-629): they enter as 0, and are present
-                if (a != a || b != b) { a = 0.0f; b = 0.0f; }
+        for (int t = 0; t < 25; ++t) {
+            const int dr = t / 5 - 2, dc = t % 5 - 2;
+            const int rr = r + dr, cc = c + dc;
+            const bool inside = rr >= 0 && rr < p.ny && cc >= 0 && cc < p.nx && abs(dr) <= h && abs(dc) <= h;
+            float a = qnanf(), b = qnanf();
+            if (inside) {
+                const bool mk = p.mask && p.mask[rr * p.nx + cc] != 0.0f;
+                if (!mk) {
+                    a = X[rr * p.nx + cc];
+                    b = Y[rr * p.nx + cc];
+                    // the reference zeroes failed vectors before its outlier tests
+                    // (cpu_instantaneous.py:627-629): they enter as 0, and are present
+                    if (a != a || b != b) { a = 0.0f; b = 0.0f; }
+                }
+                if (abs(dr) <= 1 && abs(dc) <= 1) ++present;     // finite or masked
             }
-            if (abs(dr) <= 1 && abs(dc) <= 1) ++present;     // finite or masked
+            if (t == 12) continue;
+            nu[t < 12 ? t : t - 1] = a;
+            nvv[t < 12 ? t : t - 1] = b;
         }
-        if (t == 12) continue;
-        nu[t < 12 ? t : t - 1] = a;
-        nvv[t < 12 ? t : t - 1] = b;
-    }
-    const float mu = median24(nu), mv = median24(nvv);
-    float u0 = X[w], v0 = Y[w];
-    if (u0 != u0 || v0 != v0) { u0 = 0.0f; v0 = 0.0f; }
-    const float r0 = sqrtf((u0 - mu) * (u0 - mu) + (v0 - mv) * (v0 - mv));
-    float ri[24];
+        const float mu = median24(nu), mv = median24(nvv);
+        float u0 = X[w], v0 = Y[w];
+        if (u0 != u0 || v0 != v0) { u0 = 0.0f; v0 = 0.0f; }
+        const float r0 = sqrtf((u0 - mu) * (u0 - mu) + (v0 - mv) * (v0 - mv));
+        float ri[24];
 #pragma unroll
-    for (int j = 0; j < 24; ++j)
-        ri[j] = sqrtf((nu[j] - mu) * (nu[j] - mu) + (nvv[j] - mv) * (nvv[j] - mv));
-    const float rm = median24(ri);
-    const float nr = r0 / (rm + p.med_eps);
-    const bool outlier = (nr > p.med_thr) || !isfinite(nr) || present < 6;
+        for (int j = 0; j < 24; ++j)
+            ri[j] = sqrtf((nu[j] - mu) * (nu[j] - mu) + (nvv[j] - mv) * (nvv[j] - mv));
+        const float rm = median24(ri);
+        const float nr = r0 / (rm + p.med_eps);
+        outlier = (nr > p.med_thr) || !isfinite(nr) || present < 6;
+    }
+    if (p.extra && p.extra[i]) outlier = true;
     const bool bad = p.invalid[i] || outlier;
     p.invalid[i] = bad ? 1 : 0;
     p.ux[i] = bad ? qnanf() : X[w];
@@ -538,7 +544,7 @@ PIV_EXPORT int pivb_validate_dev(const float *pk_x, const float *pk_y, const flo
     if (N <= 0 || ny <= 0 || nx <= 0 || med_size < 3 || med_size > 5 || !(med_size & 1)) return 1;
     cudaStream_t s = (cudaStream_t)stream;
     ValParams p{pk_x, pk_y, pk_h, pred_dy, pred_dx, mask, N, ny, nx, thresh_x, thresh_y, peak_thr, med_eps,
-                med_thr, med_size, ux, uy, invalid, nan_reason, (long long)ny * nx, 0};
+                med_thr, med_size, ux, uy, invalid, nan_reason, (long long)ny * nx, 0, 1, nullptr};
     const long long nv = (long long)N * ny * nx;
     gate_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, med_thr > 0.0f ? 0 : 1);
     if (med_thr > 0.0f) {
@@ -648,6 +654,250 @@ PIV_EXPORT int pivb_nearest_infill_dev(float *ux, float *uy, const unsigned char
 }
 
 // ---------------------------------------------------------------------------
+// Further outlier tests: local sigma and divergence/vorticity
+// (outlier_detection.py:246-381), on a field in which masked windows are NaN
+// and, in the primary tests, failed vectors are 0 (zero_fill) as the driver
+// zero-fills them (cpu_instantaneous.py:627-629); in the substitution rounds
+// failed vectors stay NaN.  Flags are OR-ed into `flags`.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct ExtraParams {
+    const float *X, *Y;              // (N, ny, nx)
+    const float *mask;               // (ny, nx) or null
+    int N, ny, nx, zero_fill;
+    float sigma_thr;                 // <= 0: off
+    float *div, *vort;               // work (N, ny, nx)
+    float *absdev;                   // work (N, ny, nx)
+    float *thr;                      // work (N, 2): divergence and vorticity thresholds
+    float div_thr, vort_thr;         // < 0: from the field (6 x 1.4826 x MAD)
+    unsigned char *flags;            // (N, ny, nx), OR-ed
+};
+
+// The field value the tests see at (n, r, c): NaN at masked windows, 0 for a
+// failed vector when zero_fill.
+__device__ __forceinline__ void test_field(const ExtraParams &q, long long base, int r, int c, float &a, float &b)
+{
+    const int w = r * q.nx + c;
+    if (q.mask && q.mask[w] != 0.0f) { a = qnanf(); b = qnanf(); return; }
+    a = q.X[base + w];
+    b = q.Y[base + w];
+    if (q.zero_fill && (a != a || b != b)) { a = 0.0f; b = 0.0f; }
+}
+
+// |u| of (a, b) in float32 as np.sqrt(ux**2 + uy**2), NaN kept.
+__device__ __forceinline__ float vnorm(float a, float b)
+{
+    return __fsqrt_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b)));
+}
+
+// 3-point mean along one axis as scipy's uniform_filter1d (size 3, mode
+// constant, cval 0): double sum, / 3, rounded to float32.
+__device__ __forceinline__ float mean3(float l, float c, float r)
+{
+    return (float)((((double)l + (double)c) + (double)r) / 3.0);
+}
+
+// Local 8-neighbour sigma test on the vector norm (combine 'norm';
+// outlier_detection.py:246-319): scipy's 3x3 uniform filter of v0, v0^2 and the
+// finite mask (axis 0, then axis 1), x 9, minus the centre, mean and standard
+// deviation over the finite neighbours.
+__global__ void sigma_kernel(ExtraParams q)
+{
+    const long long plane = (long long)q.ny * q.nx;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= plane * q.N) return;
+    const long long n = i / plane, base = n * plane;
+    const int w = (int)(i - base), r = w / q.nx, c = w % q.nx;
+    // first pass (axis 0) at columns c-1, c, c+1; zero outside the grid
+    float t_v[3], t_v2[3], t_f[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const int cc = c + j - 1;
+        float col_v[3], col_v2[3], col_f[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const int rr = r + k - 1;
+            col_v[k] = 0.0f; col_v2[k] = 0.0f; col_f[k] = 0.0f;
+            if (rr >= 0 && rr < q.ny && cc >= 0 && cc < q.nx) {
+                float a, b;
+                test_field(q, base, rr, cc, a, b);
+                const float v = vnorm(a, b);
+                const bool fin = isfinite(v);
+                const float v0 = fin ? v : 0.0f;
+                col_v[k] = v0;
+                col_v2[k] = __fmul_rn(v0, v0);
+                col_f[k] = fin ? 1.0f : 0.0f;
+            }
+        }
+        const bool inside = cc >= 0 && cc < q.nx;
+        t_v[j] = inside ? mean3(col_v[0], col_v[1], col_v[2]) : 0.0f;
+        t_v2[j] = inside ? mean3(col_v2[0], col_v2[1], col_v2[2]) : 0.0f;
+        t_f[j] = inside ? mean3(col_f[0], col_f[1], col_f[2]) : 0.0f;
+    }
+    const float m9_v = mean3(t_v[0], t_v[1], t_v[2]);
+    const float m9_v2 = mean3(t_v2[0], t_v2[1], t_v2[2]);
+    const float m9_f = mean3(t_f[0], t_f[1], t_f[2]);
+    float a, b;
+    test_field(q, base, r, c, a, b);
+    const float v = vnorm(a, b);
+    const bool fin = isfinite(v);
+    const float cv = fin ? v : 0.0f, cf = fin ? 1.0f : 0.0f;
+    const float sum8 = __fsub_rn(__fmul_rn(m9_v, 9.0f), cv);
+    const float sumsq8 = __fsub_rn(__fmul_rn(m9_v2, 9.0f), __fmul_rn(cv, cv));
+    const float cnt8 = __fsub_rn(__fmul_rn(m9_f, 9.0f), cf);
+    const float mean8 = __fdiv_rn(sum8, cnt8);
+    float var8 = __fsub_rn(__fdiv_rn(sumsq8, cnt8), __fmul_rn(mean8, mean8));
+    if (!(var8 != var8)) var8 = fmaxf(var8, 0.0f);      // np.maximum keeps NaN
+    const float std8 = __fsqrt_rn(var8);
+    const bool out = (fabsf(__fsub_rn(v, mean8)) > __fmul_rn(q.sigma_thr, std8)) || !fin || !isfinite(mean8) ||
+                     std8 == 0.0f || cnt8 < 1.0f;
+    if (out) q.flags[i] = 1;
+}
+
+// Central differences with periodic wrap (np.roll), float32:
+// div = dudx + dvdy, vort = dvdx - dudy (outlier_detection.py:351-358).
+__global__ void divvort_field_kernel(ExtraParams q)
+{
+    const long long plane = (long long)q.ny * q.nx;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= plane * q.N) return;
+    const long long n = i / plane, base = n * plane;
+    const int w = (int)(i - base), r = w / q.nx, c = w % q.nx;
+    const int cp = (c + 1) % q.nx, cm = (c - 1 + q.nx) % q.nx, rp = (r + 1) % q.ny, rm = (r - 1 + q.ny) % q.ny;
+    float uxp, uyp, uxm, uym, vxp, vyp, vxm, vym;
+    test_field(q, base, r, cp, uxp, uyp);     // (ux, uy) at column c+1
+    test_field(q, base, r, cm, uxm, uym);
+    test_field(q, base, rp, c, vxp, vyp);     // at row r+1
+    test_field(q, base, rm, c, vxm, vym);
+    const float dudx = __fmul_rn(0.5f, __fsub_rn(uxp, uxm));
+    const float dvdx = __fmul_rn(0.5f, __fsub_rn(uyp, uym));
+    const float dudy = __fmul_rn(0.5f, __fsub_rn(vxp, vxm));
+    const float dvdy = __fmul_rn(0.5f, __fsub_rn(vyp, vym));
+    q.div[i] = __fadd_rn(dudx, dvdy);
+    q.vort[i] = __fsub_rn(dvdx, dudy);
+}
+
+__device__ __forceinline__ unsigned fkey(float f)
+{
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__device__ __forceinline__ float fkey_inv(unsigned k)
+{
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// The k-th smallest (0-based) finite value of v[0..n) by 8-bit radix selection,
+// one CTA; every thread returns it.
+__device__ float select_kth(const float *v, long long n, long long k, unsigned *hist, unsigned *shared)
+{
+    unsigned prefix = 0, pmask = 0;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+        __syncthreads();
+        for (long long j = threadIdx.x; j < n; j += blockDim.x) {
+            const float x = v[j];
+            if (!isfinite(x)) continue;
+            const unsigned key = fkey(x);
+            if ((key & pmask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long cum = 0;
+            int b = 0;
+            for (; b < 255; ++b) {
+                if (cum + hist[b] > k) break;
+                cum += hist[b];
+            }
+            k -= cum;
+            shared[0] = prefix | ((unsigned)b << shift);
+            shared[1] = (unsigned)k;
+        }
+        __syncthreads();
+        prefix = shared[0];
+        k = shared[1];
+        pmask |= 255u << shift;
+        __syncthreads();
+    }
+    return fkey_inv(prefix);
+}
+
+// np.median of the finite values of v[0..n) (float32; mean of the two middle
+// values for an even count); count = the number of finite values.
+__device__ float median_finite(const float *v, long long n, long long count, unsigned *hist, unsigned *shared)
+{
+    if (count & 1) return select_kth(v, n, count / 2, hist, shared);
+    const float lo = select_kth(v, n, count / 2 - 1, hist, shared);
+    const float hi = select_kth(v, n, count / 2, hist, shared);
+    return __fmul_rn(__fadd_rn(lo, hi), 0.5f);
+}
+
+// Per pair (one CTA): thresholds 6 * 1.4826 * MAD of the finite divergence and
+// vorticity values (inf if none), unless given.
+__global__ void divvort_thresh_kernel(ExtraParams q)
+{
+    __shared__ unsigned hist[256];
+    __shared__ unsigned shared[2];
+    __shared__ unsigned long long cnt;
+    const long long plane = (long long)q.ny * q.nx;
+    const int n = blockIdx.x;
+    for (int f = 0; f < 2; ++f) {
+        const float given = f == 0 ? q.div_thr : q.vort_thr;
+        if (given >= 0.0f) {
+            if (threadIdx.x == 0) q.thr[2 * n + f] = given;
+            continue;
+        }
+        const float *v = (f == 0 ? q.div : q.vort) + n * plane;
+        float *ad = q.absdev + n * plane;
+        if (threadIdx.x == 0) cnt = 0;
+        __syncthreads();
+        unsigned long long mine = 0;
+        for (long long j = threadIdx.x; j < plane; j += blockDim.x) mine += isfinite(v[j]) ? 1 : 0;
+        atomicAdd(&cnt, mine);
+        __syncthreads();
+        const long long count = (long long)cnt;
+        if (count == 0) {
+            if (threadIdx.x == 0) q.thr[2 * n + f] = INFINITY;
+            __syncthreads();
+            continue;
+        }
+        const float med = median_finite(v, plane, count, hist, shared);
+        for (long long j = threadIdx.x; j < plane; j += blockDim.x)
+            ad[j] = isfinite(v[j]) ? fabsf(__fsub_rn(v[j], med)) : qnanf();
+        __syncthreads();
+        const float mad = __fmul_rn(1.4826f, median_finite(ad, plane, count, hist, shared));
+        if (threadIdx.x == 0) q.thr[2 * n + f] = __fmul_rn(6.0f, mad);
+        __syncthreads();
+    }
+}
+
+__global__ void divvort_flag_kernel(ExtraParams q)
+{
+    const long long plane = (long long)q.ny * q.nx;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= plane * q.N) return;
+    const long long n = i / plane;
+    if (fabsf(q.div[i]) > q.thr[2 * n] || fabsf(q.vort[i]) > q.thr[2 * n + 1]) q.flags[i] = 1;
+}
+
+// Run the enabled further tests on (X, Y), OR-ing into flags (zeroed here).
+void extra_outliers(ExtraParams q, int divvort, cudaStream_t s)
+{
+    const long long nv = (long long)q.N * q.ny * q.nx;
+    cudaMemsetAsync(q.flags, 0, nv, s);
+    if (q.sigma_thr > 0.0f) sigma_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);
+    if (divvort) {
+        divvort_field_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);
+        divvort_thresh_kernel<<<q.N, 1024, 0, s>>>(q);
+        divvort_flag_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
 // Secondary-peak substitution (cpu_instantaneous.py:676-760)
 // ---------------------------------------------------------------------------
 namespace {
@@ -667,6 +917,7 @@ struct SecParams {
     float *cx, *cy;                       // work: the field of the current choices
     unsigned char *active;                // work: substituted in this round
     int substitute;                       // 0: only copy each vector's current choice
+    const unsigned char *extra;           // flags of the further tests on cx/cy, or null
 };
 
 // Peak k of vector i after the gate and the predictor (NaN where masked, gated or
@@ -766,6 +1017,7 @@ __global__ void sec_median_kernel(SecParams q)
         const float nr = r0 / (rm + q.med_eps);
         outlier = outlier || (nr > q.med_thr) || !isfinite(nr) || present < 6;
     }
+    if (q.extra && q.extra[i]) outlier = true;
     if (outlier) {
         q.invalid[i] = 1;
         q.reason[i] = kSecondaryOutlier;
@@ -814,21 +1066,33 @@ __global__ void choice_init_kernel(unsigned char *choice, long long nv)
 
 // Validation of one pass whose correlation returned P >= 1 peaks per window
 // (pk_* in the correlator's layout (N, P, ny, nx)), with the reference's
-// secondary-peak substitution when `secondary` is set (config secondary_peak):
-// the primary peak is gated, predicted and tested as by pivb_validate_dev; then
-// P - 1 rounds in which every invalid vector with peaks left takes its next peak,
-// is judged afresh (NaN: reason 13), and is tested by the peak-magnitude and
-// normalised-median tests on the field of the current choices (reason 12 when it
-// fails); at the end a NaN height of the chosen peak invalidates (13).  Outputs
-// as pivb_validate_dev, plus choice (N, ny, nx): the 1-based peak each valid
-// vector took, 0 for invalid and masked ones.  work: 4*N*ny*nx floats.
-// Returns 0, or 1 for bad arguments.
+// further outlier tests and its secondary-peak substitution:
+//   * the primary peak is gated, predicted and tested as by pivb_validate_dev,
+//     plus, when enabled, the local sigma test (sigma_thr > 0) and the
+//     divergence/vorticity test (divvort; div_thr / vort_thr < 0: 6 x 1.4826 x
+//     MAD of the pair's field), all OR-ed as outliers (reason 10);
+//   * with `secondary` and P > 1, P - 1 rounds in which every invalid vector
+//     with peaks left takes its next peak, is judged afresh (NaN: reason 13) and
+//     is tested by every enabled test on the field of the current choices
+//     (reason 12 when it fails);
+//   * at the end a NaN height of the chosen peak invalidates (13).
+// Outputs as pivb_validate_dev plus choice (N, ny, nx): the 1-based peak each
+// valid vector took, 0 for invalid and masked vectors.
+// work: pivb_validate_peaks_work_floats(N, ny, nx) floats.  Returns 0, or 1 for
+// bad arguments.
+PIV_EXPORT long long pivb_validate_peaks_work_floats(int N, int ny, int nx)
+{
+    if (N <= 0 || ny <= 0 || nx <= 0) return 0;
+    return 8LL * N * ny * nx + 2LL * N;
+}
+
 PIV_EXPORT int pivb_validate_peaks_dev(const float *pk_x, const float *pk_y, const float *pk_h, int n_peaks,
                                        int secondary, const float *pred_dy, const float *pred_dx,
                                        const float *mask, int N, int ny, int nx, float thresh_x, float thresh_y,
-                                       float peak_thr, float med_eps, float med_thr, int med_size, float *ux,
-                                       float *uy, unsigned char *invalid, signed char *nan_reason,
-                                       unsigned char *choice, float *work, void *stream)
+                                       float peak_thr, float med_eps, float med_thr, int med_size, float sigma_thr,
+                                       int divvort, float div_thr, float vort_thr, float *ux, float *uy,
+                                       unsigned char *invalid, signed char *nan_reason, unsigned char *choice,
+                                       float *work, void *stream)
 {
     if (N <= 0 || ny <= 0 || nx <= 0 || n_peaks < 1 || n_peaks > 255 || med_size < 3 || med_size > 5 ||
         !(med_size & 1) || !nan_reason || !choice || !work)
@@ -836,26 +1100,41 @@ PIV_EXPORT int pivb_validate_peaks_dev(const float *pk_x, const float *pk_y, con
     cudaStream_t s = (cudaStream_t)stream;
     const long long plane = (long long)ny * nx, nv = (long long)N * plane;
     const bool sec = secondary && n_peaks > 1;
+    const bool extra_on = sigma_thr > 0.0f || divvort != 0;
+    float *gx = work, *gy = work + nv, *cx = work + 2 * nv, *cy = work + 3 * nv;
+    float *divf = work + 4 * nv, *vortf = work + 5 * nv, *absdev = work + 6 * nv;
+    unsigned char *flags = reinterpret_cast<unsigned char *>(work + 7 * nv);
+    unsigned char *active = flags + nv;
+    float *thr = work + 8 * nv;
     ValParams p{pk_x, pk_y, pk_h, pred_dy, pred_dx, mask, N, ny, nx, thresh_x, thresh_y, peak_thr, med_eps,
-                med_thr, med_size, ux, uy, invalid, nan_reason, (long long)n_peaks * plane, sec ? 1 : 0};
-    gate_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, (med_thr > 0.0f || sec) ? 0 : 1);
-    if (med_thr > 0.0f) {
-        float *gx = work, *gy = work + nv;
+                med_thr, med_size, ux, uy, invalid, nan_reason, (long long)n_peaks * plane, sec ? 1 : 0,
+                med_thr > 0.0f ? 1 : 0, extra_on ? flags : nullptr};
+    const bool finalize = med_thr > 0.0f || extra_on;
+    gate_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, (finalize || sec) ? 0 : 1);
+    if (finalize) {
         cudaMemcpyAsync(gx, ux, nv * 4, cudaMemcpyDeviceToDevice, s);
         cudaMemcpyAsync(gy, uy, nv * 4, cudaMemcpyDeviceToDevice, s);
+        if (extra_on) {
+            ExtraParams e{gx, gy, mask, N, ny, nx, 1, sigma_thr, divf, vortf, absdev, thr, div_thr, vort_thr, flags};
+            extra_outliers(e, divvort, s);
+        }
         median_kernel<<<blocks(nv, 256), 256, 0, s>>>(p, gx, gy);
     }
     choice_init_kernel<<<blocks(nv, 256), 256, 0, s>>>(choice, nv);
     SecParams q{pk_x, pk_y, pk_h, n_peaks, pred_dy, pred_dx, mask, N, ny, nx, thresh_x, thresh_y, peak_thr,
-                med_eps, med_thr, med_size, ux, uy, invalid, nan_reason, choice, work + 2 * nv, work + 3 * nv,
-                reinterpret_cast<unsigned char *>(work), sec ? 1 : 0};
+                med_eps, med_thr, med_size, ux, uy, invalid, nan_reason, choice, cx, cy, active, sec ? 1 : 0,
+                extra_on ? flags : nullptr};
     if (sec) {
         for (int round = 1; round < n_peaks; ++round) {
             subst_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);
+            if (extra_on) {
+                ExtraParams e{cx, cy, mask, N, ny, nx, 0, sigma_thr, divf, vortf, absdev, thr, div_thr, vort_thr,
+                              flags};
+                extra_outliers(e, divvort, s);
+            }
             sec_median_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);
         }
     } else {
-        // the primary peak only: the current field is peak 1
         subst_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);   // substitute = 0: copies peak 1
     }
     sec_final_kernel<<<blocks(nv, 256), 256, 0, s>>>(q);

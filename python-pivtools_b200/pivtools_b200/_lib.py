@@ -216,7 +216,9 @@ def pass_lib() -> ctypes.CDLL:
     L.pivb_decode_frames_dev.argtypes = [vp, cll, ci, ci, ci, ci, ci, vp, cll, ci, ci, vp, cll, vp]
     L.pivb_decode_frames_dev.restype = ci
     L.pivb_validate_peaks_dev.argtypes = [vp, vp, vp, ci, ci, vp, vp, vp, ci, ci, ci, fl, fl, fl, fl, fl, ci,
-                                          vp, vp, vp, vp, vp, vp, vp]
+                                          fl, ci, fl, fl, vp, vp, vp, vp, vp, vp, vp]
+    L.pivb_validate_peaks_work_floats.argtypes = [ci, ci, ci]
+    L.pivb_validate_peaks_work_floats.restype = cll
     L.pivb_validate_peaks_dev.restype = ci
     L.pivb_nearest_infill_dev.argtypes = [vp, vp, vp, vp, ci, ci, ci, ctypes.c_double, ctypes.c_double, vp]
     L.pivb_nearest_infill_dev.restype = ci

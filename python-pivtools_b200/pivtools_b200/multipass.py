@@ -47,6 +47,10 @@ class MultipassConfig:
     final_infill: bool = True
     predictor_fill: str = "harmonic"  # masked windows in the predictor: "harmonic", "nearest" or "none" (kept at 0)
     engine_32: str = "fft"          # 32 px passes: "fft" (FP32 FFT) or "dft" (tensor-core DFT-as-GEMM)
+    sigma_threshold: float = 0.0    # > 0: the reference's `sigma` outlier method with this threshold
+    div_vort: bool = False          # the reference's `div_vort` outlier method
+    div_thresh: float | None = None  # its thresholds (None: 6 x 1.4826 x MAD of each pair's field)
+    vort_thresh: float | None = None
     n_peaks: int = 1                # correlation peaks per window (the reference's num_peaks)
     secondary_peak: bool = False    # substitute the next peak for an invalid vector (needs n_peaks > 1)
 
@@ -99,6 +103,8 @@ class MultipassPIV:
         if P > 1 and self.cfg.engine_32 == "dft":
             raise ValueError("the tensor-core engine returns one peak per window: use engine_32='fft' with n_peaks > 1")
         self.P = P
+        # the extended validation entry point: several peaks or further outlier tests
+        self.full_validate = P > 1 or self.cfg.sigma_threshold > 0 or self.cfg.div_vort
         self.Ld = _lib.dft_lib() if self.cfg.engine_32 == "dft" else None
         dev, f32 = self.device, torch.float32
         # device status word of the tensor-core engine (1 = an MMA completion was not observed)
@@ -135,7 +141,8 @@ class MultipassPIV:
                 # large-displacement gate: half the window on the first pass, a quarter
                 # after (cpu_instantaneous.py:575-585), per axis
                 thr=(g.window_size[1] / (2.0 if k == 0 else 4.0), g.window_size[0] / (2.0 if k == 0 else 4.0)),
-                choice=torch.empty((N, ny, nx), dtype=torch.uint8, device=dev) if P > 1 else None,
+                choice=(torch.empty((N, ny, nx), dtype=torch.uint8, device=dev) if self.full_validate
+                        else None),
             )
             bm = None if vector_masks is None else np.asarray(vector_masks[k], bool)
             if bm is not None and bm.shape != (ny, nx):
@@ -174,7 +181,8 @@ class MultipassPIV:
             max_infill = max(max_infill, int(self.Lp.pivb_infill_work_bytes(N, ny, nx)))
             self.passes.append(p)
         self.scratch = torch.empty(max(max_scratch, 256), dtype=torch.uint8, device=dev)
-        self.work = torch.empty(max((4 if P > 1 else 2) * max_vec, max_pad), dtype=f32, device=dev)
+        nval = 8 * max_vec + 2 * N if self.full_validate else 2 * max_vec
+        self.work = torch.empty(max(nval, max_pad), dtype=f32, device=dev)
         self.infill_work = torch.empty(max(max_infill, 256), dtype=torch.uint8, device=dev)
         # predictor copies with the masked windows filled (the stored field keeps 0 there)
         self.fill = (torch.empty((2, max_vec), dtype=f32, device=dev)
@@ -229,8 +237,13 @@ class MultipassPIV:
             n += 1                                        # correlation
             n += 1 if (3 <= self.cfg.peak_finder <= 6) else 0  # deferred fit (record kernel)
             n += 2 if self.cfg.median_threshold > 0 else 1  # validate (+ median)
-            if self.P > 1:                                # choices, substitution rounds, final
-                n += 2 + (2 * (self.P - 1) if self.cfg.secondary_peak else 1)
+            if self.full_validate:                        # choices, substitution rounds, final
+                extra = (1 if self.cfg.sigma_threshold > 0 else 0) + (3 if self.cfg.div_vort else 0)
+                n += 2 + (2 * (self.P - 1) if self.cfg.secondary_peak and self.P > 1 else 1) + extra
+                if self.cfg.secondary_peak and self.P > 1:
+                    n += extra * (self.P - 1)
+                if self.cfg.median_threshold <= 0 and extra:
+                    n += 1                                # the finalising pass of the median kernel
             if k + 1 < len(self.geo) or self.cfg.final_infill:
                 n += 1                                    # infill
             if k + 1 < len(self.geo):
@@ -326,12 +339,15 @@ class MultipassPIV:
         pred_dy = p["pred_dy"] if k > 0 else None
         pred_dx = p["pred_dx"] if k > 0 else None
         thr_x, thr_y = p["thr"]
-        if self.P > 1:
+        if self.full_validate:
             self._ok(self.Lp.pivb_validate_peaks_dev(
                 o["pk_loc_x"].data_ptr(), o["pk_loc_y"].data_ptr(), o["pk_height"].data_ptr(), self.P,
                 int(bool(cfg.secondary_peak)), None if pred_dy is None else pred_dy.data_ptr(),
                 None if pred_dx is None else pred_dx.data_ptr(), mptr, N, p["ny"], p["nx"], thr_x, thr_y,
                 cfg.peak_mag_threshold, cfg.median_epsilon, cfg.median_threshold, cfg.median_size,
+                float(cfg.sigma_threshold), int(bool(cfg.div_vort)),
+                -1.0 if cfg.div_thresh is None else float(cfg.div_thresh),
+                -1.0 if cfg.vort_thresh is None else float(cfg.vort_thresh),
                 p["ux"].data_ptr(), p["uy"].data_ptr(), p["invalid"].data_ptr(), p["reason"].data_ptr(),
                 p["choice"].data_ptr(), self.work.data_ptr(), s), "validate (peaks)")
         else:
@@ -415,7 +431,7 @@ class MultipassPIV:
                 gone = (np.abs(o["pk_loc_x"]) > thr_x) | (np.abs(o["pk_loc_y"]) > thr_y)
             gone |= p["b_mask"][None, None]
             peak_mag = np.where(gone, np.float32(np.nan), o["pk_height"])
-            if self.P > 1:
+            if self.full_validate:
                 choice = p["choice"][:n].cpu().numpy().astype(np.intp)
             else:
                 choice = np.where(nan_mask, 0, 1).astype(np.intp)

@@ -18,6 +18,7 @@ Python package).  The fixtures are committed; tests never need the reference.
     python tests/golden/make_golden.py xcorr      # xcorr_ref.npz, triple_ref.npz
     python tests/golden/make_golden.py lavision   # lavision_ref.npz
     python tests/golden/make_golden.py pfill      # pfill_ref.npz
+    python tests/golden/make_golden.py outliers   # outliers_ref.npz
 
 The reference checkout is named by $PIVTOOLS_REF (its libraries are built from it
 by `make -C oracle ref PIVTOOLS_REF=...`).
@@ -761,6 +762,49 @@ def make_pfill():
     print("pfill_ref.npz written")
 
 
+def make_outliers():
+    """Outputs of the reference's sigma_outlier_detection and div_vort_outliers
+    (pivtools_cli/piv/piv_backend/outlier_detection.py:246-381) on seeded fields
+    with outliers, zeros and NaN holes (fixture outliers_ref.npz).  The module's
+    median binding (bottleneck, absent here; unused by these two tests) is given
+    NumPy's nanmedian."""
+    import importlib.util
+    import types
+
+    bn = types.ModuleType("bottleneck")
+    bn.nanmedian = np.nanmedian
+    sys.modules.setdefault("bottleneck", bn)
+
+    path = os.path.join(REF_ROOT, "pivtools_cli/piv/piv_backend/outlier_detection.py")
+    spec = importlib.util.spec_from_file_location("ref_outliers", path)
+    od = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(od)
+    rng = np.random.default_rng(616)
+    out = {}
+    for k, (ny, nx) in enumerate([(31, 31), (40, 57), (63, 63), (9, 12)]):
+        yy, xx = np.mgrid[0:ny, 0:nx]
+        ux = (2.0 + np.sin(xx / 5.0) + 0.1 * rng.normal(size=(ny, nx))).astype(np.float32)
+        uy = (-1.0 + np.cos(yy / 4.0) + 0.1 * rng.normal(size=(ny, nx))).astype(np.float32)
+        bad = rng.random((ny, nx)) < 0.05
+        ux[bad] += rng.uniform(-8, 8, bad.sum()).astype(np.float32)
+        uy[bad] += rng.uniform(-8, 8, bad.sum()).astype(np.float32)
+        if k % 2:
+            holes = rng.random((ny, nx)) < 0.04
+            ux[holes] = np.nan
+            uy[holes] = np.nan
+        zero = rng.random((ny, nx)) < 0.03
+        ux[zero] = 0.0
+        uy[zero] = 0.0
+        out[f"c{k}_ux"], out[f"c{k}_uy"] = ux, uy
+        for thr in (1.5, 2.0, 3.0):
+            out[f"c{k}_sigma_{thr}"] = od.sigma_outlier_detection(ux, uy, sigma_threshold=thr)
+        out[f"c{k}_divvort"] = od.div_vort_outliers(ux, uy)
+        out[f"c{k}_divvort_given"] = od.div_vort_outliers(ux, uy, div_thresh=0.5, vort_thresh=0.7)
+    out["n_cases"] = np.array(4)
+    np.savez_compressed(os.path.join(HERE, "outliers_ref.npz"), **out)
+    print("outliers_ref.npz written")
+
+
 def make_lavision():
     """Fixtures of the LaVision decode: .im7 files of every pack type (written by
     oracle/lavision_oracle.py) with the reference reader's read_im7 and
@@ -882,3 +926,5 @@ if __name__ == "__main__":
         make_lavision()
     if "pfill" in what:
         make_pfill()
+    if "outliers" in what:
+        make_outliers()

@@ -1,6 +1,7 @@
-"""Several correlation peaks per window and the secondary-peak substitution of
-the resident multipass (pivb_validate_peaks_dev, MultipassConfig(n_peaks,
-secondary_peak)) against the oracle's restatement of the reference driver
+"""Several correlation peaks per window, the secondary-peak substitution and the
+further outlier tests (local sigma, divergence/vorticity) of the resident
+multipass (pivb_validate_peaks_dev, MultipassConfig(n_peaks, secondary_peak,
+sigma_threshold, div_vort)) against the oracle's restatement of the reference driver
 (oracle/ref_multipass.validate_peaks: cpu_instantaneous.py:589-760) and against
 the reference's pass loop over its compiled libraries."""
 
@@ -41,9 +42,11 @@ def _peaks(rng, N, P, ny, nx):
     return x, y, h
 
 
-@pytest.mark.parametrize("P,secondary,with_pred", [(3, True, True), (2, True, False), (3, False, True),
-                                                   (4, True, True)])
-def test_validate_peaks_matches_oracle(cuda, P, secondary, with_pred):
+@pytest.mark.parametrize("P,secondary,with_pred,sigma,divvort", [
+    (3, True, True, 0.0, False), (2, True, False, 0.0, False), (3, False, True, 0.0, False),
+    (4, True, True, 0.0, False), (3, True, True, 2.0, False), (3, True, True, 0.0, True),
+    (1, False, True, 2.0, True), (3, True, False, 1.5, True)])
+def test_validate_peaks_matches_oracle(cuda, P, secondary, with_pred, sigma, divvort):
     import torch
 
     import ref_multipass as RM
@@ -56,7 +59,8 @@ def test_validate_peaks_matches_oracle(cuda, P, secondary, with_pred):
         pdy = rng.normal(0, 1.0, (N, ny, nx)).astype(np.float32)
         pdx = rng.normal(0, 1.0, (N, ny, nx)).astype(np.float32)
     thr_x, thr_y = 4.0, 4.0
-    ox, oy, obad, oreason, ochoice = RM.validate_peaks(x, y, h, pdy, pdx, thr_x, thr_y, secondary=secondary)
+    ox, oy, obad, oreason, ochoice = RM.validate_peaks(x, y, h, pdy, pdx, thr_x, thr_y, secondary=secondary,
+                                                       sigma_thr=sigma, divvort=divvort)
     L = _lib.pass_lib()
     dev = cuda
     t = {k: torch.tensor(v, device=dev) for k, v in (("x", x), ("y", y), ("h", h))}
@@ -66,13 +70,13 @@ def test_validate_peaks_matches_oracle(cuda, P, secondary, with_pred):
     inv = torch.empty((N, ny, nx), dtype=torch.uint8, device=dev)
     rc = torch.empty((N, ny, nx), dtype=torch.int8, device=dev)
     ch = torch.empty((N, ny, nx), dtype=torch.uint8, device=dev)
-    work = torch.empty(4 * N * ny * nx, device=dev)
+    work = torch.empty(int(L.pivb_validate_peaks_work_floats(N, ny, nx)), device=dev)
     s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     ptr = lambda v: None if v is None else v.data_ptr()   # noqa: E731
     assert L.pivb_validate_peaks_dev(t["x"].data_ptr(), t["y"].data_ptr(), t["h"].data_ptr(), P, int(secondary),
                                      ptr(tp["dy"]), ptr(tp["dx"]), None, N, ny, nx, thr_x, thr_y, 0.25, 0.1, 2.0, 5,
-                                     ux.data_ptr(), uy.data_ptr(), inv.data_ptr(), rc.data_ptr(), ch.data_ptr(),
-                                     work.data_ptr(), s) == 0
+                                     sigma, int(divvort), -1.0, -1.0, ux.data_ptr(), uy.data_ptr(), inv.data_ptr(),
+                                     rc.data_ptr(), ch.data_ptr(), work.data_ptr(), s) == 0
     torch.cuda.synchronize()
     gbad = inv.cpu().numpy().astype(bool)
     assert np.array_equal(gbad, obad)
@@ -80,7 +84,7 @@ def test_validate_peaks_matches_oracle(cuda, P, secondary, with_pred):
     assert np.array_equal(ch.cpu().numpy().astype(np.intp), ochoice)
     assert np.array_equal(ux.cpu().numpy(), ox, equal_nan=True)
     assert np.array_equal(uy.cpu().numpy(), oy, equal_nan=True)
-    if secondary:
+    if secondary and P > 1:
         assert (ochoice > 1).sum() > 20          # the case exercises the substitution
         assert (oreason == 12).sum() > 0 and (oreason == 13).sum() > 0
 
@@ -102,13 +106,13 @@ def test_one_peak_path_equals_validate_dev(cuda):
         uy = torch.empty_like(ux)
         inv = torch.empty((N, ny, nx), dtype=torch.uint8, device=dev)
         rc = torch.empty((N, ny, nx), dtype=torch.int8, device=dev)
-        work = torch.empty(4 * N * ny * nx, device=dev)
+        work = torch.empty(int(L.pivb_validate_peaks_work_floats(N, ny, nx)), device=dev)
         if multi:
             ch = torch.empty((N, ny, nx), dtype=torch.uint8, device=dev)
             assert L.pivb_validate_peaks_dev(t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), 1, 1, None, None,
-                                             None, N, ny, nx, 4.0, 4.0, 0.25, 0.1, 2.0, 5, ux.data_ptr(),
-                                             uy.data_ptr(), inv.data_ptr(), rc.data_ptr(), ch.data_ptr(),
-                                             work.data_ptr(), s) == 0
+                                             None, N, ny, nx, 4.0, 4.0, 0.25, 0.1, 2.0, 5, 0.0, 0, -1.0, -1.0,
+                                             ux.data_ptr(), uy.data_ptr(), inv.data_ptr(), rc.data_ptr(),
+                                             ch.data_ptr(), work.data_ptr(), s) == 0
         else:
             assert L.pivb_validate_dev(t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr(), None, None, None, N, ny,
                                        nx, 4.0, 4.0, 0.25, 0.1, 2.0, 5, ux.data_ptr(), uy.data_ptr(), inv.data_ptr(),
