@@ -42,6 +42,18 @@ int pivb_zlib_inflate_exact(const uint8_t *src, long long n, uint8_t *dst, long 
  * (im7_reader.py:534-566). */
 long long pivb_zlib_inflate_prefix(const uint8_t *src, long long n, uint8_t *dst, long long cap);
 
+/* A run of int32-size-prefixed zlib blocks (.im7 pack 2) in one buffer: skip
+ * skip_before blocks, inflate the next n_blocks (each exactly block_bytes,
+ * ending at its declared size) into dst on up to n_threads host threads, skip
+ * skip_after blocks; *consumed = the bytes walked.  Returns 0; -1 bad arguments;
+ * -2 a size prefix cut off, not positive or past the buffer (*err_block = its
+ * index); 10 + the pivb_zlib_inflate_exact code of the first failing block
+ * (*err_block = its index among the n_blocks).  Replaces the per-block loop of
+ * _read_pixels_zlib (im7_reader.py:607-635). */
+int pivb_zlib_blocks_decode(const uint8_t *buf, long long n, long long skip_before, long long n_blocks,
+                            long long skip_after, uint8_t *dst, long long block_bytes, int n_threads,
+                            long long *consumed, long long *err_block);
+
 #ifdef __cplusplus
 }
 #endif

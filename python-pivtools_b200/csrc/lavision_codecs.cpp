@@ -207,3 +207,62 @@ PIV_EXPORT long long pivb_zlib_inflate_prefix(const uint8_t *src, long long n, u
     if (rc == Z_DATA_ERROR || rc == Z_NEED_DICT || rc == Z_STREAM_ERROR || rc == Z_MEM_ERROR) return -1;
     return produced;
 }
+
+#include <atomic>
+#include <thread>
+#include <vector>
+
+// A run of int32-size-prefixed zlib blocks (.im7 pack 2) in one buffer: skip
+// `skip_before` blocks, inflate the next n_blocks (each exactly block_bytes,
+// ending at its declared size) into dst on up to n_threads host threads, then
+// skip `skip_after` blocks.  *consumed receives the bytes walked (where the
+// attribute records begin when every block of the file was walked).  Returns 0;
+// -1 for bad arguments; -2 if a size prefix is cut off, not positive or runs
+// past the buffer (*err_block = its index); or, for the first block (by index)
+// that does not inflate as required, 10 + its pivb_zlib_inflate_exact code with
+// *err_block = its index among the n_blocks.
+PIV_EXPORT int pivb_zlib_blocks_decode(const uint8_t *buf, long long n, long long skip_before, long long n_blocks,
+                                       long long skip_after, uint8_t *dst, long long block_bytes, int n_threads,
+                                       long long *consumed, long long *err_block)
+{
+    if (!buf || n < 0 || skip_before < 0 || n_blocks < 0 || skip_after < 0 || block_bytes < 0 ||
+        (n_blocks > 0 && !dst) || !consumed || !err_block)
+        return -1;
+    std::vector<long long> start((size_t)n_blocks), size((size_t)n_blocks);
+    long long pos = 0;
+    const long long total = skip_before + n_blocks + skip_after;
+    for (long long b = 0; b < total; ++b) {
+        if (n - pos < 4) { *err_block = b; return -2; }
+        int32_t s;
+        memcpy(&s, buf + pos, 4);
+        pos += 4;
+        if (s <= 0 || s > n - pos) { *err_block = b; return -2; }
+        if (b >= skip_before && b < skip_before + n_blocks) {
+            start[(size_t)(b - skip_before)] = pos;
+            size[(size_t)(b - skip_before)] = s;
+        }
+        pos += s;
+    }
+    *consumed = pos;
+    std::atomic<long long> next{0};
+    std::vector<int> code((size_t)n_blocks, 0);
+    auto work = [&]() {
+        for (long long b = next.fetch_add(1); b < n_blocks; b = next.fetch_add(1))
+            code[(size_t)b] = pivb_zlib_inflate_exact(buf + start[(size_t)b], size[(size_t)b],
+                                                      dst + b * block_bytes, block_bytes);
+    };
+    const int nt = n_threads < 1 ? 1 : (n_threads > 64 ? 64 : n_threads);
+    if (nt == 1 || n_blocks < 2) {
+        work();
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < nt; ++t) pool.emplace_back(work);
+        for (auto &th : pool) th.join();
+    }
+    for (long long b = 0; b < n_blocks; ++b)
+        if (code[(size_t)b]) {
+            *err_block = b;
+            return 10 + code[(size_t)b];
+        }
+    return 0;
+}

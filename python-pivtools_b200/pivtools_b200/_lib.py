@@ -246,6 +246,8 @@ def lavision_lib() -> ctypes.CDLL:
     L.pivb_zlib_inflate_exact.restype = ci
     L.pivb_zlib_inflate_prefix.argtypes = [vp, cll, vp, cll]
     L.pivb_zlib_inflate_prefix.restype = cll
+    L.pivb_zlib_blocks_decode.argtypes = [vp, cll, cll, cll, cll, vp, cll, ci, llp, llp]
+    L.pivb_zlib_blocks_decode.restype = ci
     L._pivb_bound = True
     return L
 

@@ -36,7 +36,7 @@ TARGETS = {
 
 # host-only translation units: the system C++ compiler, zlib
 HOST_FLAGS = ["-O3", "-std=c++17", "-fPIC", "-fvisibility=hidden", "-shared"]
-HOST_LIBS = ["-lz"]
+HOST_LIBS = ["-lz", "-pthread"]
 
 
 def _nvcc() -> str:

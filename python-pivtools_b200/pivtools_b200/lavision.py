@@ -286,40 +286,30 @@ def _zlib_block_bytes(f, h) -> int:
     raise IOError(f"First zlib block inflated to {head} bytes; expected one row ({row}) or one frame ({frame})")
 
 
-def _next_zlib_block(f) -> bytes:
-    raw = f.read(4)
-    if len(raw) < 4:
-        raise IOError("Unexpected EOF reading compressed size")
-    n = struct.unpack("<i", raw)[0]
-    if n <= 0:
-        raise IOError(f"invalid zlib block size: {n}")
-    comp = f.read(n)
-    if len(comp) != n:
-        raise IOError("Unexpected EOF reading compressed data")
-    return comp
-
-
-def _skip_zlib_blocks(f, n_blocks: int) -> None:
-    for _ in range(n_blocks):
-        raw = f.read(4)
-        if len(raw) < 4:
-            raise IOError("Unexpected EOF skipping compressed blocks")
-        f.seek(struct.unpack("<i", raw)[0], 1)
-
-
 def _read_zlib(f, h, source, start, end, dst):
+    """Pack 2: every block's size prefix walked and the kept frames' blocks
+    inflated in parallel by one native call; f is left at the attribute records."""
     fb = _frame_bytes(h)
     bb = _zlib_block_bytes(f, h)
     per = fb // bb
-    _skip_zlib_blocks(f, start * per)
-    comps = [_next_zlib_block(f) for _ in range((end - start) * per)]
-    _skip_zlib_blocks(f, (h.size_f - end) * per)
-    flat = dst.reshape(-1)
-
-    def one(i):
-        zlib_inflate_into(comps[i], flat[i * bb:(i + 1) * bb], bb, f"{source}: zlib block {i}")
-
-    list(_pool().map(one, range(len(comps))))
+    base = f.tell()
+    rest = np.empty(os.fstat(f.fileno()).st_size - base, np.uint8)
+    if f.readinto(memoryview(rest)) != rest.size:
+        raise IOError(f"{source}: short read of the zlib blocks")
+    L = _lib.lavision_lib()
+    consumed, err = ctypes.c_longlong(0), ctypes.c_longlong(-1)
+    rc = L.pivb_zlib_blocks_decode(rest.ctypes.data if rest.size else 1, rest.size, start * per, (end - start) * per,
+                                   (h.size_f - end) * per, _ptr(dst), bb, max(1, min(16, os.cpu_count() or 1)),
+                                   ctypes.byref(consumed), ctypes.byref(err))
+    if rc == -2:
+        raise IOError(f"{source}: zlib block {err.value}: unexpected EOF or invalid size prefix")
+    if rc in (11, 12, 14):
+        raise IOError(f"{source}: zlib block {err.value} did not inflate to {bb} bytes")
+    if rc in (13, 15):
+        raise IOError(f"{source}: zlib block {err.value} does not end at its declared size")
+    if rc:
+        raise IOError(f"{source}: zlib blocks could not be decoded ({rc})")
+    f.seek(base + consumed.value)
 
 
 def _read_lz4(f, h, source, start, end, dst):
@@ -558,10 +548,10 @@ def get_im7_frame_shape(filepath) -> tuple:
 # ---------------------------------------------------------------------------
 
 class _Staging:
-    """One growing page-locked buffer per device; a call waits for the previous
-    call's copy out of it (an event) before decoding into it again.  `lock` is held
-    by a call from its decode into the buffer until its copy is enqueued, so host
-    threads decoding for the same device take turns on the buffer."""
+    """One growing page-locked buffer per device and host thread; a call waits for
+    the previous call's copy out of it (an event) before decoding into it again.
+    `lock` is held by a call from its decode into the buffer until its copy is
+    enqueued."""
 
     def __init__(self, torch, device):
         import threading
@@ -585,7 +575,11 @@ _STAGING_LOCK = __import__("threading").Lock()
 
 
 def _staging(torch, device) -> _Staging:
-    key = (device.type, device.index)
+    import threading
+
+    # one buffer per device and host thread, so threads decoding different
+    # files overlap
+    key = (device.type, device.index, threading.get_ident())
     with _STAGING_LOCK:
         if key not in _STAGING:
             _STAGING[key] = _Staging(torch, device)
