@@ -53,6 +53,10 @@ def _args():
                     help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
                          "serve: Poisson request stream with continuous batching")
     ap.add_argument("--chunk", type=int, default=32, help="e2e: pairs per host-to-device chunk")
+    ap.add_argument("--ensemble-bg", default="correlation+dc_zero",
+                    choices=["correlation", "correlation+dc_zero", "window_mean", "correlation+window_mean", "image",
+                             "image+window_mean", "image+dc_zero"],
+                    help="ensemble: background subtraction method (the 'image' ones sweep each batch twice)")
     ap.add_argument("--no-dft-leg", action="store_true",
                     help="skip the tensor-core workload leg of the default run")
     ap.add_argument("--dft-frames", type=int, nargs=2, default=[49, 13], metavar=("F64", "F32"),
@@ -542,12 +546,30 @@ def run_ensemble(args):
     A = torch.stack([f[0] for f in frames]).contiguous()
     B = torch.stack([f[1] for f in frames]).contiguous()
     del frames
-    ep = ensemble.EnsemblePIV(shape, (16, 16), 75, "square", background="correlation+dc_zero", device=dev)
+    bg = args.ensemble_bg
+    ep = ensemble.EnsemblePIV(shape, (16, 16), 75, "square", background=bg, device=dev)
+    two = ep.two_sweep
+
+    def end_means():
+        if ws > 1:
+            ep.end_means_distributed()           # one all-reduce of the frame sums
+        else:
+            ep.end_means()
+
+    def sweeps(n):
+        """n batches accumulated; the 'image' methods sweep them twice (frame sums,
+        then the mean-subtracted correlation)."""
+        if two:
+            for _ in range(n):
+                ep.accumulate_means(A, B)
+            end_means()
+        for _ in range(n):
+            ep.accumulate(A, B)
+
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
-        for _ in range(max(args.warmup, 1)):
-            ep.accumulate(A, B)
+        sweeps(max(args.warmup, 1))
     stream.synchronize()
     ep.reset()
     if ws > 1:
@@ -557,8 +579,7 @@ def run_ensemble(args):
     with ClockSampler(local) as clk:
         with torch.cuda.stream(stream):
             e0.record(stream)
-            for _ in range(args.steps):
-                ep.accumulate(A, B)
+            sweeps(args.steps)
             e1.record(stream)
         stream.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
@@ -588,21 +609,31 @@ def run_ensemble(args):
     Bh = B.round().clamp(0, 65535).to(torch.int32).to(torch.uint16).cpu().pin_memory()
     if not (Ah.is_pinned() and Bh.is_pinned()):
         raise RuntimeError("host frames are not page-locked")
+    def host_sweeps(n):
+        if two:
+            ep.reset()
+            for _ in range(n):
+                ep.accumulate_means_host(Ah, Bh, chunk=16)
+            end_means()
+        for _ in range(n):
+            ep.accumulate_host(Ah, Bh, chunk=16)
+
+    n_e2e = max(2, min(args.steps, 5))
     with torch.cuda.stream(stream):
-        ep.accumulate_host(Ah, Bh, chunk=16)             # warm the staging buffers
+        host_sweeps(1)                                   # warm the staging buffers
         q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         q0.record(stream)
-        for _ in range(max(2, min(args.steps, 5))):
-            ep.accumulate_host(Ah, Bh, chunk=16)
+        host_sweeps(n_e2e)
         q1.record(stream)
     stream.synchronize()
-    e2e_ms = q0.elapsed_time(q1) / max(2, min(args.steps, 5))
+    e2e_ms = q0.elapsed_time(q1) / n_e2e
     if ws > 1:
         t = torch.tensor([e2e_ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    h2d_bytes = 2 * P * shape[0] * shape[1] * 2
-    alg_bytes = 2 * P * shape[0] * shape[1] * 4
+    sweeps_per_step = 2 if two else 1
+    h2d_bytes = 2 * P * shape[0] * shape[1] * 2 * sweeps_per_step
+    alg_bytes = 2 * P * shape[0] * shape[1] * 4 * sweeps_per_step
     hbm_peak, _, peak_kind = _peaks()
     cpu = None
     if rank == 0 and ws == 1 and os.environ.get("PIVB_SKIP_CPU") != "1":
@@ -639,7 +670,8 @@ def run_ensemble(args):
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "ensemble pass, 1024x1024 pairs at 0.02 ppp, 16 px square windows at 75% "
-                                   "(64,009 windows), correlation+dc_zero background, k-space fit (flat floor)",
+                                   f"(64,009 windows), {bg} background"
+                                   f"{' (two sweeps per batch)' if two else ''}, k-space fit (flat floor)",
                        "pairs_per_step_per_gpu": P, "l2": f"{P} distinct pairs cycled ({2 * P * 4} MB > L2)",
                        "parallelism": f"dp{ws} (pairs)"},
             "finalize_ms": fin_ms, "fit_ms": fit_ms, "fit_windows_per_s": ep.n_win / (fit_ms * 1e-3),
@@ -648,10 +680,11 @@ def run_ensemble(args):
             "projected_5000_pairs_s": 5000 / value + (fin_ms + fit_ms) * 1e-3,
             "roofline": {"bound": "hbm", "achieved": alg_bytes / (ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                          "frac": alg_bytes / (ms * 1e-3) / 1e9 / hbm_peak, "traffic": None, "peak_kind": peak_kind,
-                         "kernel": "accum_kernel<16> + frame sums", "algorithmic_bytes": alg_bytes},
+                         "kernel": "accum_kernel<16> + frame sums" + (" + mean-image subtraction" if two else ""),
+                         "algorithmic_bytes": alg_bytes},
             "e2e": {"value": P * ws / (e2e_ms * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": h2d_bytes,
                     "d2h_bytes_per_step": 0, "frames": "uint16", "chunk_pairs": 16},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": (5 * args.steps + 2) if two else 3 * args.steps,
             "clocks": clk.summary(),
         }
         if cpu is not None:

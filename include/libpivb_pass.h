@@ -65,6 +65,15 @@ int pivb_frame_sum_dev(const float *frames, long long stride, int n_frames, long
 /* out = sum / n: the mean frame of n accumulated pairs. */
 int pivb_frame_mean_dev(const float *sum, long long npix, int n, float *out, void *stream);
 
+/* The two-sweep 'image' background methods ('image', 'image+window_mean',
+ * 'image+dc_zero'): dst frame k = src frame k - mean for n_frames frames of npix
+ * pixels (strides src_stride / dst_stride elements), one float32 subtraction per
+ * pixel as the reference's `images -= A_mean` before correlating
+ * (pivtools_cli/piv/piv_backend/cpu_ensemble.py:1290-1291).  In place when
+ * dst == src (equal strides); returns 1 on bad arguments. */
+int pivb_center_frames_dev(const float *src, long long src_stride, int n_frames, long long npix, const float *mean,
+                           float *dst, long long dst_stride, void *stream);
+
 /* Finalise of one ensemble pass (std mode): average the accumulated AB/AA/BB sums
  * of n_win windows of h x w over n_pairs, subtract the background planes (all three
  * or none), optionally zero each plane's mean (the '+dc_zero' methods), divide by

@@ -420,6 +420,25 @@ def ensemble_finalize(sum_ab, sum_aa, sum_bb, n_pairs, bg=None, dc_zero=False, e
     return R[0], R[1], R[2], norm
 
 
+def image_method_means(batches_a, batches_b):
+    """Phase A of the two-sweep 'image' background methods: the float32 frame sums
+    of each batch (numpy sum over the pair axis, cpu_ensemble.py:1176-1177), summed
+    across batches in float32 (dask_pipeline.py:1028-1033, 806-830), divided by the
+    pair count and cast to float32 (pivtools_core/ensemble.py:199-200)."""
+    tot, n = [None, None], 0
+    for A, B in zip(batches_a, batches_b):
+        for k, F in enumerate((A, B)):
+            s = np.asarray(F, np.float32).sum(axis=0)
+            tot[k] = s.copy() if tot[k] is None else tot[k] + s
+        n += np.asarray(A).shape[0]
+    return (tot[0] / n).astype(np.float32), (tot[1] / n).astype(np.float32)
+
+
+def center_frames(frames, mean):
+    """Phase B's `images -= A_mean` in float32 (cpu_ensemble.py:1290-1291)."""
+    return np.asarray(frames, np.float32) - np.asarray(mean, np.float32)[None]
+
+
 # ---------------------------------------------------------------------------
 # Camera payload decode (pivtools_core/image_handling/readers/pivraw_reader.py:896-960,
 # set_reader.py:1296-1345)

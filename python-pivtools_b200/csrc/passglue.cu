@@ -1370,6 +1370,19 @@ __global__ void frame_mean_kernel(const float *__restrict__ sum, long long npix,
         out[p] = sum[p] / n;
 }
 
+// dst[k] = src[k] - mean for n frames: one float32 subtraction per pixel, the
+// reference's in-place `images -= A_mean` of the 'image' background methods
+// (cpu_ensemble.py:1290-1291).  dst may equal src.
+__global__ void center_frames_kernel(const float *src, long long src_stride, int n_frames, long long npix,
+                                     const float *__restrict__ mean, float *dst, long long dst_stride)
+{
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npix;
+         p += (long long)gridDim.x * blockDim.x) {
+        const float m = __ldg(mean + p);
+        for (int k = 0; k < n_frames; ++k) dst[(long long)k * dst_stride + p] = src[(long long)k * src_stride + p] - m;
+    }
+}
+
 struct FinParams {
     const float *sum_ab, *sum_aa, *sum_bb;     // (n_win, h, w) accumulated sums
     const float *bg_ab, *bg_aa, *bg_bb;        // background planes or null
@@ -1444,6 +1457,21 @@ PIV_EXPORT int pivb_frame_mean_dev(const float *sum, long long npix, int n, floa
     const long long want = (npix + 255) / 256;
     const unsigned grid = (unsigned)(want < 148 * 16 ? want : 148 * 16);
     frame_mean_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(sum, npix, (float)n, out);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
+// Mean-image subtraction of the two-sweep 'image' background methods: dst frame
+// k = src frame k - mean, n_frames frames of npix pixels at the given strides
+// (in place when dst == src; otherwise the ranges must not overlap).
+PIV_EXPORT int pivb_center_frames_dev(const float *src, long long src_stride, int n_frames, long long npix,
+                                      const float *mean, float *dst, long long dst_stride, void *stream)
+{
+    if (n_frames <= 0 || npix <= 0 || src_stride < npix || dst_stride < npix || !src || !mean || !dst) return 1;
+    if (dst == src && dst_stride != src_stride) return 1;
+    const long long want = (npix + 255) / 256;
+    const unsigned grid = (unsigned)(want < 148 * 16 ? want : 148 * 16);
+    center_frames_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(src, src_stride, n_frames, npix, mean, dst,
+                                                                 dst_stride);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 

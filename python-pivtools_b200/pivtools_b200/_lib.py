@@ -211,6 +211,8 @@ def pass_lib() -> ctypes.CDLL:
     L.pivb_frame_sum_dev.restype = ci
     L.pivb_frame_mean_dev.argtypes = [vp, cll, ci, vp, vp]
     L.pivb_frame_mean_dev.restype = ci
+    L.pivb_center_frames_dev.argtypes = [vp, cll, ci, cll, vp, vp, cll, vp]
+    L.pivb_center_frames_dev.restype = ci
     L.pivb_ensemble_finalize_dev.argtypes = [vp, vp, vp, vp, vp, vp, ci, ci, ci, ci, ci, vp, vp, vp, vp, vp, vp, vp]
     L.pivb_ensemble_finalize_dev.restype = ci
     L.pivb_decode_frames_dev.argtypes = [vp, cll, ci, ci, ci, ci, ci, vp, cll, ci, ci, vp, cll, vp]

@@ -8,6 +8,10 @@ kspace_lm_fitting.py:804-961):
   accumulate  per batch of pairs: the AB, AA and BB correlation sums of every
               window (bulkxcorr2d_accumulate_triple, Kahan-compensated FP32 across
               batches) and the frame sums for the mean images;
+  two sweeps  the 'image' background methods (pivtools_core/ensemble.py:142-204,
+              cpu_ensemble.py:1104-1330): a first sweep sums the frames only
+              (accumulate_means), end_means forms the mean images, and the second
+              sweep (accumulate) correlates each frame minus its mean image;
   finalise    mean images, their correlation as the background term ('correlation'
               methods), the per-window plane-mean removal ('+dc_zero'), the
               optional pair-count envelope divide, the normalisation by the auto
@@ -28,11 +32,16 @@ from . import _lib, geometry
 
 _METHODS = {
     # method: (per-pair window-mean removal in the correlator, subtract the
-    #          mean-image correlation at finalise, zero the plane means)
-    "correlation": (0, True, False),
-    "correlation+dc_zero": (0, True, True),
-    "window_mean": (1, False, False),
-    "correlation+window_mean": (1, True, False),
+    #          mean-image correlation at finalise, zero the plane means, two
+    #          sweeps with the mean images subtracted from each frame)
+    # (pivtools_core/config.py:2495-2631, single_pass_accumulator.py:575-680)
+    "correlation": (0, True, False, False),
+    "correlation+dc_zero": (0, True, True, False),
+    "window_mean": (1, False, False, False),
+    "correlation+window_mean": (1, True, False, False),
+    "image": (0, False, False, True),
+    "image+window_mean": (1, False, False, True),
+    "image+dc_zero": (0, False, True, True),
 }
 
 
@@ -61,13 +70,14 @@ class EnsemblePIV:
         import torch
 
         if background not in _METHODS:
-            raise ValueError(f"background method {background!r} not supported on the GPU path "
-                             f"(supported: {sorted(_METHODS)})")
+            raise ValueError(f"Invalid ensemble_background_subtraction_method {background!r}. "
+                             f"Must be one of {sorted(_METHODS)}")
         self.torch = torch
         self.device = torch.device("cuda" if device is None else device)
         self.H, self.W = image_shape
         self.win = tuple(window)
-        self.mean_subtract, self.use_bg, self.dc_zero = _METHODS[background]
+        self.mean_subtract, self.use_bg, self.dc_zero, self.two_sweep = _METHODS[background]
+        self.background = background
         self.grid = geometry.compute_window_centers(image_shape, self.win, overlap)
         g = self.grid
         self.n_win = g.n_win_y * g.n_win_x
@@ -94,6 +104,9 @@ class EnsemblePIV:
         sb = int(self.Lx.pivb_accumulate_scratch_bytes(h, self.n_win))
         self.scratch = torch.empty(max(sb, 256), dtype=torch.uint8, device=dev)
         self.n_pairs = 0
+        self.n_means = 0              # pairs of the first sweep (two-sweep methods)
+        self.means_ready = False
+        self._centered = None         # (2, n, H, W) centred frames of the second sweep
         # zero fills above ran on the construction stream: finish them before use
         # from another stream
         torch.cuda.current_stream(self.device).synchronize()
@@ -110,6 +123,8 @@ class EnsemblePIV:
         for t in (self.sums, self.comp, self.fsum, self.fcomp):
             t.zero_()
         self.n_pairs = 0
+        self.n_means = 0
+        self.means_ready = False
 
     def _triple(self, A, B, n, mean_subtract, out, comp, s):
         g = self.grid
@@ -122,15 +137,101 @@ class EnsemblePIV:
             None if comp is None else comp.data_ptr(), self.scratch.data_ptr(), self.scratch.numel(), s),
             "accumulate_triple")
 
-    def accumulate(self, A, B):
-        """Add a batch of pairs: A, B (n, H, W) float32 CUDA tensors."""
-        n = int(A.shape[0])
-        s = self._stream()
-        self._triple(A, B, n, self.mean_subtract, self.sums, self.comp, s)
+    def _frame_sums(self, A, B, n, s):
         npix = self.H * self.W
         for k, F in enumerate((A, B)):
             self._ok(self.Lp.pivb_frame_sum_dev(F.data_ptr(), npix, n, npix, self.fsum[k].data_ptr(),
                                                 self.fcomp[k].data_ptr(), s), "frame sum")
+
+    def _check_batch(self, A, B):
+        torch = self.torch
+        if A.shape != B.shape or A.dim() != 3 or tuple(A.shape[1:]) != (self.H, self.W):
+            raise ValueError(f"frames must be (n, {self.H}, {self.W}) pairs of one shape")
+        if A.dtype != torch.float32 or B.dtype != torch.float32 or not (A.is_contiguous() and B.is_contiguous()):
+            raise ValueError("frames must be contiguous float32 tensors")
+
+    def accumulate_means(self, A, B):
+        """First sweep of the 'image' methods: add a batch of pairs (n, H, W)
+        float32 to the frame sums only (compute_warp_sums_only,
+        cpu_ensemble.py:1104-1190)."""
+        if not self.two_sweep:
+            raise ValueError(f"accumulate_means belongs to the two-sweep 'image' methods, not {self.background!r}")
+        if self.means_ready:
+            raise RuntimeError("the first sweep is closed (end_means was called); reset() starts over")
+        self._check_batch(A, B)
+        n = int(A.shape[0])
+        self._frame_sums(A, B, n, self._stream())
+        self.n_means += n
+
+    def end_means(self):
+        """Close the first sweep: the mean images sum / n (pivtools_core/ensemble.py:
+        199-200) of this process's pairs."""
+        return self._end_means(self.fsum, self.n_means)
+
+    def end_means_distributed(self, group=None):
+        """Close the first sweep across the ranks of `group` (pairs sharded): one
+        all-reduce combines the frame sums and pair counts, so every rank
+        subtracts the ensemble's mean images (the reference reduces the workers'
+        warp sums the same way, pivtools_core/ensemble.py:179-200)."""
+        from . import ensemble_dist as ed
+
+        if not self.two_sweep:
+            raise ValueError(f"end_means belongs to the two-sweep 'image' methods, not {self.background!r}")
+        fsum, n = ed.all_reduce_frame_sums(self.fsum, self.fcomp, self.n_means, group)
+        return self._end_means(fsum, n)
+
+    def _end_means(self, fsum, n):
+        if not self.two_sweep:
+            raise ValueError(f"end_means belongs to the two-sweep 'image' methods, not {self.background!r}")
+        if self.means_ready:
+            raise RuntimeError("end_means was already called")
+        if n == 0:
+            raise RuntimeError("end_means before any accumulate_means")
+        s = self._stream()
+        npix = self.H * self.W
+        for k in range(2):
+            self._ok(self.Lp.pivb_frame_mean_dev(fsum[k].data_ptr(), npix, n, self.fmean[k].data_ptr(), s),
+                     "frame mean")
+        self.n_means = n
+        self.means_ready = True
+        return {"A_mean": self.fmean[0].view(self.H, self.W), "B_mean": self.fmean[1].view(self.H, self.W),
+                "n_pairs": n}
+
+    def _center(self, A, B, n, s, in_place):
+        """A - A_mean, B - B_mean (cpu_ensemble.py:1290-1291): in place for the
+        pipeline's own staging buffers, else into a scratch pair of batches."""
+        npix = self.H * self.W
+        if in_place:
+            outs = (A, B)
+        else:
+            if self._centered is None or self._centered.shape[1] < n:
+                self._centered = self.torch.empty((2, n, self.H, self.W), dtype=self.torch.float32,
+                                                  device=self.device)
+            outs = (self._centered[0, :n], self._centered[1, :n])
+        for k, (F, O) in enumerate(zip((A, B), outs)):
+            self._ok(self.Lp.pivb_center_frames_dev(F.data_ptr(), npix, n, npix, self.fmean[k].data_ptr(),
+                                                    O.data_ptr(), npix, s), "centre frames")
+        return outs
+
+    def accumulate(self, A, B):
+        """Add a batch of pairs: A, B (n, H, W) float32 CUDA tensors.  For the
+        'image' methods this is the second sweep: each frame minus the mean
+        images of the first is correlated (correlate_mean_subtracted_batch,
+        cpu_ensemble.py:1192-1330); the caller's tensors are not modified."""
+        self._accumulate(A, B, in_place=False)
+
+    def _accumulate(self, A, B, in_place):
+        self._check_batch(A, B)
+        n = int(A.shape[0])
+        s = self._stream()
+        if self.two_sweep:
+            if not self.means_ready:
+                raise RuntimeError(f"{self.background!r} sweeps twice: accumulate_means over every pair, then "
+                                   "end_means, before accumulate")
+            A, B = self._center(A, B, n, s, in_place)
+        else:
+            self._frame_sums(A, B, n, s)
+        self._triple(A, B, n, self.mean_subtract, self.sums, self.comp, s)
         self.n_pairs += n
 
     def accumulate_host(self, Ah, Bh, chunk: int = 16):
@@ -138,7 +239,18 @@ class EnsemblePIV:
         cross PCIe on a copy stream into two alternating staging slots while the
         previous chunk is converted to float32 on the GPU and accumulated on the
         caller's stream.  Equal, bit for bit, to accumulate() called on the same
-        frames in float32, chunk by chunk."""
+        frames in float32, chunk by chunk (for the 'image' methods the mean images
+        are subtracted in the staging buffers)."""
+        self._stream_host(Ah, Bh, chunk, lambda a, b: self._accumulate(a, b, in_place=True))
+
+    def accumulate_means_host(self, Ah, Bh, chunk: int = 16):
+        """The first sweep of the 'image' methods from page-locked uint16 host
+        frames, staged as in accumulate_host."""
+        if not self.two_sweep:
+            raise ValueError(f"accumulate_means belongs to the two-sweep 'image' methods, not {self.background!r}")
+        self._stream_host(Ah, Bh, chunk, self.accumulate_means)
+
+    def _stream_host(self, Ah, Bh, chunk, sink):
         import ctypes as C
 
         torch = self.torch
@@ -174,7 +286,7 @@ class EnsemblePIV:
                 self._ok(self.Lp.pivb_u16_to_f32_dev(st["u16"][sl][j].data_ptr(), st["f32"][j].data_ptr(), k * H * W,
                                                      cs), "u16 -> f32")
             st["ev_conv"][sl].record(comp)
-            self.accumulate(st["f32"][0][:k], st["f32"][1][:k])
+            sink(st["f32"][0][:k], st["f32"][1][:k])
 
     def finalize(self):
         """Background, DC zero, envelope, normalisation -> FP64 planes (AA, BB, AB)

@@ -90,6 +90,19 @@ def exchange_sums(sums, comps, fsum, fcomp, n_pairs, n_win, hw, group=None):
     return block, fr.float(), int(round(n.item())), blocks[rank]
 
 
+def all_reduce_frame_sums(fsum, fcomp, n_pairs, group=None):
+    """Frame sums (2, H * W) float32 with their Kahan compensations and the pair
+    count, summed over the ranks (the first sweep of the 'image' background
+    methods).  Returns (frame sums float32, total pair count)."""
+    import torch
+
+    fr = fsum.double() - fcomp.double()
+    _all_reduce(fr, group)
+    n = torch.tensor([float(n_pairs)], dtype=torch.float64, device=fsum.device)
+    _all_reduce(n, group)
+    return fr.float(), int(round(n.item()))
+
+
 def gather_rows(local, n_win, group=None):
     """All-gather per-window rows (n_block, ...) of every rank into (n_win, ...)."""
     import torch

@@ -36,7 +36,8 @@ def _worker(rank, world, port, q):
         block, fr, n_tot, (a, b) = ed.exchange_sums(sums, comps, fsum, fcomp, n, N_WIN, HW)
         rows = torch.arange(a, b, dtype=torch.float64)[:, None] * torch.ones((1, 16), dtype=torch.float64)
         full = ed.gather_rows(rows, N_WIN)
-        q.put((rank, block.numpy(), fr.numpy(), n_tot, (a, b), full.numpy()))
+        fm, n_m = ed.all_reduce_frame_sums(fsum, fcomp, n, None)     # first sweep of the 'image' methods
+        q.put((rank, block.numpy(), fr.numpy(), n_tot, (a, b), full.numpy(), fm.numpy(), n_m))
     finally:
         torch.distributed.destroy_process_group()
 
@@ -73,8 +74,9 @@ def test_two_rank_exchange_gloo():
     data = [_rank_data(r) for r in range(world)]
     tot = sum((d[0].double() - d[1].double()) for d in data).reshape(3, N_WIN, HW)
     ftot = sum((d[2].double() - d[3].double()) for d in data)
-    for rank, block, fr, n_tot, (a, b), full in res:
-        assert n_tot == sum(d[4] for d in data)
+    for rank, block, fr, n_tot, (a, b), full, fm, n_m in res:
+        assert n_tot == n_m == sum(d[4] for d in data)
         np.testing.assert_allclose(block, tot[:, a:b].float().numpy(), rtol=1e-6, atol=1e-6)
         np.testing.assert_allclose(fr, ftot.float().numpy(), rtol=1e-6, atol=1e-6)
+        assert np.array_equal(fm, fr)
         assert np.array_equal(full[:, 0], np.arange(N_WIN, dtype=np.float64))

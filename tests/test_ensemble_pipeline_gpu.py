@@ -17,15 +17,27 @@ def _pairs(n, shape, seed):
     return np.stack([p[0] for p in out]).astype(np.float32), np.stack([p[1] for p in out]).astype(np.float32)
 
 
-@pytest.mark.parametrize("method,env", [("correlation+dc_zero", False), ("correlation", True), ("window_mean", False)])
+@pytest.mark.parametrize("method,env", [("correlation+dc_zero", False), ("correlation", True), ("window_mean", False),
+                                        ("image", False), ("image+window_mean", True), ("image+dc_zero", False)])
 def test_ensemble_pass_matches_oracle(oracle, cuda, method, env):
     import torch
 
     shape, win = (128, 160), (16, 16)
     A, B = _pairs(10, shape, 700)
     ep = ensemble.EnsemblePIV(shape, win, 75, "square", background=method, envelope_divide=env, device=cuda)
-    for sl in (slice(0, 4), slice(4, 10)):                      # two batches
-        ep.accumulate(torch.tensor(A[sl], device=cuda), torch.tensor(B[sl], device=cuda))
+    ms, use_bg, dc, two = ensemble._METHODS[method]
+    if two:                                  # stationary structure for the mean images to remove
+        A += np.linspace(0, 40, shape[1], dtype=np.float32)[None, None]
+        B += np.linspace(0, 40, shape[1], dtype=np.float32)[None, None]
+    batches = (slice(0, 4), slice(4, 10))
+    dA = [torch.tensor(A[sl], device=cuda) for sl in batches]
+    dB = [torch.tensor(B[sl], device=cuda) for sl in batches]
+    if two:                                                     # first sweep: the mean images
+        for a, b in zip(dA, dB):
+            ep.accumulate_means(a, b)
+        means = ep.end_means()
+    for a, b in zip(dA, dB):                                    # two batches
+        ep.accumulate(a, b)
     fin = ep.finalize()
     fit = ep.fit()
     torch.cuda.synchronize()
@@ -33,8 +45,15 @@ def test_ensemble_pass_matches_oracle(oracle, cuda, method, env):
     g = ep.grid
     w = geometry.window_weight(win, "square")
     mask = np.zeros((g.n_win_y, g.n_win_x), np.float32)
-    ms, use_bg, dc = ensemble._METHODS[method]
-    s_ab, s_aa, s_bb = oracle.accumulate_triple(A, B, mask, g.win_ctrs_x, g.win_ctrs_y, win, w, w, w, w,
+    CA, CB = A, B
+    if two:
+        mA, mB = oracle.image_method_means([A[sl] for sl in batches], [B[sl] for sl in batches])
+        assert means["n_pairs"] == 10
+        np.testing.assert_allclose(means["A_mean"].cpu().numpy(), mA, rtol=1e-6)
+        np.testing.assert_allclose(means["B_mean"].cpu().numpy(), mB, rtol=1e-6)
+        CA, CB = oracle.center_frames(A, mA), oracle.center_frames(B, mB)
+        assert np.array_equal(dA[1].cpu().numpy(), A[4:10])     # the caller's frames are untouched
+    s_ab, s_aa, s_bb = oracle.accumulate_triple(CA, CB, mask, g.win_ctrs_x, g.win_ctrs_y, win, w, w, w, w,
                                                 mean_subtract=ms)
     n_win = g.n_win_y * g.n_win_x
     bg = None
@@ -65,9 +84,60 @@ def test_ensemble_pass_matches_oracle(oracle, cuda, method, env):
     np.testing.assert_allclose(gg[:, 9:12], go[:, 9:12], rtol=5e-3, atol=1e-4)
 
 
-def test_ensemble_rejects_two_sweep_methods(cuda):
-    with pytest.raises(ValueError):
-        ensemble.EnsemblePIV((64, 64), (16, 16), 75, "square", background="image", device=cuda)
+def test_two_sweep_order_and_refusals(cuda):
+    import torch
+
+    with pytest.raises(ValueError, match="Invalid ensemble_background_subtraction_method"):
+        ensemble.EnsemblePIV((64, 64), (16, 16), 75, "square", background="image+correlation", device=cuda)
+    a = torch.rand((2, 64, 64), device=cuda)
+    ep = ensemble.EnsemblePIV((64, 64), (16, 16), 75, "square", background="image", device=cuda)
+    with pytest.raises(RuntimeError, match="sweeps twice"):
+        ep.accumulate(a, a)                                    # second sweep before the means
+    with pytest.raises(RuntimeError, match="before any accumulate_means"):
+        ep.end_means()
+    ep.accumulate_means(a, a)
+    ep.end_means()
+    with pytest.raises(RuntimeError, match="closed"):
+        ep.accumulate_means(a, a)
+    with pytest.raises(RuntimeError, match="already"):
+        ep.end_means()
+    with pytest.raises(ValueError, match="float32"):
+        ep.accumulate(a.double(), a.double())
+    ep.accumulate(a, a)
+    ep.reset()
+    assert not ep.means_ready and ep.n_pairs == 0
+    plain = ensemble.EnsemblePIV((64, 64), (16, 16), 75, "square", background="correlation", device=cuda)
+    with pytest.raises(ValueError, match="two-sweep"):
+        plain.accumulate_means(a, a)
+
+
+def test_image_method_from_uint16_host_frames(cuda):
+    """Both sweeps of the 'image' method streamed from page-locked uint16 host
+    frames equal the float32 device path bit for bit."""
+    import torch
+
+    shape, win = (128, 160), (16, 16)
+    A, B = _pairs(7, shape, 740)
+    A16 = np.clip(np.round(A), 0, 65535).astype(np.int32)
+    B16 = np.clip(np.round(B), 0, 65535).astype(np.int32)
+    Ah = torch.tensor(A16).to(torch.uint16).pin_memory()
+    Bh = torch.tensor(B16).to(torch.uint16).pin_memory()
+    host = ensemble.EnsemblePIV(shape, win, 75, "square", background="image+dc_zero", device=cuda)
+    dev = ensemble.EnsemblePIV(shape, win, 75, "square", background="image+dc_zero", device=cuda)
+    host.accumulate_means_host(Ah, Bh, chunk=3)
+    host.end_means()
+    host.accumulate_host(Ah, Bh, chunk=3)
+    fa = [torch.tensor(A16[c0:c0 + 3], dtype=torch.float32, device=cuda) for c0 in range(0, 7, 3)]
+    fb = [torch.tensor(B16[c0:c0 + 3], dtype=torch.float32, device=cuda) for c0 in range(0, 7, 3)]
+    for a, b in zip(fa, fb):
+        dev.accumulate_means(a, b)
+    dev.end_means()
+    for a, b in zip(fa, fb):
+        dev.accumulate(a, b)
+    torch.cuda.synchronize()
+    assert host.n_pairs == dev.n_pairs == 7 and host.n_means == 7
+    for x, y in ((host.sums, dev.sums), (host.comp, dev.comp), (host.fmean, dev.fmean)):
+        assert torch.equal(x, y)
 
 
 def test_distributed_finalise_single_rank_equals_local(cuda):
