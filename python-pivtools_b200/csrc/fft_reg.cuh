@@ -102,10 +102,10 @@ struct RegFFT {
     }
 };
 
-// Cross-lane completion of a length N = P*M transform.  On entry lane p (p = lane
-// index mod P; the P lanes of one transform are adjacent) holds the length-M
-// transform of samples x[P*n + p].  On exit it holds X[M*q + k], k = 0..M-1, for
-// the block q = out_block<P>(p).
+// Cross-lane completion of a length N = P*M transform.  On entry lane p holds
+// the length-M transform of samples x[P*n + p]; the P lanes of one transform are
+// adjacent (lane index mod P = p), or, for P = 2 with XM = 16, lanes l and l + 16.
+// On exit it holds X[M*q + k], k = 0..M-1, for the block q = out_block<P>(p).
 template <int P>
 __device__ __forceinline__ int out_block(int p)
 {
@@ -113,7 +113,7 @@ __device__ __forceinline__ int out_block(int p)
     else return p;
 }
 
-template <int P, int M, int SIGN>
+template <int P, int M, int SIGN, int XM = 1>
 __device__ __forceinline__ void lane_combine(float2 (&y)[M], int p)
 {
     if constexpr (P == 1) {
@@ -139,8 +139,8 @@ __device__ __forceinline__ void lane_combine(float2 (&y)[M], int p)
 #pragma unroll
             for (int k = 0; k < M; ++k) {
                 float2 o;
-                o.x = __shfl_xor_sync(0xffffffffu, y[k].x, 1);
-                o.y = __shfl_xor_sync(0xffffffffu, y[k].y, 1);
+                o.x = __shfl_xor_sync(0xffffffffu, y[k].x, XM);
+                o.y = __shfl_xor_sync(0xffffffffu, y[k].y, XM);
                 y[k] = p ? c_sub(o, y[k]) : c_add(y[k], o);
             }
         } else {  // P == 4: radix-2 over p1 (xor 2), twiddle, radix-2 over p0 (xor 1)

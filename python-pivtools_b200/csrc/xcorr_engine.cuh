@@ -49,12 +49,19 @@ struct WinGeo {
     // distinct words one bank holds among 16 lanes, summed over the two halves.
     // Chosen per size (cost summed over the phases, 14 = no conflict): 48 ->
     // ST 50, skew per 32 columns (19.5); 96 -> 100, rotation 4, skew per 32
-    // (20.0; the former 102 ran 6% longer); 128 at two lanes -> 134 without
-    // rotation or skew (22; the skewed 133 scored 28 and ran 6% longer).  At 128
-    // px rotation 8 with a skew per 64 columns scores 16.6 but measured no faster:
-    // its index arithmetic costs what the conflicts did.
-    static constexpr int ST = N + ((P == 1) ? 1 : (P == 2 ? (N == 128 ? 6 : 2) : 4));
-    static constexpr int SKEW = (P == 1 || (P == 2 && N == 128)) ? 0 : 1;
+    // (20.0; the former 102 ran 6% longer).  128 px takes the split lane layout
+    // below with ST 129 (no conflict in any phase): shared-memory bank conflicts
+    // fell from 35.6 M to 4.0 M of the launch's wavefronts and the pass from
+    // 1.157 to 1.051 ms against the adjacent-lane layout's best stride, 134.
+    // At 128 px the two lanes of a column sit in opposite half-warps (lane l and
+    // l + 16), so each half-warp holds 16 consecutive lines of one sample block:
+    // with an odd stride every store and load phase is then free of bank
+    // conflicts (a 64-bit access is served per half-warp; rows i apart start
+    // 2 * ST * i words apart, distinct even banks for 16 rows).
+    static constexpr bool SPLIT = (N == 128);
+    static constexpr int XM = SPLIT ? 16 : 1;                           // partner-lane xor mask
+    static constexpr int ST = N + ((P == 1 || SPLIT) ? 1 : (P == 2 ? 2 : 4));
+    static constexpr int SKEW = (P == 1 || SPLIT) ? 0 : 1;
     static constexpr int SKB = 5;
     static constexpr int ROT = (P == 4) ? 4 : 0;
     static_assert(N - 1 + SKEW * ((N - 1) >> SKB) < ST, "a skewed plane row must fit its stride");
@@ -169,6 +176,9 @@ __device__ __forceinline__ void lane_slot(int t, int &line, int &p)
     if constexpr (G::P == 1) {
         line = t;
         p = 0;
+    } else if constexpr (G::SPLIT) {
+        line = (t >> 5) * 16 + (t & 15);
+        p = (t >> 4) & 1;
     } else {
         line = (t >> 5) * (32 / G::P) + (t & 31) / G::P;
         p = t % G::P;
@@ -197,7 +207,7 @@ __device__ __forceinline__ void fft2_forward(const Group<N> &g, float2 *S, const
 #pragma unroll
     for (int n = 0; n < M; ++n) z[n] = make_float2(a[n], b[n]);
     RegFFT<M, -1>::run(z);                       // column transform (over rows)
-    lane_combine<P, M, -1>(z, p);
+    lane_combine<P, M, -1, G::XM>(z, p);
     if (active) {
 #pragma unroll
         for (int k = 0; k < M; ++k) S[(M * q + k) * ST + line] = z[k];
@@ -208,7 +218,7 @@ __device__ __forceinline__ void fft2_forward(const Group<N> &g, float2 *S, const
         for (int n = 0; n < M; ++n) z[n] = S[line * ST + P * n + p];
     }
     RegFFT<M, -1>::run(z);                       // row transform
-    lane_combine<P, M, -1>(z, p);
+    lane_combine<P, M, -1, G::XM>(z, p);
     g.sync();
     if (active) {
 #pragma unroll
@@ -265,7 +275,7 @@ __device__ __forceinline__ void fft2_inverse(const Group<N> &g, float2 *S, float
     lane_slot<N>(active ? g.t : 0, line, p);
     const int q = out_block<P>(p);
     RegFFT<M, +1>::run(z);
-    lane_combine<P, M, +1>(z, p);
+    lane_combine<P, M, +1, G::XM>(z, p);
     if (active) {
 #pragma unroll
         for (int k = 0; k < M; ++k) S[line * ST + M * q + k] = z[k];
@@ -276,7 +286,7 @@ __device__ __forceinline__ void fft2_inverse(const Group<N> &g, float2 *S, float
         for (int n = 0; n < M; ++n) z[n] = S[(P * n + p) * ST + line];
     }
     RegFFT<M, +1>::run(z);
-    lane_combine<P, M, +1>(z, p);
+    lane_combine<P, M, +1, G::XM>(z, p);
     g.sync();
 }
 
@@ -341,7 +351,7 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
     for (int pass = 0;; ++pass) {
         RegFFT<M, -1>::run(z);
         if constexpr (G::TW_BYTES > 0) lane_combine_fwd_tab<P, M>(z, p, tw);
-        else lane_combine<P, M, -1>(z, p);
+        else lane_combine<P, M, -1, G::XM>(z, p);
         if (pass == 3) break;
         g.sync();
         if (active) {
