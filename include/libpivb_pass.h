@@ -74,16 +74,26 @@ int pivb_frame_mean_dev(const float *sum, long long npix, int n, float *out, voi
 int pivb_center_frames_dev(const float *src, long long src_stride, int n_frames, long long npix, const float *mean,
                            float *dst, long long dst_stride, void *stream);
 
-/* Finalise of one ensemble pass (std mode): average the accumulated AB/AA/BB sums
- * of n_win windows of h x w over n_pairs, subtract the background planes (all three
- * or none), optionally zero each plane's mean (the '+dc_zero' methods), divide by
- * the pair-count envelopes (nullable; env_ab defaults to env_auto), normalise by
+/* Finalise of one ensemble pass: average the accumulated AB/AA/BB sums of n_win
+ * windows of h x w over n_pairs, subtract the background planes (all three or
+ * none), optionally zero each plane's mean (the '+dc_zero' methods), divide by the
+ * pair-count envelopes (nullable; env_ab defaults to env_auto), scale the AB plane
+ * by ab_scale (single mode: sum-window area / particle-window area,
+ * single_pass_accumulator.py:760-780; 1 in std mode), normalise by
  * sqrt(max(AA_c BB_c, 1e-12)) at the centre bin and write FP64 planes for
  * pivb_kspace_fit_dev.  norm (nullable) receives the per-window factors. */
 int pivb_ensemble_finalize_dev(const float *sum_ab, const float *sum_aa, const float *sum_bb, const float *bg_ab,
                                const float *bg_aa, const float *bg_bb, int n_pairs, int n_win, int h, int w,
                                int dc_zero, const float *env_auto, const float *env_ab, double *out_ab,
-                               double *out_aa, double *out_bb, float *norm, void *stream);
+                               double *out_aa, double *out_bb, float *norm, float ab_scale, void *stream);
+
+/* Ensemble single mode: zero-padded copies of n_frames frames (H x W at
+ * src_stride elements) into Hp x Wp frames at dst_stride, the source placed at
+ * (pad_top, pad_left); with a mean frame (nullable) each source pixel has it
+ * subtracted first, the 'image' methods' order (cpu_ensemble.py:1290-1324,
+ * pivtools_core/window_utils.py:466-525). */
+int pivb_pad_frames_dev(const float *src, long long src_stride, int n_frames, int H, int W, const float *mean,
+                        int pad_top, int pad_left, float *dst, int Hp, int Wp, long long dst_stride, void *stream);
 
 /* Decode n_frames camera payloads (frame k at raw + k * stride bytes) into float32
  * frames, as the reference's PIVTOOLs Acquisition reader does on the host

@@ -396,11 +396,13 @@ def zero_plane_means(planes):
     return p - p.mean(axis=(1, 2), keepdims=True, dtype=np.float64).astype(np.float32)
 
 
-def ensemble_finalize(sum_ab, sum_aa, sum_bb, n_pairs, bg=None, dc_zero=False, env_auto=None, env_ab=None):
+def ensemble_finalize(sum_ab, sum_aa, sum_bb, n_pairs, bg=None, dc_zero=False, env_auto=None, env_ab=None,
+                      ab_scale=None):
     """Averaged, background-subtracted, optionally DC-zeroed and envelope-divided,
     normalised ensemble planes, in float32 as the reference computes them
-    (single_pass_accumulator.py:564-800, std mode): R = sum / N - bg; R -= mean;
-    R /= E; R /= sqrt(max(AA_c * BB_c, 1e-12)).  Inputs (n, h, w); returns
+    (single_pass_accumulator.py:564-800): R = sum / N - bg; R -= mean; R /= E;
+    single mode: R_AB *= sum area / particle area (ab_scale, :760-780);
+    R /= sqrt(max(AA_c * BB_c, 1e-12)).  Inputs (n, h, w); returns
     (R_AA, R_BB, R_AB, norm)."""
     n = np.float32(n_pairs)
     R = [np.asarray(s, np.float32) / n for s in (sum_aa, sum_bb, sum_ab)]
@@ -416,6 +418,8 @@ def ensemble_finalize(sum_ab, sum_aa, sum_bb, n_pairs, bg=None, dc_zero=False, e
     h, w = R[0].shape[1:]
     c = (h // 2, w // 2)
     norm = np.sqrt(np.maximum(R[0][:, c[0], c[1]] * R[1][:, c[0], c[1]], np.float32(1e-12)))
+    if ab_scale is not None:
+        R[2] = R[2] * np.float32(ab_scale)
     R = [r / norm[:, None, None] for r in R]
     return R[0], R[1], R[2], norm
 

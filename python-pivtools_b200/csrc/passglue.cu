@@ -1391,6 +1391,7 @@ struct FinParams {
     int n_win, hw, centre, dc_zero;
     double *out_aa, *out_bb, *out_ab;          // normalised planes for the k-space fit
     float *norm;                               // (n_win) normalisation factors, nullable
+    float ab_scale;                            // single mode: sum area / particle area, else 1
 };
 
 // One warp per window; float32 arithmetic in the reference's order.
@@ -1431,6 +1432,7 @@ __global__ void ensemble_finalize_kernel(FinParams p)
             if (bgs[q]) v = v - bgs[q][base + k];
             if (p.dc_zero) v = v - mean[q];
             if (env) v = v / env[k];
+            if (q == 2 && p.ab_scale != 1.0f) v = v * p.ab_scale;     // single_pass_accumulator.py:765-780
             outs[q][base + k] = (double)(v / nf);
         }
     }
@@ -1475,6 +1477,43 @@ PIV_EXPORT int pivb_center_frames_dev(const float *src, long long src_stride, in
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
+// Zero-padded copies of n frames for ensemble single mode
+// (window_utils.py:466-525, apply_single_mode_padding with pad value 0): dst frame
+// k (Hp x Wp) holds src frame k (H x W, minus the mean frame when mean is given,
+// the 'image' methods' subtraction that precedes the padding) at (pad_top,
+// pad_left) and zeros elsewhere.
+__global__ void pad_frames_kernel(const float *__restrict__ src, long long src_stride, int n_frames, int H, int W,
+                                  const float *__restrict__ mean, int pad_top, int pad_left, float *__restrict__ dst,
+                                  int Hp, int Wp, long long dst_stride)
+{
+    const long long npix = (long long)Hp * Wp;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < npix;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(q / Wp) - pad_top, c = (int)(q % Wp) - pad_left;
+        const bool in = r >= 0 && r < H && c >= 0 && c < W;
+        const long long s = (long long)r * W + c;
+        const float m = (in && mean) ? __ldg(mean + s) : 0.0f;
+        for (int k = 0; k < n_frames; ++k)
+            dst[(long long)k * dst_stride + q] = in ? (mean ? src[(long long)k * src_stride + s] - m
+                                                            : src[(long long)k * src_stride + s])
+                                                    : 0.0f;
+    }
+}
+
+PIV_EXPORT int pivb_pad_frames_dev(const float *src, long long src_stride, int n_frames, int H, int W,
+                                   const float *mean, int pad_top, int pad_left, float *dst, int Hp, int Wp,
+                                   long long dst_stride, void *stream)
+{
+    if (n_frames <= 0 || H <= 0 || W <= 0 || pad_top < 0 || pad_left < 0 || !src || !dst) return 1;
+    if (Hp < H + pad_top || Wp < W + pad_left || src_stride < (long long)H * W || dst_stride < (long long)Hp * Wp)
+        return 1;
+    const long long want = ((long long)Hp * Wp + 255) / 256;
+    const unsigned grid = (unsigned)(want < 148 * 16 ? want : 148 * 16);
+    pad_frames_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(src, src_stride, n_frames, H, W, mean, pad_top,
+                                                              pad_left, dst, Hp, Wp, dst_stride);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}
+
 // Finalise of one ensemble pass for n_win windows of h x w planes: average the
 // sums over n_pairs, subtract the background planes (nullable), optionally zero
 // each plane's mean, divide by the envelopes (nullable), normalise by
@@ -1484,13 +1523,15 @@ PIV_EXPORT int pivb_ensemble_finalize_dev(const float *sum_ab, const float *sum_
                                           const float *bg_ab, const float *bg_aa, const float *bg_bb, int n_pairs,
                                           int n_win, int h, int w, int dc_zero, const float *env_auto,
                                           const float *env_ab, double *out_ab, double *out_aa, double *out_bb,
-                                          float *norm, void *stream)
+                                          float *norm, float ab_scale, void *stream)
 {
     if (n_pairs <= 0 || n_win <= 0 || h <= 0 || w <= 0) return 1;
     if (!sum_ab || !sum_aa || !sum_bb || !out_ab || !out_aa || !out_bb) return 1;
     if ((bg_ab == nullptr) != (bg_aa == nullptr) || (bg_aa == nullptr) != (bg_bb == nullptr)) return 1;
+    if (!(ab_scale > 0.0f) || !isfinite(ab_scale)) return 1;
     FinParams p{sum_ab, sum_aa, sum_bb, bg_ab, bg_aa, bg_bb, env_auto, env_ab ? env_ab : env_auto,
-                (float)n_pairs, n_win, h * w, (h / 2) * w + w / 2, dc_zero ? 1 : 0, out_aa, out_bb, out_ab, norm};
+                (float)n_pairs, n_win, h * w, (h / 2) * w + w / 2, dc_zero ? 1 : 0, out_aa, out_bb, out_ab, norm,
+                ab_scale};
     const long long threads = (long long)n_win * 32;
     ensemble_finalize_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(p);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;

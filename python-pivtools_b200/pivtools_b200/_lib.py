@@ -213,7 +213,10 @@ def pass_lib() -> ctypes.CDLL:
     L.pivb_frame_mean_dev.restype = ci
     L.pivb_center_frames_dev.argtypes = [vp, cll, ci, cll, vp, vp, cll, vp]
     L.pivb_center_frames_dev.restype = ci
-    L.pivb_ensemble_finalize_dev.argtypes = [vp, vp, vp, vp, vp, vp, ci, ci, ci, ci, ci, vp, vp, vp, vp, vp, vp, vp]
+    L.pivb_ensemble_finalize_dev.argtypes = [vp, vp, vp, vp, vp, vp, ci, ci, ci, ci, ci, vp, vp, vp, vp, vp, vp,
+                                             ctypes.c_float, vp]
+    L.pivb_pad_frames_dev.argtypes = [vp, cll, ci, ci, ci, vp, ci, ci, vp, ci, ci, cll, vp]
+    L.pivb_pad_frames_dev.restype = ci
     L.pivb_ensemble_finalize_dev.restype = ci
     L.pivb_decode_frames_dev.argtypes = [vp, cll, ci, ci, ci, ci, ci, vp, cll, ci, ci, vp, cll, vp]
     L.pivb_decode_frames_dev.restype = ci

@@ -53,42 +53,97 @@ def pair_envelope(wa, wb, corr_size):
     wb = np.asarray(wb, np.float64)
     h, w = wa.shape
     ch, cw = corr_size
+    if wa.shape != wb.shape:
+        raise ValueError(f"window weights must share a shape, got {wa.shape} vs {wb.shape}")
+    if ch > h or cw > w:
+        raise ValueError(f"corr_size {tuple(corr_size)} exceeds envelope support {(h, w)}")
     full = np.fft.fftshift(np.fft.ifft2(np.fft.fft2(wa, s=(2 * h, 2 * w)) *
                                         np.conj(np.fft.fft2(wb, s=(2 * h, 2 * w)))).real)
     env = full[h - ch // 2:h - ch // 2 + ch, w - cw // 2:w - cw // 2 + cw]
-    env = env / env[ch // 2, cw // 2]
+    centre = env[ch // 2, cw // 2]
+    if abs(centre - env.max()) > 1e-9 * env.max():
+        raise ValueError(f"envelope centre {centre:.12f} != max {env.max():.12f}: centering is off")
+    env = env / centre
     if np.any(env <= 0.0):
         raise ValueError("pair-count envelope has non-positive entries inside the plane")
     return env
 
 
 class EnsemblePIV:
-    """One std-mode ensemble pass over frames of one size on one GPU."""
+    """One ensemble pass over frames of one size on one GPU: std mode (both frames
+    weighted by one window) or single mode (cpu_ensemble.py:188-225, 700-760:
+    frame A weighted by the small window centred in the sum window ('singlepix'),
+    frame B and both auto planes by the whole sum window ('bsingle'), frames
+    zero-padded so the sum window fits around every small window, planes stored
+    at the fitting window)."""
 
     def __init__(self, image_shape, window=(16, 16), overlap=75, window_type="square",
-                 background="correlation+dc_zero", envelope_divide=False, device=None):
+                 background="correlation+dc_zero", envelope_divide=False, device=None, runtype="std",
+                 sum_window=None, fit_window=None, per_pair_normalization=False):
         import torch
 
         if background not in _METHODS:
             raise ValueError(f"Invalid ensemble_background_subtraction_method {background!r}. "
                              f"Must be one of {sorted(_METHODS)}")
+        if runtype not in ("std", "single"):
+            raise ValueError(f"ensemble_type must be 'std' or 'single', got {runtype!r}")
+        if per_pair_normalization and background != "window_mean":
+            # pivtools_core/validation.py:544-552
+            raise ValueError("ensemble_piv.per_pair_normalization requires background_subtraction_method exactly "
+                             f"'window_mean', got {background!r}")
         self.torch = torch
         self.device = torch.device("cuda" if device is None else device)
         self.H, self.W = image_shape
         self.win = tuple(window)
+        self.runtype = runtype
         self.mean_subtract, self.use_bg, self.dc_zero, self.two_sweep = _METHODS[background]
+        self.per_pair_norm = 1 if per_pair_normalization else 0
         self.background = background
-        self.grid = geometry.compute_window_centers(image_shape, self.win, overlap)
+        if runtype == "single":
+            if sum_window is None:
+                raise ValueError("ensemble_sum_window must be defined when using 'single' mode in ensemble_type")
+            self.sum_window = tuple(int(v) for v in sum_window)
+            self.corr = tuple(int(v) for v in (fit_window if fit_window is not None else self.sum_window))
+            if self.corr[0] > self.sum_window[0] or self.corr[1] > self.sum_window[1]:
+                raise ValueError(f"sum_fitting_window {self.corr} must be <= sum_window {self.sum_window}")
+            # grid and padding of the padded frame (window_utils.py:276-463)
+            self.grid, self.padding = geometry.compute_window_centers_single_mode(image_shape, self.win,
+                                                                                  self.sum_window, overlap)
+            wa = geometry.window_weight(self.win, "singlepix", self.sum_window)
+            wb = geometry.window_weight(self.sum_window, "bsingle", self.sum_window)
+            self.comp_size = self.sum_window
+            # the AB plane's normalisation correction (single_pass_accumulator.py:760-780)
+            self.ab_scale = float(np.float32((self.sum_window[0] * self.sum_window[1]) / (self.win[0] * self.win[1])))
+        else:
+            if fit_window is not None or sum_window is not None:
+                raise ValueError("sum_window and fit_window belong to single mode")
+            self.sum_window = None
+            self.corr = self.win
+            self.grid = geometry.compute_window_centers(image_shape, self.win, overlap)
+            self.padding = (0, 0, 0, 0)
+            wa = wb = geometry.window_weight(self.win, window_type)
+            self.comp_size = self.win
+            self.ab_scale = 1.0
+        if self.comp_size[0] != self.comp_size[1]:
+            raise ValueError(f"the GPU accumulation takes square computation windows, got {self.comp_size}")
+        pt, pb, pl, pr = self.padding
+        self.Hp, self.Wp = self.H + pt + pb, self.W + pl + pr       # frame size the correlator reads
         g = self.grid
         self.n_win = g.n_win_y * g.n_win_x
-        h, w = self.win
+        h, w = self.corr
         dev, f32 = self.device, torch.float32
-        wt = geometry.window_weight(self.win, window_type)
-        self.weight = torch.tensor(wt, dtype=f32, device=dev)
+        self.weight_a = torch.tensor(wa, dtype=f32, device=dev)       # AB weight of frame A
+        self.weight = torch.tensor(wb, dtype=f32, device=dev)         # AB weight of frame B, both auto planes
+        self._wb_host = np.asarray(wb, np.float64)
         self.cx = torch.tensor(g.win_ctrs_x, dtype=f32, device=dev)
         self.cy = torch.tensor(g.win_ctrs_y, dtype=f32, device=dev)
-        self.env = (torch.tensor(pair_envelope(wt, wt, self.win), dtype=f32, device=dev)
-                    if envelope_divide else None)
+        self.env = self.env_ab = None
+        if envelope_divide:
+            # std: every plane shares E = W * W; single: the autos E = B * B, AB the
+            # A * B trapezoid (single_pass_accumulator.py:690-730)
+            self.env = torch.tensor(pair_envelope(wb, wb, self.corr), dtype=f32, device=dev)
+            self.env_ab = (torch.tensor(pair_envelope(wa, wb, self.corr), dtype=f32, device=dev)
+                           if runtype == "single" else self.env)
         plane = self.n_win * h * w
         self.sums = torch.zeros((3, plane), dtype=f32, device=dev)       # AB, AA, BB
         self.comp = torch.zeros((3, plane), dtype=f32, device=dev)
@@ -101,15 +156,21 @@ class EnsemblePIV:
         self.Lx = _lib.bulkxcorr2d_lib()
         self.Lp = _lib.pass_lib()
         self.Lk = _lib.kspacefit_lib()
-        sb = int(self.Lx.pivb_accumulate_scratch_bytes(h, self.n_win))
+        sb = int(self.Lx.pivb_accumulate_scratch_bytes(self.comp_size[0], self.n_win))
         self.scratch = torch.empty(max(sb, 256), dtype=torch.uint8, device=dev)
         self.n_pairs = 0
         self.n_means = 0              # pairs of the first sweep (two-sweep methods)
         self.means_ready = False
-        self._centered = None         # (2, n, H, W) centred frames of the second sweep
+        self._centered = None         # (2, n, Hp, Wp) centred / padded frames the correlator reads
         # zero fills above ran on the construction stream: finish them before use
         # from another stream
         torch.cuda.current_stream(self.device).synchronize()
+
+    @property
+    def window_centres(self):
+        """Window centres (x, y) in the coordinates of the unpadded frame."""
+        pt, _, pl, _ = self.padding
+        return self.grid.win_ctrs_x - pl, self.grid.win_ctrs_y - pt
 
     def _stream(self):
         return ctypes.c_void_p(self.torch.cuda.current_stream(self.device).cuda_stream)
@@ -127,13 +188,16 @@ class EnsemblePIV:
         self.means_ready = False
 
     def _triple(self, A, B, n, mean_subtract, out, comp, s):
+        """bulkxcorr2d_accumulate_triple over n frames of the correlator's size
+        (Hp x Wp): AB weights (A, B), auto weights (B, B) (cpu_ensemble.py:1000-1013)."""
         g = self.grid
-        h, w = self.win
-        wp = self.weight.data_ptr()
+        ch, cw = self.comp_size
+        h, w = self.corr
+        wa, wb = self.weight_a.data_ptr(), self.weight.data_ptr()
         self._ok(self.Lx.pivb_accumulate_triple_dev(
-            A.data_ptr(), B.data_ptr(), self.H * self.W, None, self.H, self.W, n, self.cx.data_ptr(),
-            self.cy.data_ptr(), g.n_win_y, g.n_win_x, wp, wp, wp, wp, h, w, h, w, mean_subtract, 0,
-            out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(),
+            A.data_ptr(), B.data_ptr(), self.Hp * self.Wp, None, self.Hp, self.Wp, n, self.cx.data_ptr(),
+            self.cy.data_ptr(), g.n_win_y, g.n_win_x, wa, wb, wb, wb, ch, cw, h, w, mean_subtract,
+            self.per_pair_norm, out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(),
             None if comp is None else comp.data_ptr(), self.scratch.data_ptr(), self.scratch.numel(), s),
             "accumulate_triple")
 
@@ -197,17 +261,29 @@ class EnsemblePIV:
         return {"A_mean": self.fmean[0].view(self.H, self.W), "B_mean": self.fmean[1].view(self.H, self.W),
                 "n_pairs": n}
 
-    def _center(self, A, B, n, s, in_place):
-        """A - A_mean, B - B_mean (cpu_ensemble.py:1290-1291): in place for the
-        pipeline's own staging buffers, else into a scratch pair of batches."""
+    def _scratch_pair(self, n):
+        if self._centered is None or self._centered.shape[1] < n:
+            self._centered = self.torch.empty((2, n, self.Hp, self.Wp), dtype=self.torch.float32, device=self.device)
+        return self._centered[0, :n], self._centered[1, :n]
+
+    def _prepare(self, A, B, n, s, in_place):
+        """The frames the correlator reads: as given (std mode); minus the mean
+        images for the 'image' methods (cpu_ensemble.py:1290-1291), in place for
+        the pipeline's own staging buffers, else into scratch; in single mode
+        zero-padded (and centred first) into scratch (cpu_ensemble.py:962-972,
+        1314-1324).  The caller's tensors are never modified."""
         npix = self.H * self.W
-        if in_place:
-            outs = (A, B)
-        else:
-            if self._centered is None or self._centered.shape[1] < n:
-                self._centered = self.torch.empty((2, n, self.H, self.W), dtype=self.torch.float32,
-                                                  device=self.device)
-            outs = (self._centered[0, :n], self._centered[1, :n])
+        if self.runtype == "single":
+            outs = self._scratch_pair(n)
+            for k, (F, O) in enumerate(zip((A, B), outs)):
+                self._ok(self.Lp.pivb_pad_frames_dev(F.data_ptr(), npix, n, self.H, self.W,
+                                                     self.fmean[k].data_ptr() if self.two_sweep else None,
+                                                     self.padding[0], self.padding[2], O.data_ptr(), self.Hp,
+                                                     self.Wp, self.Hp * self.Wp, s), "pad frames")
+            return outs
+        if not self.two_sweep:
+            return A, B
+        outs = (A, B) if in_place else self._scratch_pair(n)
         for k, (F, O) in enumerate(zip((A, B), outs)):
             self._ok(self.Lp.pivb_center_frames_dev(F.data_ptr(), npix, n, npix, self.fmean[k].data_ptr(),
                                                     O.data_ptr(), npix, s), "centre frames")
@@ -228,9 +304,9 @@ class EnsemblePIV:
             if not self.means_ready:
                 raise RuntimeError(f"{self.background!r} sweeps twice: accumulate_means over every pair, then "
                                    "end_means, before accumulate")
-            A, B = self._center(A, B, n, s, in_place)
         else:
-            self._frame_sums(A, B, n, s)
+            self._frame_sums(A, B, n, s)        # of the unpadded frames (cpu_ensemble.py:955-960)
+        A, B = self._prepare(A, B, n, s, in_place)
         self._triple(A, B, n, self.mean_subtract, self.sums, self.comp, s)
         self.n_pairs += n
 
@@ -303,7 +379,7 @@ class EnsemblePIV:
         (start, stop); `fit` then fits the block and `gather_fit` joins them."""
         from . import ensemble_dist as ed
 
-        h, w = self.win
+        h, w = self.corr
         block, fsum, n_tot, (a, b) = ed.exchange_sums(self.sums, self.comp, self.fsum, self.fcomp, self.n_pairs,
                                                       self.n_win, h * w, group)
         torch = self.torch
@@ -320,7 +396,7 @@ class EnsemblePIV:
         """Finalise windows [w0, w1): sums (3, (w1 - w0) * h * w) for those windows,
         fsum (2, H * W) frame sums over n_pairs pairs."""
         s = self._stream()
-        h, w = self.win
+        h, w = self.corr
         hw = h * w
         bg = None
         if self.use_bg:
@@ -330,14 +406,22 @@ class EnsemblePIV:
                          "frame mean")
             self.bg.zero_()
             MA, MB = self.fmean[0].view(1, self.H, self.W), self.fmean[1].view(1, self.H, self.W)
+            if self.runtype == "single":        # padded like the pairs (single_pass_accumulator.py:402-410)
+                PA, PB = self._scratch_pair(1)
+                for F, O in ((MA, PA), (MB, PB)):
+                    self._ok(self.Lp.pivb_pad_frames_dev(F.data_ptr(), npix, 1, self.H, self.W, None,
+                                                         self.padding[0], self.padding[2], O.data_ptr(), self.Hp,
+                                                         self.Wp, self.Hp * self.Wp, s), "pad frames")
+                MA, MB = PA, PB
             self._triple(MA, MB, 1, self.mean_subtract, self.bg, None, s)
             bg = self.bg[:, w0 * hw:w1 * hw]
         env = None if self.env is None else self.env.data_ptr()
+        env_ab = None if self.env_ab is None else self.env_ab.data_ptr()
         self._ok(self.Lp.pivb_ensemble_finalize_dev(
             sums[0].data_ptr(), sums[1].data_ptr(), sums[2].data_ptr(),
             None if bg is None else bg[0].data_ptr(), None if bg is None else bg[1].data_ptr(),
-            None if bg is None else bg[2].data_ptr(), n_pairs, w1 - w0, h, w, int(self.dc_zero), env, env,
-            planes[2].data_ptr(), planes[0].data_ptr(), planes[1].data_ptr(), norm.data_ptr(), s),
+            None if bg is None else bg[2].data_ptr(), n_pairs, w1 - w0, h, w, int(self.dc_zero), env, env_ab,
+            planes[2].data_ptr(), planes[0].data_ptr(), planes[1].data_ptr(), norm.data_ptr(), self.ab_scale, s),
             "ensemble finalize")
 
     def gather_fit(self, fit, group=None):
@@ -357,7 +441,7 @@ class EnsemblePIV:
 
         torch = self.torch
         dev = self.device
-        h, w = self.win
+        h, w = self.corr
         a, b = getattr(self, "block", (0, self.n_win))
         n = b - a
         pdy = pdx = None
@@ -374,8 +458,10 @@ class EnsemblePIV:
         key = (nf, warp_kernel, hole)
         cache = self.__dict__.setdefault("_p_grids", {})
         if key not in cache:
+            # the auto envelope and the frame-B weight: the sum window in single mode
+            # (single_pass_accumulator.py:863-874)
             env = self.env.cpu().numpy().astype(np.float64) if self.env is not None else np.ones((h, w))
-            fs, P = floor_psd.build_p_grid(env, warp_kernel, hole, self.weight.cpu().numpy(), n_fracs=nf)
+            fs, P = floor_psd.build_p_grid(env, warp_kernel, hole, self._wb_host.astype(np.float32), n_fracs=nf)
             cache[key] = (torch.tensor(fs, dtype=torch.float64, device=dev),
                           torch.tensor(P, dtype=torch.float64, device=dev).contiguous())
         fs_d, P_d = cache[key]
@@ -393,7 +479,7 @@ class EnsemblePIV:
         (n_win,), plus diagnostics."""
         torch = self.torch
         dev = self.device
-        h, w = self.win
+        h, w = self.corr
         n = int(self.planes.shape[1])
         if floor not in ("flat", "coloured"):
             raise ValueError(f"kspace floor {floor!r} (valid: 'flat', 'coloured')")

@@ -3,7 +3,9 @@
 Restates the reference's interrogation-grid rules so that the GPU path receives
 exactly the arrays the reference drivers pass to its C libraries:
 
-* window centres: pivtools_core/window_utils.py:142-274 (compute_window_centers)
+* window centres: pivtools_core/window_utils.py:142-274 (compute_window_centers),
+  and for ensemble single mode window_utils.py:79-128, 276-525
+  (compute_padding_for_single_mode, compute_window_centers_single_mode)
 * window weights: pivtools_cli/piv/piv_backend/base.py:52-134 (_window_weight_fun)
 * padded predictor grids and smoothing kernels: base.py:136-318
   (_cache_window_padding_unified)
@@ -50,6 +52,43 @@ def compute_window_centers(image_shape, window_size, overlap) -> WindowGrid:
     cx = np.linspace(fx, fx + sx * (nx - 1), nx, dtype=np.float32)
     cy = np.linspace(ly - sy * (ny - 1), ly, ny, dtype=np.float32)
     return WindowGrid(cx, cy, nx, ny, sx, sy)
+
+
+def compute_padding_for_single_mode(window_size, sum_window):
+    """(top, bottom, left, right) zero padding that lets the sum window sit around
+    every small window (window_utils.py:79-128): ceil on top/left, floor on
+    bottom/right of half the size difference."""
+    dh, dw = sum_window[0] - window_size[0], sum_window[1] - window_size[1]
+    return (int(np.ceil(dh / 2)), int(np.floor(dh / 2)), int(np.ceil(dw / 2)), int(np.floor(dw / 2)))
+
+
+def compute_window_centers_single_mode(image_shape, window_size, sum_window, overlap):
+    """Ensemble single-mode grid (window_utils.py:276-463): spacing from the small
+    window, centres in the coordinates of the zero-padded frame (the small
+    window's standard-mode centres shifted by the padding; y anchored to the
+    bottom and ascending).  Returns (WindowGrid in padded coordinates, padding)."""
+    H, W = image_shape
+    wh, ww = window_size
+    sh, sw = sum_window
+    if sh < wh or sw < ww:
+        raise ValueError(f"SumWindow {tuple(sum_window)} must be >= window_size {tuple(window_size)} for single mode")
+    if wh > H or ww > W:
+        raise ValueError(f"Window size {window_size} exceeds image dimensions {image_shape}")
+    if overlap < 0 or overlap >= 100:
+        raise ValueError(f"Overlap must be in range [0, 100), got {overlap}")
+    pt, pb, pl, pr = compute_padding_for_single_mode(window_size, sum_window)
+    Nx, Ny = W + pl + pr, H + pt + pb
+    sx = max(1, round((1 - overlap / 100) * ww))
+    sy = max(1, round((1 - overlap / 100) * wh))
+    fx, fy = pl + (ww - 1) / 2.0, pt + (wh - 1) / 2.0
+    lx, ly = pl + W - (ww + 1) / 2.0, pt + H - (wh + 1) / 2.0
+    nx = max(1, int(np.floor((lx - fx) / sx)) + 1)
+    ny = max(1, int(np.floor((ly - fy) / sy)) + 1)
+    cx = np.linspace(fx, fx + sx * (nx - 1), nx, dtype=np.float32)
+    cy = np.linspace(ly - sy * (ny - 1), ly, ny, dtype=np.float32)
+    if cx[-1] + (sw - 1) / 2.0 >= Nx or cy[-1] + (sh - 1) / 2.0 >= Ny:
+        raise ValueError("Single mode window centers exceed padded image bounds")
+    return WindowGrid(cx, cy, nx, ny, sx, sy), (pt, pb, pl, pr)
 
 
 def compute_vector_masks(pixel_mask, image_shape, window_sizes, overlaps, threshold=0.5):

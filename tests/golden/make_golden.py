@@ -305,6 +305,38 @@ def make_ensemble():
     planes = rng.standard_normal(7 * 16 * 16).astype(np.float32) + 3.0
     out["dc_in"] = planes
     out["dc_out"] = dc_fn(planes.copy(), 7, (16, 16))
+    # single mode: the reference's grid and padding (window_utils.py), its
+    # singlepix / bsingle weights (base.py:_window_weight_fun, a static method
+    # compiled here on its own) and the envelopes the finalise divides by
+    import ast
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("ref_window_utils",
+                                                  os.path.join(REF_ROOT, "pivtools_core/window_utils.py"))
+    wu = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(wu)
+    base = os.path.join(REF_ROOT, "pivtools_cli/piv/piv_backend/base.py")
+    tree = ast.parse(open(base).read())
+    fn = [m for c in tree.body if isinstance(c, ast.ClassDef) for m in c.body
+          if isinstance(m, ast.FunctionDef) and m.name == "_window_weight_fun"][0]
+    fn.decorator_list = []
+    ns = {"np": np}
+    exec(compile(ast.Module(body=[fn], type_ignores=[]), base, "exec"), ns)
+    wfun = ns["_window_weight_fun"]
+    cases = [((512, 384), (4, 4), (16, 16), 50), ((300, 257), (6, 4), (17, 15), 75), ((128, 160), (8, 8), (32, 32), 0),
+             ((256, 256), (1, 1), (16, 16), 50)]
+    for k, (shape, win, sumw, ov) in enumerate(cases):
+        r = wu.compute_window_centers_single_mode(shape, win, sumw, ov)
+        out[f"single{k}_cx"], out[f"single{k}_cy"] = r.win_ctrs_x, r.win_ctrs_y
+        out[f"single{k}_meta"] = np.array([r.n_win_x, r.n_win_y, r.win_spacing_x, r.win_spacing_y, *r.padding])
+        out[f"single{k}_case"] = np.array([*shape, *win, *sumw, ov])
+    for win, sumw, fit in (((4, 4), (16, 16), (16, 16)), ((8, 8), (32, 32), (24, 24)), ((5, 5), (16, 16), (12, 12))):
+        wa = wfun(win, "singlepix", sumw)
+        wb = wfun(sumw, "bsingle", sumw)
+        key = f"sp_{win[0]}_{sumw[0]}_{fit[0]}"
+        out[key + "_wa"], out[key + "_wb"] = wa, wb
+        out[key + "_env_auto"] = env_fn(wb, wb, fit)
+        out[key + "_env_ab"] = env_fn(wa, wb, fit)
     np.savez_compressed(os.path.join(HERE, "ensemble_ref.npz"), **out)
     print("ensemble_ref.npz written")
 

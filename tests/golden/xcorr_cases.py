@@ -157,6 +157,17 @@ def triple_cases():
     sq = geometry.window_weight((32, 32), "square")
     out.append(dict(name="t32_crop_ms1_pn1", A=A, B=B, cx=cx, cy=cy, win=(32, 32), fit=(24, 24),
                     w=(g, sq, sq, sq), ms=1, pn=1, keep=np.arange(len(cx) * len(cy))))
+    # ensemble single mode: 4 px particle windows at 50% inside a 16 px sum window,
+    # zero-padded frames, singlepix frame-A weight, bsingle elsewhere, 12 x 12 crop
+    grid, (pt, pb, pl, pr) = geometry.compute_window_centers_single_mode(A.shape[1:], (4, 4), (16, 16), 50)
+    PA = np.pad(A, ((0, 0), (pt, pb), (pl, pr)))
+    PB = np.pad(B, ((0, 0), (pt, pb), (pl, pr)))
+    sp = geometry.window_weight((4, 4), "singlepix", (16, 16))
+    bs = geometry.window_weight((16, 16), "bsingle", (16, 16))
+    for ms in (0, 1):
+        out.append(dict(name=f"t16_single_ms{ms}", A=PA, B=PB, cx=grid.win_ctrs_x, cy=grid.win_ctrs_y, win=(16, 16),
+                        fit=(12, 12), w=(sp, bs, bs, bs), ms=ms, pn=0,
+                        keep=np.arange(0, grid.n_win_x * grid.n_win_y, 7)))
     return out
 
 

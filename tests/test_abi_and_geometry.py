@@ -84,3 +84,41 @@ def test_window_weights(wt):
     assert w.shape == (32, 32) and w.dtype == np.float32 and np.all(w >= 0)
     if wt == "gaussian":
         assert abs(float(w[15, 15]) - np.exp(-0.5 * 2 * (0.5 / 16) ** 2)) < 1e-6
+
+
+def test_single_mode_grid_weights_and_envelopes():
+    """Ensemble single mode against the reference's own functions
+    (tests/golden/make_golden.py ensemble): the padded grid and its padding
+    (window_utils.py), the singlepix / bsingle weights (base.py) and the two
+    envelopes of the finalise (single_pass_accumulator.py:52-102, 706-716)."""
+    from pivtools_b200 import ensemble
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "ensemble_ref.npz"))
+    k = 0
+    while f"single{k}_case" in g.files:
+        H, W, wh, ww, sh, sw, ov = (int(v) for v in g[f"single{k}_case"])
+        grid, pad = geometry.compute_window_centers_single_mode((H, W), (wh, ww), (sh, sw), ov)
+        meta = g[f"single{k}_meta"]
+        assert [grid.n_win_x, grid.n_win_y, grid.win_spacing_x, grid.win_spacing_y, *pad] == meta.tolist(), k
+        assert np.array_equal(grid.win_ctrs_x, g[f"single{k}_cx"]) and np.array_equal(grid.win_ctrs_y, g[f"single{k}_cy"])
+        k += 1
+    assert k == 4
+    for key in [f for f in g.files if f.startswith("sp_") and f.endswith("_wa")]:
+        _, win, sumw, fit = key[:-3].split("_")
+        win, sumw, fit = (int(win),) * 2, (int(sumw),) * 2, (int(fit),) * 2
+        wa = geometry.window_weight(win, "singlepix", sumw)
+        wb = geometry.window_weight(sumw, "bsingle", sumw)
+        assert np.array_equal(wa, g[key]) and np.array_equal(wb, g[key[:-3] + "_wb"])
+        np.testing.assert_allclose(ensemble.pair_envelope(wb, wb, fit), g[key[:-3] + "_env_auto"], rtol=1e-12,
+                                   atol=1e-14)
+        np.testing.assert_allclose(ensemble.pair_envelope(wa, wb, fit), g[key[:-3] + "_env_ab"], rtol=1e-12,
+                                   atol=1e-14)
+    with pytest.raises(ValueError, match="must be >="):
+        geometry.compute_window_centers_single_mode((64, 64), (16, 16), (8, 8), 50)
+    with pytest.raises(ValueError, match="exceeds envelope support"):
+        ensemble.pair_envelope(np.ones((8, 8)), np.ones((8, 8)), (16, 16))
+    wa, wb = np.zeros((16, 16)), np.zeros((16, 16))
+    wa[0:4, 0:4] = 1.0                                   # windows 8 px apart: the envelope peak leaves the centre
+    wb[8:12, 8:12] = 1.0
+    with pytest.raises(ValueError, match="centering is off"):
+        ensemble.pair_envelope(wa, wb, (16, 16))

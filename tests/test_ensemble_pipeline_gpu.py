@@ -84,6 +84,83 @@ def test_ensemble_pass_matches_oracle(oracle, cuda, method, env):
     np.testing.assert_allclose(gg[:, 9:12], go[:, 9:12], rtol=5e-3, atol=1e-4)
 
 
+@pytest.mark.parametrize("method,env,win,sumw,fit", [
+    ("correlation+dc_zero", False, (4, 4), (16, 16), None), ("window_mean", True, (4, 4), (16, 16), (12, 12)),
+    ("image", True, (8, 8), (32, 32), (24, 24)), ("correlation", True, (5, 5), (16, 16), None),
+    ("image+dc_zero", False, (6, 6), (16, 16), (16, 16))])
+def test_single_mode_matches_oracle(oracle, cuda, method, env, win, sumw, fit):
+    """Ensemble single mode (singlepix frame-A weight inside the sum window,
+    bsingle frame B and auto planes, zero-padded frames, planes at the fitting
+    window, the AB area correction) against the oracle's restatement of the
+    reference's steps on the same pairs."""
+    import torch
+
+    shape = (96, 112)
+    A, B = _pairs(6, shape, 770)
+    ep = ensemble.EnsemblePIV(shape, win, 50, "square", background=method, envelope_divide=env, device=cuda,
+                              runtype="single", sum_window=sumw, fit_window=fit)
+    ms, use_bg, dc, two = ensemble._METHODS[method]
+    batches = (slice(0, 2), slice(2, 6))
+    dA = [torch.tensor(A[sl], device=cuda) for sl in batches]
+    dB = [torch.tensor(B[sl], device=cuda) for sl in batches]
+    if two:
+        for a, b in zip(dA, dB):
+            ep.accumulate_means(a, b)
+        ep.end_means()
+    for a, b in zip(dA, dB):
+        ep.accumulate(a, b)
+    fin = ep.finalize()
+    torch.cuda.synchronize()
+
+    g = ep.grid
+    corr = fit or sumw
+    assert tuple(fin["R_AB"].shape[1:]) == corr
+    pt, pb, pl, pr = ep.padding
+    wa = geometry.window_weight(win, "singlepix", sumw)
+    wb = geometry.window_weight(sumw, "bsingle", sumw)
+    mask = np.zeros((g.n_win_y, g.n_win_x), np.float32)
+    pad = lambda F: np.pad(F, ((0, 0), (pt, pb), (pl, pr)))      # noqa: E731
+    CA, CB = A, B
+    if two:
+        mA, mB = oracle.image_method_means([A[sl] for sl in batches], [B[sl] for sl in batches])
+        CA, CB = oracle.center_frames(A, mA), oracle.center_frames(B, mB)
+    s_ab, s_aa, s_bb = oracle.accumulate_triple(pad(CA), pad(CB), mask, g.win_ctrs_x, g.win_ctrs_y, sumw, wa, wb,
+                                                wb, wb, fit_size=corr, mean_subtract=ms)
+    n_win = g.n_win_y * g.n_win_x
+    bg = None
+    if use_bg:
+        mA = (A.astype(np.float64).sum(0) / 6).astype(np.float32)
+        mB = (B.astype(np.float64).sum(0) / 6).astype(np.float32)
+        b_ab, b_aa, b_bb = oracle.accumulate_triple(pad(mA[None]), pad(mB[None]), mask, g.win_ctrs_x, g.win_ctrs_y,
+                                                    sumw, wa, wb, wb, wb, fit_size=corr, mean_subtract=ms)
+        bg = [x.reshape(n_win, *corr) for x in (b_aa, b_bb, b_ab)]
+    e_auto = oracle.pair_envelope(wb, wb, corr) if env else None
+    e_ab = oracle.pair_envelope(wa, wb, corr) if env else None
+    R_AA, R_BB, R_AB, norm = oracle.ensemble_finalize(
+        s_ab.reshape(n_win, *corr), s_aa.reshape(n_win, *corr), s_bb.reshape(n_win, *corr), 6, bg=bg, dc_zero=dc,
+        env_auto=e_auto, env_ab=e_ab, ab_scale=(sumw[0] * sumw[1]) / (win[0] * win[1]))
+    for got, ref in ((fin["R_AA"], R_AA), (fin["R_BB"], R_BB), (fin["R_AB"], R_AB)):
+        got = got.cpu().numpy()
+        scale = np.abs(ref).reshape(n_win, -1).max(axis=1)[:, None, None]
+        assert np.all(np.abs(got - ref) <= 2e-4 * scale + 1e-7), float(np.max(np.abs(got - ref) / scale))
+    np.testing.assert_allclose(fin["norm"].cpu().numpy(), norm, rtol=2e-4)
+    cx, cy = ep.window_centres                                  # unpadded-frame coordinates
+    assert float(cx[0]) == (win[1] - 1) / 2.0
+
+
+def test_single_mode_refusals(cuda):
+    with pytest.raises(ValueError, match="sum_window must be defined"):
+        ensemble.EnsemblePIV((64, 64), (4, 4), 50, runtype="single", device=cuda)
+    with pytest.raises(ValueError, match="must be <="):
+        ensemble.EnsemblePIV((64, 64), (4, 4), 50, runtype="single", sum_window=(16, 16), fit_window=(20, 20),
+                             device=cuda)
+    with pytest.raises(ValueError, match="square"):
+        ensemble.EnsemblePIV((64, 64), (4, 4), 50, runtype="single", sum_window=(16, 32), device=cuda)
+    with pytest.raises(ValueError, match="per_pair_normalization"):
+        ensemble.EnsemblePIV((64, 64), (16, 16), 75, background="correlation", per_pair_normalization=True,
+                             device=cuda)
+
+
 def test_two_sweep_order_and_refusals(cuda):
     import torch
 
