@@ -15,6 +15,11 @@ libpivb_lavision codecs and the GPU unpack).
   nibble runs ended by a low nibble 8 or by the value count).
 * Writers of Image_Header_7 files (im7_reader.py:33-118, 722-869) for packs 0, 1,
   2 and 20 (versions 0 and 1, with the version-1 mask trailer).
+* A host reader of camera frames for packs 0 and 2 (version 0), restating the
+  reference's read_im7_camera (im7_reader.py:982-1160: header, per-frame reads or
+  per-row / per-frame zlib blocks with exact ends, the attribute walk for the
+  SCALE_I record, float32 frames with the scale applied in place): the CPU
+  baseline of the ingest measurement and a checker of the fixtures.
 """
 
 from __future__ import annotations
@@ -318,3 +323,107 @@ def im7_pack20_v1(frames: np.ndarray, attrs: bytes, masks=None) -> bytes:
     slots[0], slots[1], slots[7] = attr_at, attr_at - 8 * F, mtab
     buf += struct.pack("<8q", *slots) + bytes(256 - 64)
     return bytes(buf)
+
+
+# ---------------------------------------------------------------------------
+# Host reader (packs 0 and 2, version 0)
+# ---------------------------------------------------------------------------
+
+def _intensity_scale(f):
+    """(slope, offset) from the attribute records at f's position (im7_reader.py:
+    747-868): records of int32 type, int32 size and data up to IEH_END or EOF;
+    type 4 holds 'slope offset\\0unit\\0'."""
+    slope, offset, first = 1.0, 0.0, True
+    while True:
+        t = f.read(4)
+        if not t:
+            break
+        if len(t) < 4:
+            raise IOError("stray bytes after the pixel data")
+        typ = struct.unpack("<i", t)[0]
+        if typ == 0:
+            if first:
+                raise IOError("empty record list after the pixel data")
+            break
+        if not 1 <= typ <= 13:
+            raise IOError(f"record type {typ} after the pixel data")
+        size = struct.unpack("<i", f.read(4))[0]
+        data = f.read(size)
+        if size < 0 or len(data) != size:
+            raise IOError("attribute record past the end of the file")
+        if typ == 4:
+            words = data.split(b"\x00")[0].decode("utf-8", "replace").split()
+            try:
+                if len(words) >= 1:
+                    slope = float(words[0])
+                if len(words) >= 2:
+                    offset = float(words[1])
+            except ValueError:
+                pass
+        first = False
+    return slope, offset
+
+
+def _zlib_exact(comp: bytes, want: int) -> bytes:
+    d = zlib.decompressobj()
+    out = d.decompress(comp)
+    if not d.eof or d.unused_data or len(out) != want:
+        raise IOError("zlib block does not inflate to its block size at its declared end")
+    return out
+
+
+def read_im7_camera_host(path, camera_no: int = 1, frames_per_camera: int = 2, frames=None) -> np.ndarray:
+    """Float32 frames (n, H, W) of one camera of a pack-0 or pack-2 version-0
+    file, scale applied as result *= slope; result += offset."""
+    with open(path, "rb") as f:
+        head = f.read(256)
+        ver, pack, fmt, _, W, H, Z, F = struct.unpack_from("<hhhh iiii", head, 0)
+        if ver != 0 or pack not in (0, 2) or min(W, H, Z, F) < 1:
+            raise ValueError(f"host reader: version {ver} pack {pack} not restated")
+        dt = np.dtype("<u2") if fmt == -4 else np.dtype("<f4")
+        row = W * dt.itemsize
+        fb = row * H * Z
+        start = (camera_no - 1) * frames_per_camera
+        if start >= F:
+            raise ValueError("camera beyond the file's frames")
+        n = min(frames_per_camera if frames is None else min(frames, frames_per_camera), F - start)
+        out = np.empty((n, H, W), np.float32)
+        if pack == 0:
+            f.seek(256 + start * fb)
+            for i in range(n):
+                raw = f.read(fb)
+                if len(raw) != fb:
+                    raise IOError("truncated frame")
+                out[i] = np.frombuffer(raw, dt).reshape(Z, H, W)[0]
+            f.seek(256 + F * fb)
+        else:
+            pos = f.tell()
+            c0 = struct.unpack("<i", f.read(4))[0]
+            probe = zlib.decompressobj().decompress(f.read(c0), row + 1)
+            f.seek(pos)
+            block = fb if len(probe) > row else row
+            if len(probe) < row:
+                raise IOError("first zlib block is shorter than a row")
+            per_frame = fb // block
+
+            def skip(k):
+                for _ in range(k):
+                    c = struct.unpack("<i", f.read(4))[0]
+                    f.seek(c, 1)
+
+            skip(start * per_frame)
+            for i in range(n):
+                parts = []
+                for _ in range(per_frame):
+                    c = struct.unpack("<i", f.read(4))[0]
+                    if c <= 0:
+                        raise IOError("invalid zlib block size")
+                    parts.append(_zlib_exact(f.read(c), block))
+                out[i] = np.frombuffer(b"".join(parts), dt).reshape(Z, H, W)[0]
+            skip((F - start - n) * per_frame)
+        slope, offset = _intensity_scale(f)
+    if slope != 1.0:
+        out *= slope
+    if offset != 0.0:
+        out += offset
+    return out

@@ -176,3 +176,22 @@ def test_header_refusals(tmp_path):
     p.write_bytes(good[:-20])                       # a record cut off: the decode did not end right
     with pytest.raises(IOError, match="attribute records"):
         LV.read_im7(p)
+
+
+def test_host_reader_restatement_matches_reference(gold, tmp_path):
+    """The oracle's host reader (the ingest measurement's CPU baseline) equals the
+    reference reader's float32 camera frames on the pack-0 and pack-2 fixtures."""
+    import lavision_oracle as LO
+
+    z, meta = gold
+    n = 0
+    for case in meta["im7"]:
+        name = case["name"]
+        if not name.startswith(("p0_", "p2_")):
+            continue
+        p = _write(tmp_path, name, z[name + "_file"])
+        for i, (cam, fpc, nfr) in enumerate(case["cams"]):
+            got = LO.read_im7_camera_host(p, cam, fpc, nfr)
+            assert got.dtype == np.float32 and np.array_equal(got, z[f"{name}_cam{i}"]), (name, i)
+            n += 1
+    assert n >= 6
