@@ -396,11 +396,11 @@ def run_b200(args):
     fp32_flops = windows * 80.1e3
     # DRAM traffic of one launch pair (correlation + deferred fits): dram__bytes_read.sum
     # + dram__bytes_write.sum of the same kernels and pass captured by ncu on 8 pairs
-    # (xcorr_kernel<32>: 362.9 + 63.0 MB, lm_records_kernel: 65.6 + 4.8 MB, for
+    # (xcorr_kernel<32>: 386.7 + 62.8 MB, lm_records_kernel: 65.6 + 4.8 MB, for
     # 512,072 windows; profiles/xcorr_kernel32_pass4_8pairs.md,
     # profiles/lm_records_gauss3_8pairs.md), scaled by windows processed (frames,
     # records and outputs all grow with the pair count).
-    traffic = (362.904064e6 + 63.008768e6 + 65.61664e6 + 4.807424e6) / 512072 * windows
+    traffic = (386.735616e6 + 62.808576e6 + 65.61664e6 + 4.807424e6) / 512072 * windows
 
     # ---- end to end through host buffers: every step copies its 64 pairs of
     # uint16 frames from pinned memory (chunked, overlapped with compute), converts

@@ -344,6 +344,16 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
         }
     };
     const int lb = line / M, rb = rm / M;
+    // One lane per column (32 and 64 px): the last pass is a complex-to-real
+    // transform.  After the row pass, column x holds E(ky) = conj(D(ky, x)) with D
+    // Hermitian in ky (C is), so the real column c(., x) follows from ky = 0..N/2
+    // alone: Z(k) = conj(E(k)) + E(N/2 - k) + i (conj(E(k)) - E(N/2 - k)) W_N^{-k}
+    // for k < N/2, z = the unnormalised length-N/2 inverse of Z, and
+    // c(2m, x) = Re z(m), c(2m + 1, x) = Im z(m): half-length butterflies in place
+    // of a full-length transform whose imaginary output was discarded.
+    constexpr bool C2R = (P == 1) && (N == 32 || N == 64);
+    constexpr int MH = C2R ? M / 2 : 1;
+    float2 zh[MH];
     float2 z[M];
 #pragma unroll
     for (int n = 0; n < M; ++n) z[n] = zab[n];
@@ -386,20 +396,40 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
             if (pass == 0) {
 #pragma unroll
                 for (int n = 0; n < M; ++n) z[n] = S[at(line, lb, P * n + p)];
+            } else if constexpr (C2R) {
+                sfor<MH>([&](auto kc) {
+                    constexpr int k = decltype(kc)::value;
+                    const float2 e = S[k * ST + line], f = S[(MH - k) * ST + line];
+                    const float2 s = make_float2(e.x + f.x, f.y - e.y);        // conj(E(k)) + E(N/2 - k)
+                    const float2 d = c_twiddle<N, k, +1>(make_float2(e.x - f.x, -e.y - f.y));
+                    zh[k] = make_float2(s.x - d.y, s.y + d.x);                // s + i d
+                });
+                RegFFT<MH, +1>::run(zh);
+                break;
             } else {
 #pragma unroll
                 for (int n = 0; n < M; ++n) z[n] = S[at(P * n + p, (P * n) / M, line)];
             }
+        } else if constexpr (C2R) {
+            if (pass == 2) break;
         }
     }
     g.sync();
     float *pl = reinterpret_cast<float *>(S);
     if (active) {
         const int col = (line + N / 2) % N;
+        if constexpr (C2R) {
 #pragma unroll
-        for (int k = 0; k < M; ++k) {
-            const int row = (M * q + k + N / 2) % N;
-            pl[row * G::STF + col] = (z[k].x * 0.25f) * scale;
+            for (int m = 0; m < MH; ++m) {
+                pl[((2 * m + N / 2) % N) * G::STF + col] = (zh[m].x * 0.25f) * scale;
+                pl[((2 * m + 1 + N / 2) % N) * G::STF + col] = (zh[m].y * 0.25f) * scale;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < M; ++k) {
+                const int row = (M * q + k + N / 2) % N;
+                pl[row * G::STF + col] = (z[k].x * 0.25f) * scale;
+            }
         }
     }
     g.sync();
