@@ -344,14 +344,16 @@ __device__ __forceinline__ void correlate_plane(const Group<N> &g, float2 *S, co
         }
     };
     const int lb = line / M, rb = rm / M;
-    // One lane per column (32 and 64 px): the last pass is a complex-to-real
+    // One lane per column (8 to 64 px but 12): the last pass is a complex-to-real
     // transform.  After the row pass, column x holds E(ky) = conj(D(ky, x)) with D
     // Hermitian in ky (C is), so the real column c(., x) follows from ky = 0..N/2
     // alone: Z(k) = conj(E(k)) + E(N/2 - k) + i (conj(E(k)) - E(N/2 - k)) W_N^{-k}
     // for k < N/2, z = the unnormalised length-N/2 inverse of Z, and
     // c(2m, x) = Re z(m), c(2m + 1, x) = Im z(m): half-length butterflies in place
-    // of a full-length transform whose imaginary output was discarded.
-    constexpr bool C2R = (P == 1) && (N == 32 || N == 64);
+    // of a full-length transform whose imaginary output was discarded (measured
+    // on B200: 32 px final pass -5.5%, 8 / 16 / 24 px -1 to -2%; 12 px spills at
+    // its register cap and ran 3.7% slower, so it keeps the full transform).
+    constexpr bool C2R = (P == 1) && (N % 2 == 0) && (N != 12);
     constexpr int MH = C2R ? M / 2 : 1;
     float2 zh[MH];
     float2 z[M];
