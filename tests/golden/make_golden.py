@@ -145,7 +145,7 @@ def make_peakfit():
         out[f"s{si}_loc"] = loc
         out[f"s{si}_sd"] = sd
         out[f"s{si}_ratio"] = ratio
-    # batch route (reference lockstep fitter, 8 lanes in this build)
+    # batch route (reference lockstep fitter; 8 lanes as the reference library is compiled here)
     W = R.peakfit_batch_lanes()
     rng = np.random.default_rng(7)
     bplanes, btypes, bloc, bsd = [], [], [], []
@@ -196,7 +196,7 @@ def make_warp():
             RW.fused_symmetric_warp_batch(ia, ib, ra, rb, pdy, pdx, N, H, W, 8, 10, cy, cx, mode, 0, rs)
             out[f"out_a_m{mode}_r{rs}"] = ra
             out[f"out_b_m{mode}_r{rs}"] = rb
-    # the reference's default SIMD route (AVX2 interior association in this build)
+    # the reference's default SIMD route (AVX2 interior association as compiled here)
     RW.fused_warp_set_impl(1)
     for mode in (0, 1):
         ra = np.zeros_like(ia)
