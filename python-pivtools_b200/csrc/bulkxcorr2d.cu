@@ -128,6 +128,63 @@ int size_index(int n)
 std::atomic<int> g_ctas_cap[9];
 std::atomic<int> g_record_block{128};
 
+// Resident 128-thread CTAs per SM of lm_fit_kernel<T, MODE> on `dev`, once per device.
+template <int T, int MODE>
+int lm_fit_blocks_per_sm(int dev)
+{
+    static PerDeviceOnce per_sm;
+    return per_sm.get(dev, [] {
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, lm_fit_kernel<T, MODE>, 128, 0) != cudaSuccess)
+            return -1;
+        return nb > 0 ? nb : 1;
+    });
+}
+
+bool lm_fit_setup(int dev)
+{
+    return lm_fit_blocks_per_sm<4, 0>(dev) >= 0 && lm_fit_blocks_per_sm<5, 0>(dev) >= 0 &&
+           lm_fit_blocks_per_sm<6, 0>(dev) >= 0 && lm_fit_blocks_per_sm<4, 1>(dev) >= 0 &&
+           lm_fit_blocks_per_sm<5, 1>(dev) >= 0 && lm_fit_blocks_per_sm<6, 1>(dev) >= 0;
+}
+
+template <int T, int MODE>
+int launch_lm_fit(const XcorrParams &p, int win, cudaStream_t s)
+{
+    const int dev = current_device();
+    if (dev < 0) return PIV_ERROR_CUDA;
+    const int per_sm = lm_fit_blocks_per_sm<T, MODE>(dev);
+    if (per_sm < 0) return PIV_ERROR_CUDA;
+    // every resident warp owns a contiguous run of at least 64 records
+    const long long resident = (long long)device_sms(dev) * per_sm * 4;
+    long long warps = (p.total + 63) / 64;
+    if (warps > resident) warps = resident;
+    const long long chunk = (p.total + warps - 1) / warps;
+    const unsigned blocks = (unsigned)((warps + 3) / 4);
+    lm_fit_kernel<T, MODE><<<blocks, 128, 0, s>>>(p, win, chunk);
+    return cudaGetLastError() == cudaSuccess ? PIV_ERROR_NONE : PIV_ERROR_CUDA;
+}
+
+// The deferred fits of a single-peak call: LM types on the persistent refill
+// kernel, 3-point fits one thread per record.
+int launch_records(const XcorrParams &p, int win, int peakfit_impl, int tb, cudaStream_t s)
+{
+    const int impl = peakfit_impl ? 1 : 0;
+    switch (p.finder * 2 + impl) {
+    case 8: return launch_lm_fit<4, 0>(p, win, s);
+    case 9: return launch_lm_fit<4, 1>(p, win, s);
+    case 10: return launch_lm_fit<5, 0>(p, win, s);
+    case 11: return launch_lm_fit<5, 1>(p, win, s);
+    case 12: return launch_lm_fit<6, 0>(p, win, s);
+    case 13: return launch_lm_fit<6, 1>(p, win, s);
+    default: break;
+    }
+    const unsigned blocks = (unsigned)((p.total + tb - 1) / tb);
+    if (impl) lm_records_kernel<1><<<blocks, tb, 0, s>>>(p, win);
+    else lm_records_kernel<0><<<blocks, tb, 0, s>>>(p, win);
+    return cudaGetLastError() == cudaSuccess ? PIV_ERROR_NONE : PIV_ERROR_CUDA;
+}
+
 template <int N, bool MULTI>
 int launch_xcorr_n(const XcorrParams &p, cudaStream_t s)
 {
@@ -556,11 +613,8 @@ PIV_EXPORT int pivb_xcorr_dev(const float *d_A, const float *d_B, long long img_
     if (e) return e;
     if (timing) cudaEventRecord(tw->ev[1], s);
     if (defer) {
-        const int tb = g_record_block.load(std::memory_order_relaxed);
-        const unsigned blocks = (unsigned)((total + tb - 1) / tb);
-        if (peakfit_impl) lm_records_kernel<1><<<blocks, tb, 0, s>>>(p, win_h);
-        else lm_records_kernel<0><<<blocks, tb, 0, s>>>(p, win_h);
-        if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
+        const int er = launch_records(p, win_h, peakfit_impl, g_record_block.load(std::memory_order_relaxed), s);
+        if (er) return er;
     }
     if (timing) {
         cudaEventRecord(tw->ev[2], s);
@@ -1160,7 +1214,7 @@ void *noalloc_setup()
             cudaGetLastError();
             return nullptr;
         }
-        if (!setup_all_sizes<false>(dev) || !setup_all_sizes<true>(dev)) {
+        if (!setup_all_sizes<false>(dev) || !setup_all_sizes<true>(dev) || !lm_fit_setup(dev)) {
             cudaGetLastError();
             return nullptr;
         }
@@ -1213,10 +1267,8 @@ PIV_EXPORT int pivb_xcorr_dev_noalloc(const float *d_A, const float *d_B, long l
     const int e = (n_peaks > 1 && !ensemble) ? launch_xcorr<true>(win_h, p, s) : launch_xcorr<false>(win_h, p, s);
     if (e) return e;
     if (lm) {
-        const unsigned blocks = (unsigned)((total + 127) / 128);
-        if (peakfit_impl) lm_records_kernel<1><<<blocks, 128, 0, s>>>(p, win_h);
-        else lm_records_kernel<0><<<blocks, 128, 0, s>>>(p, win_h);
-        if (cudaGetLastError() != cudaSuccess) return PIV_ERROR_CUDA;
+        const int er = launch_records(p, win_h, peakfit_impl, 128, s);
+        if (er) return er;
     }
     return PIV_ERROR_NONE;
 }

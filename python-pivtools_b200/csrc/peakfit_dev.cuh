@@ -32,6 +32,9 @@ __device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a,
 constexpr int PKW = 5;              // fit patch side (peak_locate_lm.h:16-17)
 constexpr int PKN = PKW * PKW;
 
+// Row-major index of (i, j), j <= i, in a packed lower triangle.
+__host__ __device__ constexpr int tri(int i, int j) { return i * (i + 1) / 2 + j; }
+
 // Correctly rounded float exponential via double.
 __device__ __forceinline__ float expf_cr(float x) { return (float)exp((double)x); }
 
@@ -138,7 +141,7 @@ __device__ __forceinline__ void lm_jac(const float *sub, const float *p, const f
 {
     constexpr int n = (T == 4) ? 4 : (T == 5 ? 5 : 6);
 #pragma unroll
-    for (int a = 0; a < n * n; ++a) JtJ[a] = 0.0;
+    for (int a = 0; a < n * (n + 1) / 2; ++a) JtJ[a] = 0.0;
 #pragma unroll
     for (int a = 0; a < n; ++a) Jtr[a] = 0.0;
 #pragma unroll 1
@@ -177,37 +180,36 @@ __device__ __forceinline__ void lm_jac(const float *sub, const float *p, const f
         for (int a = 0; a < n; ++a) {
             Jtr[a] = dadd(Jtr[a], dmul((double)J[a], (double)r));
 #pragma unroll
-            for (int b = 0; b <= a; ++b) JtJ[a * n + b] = dadd(JtJ[a * n + b], dmul((double)J[a], (double)J[b]));
+            for (int b = 0; b <= a; ++b) JtJ[tri(a, b)] = dadd(JtJ[tri(a, b)], dmul((double)J[a], (double)J[b]));
         }
     }
-#pragma unroll
-    for (int a = 0; a < n; ++a)
-#pragma unroll
-        for (int b = a + 1; b < n; ++b) JtJ[a * n + b] = JtJ[b * n + a];
 }
 
 // (JtJ + lambda diag) delta = -Jtr by FP64 Cholesky (peak_locate_lm.c:342-393).
+// JtJ is the packed lower triangle; the factor overwrites a working copy of it
+// entry by entry (each entry is read once, just before its factor value is
+// written), the reference's operation order throughout.
 template <int n>
 __device__ __forceinline__ bool lm_solve(const double *JtJ, const double *Jtr, float lambda, float *delta)
 {
-    double A[n * n], L[n * n], y[n], d[n];
+    double L[n * (n + 1) / 2], y[n], d[n];
     const double l1 = dadd(1.0, (double)lambda);
 #pragma unroll
-    for (int a = 0; a < n * n; ++a) { A[a] = JtJ[a]; L[a] = 0.0; }
+    for (int a = 0; a < n * (n + 1) / 2; ++a) L[a] = JtJ[a];
 #pragma unroll
-    for (int i = 0; i < n; ++i) A[i * n + i] = dmul(A[i * n + i], l1);
+    for (int i = 0; i < n; ++i) L[tri(i, i)] = dmul(L[tri(i, i)], l1);
 #pragma unroll
     for (int i = 0; i < n; ++i) {
 #pragma unroll
         for (int j = 0; j <= i; ++j) {
-            double s = A[i * n + j];
+            double s = L[tri(i, j)];
 #pragma unroll
-            for (int k = 0; k < j; ++k) s = dsub(s, dmul(L[i * n + k], L[j * n + k]));
+            for (int k = 0; k < j; ++k) s = dsub(s, dmul(L[tri(i, k)], L[tri(j, k)]));
             if (i == j) {
                 if (s <= 0.0) return false;
-                L[i * n + i] = sqrt(s);
+                L[tri(i, i)] = sqrt(s);
             } else {
-                L[i * n + j] = ddiv(s, L[j * n + j]);
+                L[tri(i, j)] = ddiv(s, L[tri(j, j)]);
             }
         }
     }
@@ -215,15 +217,15 @@ __device__ __forceinline__ bool lm_solve(const double *JtJ, const double *Jtr, f
     for (int i = 0; i < n; ++i) {
         double s = -Jtr[i];
 #pragma unroll
-        for (int j = 0; j < i; ++j) s = dsub(s, dmul(L[i * n + j], y[j]));
-        y[i] = ddiv(s, L[i * n + i]);
+        for (int j = 0; j < i; ++j) s = dsub(s, dmul(L[tri(i, j)], y[j]));
+        y[i] = ddiv(s, L[tri(i, i)]);
     }
 #pragma unroll
     for (int i = n - 1; i >= 0; --i) {
         double s = y[i];
 #pragma unroll
-        for (int j = i + 1; j < n; ++j) s = dsub(s, dmul(L[j * n + i], d[j]));
-        d[i] = ddiv(s, L[i * n + i]);
+        for (int j = i + 1; j < n; ++j) s = dsub(s, dmul(L[tri(j, i)], d[j]));
+        d[i] = ddiv(s, L[tri(i, i)]);
     }
 #pragma unroll
     for (int i = 0; i < n; ++i) delta[i] = (float)d[i];
@@ -231,76 +233,104 @@ __device__ __forceinline__ bool lm_solve(const double *JtJ, const double *Jtr, f
 }
 
 // Marquardt fit of a compensated 5x5 patch (peak_locate_lm.c:412-712 for MODE 0,
-// peak_locate_lm_batch.c:362-588 per lane for MODE 1).  Returns true if trusted.
+// peak_locate_lm_batch.c:362-588 per lane for MODE 1), in three pieces so that a
+// caller can interleave the iterations of many fits: lm_init (start values from
+// the 3-point fit, residual, normal equations), lm_step (one damped step) and
+// lm_finish (the trust test).  lm_fit runs them in sequence.
+template <int T>
+struct LmState {
+    static constexpr int n = (T == 4) ? 4 : (T == 5 ? 5 : 6);
+    float p[6];
+    double JtJ[n * (n + 1) / 2], Jtr[n];      // normal equations, packed lower triangle
+    double resid;
+    float lambda;
+    int it;
+};
+
 template <int T, int MODE>
-__device__ bool lm_fit(const float *sub, float *off, float *sig, float *fitval)
+__device__ __forceinline__ void lm_init(const float *sub, LmState<T> &st, float *pred)
 {
-    constexpr int n = (T == 4) ? 4 : (T == 5 ? 5 : 6);
-    float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     float pk[2], A, sx, sy;
     three_point(sub, PKW, PKW, PKW, pk, &A, &sx, &sy);
-    p[0] = A;
-    p[1] = fminf(fmaxf(pk[0], -2.0f), 2.0f);
-    p[2] = fminf(fmaxf(pk[1], -2.0f), 2.0f);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) st.p[k] = 0.0f;
+    st.p[0] = A;
+    st.p[1] = fminf(fmaxf(pk[0], -2.0f), 2.0f);
+    st.p[2] = fminf(fmaxf(pk[1], -2.0f), 2.0f);
     if constexpr (T == 4) {
         float s = sqrtf(fadd(fmul(sx, sx), fmul(sy, sy)));
-        p[3] = fminf(fmaxf(s, 0.5f), 3.0f);
+        st.p[3] = fminf(fmaxf(s, 0.5f), 3.0f);
     } else if constexpr (T == 5) {
-        p[3] = fminf(fmaxf(sx, 0.5f), 3.0f);
-        p[4] = fminf(fmaxf(sy, 0.5f), 3.0f);
+        st.p[3] = fminf(fmaxf(sx, 0.5f), 3.0f);
+        st.p[4] = fminf(fmaxf(sy, 0.5f), 3.0f);
     } else {
-        p[3] = fminf(fmaxf(fmul(sx, sx), 0.25f), 9.0f);
-        p[4] = fminf(fmaxf(fmul(sy, sy), 0.25f), 9.0f);
+        st.p[3] = fminf(fmaxf(fmul(sx, sx), 0.25f), 9.0f);
+        st.p[4] = fminf(fmaxf(fmul(sy, sy), 0.25f), 9.0f);
     }
-    float pred[PKN];
-    double JtJ[n * n], Jtr[n];
+    st.lambda = 0.01f;
+    st.it = 0;
+    st.resid = lm_resid<T, MODE>(sub, st.p, pred);
+    lm_jac<T>(sub, st.p, pred, st.JtJ, st.Jtr);
+}
+
+// One iteration of at most 50: 0 = go on, 1 = converged, 2 = stopped without
+// converging (singular system, damping above 1e6 or the iteration limit).
+template <int T, int MODE>
+__device__ __forceinline__ int lm_step(const float *sub, LmState<T> &st, float *pred)
+{
+    constexpr int n = LmState<T>::n;
     float delta[n];
-    float lambda = 0.01f;
-    bool ok = false;
-    double resid = lm_resid<T, MODE>(sub, p, pred);
-    lm_jac<T>(sub, p, pred, JtJ, Jtr);
-#pragma unroll 1
-    for (int it = 0; it < 50; ++it) {
-        if (!lm_solve<n>(JtJ, Jtr, lambda, delta)) break;
-        float q[6];
+    if (!lm_solve<n>(st.JtJ, st.Jtr, st.lambda, delta)) return 2;
+    float *p = st.p;
+    float q[6];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) q[k] = p[k];
+    for (int k = 0; k < 6; ++k) q[k] = p[k];
 #pragma unroll
-        for (int k = 0; k < n; ++k) q[k] = fadd(p[k], delta[k]);
-        q[0] = cmax<MODE>(q[0], fmul(p[0], 0.5f));
-        q[1] = cmin<MODE>(cmax<MODE>(q[1], -2.5f), 2.5f);
-        q[2] = cmin<MODE>(cmax<MODE>(q[2], -2.5f), 2.5f);
-        if constexpr (T == 4) {
-            q[3] = cmin<MODE>(cmax<MODE>(q[3], 0.25f), 4.0f);
-        } else if constexpr (T == 5) {
-            q[3] = cmin<MODE>(cmax<MODE>(q[3], 0.25f), 4.0f);
-            q[4] = cmin<MODE>(cmax<MODE>(q[4], 0.25f), 4.0f);
-        } else {
-            q[3] = cmin<MODE>(cmax<MODE>(q[3], 0.1f), 16.0f);
-            q[4] = cmin<MODE>(cmax<MODE>(q[4], 0.1f), 16.0f);
-            float smax = fdiv(0.95f, sqrtf(fmul(q[3], q[4])));
-            q[5] = cmin<MODE>(cmax<MODE>(q[5], -smax), smax);
-        }
-        double nr = lm_resid<T, MODE>(sub, q, pred);
-        if (nr < resid) {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) p[k] = q[k];
-            double improve = ddiv(dsub(resid, nr), dadd(resid, (double)FLT_EPSILON));
-            resid = nr;
-            lambda = fmul(lambda, 0.5f);
-            lm_jac<T>(sub, p, pred, JtJ, Jtr);
-            if (improve < 1e-6) { ok = true; break; }
-        } else {
-            lambda = fmul(lambda, 2.0f);
-            if (lambda > 1e6f) break;
-        }
+    for (int k = 0; k < n; ++k) q[k] = fadd(p[k], delta[k]);
+    q[0] = cmax<MODE>(q[0], fmul(p[0], 0.5f));
+    q[1] = cmin<MODE>(cmax<MODE>(q[1], -2.5f), 2.5f);
+    q[2] = cmin<MODE>(cmax<MODE>(q[2], -2.5f), 2.5f);
+    if constexpr (T == 4) {
+        q[3] = cmin<MODE>(cmax<MODE>(q[3], 0.25f), 4.0f);
+    } else if constexpr (T == 5) {
+        q[3] = cmin<MODE>(cmax<MODE>(q[3], 0.25f), 4.0f);
+        q[4] = cmin<MODE>(cmax<MODE>(q[4], 0.25f), 4.0f);
+    } else {
+        q[3] = cmin<MODE>(cmax<MODE>(q[3], 0.1f), 16.0f);
+        q[4] = cmin<MODE>(cmax<MODE>(q[4], 0.1f), 16.0f);
+        float smax = fdiv(0.95f, sqrtf(fmul(q[3], q[4])));
+        q[5] = cmin<MODE>(cmax<MODE>(q[5], -smax), smax);
     }
+    const double nr = lm_resid<T, MODE>(sub, q, pred);
+    int r = 0;
+    if (nr < st.resid) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) p[k] = q[k];
+        const double improve = ddiv(dsub(st.resid, nr), dadd(st.resid, (double)FLT_EPSILON));
+        st.resid = nr;
+        st.lambda = fmul(st.lambda, 0.5f);
+        lm_jac<T>(sub, p, pred, st.JtJ, st.Jtr);
+        if (improve < 1e-6) r = 1;
+    } else {
+        st.lambda = fmul(st.lambda, 2.0f);
+        if (st.lambda > 1e6f) r = 2;
+    }
+    if (r == 0 && ++st.it == 50) r = 2;
+    return r;
+}
+
+// Trust test and outputs; `converged` is lm_step's result 1.
+template <int T, int MODE>
+__device__ __forceinline__ bool lm_finish(const LmState<T> &st, bool converged, float *off, float *sig)
+{
+    const float *p = st.p;
+    bool ok = converged;
     if (!ok) {
         if constexpr (MODE == 0) {
-            ok = resid <= (double)fmul(fmul(fmul(1e-3f, p[0]), p[0]), 25.0f);
+            ok = st.resid <= (double)fmul(fmul(fmul(1e-3f, p[0]), p[0]), 25.0f);
         } else {
             constexpr float frac = 1e-3f * 25.0f;
-            ok = resid <= (double)fmul(fmul(frac, p[0]), p[0]);
+            ok = st.resid <= (double)fmul(fmul(frac, p[0]), p[0]);
         }
     }
     if (ok) {
@@ -313,10 +343,24 @@ __device__ bool lm_fit(const float *sub, float *off, float *sig, float *fitval)
     if constexpr (T == 4) { sig[0] = p[3]; sig[1] = p[3]; sig[2] = 0.0f; }
     else if constexpr (T == 5) { sig[0] = p[3]; sig[1] = p[4]; sig[2] = 0.0f; }
     else { sig[0] = p[3]; sig[1] = p[4]; sig[2] = p[5]; }
+    return ok;
+}
+
+// The whole fit of one patch.  Returns true if trusted.
+template <int T, int MODE>
+__device__ bool lm_fit(const float *sub, float *off, float *sig, float *fitval)
+{
+    float pred[PKN];
+    LmState<T> st;
+    lm_init<T, MODE>(sub, st, pred);
+    int r = 0;
+#pragma unroll 1
+    while (r == 0) r = lm_step<T, MODE>(sub, st, pred);
+    const bool ok = lm_finish<T, MODE>(st, r == 1, off, sig);
     if (fitval) {
 #pragma unroll 1
         for (int q = 0; q < PKN; ++q)
-            fitval[q] = lm_model<T, MODE>((float)(q / PKW - 2), (float)(q % PKW - 2), p);
+            fitval[q] = lm_model<T, MODE>((float)(q / PKW - 2), (float)(q % PKW - 2), st.p);
     }
     return ok;
 }

@@ -491,6 +491,63 @@ __global__ void __launch_bounds__(128) lm_records_kernel(const __grid_constant__
     else write_peak(prm, idx, N, rec.ij >> 16, rec.ij & 0xffff, off, sig, rec.best, rec.enorm);
 }
 
+// Deferred LM fits (types 4-6) of single-peak calls, persistent: warp w owns the
+// records [w * chunk, (w + 1) * chunk) and its lanes refill as their fits end, so
+// a lane whose fit converged early takes the next record instead of idling while
+// the warp's slowest fit iterates (one thread per record left about a third of
+// the lanes active).  Each fit runs lm_init / lm_step / lm_finish, the same
+// arithmetic as lm_fit, so the results equal lm_records_kernel's.
+template <int T, int MODE>
+__global__ void __launch_bounds__(128) lm_fit_kernel(const __grid_constant__ XcorrParams prm, int N, long long chunk)
+{
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    long long next = warp * chunk;                            // warp-uniform
+    const long long end = min(prm.total, next + chunk);
+    LmState<T> st;
+    float sub[PKN], pred[PKN];
+    long long idx = 0;
+    bool active = false;
+#pragma unroll 1
+    for (;;) {
+        // lanes without a fit take the next records of the chunk; records that
+        // need no fit (flag != 1) are passed over
+#pragma unroll 1
+        for (;;) {
+            const unsigned need = __ballot_sync(0xffffffffu, !active);
+            if (need == 0u || next >= end) break;
+            const long long mine = next + __popc(need & ((1u << lane) - 1u));
+            next += __popc(need);
+            if (!active && mine < end) {
+                const LmRecord &rec = prm.lm[mine];
+                if (rec.flag == 1) {
+                    const float4 *s4 = reinterpret_cast<const float4 *>(rec.sub);
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) {
+                        const float4 v = s4[k];
+                        sub[4 * k] = v.x; sub[4 * k + 1] = v.y; sub[4 * k + 2] = v.z; sub[4 * k + 3] = v.w;
+                    }
+                    sub[24] = rec.sub[24];
+                    lm_init<T, MODE>(sub, st, pred);
+                    idx = mine;
+                    active = true;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u) break;
+        if (active) {
+            const int r = lm_step<T, MODE>(sub, st, pred);
+            if (r != 0) {
+                float off[2], sig[3];
+                const LmRecord &rec = prm.lm[idx];
+                if (!lm_finish<T, MODE>(st, r == 1, off, sig)) write_sentinel(prm, idx, rec.enorm);
+                else write_peak(prm, idx, N, rec.ij >> 16, rec.ij & 0xffff, off, sig, rec.best, rec.enorm);
+                active = false;
+            }
+        }
+    }
+}
+
 // numel / (w (*) w): linear autocorrelation of the window weight at shift
 // (r - h/2, c - w/2), FP64 sum (PIV_2d_cross_correlate.c:216-222, xcorr.c:55-122).
 // Generic two-input form; `divide` selects the reciprocal weighting.
