@@ -124,13 +124,16 @@ template <int T, int MODE>
 __device__ __forceinline__ double lm_resid(const float *sub, const float *p, float *pred)
 {
     double rs = 0.0;
+    // patch coordinates i, j in -2..2 kept as float counters (exact), row-major
+    float i = -2.0f, j = -2.0f;
 #pragma unroll 1
     for (int q = 0; q < PKN; ++q) {
-        float i = (float)(q / PKW - 2), j = (float)(q % PKW - 2);
         float v = lm_model<T, MODE>(i, j, p);
         pred[q] = v;
         float r = fsub(v, sub[q]);
         rs = dadd(rs, dmul((double)r, (double)r));
+        j += 1.0f;
+        if (j > 2.0f) { j = -2.0f; i += 1.0f; }
     }
     return rs;
 }
@@ -144,9 +147,9 @@ __device__ __forceinline__ void lm_jac(const float *sub, const float *p, const f
     for (int a = 0; a < n * (n + 1) / 2; ++a) JtJ[a] = 0.0;
 #pragma unroll
     for (int a = 0; a < n; ++a) Jtr[a] = 0.0;
+    float i = -2.0f, j = -2.0f;
 #pragma unroll 1
     for (int q = 0; q < PKN; ++q) {
-        float i = (float)(q / PKW - 2), j = (float)(q % PKW - 2);
         float v = pred[q];
         float r = fsub(v, sub[q]);
         float J[n];
@@ -182,6 +185,8 @@ __device__ __forceinline__ void lm_jac(const float *sub, const float *p, const f
 #pragma unroll
             for (int b = 0; b <= a; ++b) JtJ[tri(a, b)] = dadd(JtJ[tri(a, b)], dmul((double)J[a], (double)J[b]));
         }
+        j += 1.0f;
+        if (j > 2.0f) { j = -2.0f; i += 1.0f; }
     }
 }
 
