@@ -124,16 +124,21 @@ template <int T, int MODE>
 __device__ __forceinline__ double lm_resid(const float *sub, const float *p, float *pred)
 {
     double rs = 0.0;
-    // patch coordinates i, j in -2..2 kept as float counters (exact), row-major
-    float i = -2.0f, j = -2.0f;
+    // one patch row per iteration: its five model values are independent, so
+    // their latency overlaps; the residual sum keeps the row-major order
+    float i = -2.0f;
 #pragma unroll 1
-    for (int q = 0; q < PKN; ++q) {
-        float v = lm_model<T, MODE>(i, j, p);
-        pred[q] = v;
-        float r = fsub(v, sub[q]);
-        rs = dadd(rs, dmul((double)r, (double)r));
-        j += 1.0f;
-        if (j > 2.0f) { j = -2.0f; i += 1.0f; }
+    for (int a = 0; a < PKW; ++a) {
+        float v[PKW];
+#pragma unroll
+        for (int b = 0; b < PKW; ++b) v[b] = lm_model<T, MODE>(i, (float)(b - 2), p);
+#pragma unroll
+        for (int b = 0; b < PKW; ++b) {
+            pred[a * PKW + b] = v[b];
+            float r = fsub(v[b], sub[a * PKW + b]);
+            rs = dadd(rs, dmul((double)r, (double)r));
+        }
+        i += 1.0f;
     }
     return rs;
 }
