@@ -203,6 +203,7 @@ __global__ void pred_index_kernel(const float *ctrs, int nc, float *lut, int n)
 // with, and not correctly rounded, so a device sin would differ from it in the
 // last bit of a few hundred entries -- and copied into each call's tables.
 float g_lut_host[(kLutN + 1) * 6];
+float g_lut2_host[kLutN * 12];     // row k: the six weights at k, then the six at k + 1
 std::once_flag g_lut_once;
 void build_lut_host()
 {
@@ -220,6 +221,8 @@ void build_lut_host()
             g_lut_host[i * 6 + k] = v;
         }
     }
+    for (int i = 0; i < kLutN; ++i)
+        for (int k = 0; k < 12; ++k) g_lut2_host[i * 12 + k] = g_lut_host[i * 6 + k];   // rows i and i + 1
 }
 
 struct WarpParams {
@@ -231,6 +234,7 @@ struct WarpParams {
     int N, H, W, nPY, nPX;
     const float *ly, *lx;      // pixel -> fractional predictor index
     const float *lut;          // Lanczos table or null
+    const float4 *lut2;        // the same table as 48-byte rows {w(k), w(k + 1)}, k < kLutN
     const float4 *wyb;         // per row: predictor row weights as pairs {w0,w0,w1,w1}, {w2,w2,w3,w3}
     const int *byr;            // per row: first predictor row of the 4x4 stencil
     int round_shifts;
@@ -326,11 +330,64 @@ __global__ void __launch_bounds__(128) warp_kernel(WarpParams p)
     }
 }
 
-// warp_kernel<0, 1> with paired arithmetic: the predictor's dy and dx sums run
-// as one f32x2 chain, and the samples of frame A (.x) and frame B (.y) share
-// every weight, gather and combine instruction.  Each half performs the scalar
-// kernel's operations in its order, so the output is bit-identical to it.  When
-// either stencil touches the border both samples take the scalar routines.
+// Paired (f32x2) warp kernels: the predictor's dy and dx sums run as one f32x2
+// chain, and the samples of frame A (.x) and frame B (.y) share every weight,
+// gather and combine instruction.  Each half performs the scalar kernel's
+// operations in its order, so the output is bit-identical to warp_kernel<MODE, 1>.
+// When either stencil touches the border both samples take the scalar routines.
+//
+// Per-thread column side and per-row predictor of the paired kernels: the
+// symmetric half shifts {hy, hx} of output pixel (i, j).
+struct PredX2 {
+    float2 wxb[4];
+    int cq[4];
+    float2 pyx[4][4];      // {dy, dx} at the 4x4 predictor stencil
+    int cur_by;
+};
+
+__device__ __forceinline__ void pred_x2_init(const WarpParams &p, int j, PredX2 &st)
+{
+    using namespace piv;
+    const float fx = p.lx[j], fxf = floorf(fx);
+    const int bx = (int)fxf - 1;
+    float wx[4];
+    keys4(fs(fx, fxf), wx);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        st.wxb[q] = dup2(wx[q]);
+        st.cq[q] = min(max(bx + q, 0), p.nPX - 1);
+    }
+    st.cur_by = -0x7fffffff;
+}
+
+__device__ __forceinline__ float2 pred_x2_row(const WarpParams &p, const float *dy, const float *dx, int i,
+                                              PredX2 &st, float2 nz)
+{
+    using namespace piv;
+    const int by = p.byr[i];
+    const float4 w01 = p.wyb[2 * i], w23 = p.wyb[2 * i + 1];
+    const float2 wyb[4] = {make_float2(w01.x, w01.y), make_float2(w01.z, w01.w), make_float2(w23.x, w23.y),
+                           make_float2(w23.z, w23.w)};
+    if (by != st.cur_by) {          // warp-uniform: all lanes share row i
+        st.cur_by = by;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int r = min(max(by + m, 0), p.nPY - 1) * p.nPX;
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                st.pyx[m][q] = make_float2(__ldg(dy + r + st.cq[q]), __ldg(dx + r + st.cq[q]));
+        }
+    }
+    float2 v = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) v = add2(v, mulz2(mulz2(wyb[m], st.wxb[q], nz), st.pyx[m][q], nz));
+    float2 h = mulz2(dup2(0.5f), v, nz);     // {hy, hx}
+    if (p.round_shifts) { h.x = roundf(h.x); h.y = roundf(h.y); }
+    return h;
+}
+
 // (96 registers, 5 CTAs per SM; capping them for 6 or 8 spills and ran 5% slower)
 __global__ void __launch_bounds__(128) warp_bicubic_x2_kernel(WarpParams p)
 {
@@ -341,45 +398,15 @@ __global__ void __launch_bounds__(128) warp_bicubic_x2_kernel(WarpParams p)
     if (j >= p.W || i0 >= p.H) return;
     const float2 nz = dup2(p.neg_zero);
     const float *dy = p.pdy + n * p.pred_stride, *dx = p.pdx + n * p.pred_stride;
-    const float fx = p.lx[j], fxf = floorf(fx);
-    const int bx = (int)fxf - 1;
-    float wx[4];
-    keys4(fs(fx, fxf), wx);
-    float2 wxb[4];
-    int cq[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        wxb[q] = dup2(wx[q]);
-        cq[q] = min(max(bx + q, 0), p.nPX - 1);
-    }
-    float2 pyx[4][4];      // {dy, dx} at the 4x4 predictor stencil
-    int cur_by = -0x7fffffff;
+    PredX2 st;
+    pred_x2_init(p, j, st);
     const float *a = p.ia + n * p.img_stride, *b = p.ib + n * p.img_stride;
     const int H = p.H, W = p.W;
     const float fj = (float)j;
     const int i_end = min(i0 + p.rows, H);
 #pragma unroll 1
     for (int i = i0; i < i_end; ++i) {
-        const int by = p.byr[i];
-        const float4 w01 = p.wyb[2 * i], w23 = p.wyb[2 * i + 1];
-        const float2 wyb[4] = {make_float2(w01.x, w01.y), make_float2(w01.z, w01.w), make_float2(w23.x, w23.y),
-                               make_float2(w23.z, w23.w)};
-        if (by != cur_by) {          // warp-uniform: all lanes share row i
-            cur_by = by;
-#pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                const int r = min(max(by + m, 0), p.nPY - 1) * p.nPX;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) pyx[m][q] = make_float2(__ldg(dy + r + cq[q]), __ldg(dx + r + cq[q]));
-            }
-        }
-        float2 v = make_float2(0.0f, 0.0f);
-#pragma unroll
-        for (int m = 0; m < 4; ++m)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) v = add2(v, mulz2(mulz2(wyb[m], wxb[q], nz), pyx[m][q], nz));
-        float2 h = mulz2(dup2(0.5f), v, nz);     // {hy, hx}
-        if (p.round_shifts) { h.x = roundf(h.x); h.y = roundf(h.y); }
+        const float2 h = pred_x2_row(p, dy, dx, i, st, nz);
         const float fi = (float)i;
         const float2 Y = make_float2(fs(fi, h.x), fa(fi, h.x));     // {frame A, frame B}
         const float2 X = make_float2(fs(fj, h.y), fa(fj, h.y));
@@ -410,6 +437,83 @@ __global__ void __launch_bounds__(128) warp_bicubic_x2_kernel(WarpParams p)
             const float wxa[4] = {wx2[0].x, wx2[1].x, wx2[2].x, wx2[3].x}, wxb_[4] = {wx2[0].y, wx2[1].y, wx2[2].y, wx2[3].y};
             p.oa[o] = bicubic_from_weights(a, iya, ixa, wya, wxa, H, W);
             p.ob[o] = bicubic_from_weights(b, iyb, ixb, wyb_, wxb_, H, W);
+        }
+    }
+}
+
+// lanczos_w on two offsets at once (.x frame A, .y frame B): the table lookups
+// per frame, the interpolation in paired instructions, each half equal to
+// lanczos_w of its offset.
+__device__ __forceinline__ void lanczos_w_x2(float2 d, const float4 *lut2, float2 (&w)[6], float2 nz)
+{
+    using namespace piv;
+    const float2 pos = mulz2(d, dup2((float)kLutN), nz);
+    int ka = (int)pos.x, kb = (int)pos.y;
+    float2 fr = sub2(pos, make_float2((float)ka, (float)kb));
+    if (ka >= kLutN) { ka = kLutN - 1; fr.x = 0.0f; }
+    if (kb >= kLutN) { kb = kLutN - 1; fr.y = 0.0f; }
+    // one 48-byte row per frame holds the twelve table values the interpolation
+    // reads (three 16-byte loads instead of twelve 4-byte ones)
+    const float4 a0 = __ldg(lut2 + 3 * ka), a1 = __ldg(lut2 + 3 * ka + 1), a2 = __ldg(lut2 + 3 * ka + 2);
+    const float4 b0 = __ldg(lut2 + 3 * kb), b1 = __ldg(lut2 + 3 * kb + 1), b2 = __ldg(lut2 + 3 * kb + 2);
+    const float2 lo[6] = {make_float2(a0.x, b0.x), make_float2(a0.y, b0.y), make_float2(a0.z, b0.z),
+                          make_float2(a0.w, b0.w), make_float2(a1.x, b1.x), make_float2(a1.y, b1.y)};
+    const float2 hi[6] = {make_float2(a1.z, b1.z), make_float2(a1.w, b1.w), make_float2(a2.x, b2.x),
+                          make_float2(a2.y, b2.y), make_float2(a2.z, b2.z), make_float2(a2.w, b2.w)};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) w[q] = add2(lo[q], mulz2(fr, sub2(hi[q], lo[q]), nz));
+}
+
+// The Lanczos-3 route (interp_mode 1) of the paired kernel: 6 x 6 taps per frame,
+// sample_lanczos<1>'s fused row sums, products and combine tree.
+__global__ void __launch_bounds__(128) warp_lanczos_x2_kernel(WarpParams p)
+{
+    using namespace piv;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i0 = (blockIdx.y * blockDim.y + threadIdx.y) * p.rows;
+    const int n = blockIdx.z;
+    if (j >= p.W || i0 >= p.H) return;
+    const float2 nz = dup2(p.neg_zero);
+    const float *dy = p.pdy + n * p.pred_stride, *dx = p.pdx + n * p.pred_stride;
+    PredX2 st;
+    pred_x2_init(p, j, st);
+    const float *a = p.ia + n * p.img_stride, *b = p.ib + n * p.img_stride;
+    const int H = p.H, W = p.W;
+    const float fj = (float)j;
+    const int i_end = min(i0 + p.rows, H);
+#pragma unroll 1
+    for (int i = i0; i < i_end; ++i) {
+        const float2 h = pred_x2_row(p, dy, dx, i, st, nz);
+        const float fi = (float)i;
+        const float2 Y = make_float2(fs(fi, h.x), fa(fi, h.x));     // {frame A, frame B}
+        const float2 X = make_float2(fs(fj, h.y), fa(fj, h.y));
+        const float2 FY = make_float2(floorf(Y.x), floorf(Y.y)), FX = make_float2(floorf(X.x), floorf(X.y));
+        const int iya = (int)FY.x - 2, iyb = (int)FY.y - 2, ixa = (int)FX.x - 2, ixb = (int)FX.y - 2;
+        const long long o = n * p.img_stride + (long long)i * W + j;
+        const bool inside = iya >= 0 && iya + 5 < H && ixa >= 0 && ixa + 5 < W && iyb >= 0 && iyb + 5 < H &&
+                            ixb >= 0 && ixb + 5 < W;
+        if (inside) {
+            float2 wy2[6], wx2[6];
+            lanczos_w_x2(sub2(Y, FY), p.lut2, wy2, nz);
+            lanczos_w_x2(sub2(X, FX), p.lut2, wx2, nz);
+            const float *ra = a + (iya * W + ixa), *rb = b + (iyb * W + ixb);
+            float2 c[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) c[q] = make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int m = 0; m < 6; ++m)
+#pragma unroll
+                for (int q = 0; q < 6; ++q)
+                    c[q] = fma2(make_float2(__ldg(ra + m * W + q), __ldg(rb + m * W + q)), wy2[m], c[q]);
+            float2 pr[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) pr[q] = mulz2(c[q], wx2[q], nz);
+            const float2 r = add2(add2(add2(pr[0], pr[4]), add2(pr[1], pr[5])), add2(pr[2], pr[3]));
+            p.oa[o] = r.x;
+            p.ob[o] = r.y;
+        } else {
+            p.oa[o] = sample_lanczos<1>(a, Y.x, X.x, H, W, p.lut);
+            p.ob[o] = sample_lanczos<1>(b, Y.y, X.y, H, W, p.lut);
         }
     }
 }
@@ -451,16 +555,18 @@ PIV_EXPORT void fused_warp_set_impl(int impl) { g_impl = impl ? 1 : 0; }
 PIV_EXPORT int fused_warp_get_impl(void) { return g_impl; }
 
 // Bytes of device tables pivb_warp_dev needs: lut_y [H], lut_x [W], Lanczos
-// [4097*6], predictor row weight pairs [H*8], predictor stencil rows [H].
+// [4097*6] and its paired rows [4096*12], predictor row weight pairs [H*8],
+// predictor stencil rows [H].
 PIV_EXPORT size_t pivb_warp_table_bytes(int H, int W)
 {
     return pad256((size_t)H * 4) + pad256((size_t)W * 4) + pad256((size_t)(kLutN + 1) * 6 * 4) +
-           pad256((size_t)H * 32) + pad256((size_t)H * 4);
+           pad256((size_t)kLutN * 12 * 4) + pad256((size_t)H * 32) + pad256((size_t)H * 4);
 }
 
 namespace {
 struct WarpTables {
     float *ly, *lx, *lut;
+    float4 *lut2;
     float4 *wyb;
     int *byr;
 };
@@ -472,6 +578,7 @@ WarpTables warp_tables(void *t_, int H, int W)
     r.ly = reinterpret_cast<float *>(t + off); off += pad256((size_t)H * 4);
     r.lx = reinterpret_cast<float *>(t + off); off += pad256((size_t)W * 4);
     r.lut = reinterpret_cast<float *>(t + off); off += pad256((size_t)(kLutN + 1) * 6 * 4);
+    r.lut2 = reinterpret_cast<float4 *>(t + off); off += pad256((size_t)kLutN * 12 * 4);
     r.wyb = reinterpret_cast<float4 *>(t + off); off += pad256((size_t)H * 32);
     r.byr = reinterpret_cast<int *>(t + off);
     return r;
@@ -490,6 +597,7 @@ PIV_EXPORT int pivb_warp_setup_dev(const float *d_ctrs_y, int nPY, const float *
     row_weights_kernel<<<(H + 255) / 256, 256, 0, s>>>(t.ly, H, t.wyb, t.byr);
     std::call_once(g_lut_once, build_lut_host);
     if (cudaMemcpyAsync(t.lut, g_lut_host, sizeof(g_lut_host), cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(t.lut2, g_lut2_host, sizeof(g_lut2_host), cudaMemcpyHostToDevice, s) != cudaSuccess) return 1;
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
@@ -511,7 +619,7 @@ PIV_EXPORT int pivb_warp_dev(const float *d_ia, const float *d_ib, float *d_oa, 
     p.pred_stride = shared_predictor ? 0 : (long long)nPY * nPX;
     p.img_stride = img_stride;
     p.N = N; p.H = H; p.W = W; p.nPY = nPY; p.nPX = nPX;
-    p.ly = t.ly; p.lx = t.lx; p.lut = t.lut; p.wyb = t.wyb; p.byr = t.byr;
+    p.ly = t.ly; p.lx = t.lx; p.lut = t.lut; p.lut2 = t.lut2; p.wyb = t.wyb; p.byr = t.byr;
     p.round_shifts = round_shifts;
     p.rows = g_rows.load(std::memory_order_relaxed);
     p.neg_zero = -0.0f;
@@ -522,7 +630,7 @@ PIV_EXPORT int pivb_warp_dev(const float *d_ia, const float *d_ib, float *d_oa, 
         if (impl) warp_bicubic_x2_kernel<<<grd, blk, 0, s>>>(p);
         else warp_kernel<0, 0><<<grd, blk, 0, s>>>(p);
     } else {
-        if (impl) warp_kernel<1, 1><<<grd, blk, 0, s>>>(p);
+        if (impl) warp_lanczos_x2_kernel<<<grd, blk, 0, s>>>(p);
         else warp_kernel<1, 0><<<grd, blk, 0, s>>>(p);
     }
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
