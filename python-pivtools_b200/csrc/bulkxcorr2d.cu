@@ -635,7 +635,7 @@ template <int N>
 constexpr size_t accum_smem_bytes()
 {
     // the accumulation kernel has no use for the correlator's staged weights
-    return (size_t)(WinGeo<N>::SMEM_BYTES - WinGeo<N>::WT_BYTES) + (size_t)WinGeo<N>::GROUPS_PER_CTA * 6 * N * N * 4;
+    return (size_t)(WinGeo<N>::SMEM_BYTES - WinGeo<N>::WT_BYTES) + (size_t)WinGeo<N>::GROUPS_PER_CTA * 4 * N * N * 4;
 }
 template <int N>
 constexpr bool accum_in_smem()
@@ -675,7 +675,7 @@ size_t accum_scratch_n(long long nwt)
     if (!accum_in_smem<N>()) {
         int grid = accum_grid<N>(nwt);
         if (grid < 0) return (size_t)-1;
-        b += pad256((size_t)grid * WinGeo<N>::GROUPS_PER_CTA * 6 * N * N * 4);
+        b += pad256((size_t)grid * WinGeo<N>::GROUPS_PER_CTA * 4 * N * N * 4);
     }
     return b;
 }

@@ -785,18 +785,26 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v)
     s = t;
 }
 
-// Window-stationary: one thread group per window streams all pairs of the call,
-// keeping Kahan-compensated FP32 sums of its crop in shared memory (or, for the
-// largest windows, in global scratch); one read-modify-write of the outputs per
-// call.  Per pair: two packed forward transforms (AB-weighted A + i B; AA/BB
-// auto-weighted A + i B) and two inverse transforms (the cross spectrum; the two
-// power spectra packed as |F_A|^2 + i |F_B|^2).
+// Window-stationary: one thread group per window streams all pairs of the call.
+// Correlation is linear, so the planes of a run of pairs are the inverse
+// transform of the sum of their spectra: each pair adds its cross spectrum and
+// its two power spectra (packed as |F_A|^2 + i |F_B|^2, per-pair scales
+// applied) to sums kept in shared memory (or, for the largest windows, global
+// scratch), and every kAccumBlock pairs (and at the end of the call) the sums
+// are transformed back once, cropped and added to the caller's planes with
+// Kahan compensation in FP32 (the compensation carried across calls in `comp`).
+// Per pair that leaves the two packed forward transforms (AB-weighted A + i B;
+// AA/BB auto-weighted A + i B) and the spectrum products; the inverse
+// transforms run once per block.  The spectral sums of a block are plain FP32
+// (at most kAccumBlock terms).
+constexpr int kAccumBlock = 32;
+
 template <int N, bool SMEM_ACC>
 __global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS) accum_kernel(AccumParams prm)
 {
     using G = WinGeo<N>;
-    constexpr int M = G::M, P = G::P;
-    constexpr int ACC_FLOATS = 6 * N * N;
+    constexpr int M = G::M, P = G::P, T = G::T;
+    constexpr int ACC_FLOATS = 4 * N * N;
     extern __shared__ float4 smem_raw[];
     char *smem = reinterpret_cast<char *>(smem_raw);
     int gi, t;
@@ -816,6 +824,8 @@ __global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS) accum_kernel(AccumPara
               gi * ACC_FLOATS;
     else
         acc = prm.gacc + ((long long)blockIdx.x * G::GROUPS_PER_CTA + gi) * ACC_FLOATS;
+    // spectral sums, element (lane t, sample n) at n * T + t: cross, then powers
+    float2 *sab = reinterpret_cast<float2 *>(acc), *spw = sab + N * N;
     const Group<N> g{t, red};
     const bool active = t < G::T;
     int line, p;
@@ -839,19 +849,15 @@ __global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS) accum_kernel(AccumPara
             c0 = (int)floorf(prm.ctr_x[ii] - ((float)N - 1.0f) / 2.0f + 0.5f);
             if (r0 < 0 || c0 < 0 || r0 + N > prm.H || c0 + N > prm.W) valid = false;
         }
-        // sums start from the caller's values (and carried compensation)
-        float *accs[3] = {acc, acc + 2 * N * N, acc + 4 * N * N};
-        float *outs[3] = {prm.ab, prm.aa, prm.bb};
-        const int nacc = prm.triple ? 3 : 1;
-        if (valid) {
-            for (int k = t; k < nout; k += G::GW)
-                for (int a = 0; a < nacc; ++a) {
-                    accs[a][k] = outs[a][iw * nout + k];
-                    accs[a][N * N + k] = prm.comp ? prm.comp[((long long)a * prm.nwt + iw) * nout + k] : 0.0f;
-                }
-        }
-        g.sync();
+        int in_block = 0;
         for (int n = 0; n < prm.n_img; ++n) {
+            if (in_block == 0 && active) {
+#pragma unroll
+                for (int k = 0; k < M; ++k) {
+                    sab[k * T + t] = make_float2(0.0f, 0.0f);
+                    spw[k * T + t] = make_float2(0.0f, 0.0f);
+                }
+            }
             float ra[M], rb[M];
             if (active && valid) {
                 const float *fa = prm.A + (long long)n * prm.img_stride + (long long)r0 * prm.W + c0 + line;
@@ -923,46 +929,69 @@ __global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS) accum_kernel(AccumPara
                     s_aa = 1.0f / eaa;
                     s_bb = 1.0f / ebb;
                 }
-                // autos first (x3, x4 die early)
+                // autos first (x3, x4 die early): 4 (|F_A|^2 + i |F_B|^2)
                 float2 z[M];
                 fft2_forward<N>(g, S, x3, x4);
                 spectrum_product<N, 1>(g, S, z);
-                fft2_inverse<N>(g, S, z);
-                if (valid && !skip) {
+                if (active && valid && !skip) {
 #pragma unroll
                     for (int k = 0; k < M; ++k) {
-                        const int row = (M * q + k + N / 2) % N - prm.sy0;
-                        if (col_in && row >= 0 && row < prm.out_h) {
-                            const int e = row * prm.out_w + col;
-                            kahan_add(accs[1][e], accs[1][N * N + e], s_aa * ((z[k].x * 0.25f) * inv_numel));
-                            kahan_add(accs[2][e], accs[2][N * N + e], s_bb * ((z[k].y * 0.25f) * inv_numel));
+                        float2 v = spw[k * T + t];
+                        v.x += s_aa * z[k].x;
+                        v.y += s_bb * z[k].y;
+                        spw[k * T + t] = v;
+                    }
+                }
+            }
+            // cross spectrum 4 F_B conj(F_A): slot0 = B, slot1 = A
+            {
+                float2 z[M];
+                fft2_forward<N>(g, S, x1, x2);
+                spectrum_product<N, 0>(g, S, z);
+                if (active && valid && !skip) {
+#pragma unroll
+                    for (int k = 0; k < M; ++k) {
+                        float2 v = sab[k * T + t];
+                        v.x += s_ab * z[k].x;
+                        v.y += s_ab * z[k].y;
+                        sab[k * T + t] = v;
+                    }
+                }
+            }
+            // the end of a block or of the call: one inverse of each sum, added
+            // to the caller's planes
+            if (++in_block == kAccumBlock || n + 1 == prm.n_img) {
+                in_block = 0;
+#pragma unroll 1
+                for (int pass = 0; pass < (prm.triple ? 2 : 1); ++pass) {
+                    const float2 *src = pass == 0 ? sab : spw;
+                    float2 z[M];
+#pragma unroll
+                    for (int k = 0; k < M; ++k) z[k] = active ? src[k * T + t] : make_float2(0.0f, 0.0f);
+                    fft2_inverse<N>(g, S, z);
+                    if (valid) {
+#pragma unroll
+                        for (int k = 0; k < M; ++k) {
+                            const int row = (M * q + k + N / 2) % N - prm.sy0;
+                            if (col_in && row >= 0 && row < prm.out_h) {
+                                const long long e = iw * nout + row * prm.out_w + col;
+#pragma unroll
+                                for (int h = 0; h < 2; ++h) {
+                                    if (pass == 0 && h == 1) break;           // the cross plane is real
+                                    const int a = pass == 0 ? 0 : 1 + h;      // AB, AA, BB
+                                    float *out = a == 0 ? prm.ab : (a == 1 ? prm.aa : prm.bb);
+                                    const float v = ((h == 0 ? z[k].x : z[k].y) * 0.25f) * inv_numel;
+                                    float sum = out[e];
+                                    float c = prm.comp ? prm.comp[(long long)a * prm.nwt * nout + e] : 0.0f;
+                                    kahan_add(sum, c, v);
+                                    out[e] = sum;
+                                    if (prm.comp) prm.comp[(long long)a * prm.nwt * nout + e] = c;
+                                }
+                            }
                         }
                     }
                 }
             }
-            // cross correlation: slot0 = B, slot1 = A
-            float2 z[M];
-            fft2_forward<N>(g, S, x1, x2);
-            spectrum_product<N, 0>(g, S, z);
-            fft2_inverse<N>(g, S, z);
-            if (valid && !skip) {
-#pragma unroll
-                for (int k = 0; k < M; ++k) {
-                    const int row = (M * q + k + N / 2) % N - prm.sy0;
-                    if (col_in && row >= 0 && row < prm.out_h) {
-                        const int e = row * prm.out_w + col;
-                        kahan_add(accs[0][e], accs[0][N * N + e], s_ab * ((z[k].x * 0.25f) * inv_numel));
-                    }
-                }
-            }
-        }
-        g.sync();
-        if (valid) {
-            for (int k = t; k < nout; k += G::GW)
-                for (int a = 0; a < nacc; ++a) {
-                    outs[a][iw * nout + k] = accs[a][k];
-                    if (prm.comp) prm.comp[((long long)a * prm.nwt + iw) * nout + k] = accs[a][N * N + k];
-                }
         }
         g.sync();
     }
