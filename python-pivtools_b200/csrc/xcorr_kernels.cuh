@@ -797,7 +797,7 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float v)
 // AA/BB auto-weighted A + i B) and the spectrum products; the inverse
 // transforms run once per block.  The spectral sums of a block are plain FP32
 // (at most kAccumBlock terms).
-constexpr int kAccumBlock = 32;
+constexpr int kAccumBlock = 64;
 
 template <int N, bool SMEM_ACC>
 __global__ void __launch_bounds__(WinGeo<N>::CTA_THREADS) accum_kernel(AccumParams prm)
