@@ -126,9 +126,10 @@ int pivb_xcorr_dev(const float *d_A, const float *d_B, long long img_stride, con
 /* Scratch bytes of the device accumulation entry points for one call. */
 size_t pivb_accumulate_scratch_bytes(int win, long long n_windows);
 
-/* bulkxcorr2d_accumulate_triple on device pointers.  Sums are Kahan-compensated
- * FP32 per window across the pairs of the call; d_comp (nullable, 3 arrays of the
- * sums' size) carries the compensation terms across calls. */
+/* bulkxcorr2d_accumulate_triple on device pointers.  Per window the spectra of up
+ * to 64 pairs are summed in FP32 and transformed back once; each such block is
+ * added to the sums with Kahan compensation in FP32; d_comp (nullable, 3 arrays of
+ * the sums' size) carries the compensation terms across blocks and calls. */
 int pivb_accumulate_triple_dev(const float *d_A, const float *d_B, long long img_stride,
                                const float *d_mask, int H, int W, int n_images,
                                const float *d_ctr_x, const float *d_ctr_y, int n_win_y,
