@@ -35,6 +35,7 @@ sys.path.insert(0, os.path.join(ROOT, "python-pivtools_b200"))
 METRIC = "vectors/s and p50/p99 pair latency on 1 B200 at ≤0.01 px RMS vs FP64 oracle"
 WORKLOAD = "multipass window-deformation PIV, 64 pairs 2048x2048, passes 128/64/32/32 px at 50/50/50/75%"
 HW = (2048, 2048)
+PEAK_FINDER = 3        # the multipass workload's subpixel fit (--peak-finder; 3-point by default)
 # FP32 CUDA-core peak, nominal: 148 SMs x 128 lanes x 2 flops x 1.965 GHz (no measured figure)
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
@@ -55,6 +56,8 @@ def _args():
                     help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
                          "serve: Poisson request stream with continuous batching")
     ap.add_argument("--chunk", type=int, default=32, help="e2e: pairs per host-to-device chunk")
+    ap.add_argument("--peak-finder", type=int, default=3, choices=[3, 4, 5, 6],
+                    help="multipass: subpixel fit, gauss3 (3-point) or the gauss4/5/6 Levenberg-Marquardt fits")
     ap.add_argument("--ensemble-bg", default="correlation+dc_zero",
                     choices=["correlation", "correlation+dc_zero", "window_mean", "correlation+window_mean", "image",
                              "image+window_mean", "image+dc_zero"],
@@ -144,7 +147,7 @@ def _dist():
 def _workload_config(n_pairs, ws, vec_step, win_step):
     """The workload as both arms state it (identical keys and values)."""
     return {"workload": WORKLOAD, "pairs_per_step_per_gpu": n_pairs, "image": "2048x2048 uint16 counts",
-            "passes": "128/64/32/32 px, 50/50/50/75%", "window_weight": "gaussian", "peak_finder": "gauss3",
+            "passes": "128/64/32/32 px, 50/50/50/75%", "window_weight": "gaussian", "peak_finder": f"gauss{PEAK_FINDER}",
             "warp": "bicubic symmetric, smoothed predictor",
             "validation": "gate win/2 then win/4; peak_mag 0.25; normalised median 5x5 (eps 0.1, thr 2)",
             "infill": "least squares between passes and after the last",
@@ -166,7 +169,7 @@ def _ref_pipeline():
     import ref_multipass as RM
     from pivtools_b200 import geometry, multipass
 
-    cfg = multipass.MultipassConfig()
+    cfg = multipass.MultipassConfig(peak_finder=PEAK_FINDER)
     geo = geometry.multipass_geometry(HW, cfg.window_sizes, cfg.overlaps, cfg.window_type)
     return RM, RM.RefMultipass(geo, window_type=cfg.window_type, peak_finder=cfg.peak_finder,
                                infill=cfg.infill, final_infill=cfg.final_infill)
@@ -304,7 +307,8 @@ def run_b200(args):
     dev = torch.device("cuda", local)
     N = args.pairs
     A, B = synthetic.channel_batch_torch(N, HW, seed=2026 + rank, device=dev)
-    mp = multipass.MultipassPIV(HW, N, multipass.MultipassConfig(engine_32=args.engine32), device=dev)
+    mp = multipass.MultipassPIV(HW, N, multipass.MultipassConfig(engine_32=args.engine32, peak_finder=PEAK_FINDER),
+                                device=dev)
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
@@ -408,7 +412,8 @@ def run_b200(args):
     from pivtools_b200.multipass import HostPipeline
 
     chunk = args.chunk if (args.chunk > 0 and N % args.chunk == 0) else N
-    pipe = HostPipeline(HW, chunk, multipass.MultipassConfig(engine_32=args.engine32), device=dev)
+    pipe = HostPipeline(HW, chunk, multipass.MultipassConfig(engine_32=args.engine32, peak_finder=PEAK_FINDER),
+                        device=dev)
     # frames are integer counts in [0, 65535]; every host buffer is page-locked with
     # .pin_memory() (torch.empty_like of a pinned tensor is pageable, which turns the
     # copies synchronous and serialises them with the compute)
@@ -480,7 +485,8 @@ def run_b200(args):
                     "traffic_unit": "bytes per launch (DRAM read + write)",
                     "peak_kind": "nominal FP32 (148 SMs x 128 lanes x 2 x 1.965 GHz; no measured FP32 figure)",
                     "flops_per_window": 80.1e3, "flops_per_launch": fp32_flops,
-                    "kernel": "xcorr_kernel<32> + lm_records_kernel (final pass, 4.1M windows)",
+                    "kernel": "xcorr_kernel<32> + " + ("lm_records_kernel" if PEAK_FINDER == 3 else "lm_fit_kernel") +
+                              " (final pass, 4.1M windows)",
                     "kernel_ms": kern_ms,
                     "hbm_view": {"algorithmic_bytes": alg_bytes, "achieved_gbs": achieved, "peak_gbs": hbm_peak,
                                  "frac": achieved / hbm_peak, "peak_kind": peak_kind}}
@@ -1141,7 +1147,9 @@ def run_serve(args):
 
 
 def main():
+    global PEAK_FINDER
     args = _args()
+    PEAK_FINDER = args.peak_finder
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "ensemble":
