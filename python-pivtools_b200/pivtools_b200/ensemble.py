@@ -1,7 +1,7 @@
 """GPU-resident ensemble PIV pass: accumulate, finalise, k-space fit.
 
-Follows the reference's single-pass ensemble (std mode) for one pass
-(pivtools_cli/piv/piv_backend/cpu_ensemble.py:590-676,
+Follows the reference's single-pass ensemble for one pass, std or single mode
+(pivtools_cli/piv/piv_backend/cpu_ensemble.py:188-225, 590-676, 700-760,
 single_pass_accumulator.py:292-320, 352-506, 508-800,
 kspace_lm_fitting.py:804-961):
 
