@@ -36,6 +36,7 @@ METRIC = "vectors/s and p50/p99 pair latency on 1 B200 at ≤0.01 px RMS vs FP64
 WORKLOAD = "multipass window-deformation PIV, 64 pairs 2048x2048, passes 128/64/32/32 px at 50/50/50/75%"
 HW = (2048, 2048)
 PEAK_FINDER = 3        # the multipass workload's subpixel fit (--peak-finder; 3-point by default)
+INTERP = 0             # image warp interpolation (--interp): 0 bicubic (default), 1 Lanczos-3
 # FP32 CUDA-core peak, nominal: 148 SMs x 128 lanes x 2 flops x 1.965 GHz (no measured figure)
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
@@ -56,6 +57,8 @@ def _args():
                     help="multipass: the headline line (default); ensemble: the 1024^2 16 px ensemble pass; "
                          "serve: Poisson request stream with continuous batching")
     ap.add_argument("--chunk", type=int, default=32, help="e2e: pairs per host-to-device chunk")
+    ap.add_argument("--interp", default="cubic", choices=["cubic", "lanczos"],
+                    help="multipass: image warp interpolation (the reference's image_warp_interpolation)")
     ap.add_argument("--peak-finder", type=int, default=3, choices=[3, 4, 5, 6],
                     help="multipass: subpixel fit, gauss3 (3-point) or the gauss4/5/6 Levenberg-Marquardt fits")
     ap.add_argument("--ensemble-bg", default="correlation+dc_zero",
@@ -148,7 +151,7 @@ def _workload_config(n_pairs, ws, vec_step, win_step):
     """The workload as both arms state it (identical keys and values)."""
     return {"workload": WORKLOAD, "pairs_per_step_per_gpu": n_pairs, "image": "2048x2048 uint16 counts",
             "passes": "128/64/32/32 px, 50/50/50/75%", "window_weight": "gaussian", "peak_finder": f"gauss{PEAK_FINDER}",
-            "warp": "bicubic symmetric, smoothed predictor",
+            "warp": f"{'Lanczos-3' if INTERP else 'bicubic'} symmetric, smoothed predictor",
             "validation": "gate win/2 then win/4; peak_mag 0.25; normalised median 5x5 (eps 0.1, thr 2)",
             "infill": "least squares between passes and after the last",
             "vectors_per_step_per_gpu": vec_step, "windows_per_step_per_gpu": win_step,
@@ -169,10 +172,10 @@ def _ref_pipeline():
     import ref_multipass as RM
     from pivtools_b200 import geometry, multipass
 
-    cfg = multipass.MultipassConfig(peak_finder=PEAK_FINDER)
+    cfg = multipass.MultipassConfig(peak_finder=PEAK_FINDER, interp_mode=INTERP)
     geo = geometry.multipass_geometry(HW, cfg.window_sizes, cfg.overlaps, cfg.window_type)
     return RM, RM.RefMultipass(geo, window_type=cfg.window_type, peak_finder=cfg.peak_finder,
-                               infill=cfg.infill, final_infill=cfg.final_infill)
+                               infill=cfg.infill, final_infill=cfg.final_infill, interp_mode=cfg.interp_mode)
 
 
 def _cpu_baseline(n_pairs: int):
@@ -307,8 +310,8 @@ def run_b200(args):
     dev = torch.device("cuda", local)
     N = args.pairs
     A, B = synthetic.channel_batch_torch(N, HW, seed=2026 + rank, device=dev)
-    mp = multipass.MultipassPIV(HW, N, multipass.MultipassConfig(engine_32=args.engine32, peak_finder=PEAK_FINDER),
-                                device=dev)
+    mp = multipass.MultipassPIV(HW, N, multipass.MultipassConfig(engine_32=args.engine32, peak_finder=PEAK_FINDER,
+                                                                  interp_mode=INTERP), device=dev)
     stream = torch.cuda.Stream(device=dev)
     torch.cuda.synchronize()
     with torch.cuda.stream(stream):
@@ -412,8 +415,8 @@ def run_b200(args):
     from pivtools_b200.multipass import HostPipeline
 
     chunk = args.chunk if (args.chunk > 0 and N % args.chunk == 0) else N
-    pipe = HostPipeline(HW, chunk, multipass.MultipassConfig(engine_32=args.engine32, peak_finder=PEAK_FINDER),
-                        device=dev)
+    pipe = HostPipeline(HW, chunk, multipass.MultipassConfig(engine_32=args.engine32, peak_finder=PEAK_FINDER,
+                                                           interp_mode=INTERP), device=dev)
     # frames are integer counts in [0, 65535]; every host buffer is page-locked with
     # .pin_memory() (torch.empty_like of a pinned tensor is pageable, which turns the
     # copies synchronous and serialises them with the compute)
@@ -1147,9 +1150,10 @@ def run_serve(args):
 
 
 def main():
-    global PEAK_FINDER
+    global PEAK_FINDER, INTERP
     args = _args()
     PEAK_FINDER = args.peak_finder
+    INTERP = 1 if args.interp == "lanczos" else 0
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "ensemble":

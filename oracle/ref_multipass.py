@@ -341,7 +341,7 @@ class RefMultipass:
     default, config.yaml:60-66) or 'harmonic'."""
 
     def __init__(self, geo, window_type="gaussian", peak_finder=3, infill="biharmonic", final_infill=True,
-                 smoothing=True, n_peaks=1, secondary_peak=False):
+                 smoothing=True, n_peaks=1, secondary_peak=False, interp_mode=0):
         self.bulk = O.ref_bulk()
         self.warp = O.ref_warp()
         if self.bulk is None or self.warp is None:
@@ -358,6 +358,7 @@ class RefMultipass:
         self.smoothing = smoothing
         self.n_peaks = n_peaks
         self.secondary = secondary_peak
+        self.interp_mode = interp_mode            # 0 bicubic, 1 Lanczos-3 (image_warp_interpolation)
         self.warp.fused_warp_set_impl(1)        # the SIMD route, the reference's default
 
     def run(self, A, B):
@@ -393,7 +394,7 @@ class RefMultipass:
                 ody = np.ascontiguousarray(old[..., 0])
                 odx = np.ascontiguousarray(old[..., 1])
                 if self.warp.fused_symmetric_warp_batch(A, B, fa, fb, ody, odx, N, H, W, ody.shape[1], ody.shape[2],
-                                                        prev.ctrs_y_all, prev.ctrs_x_all, 0, 0, 0) != 0:
+                                                        prev.ctrs_y_all, prev.ctrs_x_all, self.interp_mode, 0, 0) != 0:
                     raise RuntimeError("reference fused_symmetric_warp_batch failed")
             mask = np.zeros((ny, nx), np.float32)
             r = O.ref_bulkxcorr2d(fa, fb, mask, g.grid.win_ctrs_x, g.grid.win_ctrs_y, g.window_size, w, w,
