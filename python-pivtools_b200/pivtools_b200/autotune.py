@@ -122,9 +122,11 @@ def tune(mp, A, B, reps: int = 3, min_gain: float = 0.01, cache: str | None = DE
             best, t_best = cand, t
         apply(best)
 
+    # each candidate value is measured once: the default is not retried after
+    # another value has replaced it
     for rows in WARP_ROWS:
         for by in WARP_BLOCK_Y:
-            if (rows, by) != (best["warp_rows"], best["warp_block_y"]):
+            if (rows, by) != (16, 4):
                 attempt(dict(best, warp_rows=rows, warp_block_y=by))
     for n in sorted(best["ctas_per_sm"]):
         top = int(Lx.pivb_xcorr_max_ctas_per_sm(n))
@@ -134,7 +136,7 @@ def tune(mp, A, B, reps: int = 3, min_gain: float = 0.01, cache: str | None = DE
             attempt(dict(best, ctas_per_sm=cap))
     if mp.cfg.peak_finder in (3, 4, 5, 6):
         for tb in RECORD_BLOCKS:
-            if tb != best["record_block"]:
+            if tb != 128:
                 attempt(dict(best, record_block=tb))
     apply(best)
     out = {"settings": best, "step_ms_default": t0, "step_ms_tuned": t_best, "trials": len(trials), "key": key}
