@@ -134,3 +134,18 @@ def test_serving_engine_size_and_schedule():
     assert nb == int(4 * 2048 * 4096 * 20 * 1.1) + (64 << 20)
     # the largest class of the serving mix fits the 120 GB budget many times over
     assert 120e9 // nb >= 50
+
+
+def test_no_cpu_path():
+    """Without a GPU the resident pipelines refuse to start: there is no CPU
+    fallback behind them."""
+    import torch
+    from pivtools_b200 import ensemble, multipass
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    cfg = multipass.MultipassConfig(window_sizes=[(32, 32)], overlaps=[50])
+    with pytest.raises(RuntimeError):
+        multipass.MultipassPIV((256, 256), 1, cfg)
+    with pytest.raises(RuntimeError):
+        ensemble.EnsemblePIV((256, 256), window=(16, 16), overlap=75)
