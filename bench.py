@@ -80,30 +80,93 @@ def _args():
     return ap.parse_args()
 
 
+def _pci_bus_id(index):
+    """PCI bus id ("domain:bus:device.function") of CUDA device `index`, or None."""
+    try:
+        import torch
+
+        p = torch.cuda.get_device_properties(index)
+        return f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+    except Exception:
+        return None
+
+
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+    """SM clocks and throttle reasons sampled while the timed region runs.
+
+    Read-only NVML queries every `period_s` (20 ms), else `nvidia-smi` every 0.2 s
+    when NVML cannot be used.  The GPU is found by its PCI bus id, so the samples
+    are of the device the step runs on even where CUDA_VISIBLE_DEVICES renumbers
+    the devices."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period_s=0.02):
         self.index = index
+        self.period = period_s
         self.rows = []
         self._stop = threading.Event()
         self._t = None
+        self.bus_id = _pci_bus_id(index)
+        self._nvml = None
+        self._shutdown = None
+        self.source = "nvidia-smi"
+        try:
+            import pynvml as nv
+
+            nv.nvmlInit()
+            self._shutdown = nv.nvmlShutdown
+            h = nv.nvmlDeviceGetHandleByPciBusId(self.bus_id) if self.bus_id else nv.nvmlDeviceGetHandleByIndex(index)
+            self._nvml = (nv, h)
+            self.source = "nvml"
+        except Exception:
+            self._nvml = None
+
+    def _nvml_row(self):
+        nv, h = self._nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        try:
+            pw = f"{nv.nvmlDeviceGetPowerUsage(h) / 1000.0:.2f}"
+        except Exception:
+            pw = "[N/A]"
+        r = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        return [str(self.index), str(sm), str(mx), pw, hex(r)] + ["Active" if r & b else "Not Active" for b in bits]
+
+    def _smi_row(self):
+        ids = [self.bus_id, str(self.index)] if self.bus_id else [str(self.index)]
+        for i in ids:
+            out = subprocess.run(["nvidia-smi", f"--id={i}", f"--query-gpu={self.QUERY}",
+                                  "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                 timeout=5).stdout.strip()
+            row = [c.strip() for c in out.split(",")] if out else []
+            if len(row) == 9:
+                return row
+            self.bus_id = None                 # not accepted as an id: use the index from now on
+        return None
 
     def _run(self):
         while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.rows.append([c.strip() for c in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+            if self._nvml is not None:
+                try:
+                    self.rows.append(self._nvml_row())
+                except Exception:
+                    self._nvml, self.source = None, "nvidia-smi"
+                    continue
+                self._stop.wait(self.period)
+            else:
+                try:
+                    row = self._smi_row()
+                    if row:
+                        self.rows.append(row)
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -113,15 +176,21 @@ class ClockSampler:
     def __exit__(self, *a):
         self._stop.set()
         self._t.join(timeout=10)
+        if self._shutdown is not None:
+            try:
+                self._shutdown()
+            except Exception:
+                pass
+            self._shutdown = None
 
     def summary(self):
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
-                          and "Not" not in r[5 + k]})
+        rows = [r for r in self.rows if len(r) == 9]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = self.REASONS
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows), "source": self.source}
 
 
 def _peaks():
