@@ -32,9 +32,10 @@ int pivb_lz4_block_decode(const uint8_t *src, long long n, uint8_t *dst, long lo
 /* One zlib stream (.im7 pack 2 blocks, Zlib .set entries) into exactly
  * `expected` bytes, ending at its last byte.  Returns 0, 1 (invalid stream),
  * 2 (more than `expected`), 3 (no end marker), 4 (fewer than `expected`),
- * 5 (bytes after the end marker), -1 (bad arguments).  Replaces
- * _read_zlib_block (im7_reader.py:569-594) and _decompress_zlib
- * (set_reader.py:1601-1633). */
+ * 5 (bytes after the end marker), -1 (bad arguments): the bytes and codes of
+ * zlib's inflate() driven to exactly `expected` bytes, from the library's own
+ * Deflate decoder.  Replaces _read_zlib_block (im7_reader.py:569-594) and
+ * _decompress_zlib (set_reader.py:1601-1633). */
 int pivb_zlib_inflate_exact(const uint8_t *src, long long n, uint8_t *dst, long long expected);
 
 /* At most `cap` bytes from the start of one zlib stream: the bytes produced, or
