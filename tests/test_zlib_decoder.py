@@ -172,3 +172,49 @@ def test_decoder_header_and_block_errors(inflate, zlib_status):
     ]
     for c in cases:
         _check(inflate, zlib_status, c, len(raw) if c[2:3] != b"\x01" else 5)
+
+
+def test_row_blocks_in_parallel(zlib_status):
+    """pivb_zlib_blocks_decode: a pack-2 style run of size-prefixed row streams,
+    inflated on several threads, equals zlib row by row; the first damaged block
+    by index is the one reported; a bad size prefix is reported as such."""
+    import struct
+
+    from pivtools_b200 import _lib
+
+    L = _lib.lavision_lib()
+    rng = np.random.default_rng(7)
+    rows = [np.clip(rng.normal(120, 40, 512), 0, 65535).astype(np.uint16).tobytes() for _ in range(96)]
+    comp = [zlib.compress(r, int(rng.integers(1, 10))) for r in rows]
+
+    def run(blocks, skip_before, n_blocks, skip_after, threads):
+        body = b"".join(struct.pack("<i", len(c)) + c for c in blocks)
+        buf = np.frombuffer(body, np.uint8).copy()
+        dst = np.zeros(max(1, n_blocks) * 1024, np.uint8)
+        used, err = ctypes.c_longlong(0), ctypes.c_longlong(-1)
+        rc = L.pivb_zlib_blocks_decode(buf.ctypes.data, buf.size, skip_before, n_blocks, skip_after, dst.ctypes.data,
+                                       1024, threads, ctypes.byref(used), ctypes.byref(err))
+        return rc, dst, used.value, err.value, len(body)
+
+    for threads in (1, 4, 16):
+        rc, dst, used, err, total = run(comp, 8, 80, 8, threads)
+        assert rc == 0 and used == total
+        assert dst.tobytes() == b"".join(rows[8:88])
+    bad = list(comp)
+    for k in (30, 50):
+        z = bytearray(bad[k])
+        z[len(z) // 2] ^= 0x10
+        bad[k] = bytes(z)
+    want = [zlib_status(bad[k], 1024)[0] for k in (30, 50)]
+    assert any(want), "the flipped bits left both streams valid"
+    rc, _, _, err, _ = run(bad, 8, 80, 8, 8)
+    first = 30 if want[0] else 50
+    assert rc == 10 + zlib_status(bad[first], 1024)[0] and err == first - 8
+    # a size prefix that runs past the buffer
+    body = b"".join(struct.pack("<i", len(c)) + c for c in comp[:40]) + struct.pack("<i", 10 ** 6) + comp[40]
+    buf = np.frombuffer(body, np.uint8).copy()
+    dst = np.zeros(96 * 1024, np.uint8)
+    used, err = ctypes.c_longlong(0), ctypes.c_longlong(-1)
+    rc = L.pivb_zlib_blocks_decode(buf.ctypes.data, buf.size, 0, 41, 0, dst.ctypes.data, 1024, 4,
+                                   ctypes.byref(used), ctypes.byref(err))
+    assert rc == -2 and err.value == 40
